@@ -1,0 +1,262 @@
+"""FerroX inputs-file reader for the oracle (TEST INFRASTRUCTURE ONLY).
+
+A Python restatement of the subset of AMReX ParmParse that FerroX's inputs
+decks use (``key = v1 v2 ...``, ``#`` comments, double-quoted strings that may
+span lines, the last definition of a key wins), and of the defaults that
+``InitializeFerroXNamespace`` (Source/FerroX.cpp:273-572) and
+``c_GeometryProperties::ParseBasicDomainInput``
+(Source/Input/GeometryProperties/GeometryProperties.cpp:86-173) apply.
+
+Function-valued keys (``tphase_geom.tphase_geom_function(x,y,z)``,
+``angle_alpha.alpha_function(x,y,z)``, ...; Initialization.cpp:227-365) are
+evaluated with numpy over cell centres.  The AMReX Parser itself is a
+third-party component absent from the reference tree; this evaluator covers
+the grammar the example decks use (arithmetic, ``^``, comparisons, ``if``,
+the usual functions, ``my_constants.*``), so its parity is unpinned.
+
+The product library has its own C++ reader; tests compare the two.
+"""
+from __future__ import annotations
+
+import math
+import re
+
+import numpy as np
+
+# --------------------------------------------------------------- ParmParse --
+
+
+def tokenize(text: str) -> list[str]:
+    toks: list[str] = []
+    i, n = 0, len(text)
+    cur = ""
+    while i < n:
+        ch = text[i]
+        if ch == '"':
+            j = text.index('"', i + 1)
+            if cur:
+                toks.append(cur)
+                cur = ""
+            toks.append(text[i:j + 1])
+            i = j + 1
+            continue
+        if ch == "#":
+            while i < n and text[i] != "\n":
+                i += 1
+            continue
+        if ch == "=":
+            if cur:
+                toks.append(cur)
+                cur = ""
+            toks.append("=")
+            i += 1
+            continue
+        if ch.isspace():
+            if cur:
+                toks.append(cur)
+                cur = ""
+            i += 1
+            continue
+        cur += ch
+        i += 1
+    if cur:
+        toks.append(cur)
+    return toks
+
+
+def parse_table(text: str) -> dict[str, list[str]]:
+    """key -> value tokens of its last definition (quotes stripped)."""
+    toks = tokenize(text)
+    table: dict[str, list[str]] = {}
+    i = 0
+    while i < len(toks):
+        if i + 1 < len(toks) and toks[i + 1] == "=":
+            key = toks[i]
+            j = i + 2
+            vals = []
+            while j < len(toks) and not (j + 1 < len(toks) and toks[j + 1] == "="):
+                vals.append(toks[j])
+                j += 1
+            table[key] = [v[1:-1] if v.startswith('"') else v for v in vals]
+            i = j
+        else:
+            raise ValueError(f"inputs: unexpected token {toks[i]!r}")
+    return table
+
+
+# ---------------------------------------------------------- expressions ----
+
+_FUNCS = {
+    "sin": np.sin, "cos": np.cos, "tan": np.tan, "asin": np.arcsin, "acos": np.arccos,
+    "atan": np.arctan, "atan2": np.arctan2, "sinh": np.sinh, "cosh": np.cosh, "tanh": np.tanh,
+    "exp": np.exp, "log": np.log, "log10": np.log10, "sqrt": np.sqrt, "abs": np.abs,
+    "fabs": np.abs, "floor": np.floor, "ceil": np.ceil, "pow": np.power,
+    "min": np.minimum, "max": np.maximum,
+    "_if": lambda c, a, b: np.where(np.asarray(c) != 0, a, b),
+    "heaviside": lambda x, h0=0.0: np.where(np.asarray(x) > 0, 1.0, np.where(np.asarray(x) < 0, 0.0, h0)),
+}
+
+
+def _to_python(expr: str) -> str:
+    e = expr.replace("^", "**")
+    e = re.sub(r"\bif\s*\(", "_if(", e)
+    e = e.replace("&&", " & ").replace("||", " | ")
+    e = re.sub(r"\band\b", " & ", e)
+    e = re.sub(r"\bor\b", " | ", e)
+    return e
+
+
+def constants(table: dict[str, list[str]]) -> dict[str, float]:
+    out: dict[str, float] = {"pi": math.pi}
+    pending = {k[len("my_constants."):]: " ".join(v) for k, v in table.items() if k.startswith("my_constants.")}
+    for _ in range(len(pending) + 1):
+        for name, ex in list(pending.items()):
+            try:
+                out[name] = float(eval_expr(ex, out))
+                del pending[name]
+            except NameError:
+                pass
+    if pending:
+        raise ValueError(f"inputs: unresolved my_constants {sorted(pending)}")
+    return out
+
+
+def eval_expr(expr: str, consts: dict[str, float], x=None, y=None, z=None):
+    env = dict(_FUNCS)
+    env.update(consts)
+    if x is not None:
+        env.update(x=x, y=y, z=z)
+    code = _to_python(expr)
+    # comparisons yield booleans; arithmetic on them gives 0/1 as in AMReX Parser
+    val = eval(code, {"__builtins__": {}}, env)  # noqa: S307 - trusted test decks
+    return np.asarray(val, dtype=np.float64) * 1.0
+
+
+# ------------------------------------------------------------- defaults -----
+
+REQUIRED = ["TimeIntegratorOrder", "prob_type", "epsilon_0", "epsilonX_fe", "epsilonZ_fe", "epsilon_de",
+            "epsilon_si", "alpha", "beta", "gamma", "alpha_12", "alpha_112", "alpha_123", "BigGamma",
+            "g11", "g44", "g12", "g44_p", "lambda", "dt", "FE_lo", "FE_hi",
+            "domain.prob_lo", "domain.prob_hi", "domain.n_cell"]
+
+GHOST_MODES = {"extrap": 0, "face": 1, "zero": 2}
+
+
+def ferrox_params(table: dict[str, list[str]]) -> dict:
+    """Physics and domain parameters with the reference's defaults."""
+    for k in REQUIRED:
+        if k not in table:
+            raise KeyError(f"inputs: required key {k!r} missing")
+    consts = constants(table)
+
+    def num(key, default=None, cast=float):
+        if key not in table:
+            if default is None:
+                raise KeyError(key)
+            return default
+        v = table[key][0]
+        try:
+            return cast(v) if cast is int else float(v)
+        except ValueError:
+            return cast(float(eval_expr(v, consts)))
+
+    def arr(key, default=None, cast=float):
+        if key not in table:
+            return list(default)
+        out = []
+        for v in table[key][:3]:
+            try:
+                out.append(cast(v) if cast is int else float(v))
+            except ValueError:
+                out.append(cast(float(eval_expr(v, consts))))
+        return out
+
+    p: dict = {}
+    p["n_cell"] = arr("domain.n_cell", cast=int)
+    p["prob_lo"] = arr("domain.prob_lo")
+    p["prob_hi"] = arr("domain.prob_hi")
+    p["is_periodic"] = arr("domain.is_periodic", [0, 0, 0], cast=int)
+    lo, hi = p["prob_lo"], p["prob_hi"]
+
+    p["P_BC_flag_lo"] = arr("P_BC_flag_lo", [0, 0, 0], cast=int)
+    p["P_BC_flag_hi"] = arr("P_BC_flag_hi", [0, 0, 0], cast=int)
+    p["TimeIntegratorOrder"] = num("TimeIntegratorOrder", cast=int)
+    p["prob_type"] = num("prob_type", cast=int)
+    p["is_polarization_scalar"] = num("is_polarization_scalar", 1, int)
+    for k in ["epsilon_0", "epsilonX_fe", "epsilonZ_fe", "epsilon_de", "epsilon_si", "alpha", "beta", "gamma",
+              "alpha_12", "alpha_112", "alpha_123", "BigGamma", "g11", "g44", "g12", "g44_p", "lambda", "dt"]:
+        p[k] = num(k)
+    p["epsilonX_fe_tphase"] = num("epsilonX_fe_tphase", p["epsilonX_fe"])
+    p["nsteps"] = num("nsteps", 10, int)
+    p["plot_int"] = num("plot_int", -1, int)
+    p["delta"] = num("delta", 1.e-6)
+    p["inc_step"] = num("inc_step", -1, int)
+    p["random_seed"] = num("random_seed", 1, int)
+    p["voltage_sweep"] = num("voltage_sweep", 0, int)
+    p["Phi_Bc_hi"] = num("Phi_Bc_hi", 0.0)
+    p["Phi_Bc_lo"] = num("Phi_Bc_lo", 0.0)
+    p["Phi_Bc_inc"] = num("Phi_Bc_inc", 0.0)
+    p["Phi_Bc_hi_max"] = num("Phi_Bc_hi_max", 0.0)
+    p["phi_tolerance"] = num("phi_tolerance", 1.e-7)
+    p["num_Vapp_max"] = num("num_Vapp_max", 1, int)
+    p["include_Landau"] = num("include_Landau", 1, int)
+    p["include_Grad"] = num("include_Grad", 1, int)
+    p["include_Elec"] = num("include_Elec", 1, int)
+    outside_lo = [lo[i] - 1.0 for i in range(3)]
+    outside_hi = [hi[i] + 1.0 for i in range(3)]
+    p["FE_lo"] = arr("FE_lo")
+    p["FE_hi"] = arr("FE_hi")
+    p["DE_lo"] = arr("DE_lo", outside_lo)
+    p["DE_hi"] = arr("DE_hi", outside_hi)
+    p["SC_lo"] = arr("SC_lo", outside_lo)
+    p["SC_hi"] = arr("SC_hi", outside_hi)
+    p["Channel_lo"] = arr("Channel_lo", outside_lo)
+    p["Channel_hi"] = arr("Channel_hi", outside_hi)
+    p["Remnant_P"] = arr("Remnant_P", [0.0, 0.0, 0.002])
+    p["acceptor_doping"] = num("acceptor_doping", 0.0)
+    p["donor_doping"] = num("donor_doping", 0.0)
+    p["use_Fermi_Dirac"] = num("use_Fermi_Dirac", 1, int)
+    p["use_work_function"] = num("use_work_function", 0, int)
+    p["metal_work_function"] = num("metal_work_function", 4.85) if p["use_work_function"] == 1 else 0.0
+    p["Coordinate_Transformation"] = num("Coordinate_Transformation", 0, int)
+    p["use_Euler_angles"] = num("use_Euler_angles", 0, int)
+    # fx.* extensions
+    p["mg_rtol"] = num("fx.mg_rtol", 1.e-10)
+    gm = table.get("fx.phi_ghost_mode", ["extrap"])[0]
+    p["phi_ghost_mode"] = GHOST_MODES[gm]
+    p["sweep_mode"] = 1 if table.get("fx.sweep_mode", ["steady"])[0] == "fixed" else 0
+    p["steps_per_voltage"] = num("fx.steps_per_voltage", 0, int)
+    p["newton_max_iter"] = num("fx.newton_max_iter", 50, int)
+    p["mg_max_iter"] = num("fx.mg_max_iter", 200, int)
+    p["verbose"] = 0
+    return p
+
+
+def cell_centres(p: dict):
+    n = p["n_cell"]
+    dx = [(p["prob_hi"][d] - p["prob_lo"][d]) / n[d] for d in range(3)]
+    x = p["prob_lo"][0] + (np.arange(n[0]) + 0.5) * dx[0]
+    y = p["prob_lo"][1] + (np.arange(n[1]) + 0.5) * dx[1]
+    z = p["prob_lo"][2] + (np.arange(n[2]) + 0.5) * dx[2]
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    return X, Y, Z
+
+
+def function_fields(table: dict[str, list[str]], p: dict):
+    """tphase and Euler-angle fields (valid cells, shape (nz, ny, nx)) from the
+    parser keys, as Initialize_tphase_Mask / Initialize_Euler_angles do when
+    Coordinate_Transformation == 1 (Source/main.cpp:178-181)."""
+    n = p["n_cell"]
+    shape = (n[2], n[1], n[0])
+    if p["Coordinate_Transformation"] != 1:
+        z0 = np.zeros(shape)
+        return z0, z0.copy(), z0.copy(), z0.copy()
+    consts = constants(table)
+    X, Y, Z = cell_centres(p)
+    out = []
+    for key in ["tphase_geom.tphase_geom_function(x,y,z)", "angle_alpha.alpha_function(x,y,z)",
+                "angle_beta.beta_function(x,y,z)", "angle_theta.theta_function(x,y,z)"]:
+        if key not in table:
+            raise KeyError(f"inputs: {key!r} is required when Coordinate_Transformation = 1")
+        out.append(np.broadcast_to(eval_expr(" ".join(table[key]), consts, X, Y, Z), shape).astype(np.float64))
+    return tuple(out)
