@@ -1,0 +1,348 @@
+"""Coupled-step throughput of ferrox_b200 on one node.
+
+A step is one pass of FerroX's time loop (Source/main.cpp:261-621): the
+semiconductor-charge Newton loop with its Poisson multigrid solves, the fused
+TDGL update with E from phi, and the steady-state check.  The default workload
+is the 128x128x144 MFISM stack (5 nm HZO / 1 nm SiO2 / 30 nm p-Si, Boltzmann
+carriers, Newton-coupled Poisson to 1e-10 relative residual, FP64), with
+seeded synthetic initial polarization.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload mfism|mfim|polycrystal] [--precision fp64|mixed]
+
+Multi-GPU runs are independent replicas (one process per GPU, weak scaling):
+the path has no data exchange between devices.  Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "mfism": dict(shape=(128, 128, 144), label="MFISM 5nm HZO/1nm SiO2/30nm p-Si, Newton-coupled"),
+    "mfim": dict(shape=(64, 64, 36), label="MFIM 5nm HZO/4nm Al2O3"),
+    "polycrystal": dict(shape=(256, 256, 128), label="64-grain polycrystalline HZO on Al2O3"),
+}
+METRIC = "coupled-step cell-updates/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def deck(name: str):
+    from ferrox_b200 import decks
+    nx, ny, nz = WORKLOADS[name]["shape"]
+    if name == "mfism":
+        return decks.mfism(nx, ny, nz), None
+    if name == "mfim":
+        return decks.mfim(nx, ny, nz), None
+    return decks.polycrystal(nx, ny, nz, ngrains=64, seed=1)
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.idx)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, ValueError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def algorithmic_bytes(kernel: str, N: int, Nc1: int, sc: bool, scalar: bool, rot: bool, fp: int = 8) -> float:
+    """Compulsory bytes of one launch: each distinct array read once, each
+    output written once; stencil neighbours and ghosts count once."""
+    a = fp if sc else 0
+    if kernel == "smooth_l0":      # one red or black half-sweep: half of a full sweep
+        return N * (fp + fp + 1 + fp + a) / 2.0
+    if kernel == "restrict_l0":
+        return N * (fp + fp + 1 + a) + Nc1 * fp
+    if kernel == "prolong_l0":
+        return N * 2 * fp + Nc1 * fp
+    if kernel == "tdgl":
+        return N * ((3 if scalar else 7) * 8 + 1 + (1 if rot else 0))
+    if kernel == "newton":
+        return N * (8 * 5 + 4 + 1)
+    if kernel == "rho":
+        return N * (8 * 3 + 1) + (N * 24 if sc else 0)
+    if kernel == "resid64":
+        return N * (8 + 8 + 1 + a + 4)
+    if kernel == "rhs_p":
+        return N * ((1 if scalar else 3) * 8 + 1 + 8)
+    if kernel == "steady":
+        return N * 8 * 4
+    return 0.0
+
+
+def cpu_baseline(text: str, grains, steps: int) -> dict:
+    from ferrox_b200 import decks
+    from oracle import inputs as I
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    table = I.parse_table(text)
+    p = I.ferrox_params(table)
+    if grains is not None:
+        tph, ang = decks.grain_fields(grains)
+        o = O.Oracle(p, tph, tuple(ang), threads=threads)
+    else:
+        o = O.Oracle.from_text(text, threads=threads)
+    o.step(1)  # warm-up (first Newton pass from the intrinsic charge)
+    t0 = time.perf_counter()
+    for s in range(2, 2 + steps):
+        o.step(s)
+    dt = time.perf_counter() - t0
+    n = p["n_cell"][0] * p["n_cell"][1] * p["n_cell"][2]
+    return {"value": n * steps / dt, "unit": "cell-updates/s", "cores": threads, "kind": "port",
+            "sample": f"{steps} full coupled steps of the same deck after 1 warm-up step (restated CPU oracle, "
+                      f"OpenMP, {threads} threads; the reference build needs AMReX, absent)",
+            "seconds": dt}
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import inputs as I
+    from oracle import oracle as O
+    from ferrox_b200 import decks
+    text, grains = deck(args.workload)
+    threads = os.cpu_count() or 1
+    p = I.ferrox_params(I.parse_table(text))
+    if grains is not None:
+        tph, ang = decks.grain_fields(grains)
+        o = O.Oracle(p, tph, tuple(ang), threads=threads)
+    else:
+        o = O.Oracle.from_text(text, threads=threads)
+    step = 0
+    for _ in range(args.warmup):
+        step += 1
+        o.step(step)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step += 1
+        o.step(step)
+    dt = time.perf_counter() - t0
+    n = p["n_cell"][0] * p["n_cell"][1] * p["n_cell"][2]
+    v = n * args.steps / dt
+    line = {"metric": METRIC, "value": v, "unit": "cell-updates/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": f"{args.workload}-{'x'.join(map(str, WORKLOADS[args.workload]['shape']))}-fp64",
+                       "cells": n, "parallelism": "replicas"},
+            "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": threads, "kind": "port",
+                             "sample": f"{args.steps} full coupled steps after {args.warmup} warm-up steps "
+                                       f"(restated CPU oracle, OpenMP {threads} threads)"},
+            "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="mfism", choices=list(WORKLOADS))
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from ferrox_b200 import api
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    text, grains = deck(args.workload)
+    f = api.FerroX(text, precision=args.precision)
+    if grains is not None:
+        f.set_grains(grains["id"], grains["angles"], grains["tphase"])
+    stream = torch.cuda.current_stream()
+    f.set_stream(stream.cuda_stream)
+    N = f.N
+    f.step(args.warmup)
+    f.sync()
+    st0 = f.stats()
+
+    sampler = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    done = f.step(args.steps)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    ms = ev0.elapsed_time(ev1)
+    st1 = f.stats()
+    # per-launch kernel durations: the same K steps again with CUDA events
+    # around every launch (kept out of the timed region, whose cost they raise)
+    f.set_param("fx.profile", 1)
+    f.reset_kernel_times()
+    f.step(args.steps)
+    kt = f.kernel_times()
+    f.set_param("fx.profile", 0)
+    if done != args.steps:
+        raise RuntimeError(f"the reference loop ended after {done} of {args.steps} steps")
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = N * args.steps * world / (ms_max / 1e3)
+
+    # end to end through the public API with host buffers: the initial P
+    # uploaded from pinned host memory, per step the applied voltage in and the
+    # mean polarization out, the final P and phi read back
+    ke = args.e2e_steps or args.steps
+    Pz_host = torch.empty(f.shape, dtype=torch.float64, pin_memory=True).numpy()
+    Pz_host[...] = f.field("Pz")
+    out_P = torch.empty(f.shape, dtype=torch.float64, pin_memory=True).numpy()
+    out_phi = torch.empty(f.shape, dtype=torch.float64, pin_memory=True).numpy()
+    V0 = f.param("Phi_Bc_hi")
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    f.set_initial_P(None, None, Pz_host)
+    means = []
+    for q in range(ke):
+        f.set_param("Phi_Bc_hi", V0)
+        f.step(1)
+        means.append(f.mean_P()[2])
+    out_P[...] = f.field("Pz")
+    out_phi[...] = f.field("Phi")
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ems = e0.elapsed_time(e1)
+    t = torch.tensor([ems], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = N * ke * world / (float(t.item()) / 1e3)
+    h2d = (3 * N * 8 + ke * 8) / ke
+    d2h = (ke * 24 + 2 * N * 8) / ke
+
+    if rank == 0:
+        peak, peak_src = peaks()
+        sc = f.param("contains_sc") == 1.0
+        rot = f.param("num_variants") > 0
+        # dominant kernel class of the timed region and its achieved bandwidth
+        dom = max(kt, key=lambda k: kt[k][0])
+        dms, dcnt = kt[dom]
+        nz1 = WORKLOADS[args.workload]["shape"]
+        Nc1 = N // 2  # level 1 halves z on these stacks (dz < dx)
+        fp = 4 if args.precision == "mixed" and dom in ("smooth_l0", "restrict_l0", "prolong_l0") else 8
+        per_launch = algorithmic_bytes(dom, N, Nc1, sc, True, rot, fp)
+        achieved = per_launch / (dms / dcnt / 1e3) / 1e9 if dcnt else None
+        total_ms = sum(v[0] for v in kt.values())
+        roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak if achieved else None, "traffic": None,
+                "peak_source": f"{peak_src} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured"
+                else "fallback 6.65 TB/s",
+                "algorithmic_bytes_per_launch": per_launch, "launches": dcnt, "avg_launch_us": 1e3 * dms / dcnt}
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            cpu = cpu_baseline(text, grains, 3)
+        line = {
+            "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+            "data": "synthetic (seeded initial P, synthetic device stack)",
+            "config": {"workload": f"{args.workload}-{'x'.join(map(str, nz1))}-{args.precision}",
+                       "description": WORKLOADS[args.workload]["label"], "cells": N,
+                       "l2": f"inputs larger than L2: device working set {f.stats()['device_bytes'] / 1e6:.0f} MB per step",
+                       "mg_rtol": f.param("fx.mg_rtol"), "parallelism": "replicas"},
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "steps": ke},
+            "gpu_launches": int(st1["kernel_launches"] - st0["kernel_launches"]),
+            "clocks": clocks,
+            "kernel_ms_share": {k: round(v[0] / total_ms, 4) for k, v in kt.items() if v[1]},
+            "mg_cycles_per_step": (st1["mg_cycles_total"] - st0["mg_cycles_total"]) / args.steps,
+            "newton_passes_per_step": (st1["newton_iters_total"] - st0["newton_iters_total"]) / args.steps,
+        }
+        print(json.dumps(line), flush=True)
+    f.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,1212 @@
+// fx_api.cu -- context, host-side setup and the C ABI (include/ferrox_b200.h).
+//
+// Host setup restates the reference's initialization (masks, permittivity,
+// initial P, electrode values); the per-step work is the device kernels of
+// fx_kernels.cu and the multigrid of fx_mg.cu, ordered on one stream.  There
+// is no CPU compute path: every hot-path function launches device kernels
+// and returns FX_ERR_CUDA when no device is usable.
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <memory>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/ferrox_b200.h"
+#include "fx_kernels.h"
+#include "fx_mg.h"
+#include "fx_params.h"
+#include "plotfile.h"
+
+namespace fx {
+std::atomic<long long> g_launches{0};
+}
+
+using namespace fx;
+
+namespace {
+
+thread_local std::string t_create_error;
+
+// Silicon constants, Source/FerroX.cpp:534-554
+constexpr double kNc = 2.8e25, kNv = 1.83e25, kEg = 1.12, kChi = 4.05, kQ = 1.602e-19, kKb = 1.38e-23, kT = 300.0;
+constexpr double kEa = 44.0e-3, kEd = 46.0e-3;
+
+uint64_t splitmix_mix(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+// n-th draw (n >= 1) of a splitmix64 stream seeded with `seed`, in [0, 1)
+double uniform(uint64_t seed, uint64_t n) {
+    return (double)(splitmix_mix(seed + n * 0x9E3779B97F4A7C15ULL) >> 11) * (1.0 / 9007199254740992.0);
+}
+
+// rotation from Euler angles in degrees, TotalEnergyDensity.cpp:167-195
+void rotation(int use_euler, double a_deg, double b_deg, double t_deg, double R[9]) {
+    double Pi = 3.14159265358979323846;
+    double alpha_rad = Pi / 180. * a_deg, beta_rad = Pi / 180. * b_deg, theta_rad = Pi / 180. * t_deg;
+    if (use_euler) {
+        R[0] = cos(alpha_rad) * cos(theta_rad) - cos(beta_rad) * sin(alpha_rad) * sin(theta_rad);
+        R[1] = sin(alpha_rad) * cos(theta_rad) + cos(beta_rad) * cos(alpha_rad) * sin(theta_rad);
+        R[2] = sin(beta_rad) * sin(theta_rad);
+        R[3] = -cos(beta_rad) * cos(theta_rad) * sin(alpha_rad) - cos(alpha_rad) * sin(theta_rad);
+        R[4] = cos(beta_rad) * cos(alpha_rad) * cos(theta_rad) - sin(alpha_rad) * sin(theta_rad);
+        R[5] = sin(beta_rad) * cos(theta_rad);
+        R[6] = sin(alpha_rad) * sin(beta_rad);
+        R[7] = -cos(alpha_rad) * sin(beta_rad);
+        R[8] = cos(beta_rad);
+    } else {
+        R[0] = cos(beta_rad) * cos(theta_rad);
+        R[1] = sin(alpha_rad) * sin(beta_rad) * cos(theta_rad) - cos(alpha_rad) * sin(theta_rad);
+        R[2] = cos(alpha_rad) * sin(beta_rad) * cos(theta_rad) + sin(alpha_rad) * sin(theta_rad);
+        R[3] = cos(beta_rad) * sin(theta_rad);
+        R[4] = sin(beta_rad) * sin(alpha_rad) * sin(theta_rad) + cos(alpha_rad) * cos(theta_rad);
+        R[5] = cos(alpha_rad) * sin(beta_rad) * sin(theta_rad) - sin(alpha_rad) * cos(theta_rad);
+        R[6] = -sin(beta_rad);
+        R[7] = sin(alpha_rad) * cos(beta_rad);
+        R[8] = cos(alpha_rad) * cos(beta_rad);
+    }
+}
+
+struct FxError {
+    int code;
+    std::string msg;
+};
+
+}  // namespace
+
+struct fx_ctx {
+    Params par;
+    Inputs in;
+    DevParams dp{};
+    int nx = 0, ny = 0, nz = 0;
+    size_t N = 0, nxy = 0;
+    double dx[3] = {0, 0, 0};
+    std::string err;
+
+    // host setup
+    std::vector<uint8_t> code;           // (nz+2)*nxy, mask | tphase << 2
+    std::vector<double> mask_ref;        // reference ghosted mask (nx+2)(ny+2)(nz+2)
+    std::vector<double> tphase, ang[3];  // valid cells
+    std::vector<uint8_t> var;            // per-cell variant id (empty: identity R everywhere)
+    std::vector<Variant> variants;
+    std::vector<double> P0[3];
+    std::vector<uint8_t> gid;            // per-cell grain id (255: none) once grains are set
+    std::vector<double> galpha;          // per-grain Landau alpha (empty: global alpha)
+    bool scalarP = true;                 // Px = Py = 0 and is_polarization_scalar
+    bool contains_sc = false;
+    bool grains_set = false;
+    bool user_P = false;
+
+    // loop state, main.cpp:238-242
+    int step = 0;
+    int steady_state_step = 1000000;
+    int sign = 1;
+    int num_Vapp = 0;
+    int inc_step = -1;
+    double time = 0.0;
+    double Phi_Bc_hi = 0.0;
+    bool finished = false;
+    double phi_max_last = 0.0;
+
+    // stats
+    int newton_last = 0, mg_last = 0;
+    long long newton_total = 0, mg_total = 0;
+    double mg_resid_last = 0, mg_target_last = 0, phi_err_last = 0, steady_err_last = 0;
+
+    // device
+    bool dev = false;
+    cudaStream_t s = nullptr;
+    bool own_stream = true;
+    Prof prof;
+    uint8_t *d_code = nullptr, *d_var = nullptr;
+    Variant* d_vt = nullptr;
+    double* d_P[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+    int cur = 0;
+    double *d_phi = nullptr, *d_phi_old = nullptr, *d_phi_prev = nullptr, *d_rho = nullptr, *d_e = nullptr, *d_h = nullptr;
+    double *d_alpha = nullptr, *d_rhs = nullptr, *d_rhsP = nullptr, *d_dphi = nullptr, *d_E[3] = {nullptr, nullptr, nullptr};
+    float* d_alpha32 = nullptr;
+    double* d_part = nullptr;
+    unsigned int* d_counter = nullptr;
+    double* d_out = nullptr;
+    double* h_out = nullptr;
+    bool E_valid = false;
+    bool rhs_is_newton = false;
+    size_t dev_bytes = 0;
+    Multigrid mg;
+    bool mg_ready = false;
+};
+
+namespace {
+
+int set_err(fx_ctx* c, int code, const std::string& m) {
+    if (c) c->err = m;
+    return code;
+}
+
+#define FX_CUDA(ctx, call)                                                                         \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return set_err(ctx, e_ == cudaErrorMemoryAllocation ? FX_ERR_OUT_OF_MEMORY : FX_ERR_CUDA, \
+                           std::string(#call) + ": " + cudaGetErrorString(e_));                    \
+    } while (0)
+
+double eps_of_code(const Params& p, int code) {
+    // InitializePermittivity, ElectrostaticSolver.cpp:238-251
+    const int m = code & 3, tph = (code >> 2) & 1;
+    if (m == 0) return tph ? p.epsilonX_fe_tphase * p.epsilon_0 : p.epsilonX_fe * p.epsilon_0;
+    if (m == 1) return p.epsilon_de * p.epsilon_0;
+    return p.epsilon_si * p.epsilon_0;
+}
+
+double phi_ref() { return kChi + 0.5 * kEg + 0.5 * kKb * kT * log(kNc / kNv) / kQ; }
+
+// SetPhiBC_z values, ElectrostaticSolver.cpp:512-519
+void electrode_values(fx_ctx* c) {
+    const double pr = phi_ref();
+    const double phi_m = c->par.use_work_function ? c->par.metal_work_function : pr;
+    c->dp.V_lo = c->par.Phi_Bc_lo;
+    c->dp.V_hi = c->Phi_Bc_hi - (phi_m - pr);
+}
+
+// InitializeMaterialMask, Initialization.cpp:184-202 at one cell centre
+double mask_at(const Params& p, double x, double y, double z) {
+    if (x <= p.FE_hi[0] && x >= p.FE_lo[0] && y <= p.FE_hi[1] && y >= p.FE_lo[1] && z <= p.FE_hi[2] && z >= p.FE_lo[2]) return 0.;
+    if (x <= p.DE_hi[0] && x >= p.DE_lo[0] && y <= p.DE_hi[1] && y >= p.DE_lo[1] && z <= p.DE_hi[2] && z >= p.DE_lo[2]) return 1.;
+    if (x <= p.SC_hi[0] && x >= p.SC_lo[0] && y <= p.SC_hi[1] && y >= p.SC_lo[1] && z <= p.SC_hi[2] && z >= p.SC_lo[2]) {
+        if (x <= p.Channel_hi[0] && x >= p.Channel_lo[0] && y <= p.Channel_hi[1] && y >= p.Channel_lo[1] && z <= p.Channel_hi[2] && z >= p.Channel_lo[2])
+            return 3.;
+        return 2.;
+    }
+    return 1.;
+}
+
+void build_codes(fx_ctx* c) {
+    const Params& p = c->par;
+    const int nx = c->nx, ny = c->ny, nz = c->nz;
+    const size_t gx = nx + 2, gy = ny + 2;
+    c->mask_ref.assign(gx * gy * (nz + 2), 0.0);
+    auto G = [&](int i, int j, int k) -> double& { return c->mask_ref[(size_t)(i + 1) + gx * ((size_t)(j + 1) + gy * (size_t)(k + 1))]; };
+    for (int k = -1; k <= nz; ++k)
+        for (int j = -1; j <= ny; ++j)
+            for (int i = -1; i <= nx; ++i)
+                G(i, j, k) = mask_at(p, p.prob_lo[0] + (i + 0.5) * c->dx[0], p.prob_lo[1] + (j + 0.5) * c->dx[1],
+                                     p.prob_lo[2] + (k + 0.5) * c->dx[2]);
+    // FillBoundary with the x/y periodic images that are valid cells
+    for (int k = -1; k <= nz; ++k)
+        for (int j = -1; j <= ny; ++j)
+            for (int i = -1; i <= nx; ++i) {
+                const bool gxo = i < 0 || i >= nx, gyo = j < 0 || j >= ny, gzo = k < 0 || k >= nz;
+                if ((gxo || gyo) && !gzo) G(i, j, k) = G((i + nx) % nx, (j + ny) % ny, k);
+            }
+    c->code.assign((size_t)nx * ny * (nz + 2), 0);
+    for (int k = -1; k <= nz; ++k)
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                int m = (int)G(i, j, k);
+                int t = 0;
+                if (k >= 0 && k < nz) t = c->tphase[(size_t)i + nx * ((size_t)j + (size_t)ny * k)] == 1.0 ? 1 : 0;
+                c->code[(size_t)i + nx * ((size_t)j + (size_t)ny * (k + 1))] = (uint8_t)(m | (t << 2));
+            }
+    c->contains_sc = false;
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i)
+                if (G(i, j, k) >= 2.0) c->contains_sc = true;
+}
+
+// the device reads the mask of a ghost cell through periodic wrapping; check
+// that this equals the reference's ghosted mask wherever the stencils read it
+std::string check_wrapped_mask(fx_ctx* c) {
+    const int nx = c->nx, ny = c->ny, nz = c->nz;
+    const size_t gx = nx + 2, gy = ny + 2;
+    for (int k = -1; k <= nz; ++k)
+        for (int j = -1; j <= ny; ++j)
+            for (int i = -1; i <= nx; ++i) {
+                const double ref = c->mask_ref[(size_t)(i + 1) + gx * ((size_t)(j + 1) + gy * (size_t)(k + 1))];
+                const int w = c->code[(size_t)((i + nx) % nx) + nx * ((size_t)((j + ny) % ny) + (size_t)ny * (k + 1))] & 3;
+                if (ref != (double)w) {
+                    std::ostringstream o;
+                    o << "material boxes distinguish a periodic ghost corner from its image at cell (" << i << "," << j << "," << k
+                      << "): mask " << ref << " vs " << w << "; the device layout wraps x/y ghosts";
+                    return o.str();
+                }
+            }
+    return "";
+}
+
+void build_variants(fx_ctx* c, const std::vector<uint8_t>* gid, const std::vector<double>* galpha) {
+    c->var.clear();
+    c->variants.clear();
+    const size_t N = c->N;
+    bool any = false;
+    if (gid) any = true;
+    for (int d = 0; d < 3 && !any; ++d)
+        for (size_t q = 0; q < N; ++q)
+            if (c->ang[d][q] != 0.0) { any = true; break; }
+    if (!any) return;
+    std::map<std::tuple<double, double, double, double>, uint8_t> ids;
+    c->var.assign(N, 0);
+    for (size_t q = 0; q < N; ++q) {
+        double al = c->par.alpha;
+        if (gid && galpha && (*gid)[q] != 255 && (*gid)[q] < galpha->size()) al = (*galpha)[(*gid)[q]];
+        auto key = std::make_tuple(c->ang[0][q], c->ang[1][q], c->ang[2][q], al);
+        auto it = ids.find(key);
+        if (it == ids.end()) {
+            if (ids.size() >= 255) throw FxError{FX_ERR_UNSUPPORTED, "more than 255 distinct Euler-angle / alpha combinations"};
+            Variant v{};
+            rotation(c->par.use_Euler_angles, c->ang[0][q], c->ang[1][q], c->ang[2][q], v.R);
+            v.alpha = al;
+            const uint8_t id = (uint8_t)c->variants.size();
+            c->variants.push_back(v);
+            it = ids.emplace(key, id).first;
+        }
+        c->var[q] = it->second;
+    }
+}
+
+// InitializePandRho, Initialization.cpp:83-131 (random draws from the seeded
+// splitmix64 stream: the n-th draw is cell 3*idx + component + 1)
+void build_P0(fx_ctx* c) {
+    const Params& p = c->par;
+    const int nx = c->nx, ny = c->ny, nz = c->nz;
+    for (int d = 0; d < 3; ++d) c->P0[d].assign(c->N, 0.0);
+    const uint64_t seed = (uint64_t)(int64_t)p.random_seed;
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                const size_t idx = (size_t)i + nx * ((size_t)j + (size_t)ny * k);
+                const int m = c->code[idx + c->nxy] & 3;
+                double pp = 0, pq = 0, pr = 0;
+                if (m == 0) {
+                    const double x = p.prob_lo[0] + (i + 0.5) * c->dx[0];
+                    const double y = p.prob_lo[1] + (j + 0.5) * c->dx[1];
+                    const double z = p.prob_lo[2] + (k + 0.5) * c->dx[2];
+                    if (p.prob_type == 1) {
+                        const double u = uniform(seed, (uint64_t)i + (uint64_t)k * nz + 1);
+                        pp = (-1.0 + 2.0 * u) * p.Remnant_P[0];
+                        pq = (-1.0 + 2.0 * u) * p.Remnant_P[1];
+                        pr = (-1.0 + 2.0 * u) * p.Remnant_P[2];
+                    } else if (p.prob_type == 2) {
+                        pp = (-1.0 + 2.0 * uniform(seed, 3 * idx + 1)) * p.Remnant_P[0];
+                        pq = (-1.0 + 2.0 * uniform(seed, 3 * idx + 2)) * p.Remnant_P[1];
+                        pr = (-1.0 + 2.0 * uniform(seed, 3 * idx + 3)) * p.Remnant_P[2];
+                    } else {
+                        const double DEz = p.DE_hi[2];
+                        const double g = exp(-(x * x / (2.0 * 5.e-9 * 5.e-9) + y * y / (2.0 * 5.e-9 * 5.e-9) +
+                                               (z - 1.5 * DEz) * (z - 1.5 * DEz) / (2.0 * 2.0e-9 * 2.0e-9)));
+                        pp = p.Remnant_P[0] * g; pq = p.Remnant_P[1] * g; pr = p.Remnant_P[2] * g;
+                    }
+                    if (c->tphase[idx] == 1.0) pr = 0.0;
+                }
+                if (p.is_polarization_scalar == 1) { pp = 0.0; pq = 0.0; }
+                c->P0[0][idx] = pp; c->P0[1][idx] = pq; c->P0[2][idx] = pr;
+            }
+    c->scalarP = p.is_polarization_scalar == 1;
+}
+
+void fill_devparams(fx_ctx* c) {
+    const Params& p = c->par;
+    DevParams& d = c->dp;
+    d.nx = c->nx; d.ny = c->ny; d.nz = c->nz;
+    d.nxy = (long long)c->nxy; d.N = (long long)c->N;
+    long long blocks = ((long long)c->N + 255) / 256;
+    d.ngrid_red = (int)std::min<long long>(std::max<long long>(blocks, 1), 148 * 8);
+    for (int q = 0; q < 3; ++q) { d.dx[q] = c->dx[q]; d.ih2[q] = 1.0 / (c->dx[q] * c->dx[q]); }
+    d.dt = p.dt;
+    d.alpha = p.alpha; d.beta = p.beta; d.gamma = p.gamma; d.a12 = p.alpha_12; d.a112 = p.alpha_112; d.a123 = p.alpha_123;
+    d.BigGamma = p.BigGamma; d.g11 = p.g11; d.g44 = p.g44; d.g44p = p.g44_p; d.g12 = p.g12; d.lambda = p.lambda;
+    for (int q = 0; q < 3; ++q) { d.flo[q] = p.P_BC_flag_lo[q]; d.fhi[q] = p.P_BC_flag_hi[q]; }
+    d.incl_L = p.include_Landau == 1; d.incl_G = p.include_Grad == 1; d.incl_E = p.include_Elec == 1;
+    d.scalar = p.is_polarization_scalar == 1;
+    for (int q = 0; q < 8; ++q) d.eps[q] = eps_of_code(p, q);
+    d.q = kQ; d.kb = kKb; d.T = kT; d.Nc = kNc; d.Nv = kNv; d.Eg = kEg; d.Chi = kChi; d.Ea = kEa; d.Ed = kEd;
+    d.NA = p.acceptor_doping; d.ND = p.donor_doping; d.phi_ref = phi_ref(); d.use_FD = p.use_Fermi_Dirac;
+    d.delta = p.delta; d.inv_delta = 1. / p.delta; d.neg_inv_delta = -1. / p.delta;
+    d.ghost_mode = p.phi_ghost_mode;
+    electrode_values(c);
+}
+
+template <typename T>
+int dmalloc(fx_ctx* c, T** p, size_t n) {
+    cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(n, 1) * sizeof(T));
+    if (e != cudaSuccess) return set_err(c, FX_ERR_OUT_OF_MEMORY, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    c->dev_bytes += n * sizeof(T);
+    return 0;
+}
+
+int ensure_device(fx_ctx* c) {
+    if (c->dev) return FX_OK;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0)
+        return set_err(c, FX_ERR_CUDA, std::string("no usable CUDA device: ") + cudaGetErrorString(e));
+    if (c->own_stream) FX_CUDA(c, cudaStreamCreateWithFlags(&c->s, cudaStreamNonBlocking));
+    c->mg.prof = &c->prof;
+    const size_t N = c->N;
+    int r = 0;
+    r |= dmalloc(c, &c->d_code, c->code.size());
+    for (int b = 0; b < 2; ++b)
+        for (int d = 0; d < 3; ++d) r |= dmalloc(c, &c->d_P[b][d], N);
+    r |= dmalloc(c, &c->d_phi, N); r |= dmalloc(c, &c->d_phi_old, N); r |= dmalloc(c, &c->d_phi_prev, N);
+    r |= dmalloc(c, &c->d_rho, N); r |= dmalloc(c, &c->d_e, N); r |= dmalloc(c, &c->d_h, N);
+    r |= dmalloc(c, &c->d_alpha, N); r |= dmalloc(c, &c->d_alpha32, N); r |= dmalloc(c, &c->d_rhs, N);
+    r |= dmalloc(c, &c->d_rhsP, N); r |= dmalloc(c, &c->d_dphi, N);
+    r |= dmalloc(c, &c->d_part, 4 * 148 * 8 + 64);
+    r |= dmalloc(c, &c->d_counter, 4);
+    r |= dmalloc(c, &c->d_out, 8);
+    if (r) return r;
+    FX_CUDA(c, cudaMallocHost(&c->h_out, 8 * sizeof(double)));
+    if (!c->var.empty()) {
+        r |= dmalloc(c, &c->d_var, N);
+        r |= dmalloc(c, &c->d_vt, c->variants.size());
+        if (r) return r;
+        FX_CUDA(c, cudaMemcpy(c->d_var, c->var.data(), N, cudaMemcpyHostToDevice));
+        FX_CUDA(c, cudaMemcpy(c->d_vt, c->variants.data(), c->variants.size() * sizeof(Variant), cudaMemcpyHostToDevice));
+    }
+    FX_CUDA(c, cudaMemcpy(c->d_code, c->code.data(), c->code.size(), cudaMemcpyHostToDevice));
+    for (int b = 0; b < 2; ++b)
+        for (int d = 0; d < 3; ++d) FX_CUDA(c, cudaMemcpy(c->d_P[b][d], c->P0[d].data(), N * 8, cudaMemcpyHostToDevice));
+    // main.cpp:157-173 zero fields; InitializePandRho's intrinsic carriers in SC
+    std::vector<double> rho0(N, 0.0), e0(N, 0.0);
+    const double ni = std::sqrt(kNc * kNv) * exp(-0.5 * kQ * kEg / (kKb * kT));
+    for (size_t q = 0; q < N; ++q)
+        if ((c->code[q + c->nxy] & 3) >= 2) {
+            e0[q] = ni;
+            rho0[q] = kQ * (ni - ni - c->par.acceptor_doping + c->par.donor_doping);
+        }
+    FX_CUDA(c, cudaMemcpy(c->d_rho, rho0.data(), N * 8, cudaMemcpyHostToDevice));
+    FX_CUDA(c, cudaMemcpy(c->d_e, e0.data(), N * 8, cudaMemcpyHostToDevice));
+    FX_CUDA(c, cudaMemcpy(c->d_h, e0.data(), N * 8, cudaMemcpyHostToDevice));
+    for (double* a : {c->d_phi, c->d_phi_old, c->d_phi_prev, c->d_alpha, c->d_rhs, c->d_rhsP, c->d_dphi})
+        FX_CUDA(c, cudaMemset(a, 0, N * 8));
+    FX_CUDA(c, cudaMemset(c->d_alpha32, 0, N * 4));
+    FX_CUDA(c, cudaMemset(c->d_counter, 0, 4));
+    const bool mixed = c->par.precision == 1;
+    c->mg.verbose = c->par.verbose;
+    int st = c->mg.setup(c->dp, c->code, true, mixed);
+    if (st == -2) return set_err(c, FX_ERR_OUT_OF_MEMORY, "multigrid allocation failed");
+    if (st != 0) return set_err(c, FX_ERR_CUDA, "multigrid setup failed");
+    c->dev_bytes += c->mg.bytes();
+    c->mg_ready = true;
+    c->dev = true;
+    FX_CUDA(c, cudaDeviceSynchronize());
+    return FX_OK;
+}
+
+const double* const* P_in(fx_ctx* c, const double* arr[3]) {
+    arr[0] = c->scalarP ? nullptr : c->d_P[c->cur][0];
+    arr[1] = c->scalarP ? nullptr : c->d_P[c->cur][1];
+    arr[2] = c->d_P[c->cur][2];
+    return arr;
+}
+
+int k_status(fx_ctx* c, int e) {
+    if (e) return set_err(c, FX_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString((cudaError_t)e));
+    return FX_OK;
+}
+
+int read_out(fx_ctx* c, int n) {
+    FX_CUDA(c, cudaMemcpyAsync(c->h_out, c->d_out, n * sizeof(double), cudaMemcpyDeviceToHost, c->s));
+    FX_CUDA(c, cudaStreamSynchronize(c->s));
+    return FX_OK;
+}
+
+// the FE part of ComputePoissonRHS for the present P
+int compute_rhs_p(fx_ctx* c, bool norms) {
+    const double* P[3];
+    P_in(c, P);
+    if (norms) FX_CUDA(c, cudaMemsetAsync(c->d_out, 0, 2 * sizeof(double), c->s));
+    ++g_launches;
+    c->prof.begin(PROF_RHS_P, c->s);
+    int e = launch_rhs_p(c->dp, c->d_code, c->d_var, c->d_vt, P, c->d_rhsP, norms ? c->d_out : nullptr, c->s);
+    c->prof.end(c->s);
+    return k_status(c, e);
+}
+
+int mg_solve(fx_ctx* c, const double* rhs, double nb, double nbp) {
+    const double target = std::max(c->par.mg_rtol, 1e-16) * std::max(nb, nbp);
+    if (!c->par.warm_start) FX_CUDA(c, cudaMemsetAsync(c->d_phi, 0, c->N * 8, c->s));
+    MGStats st;
+    int r = c->par.precision == 1
+                ? c->mg.solve_mixed(c->dp, c->d_code, c->d_phi, rhs, target, c->par.mg_max_iter, c->s, &st)
+                : c->mg.solve64(c->dp, c->d_code, c->d_phi, rhs, target, c->par.mg_max_iter, c->s, &st);
+    c->mg_last += st.cycles;
+    c->mg_total += st.cycles;
+    c->mg_resid_last = st.resid;
+    c->mg_target_last = target;
+    if (r == -3) {
+        std::ostringstream o;
+        o << "Poisson multigrid did not reach |r| <= " << target << " in " << c->par.mg_max_iter << " cycles (|r| = " << st.resid << ")";
+        return set_err(c, std::isfinite(st.resid) ? FX_ERR_NO_CONVERGENCE : FX_ERR_NONFINITE, o.str());
+    }
+    if (r) return set_err(c, FX_ERR_CUDA, std::string("multigrid: ") + cudaGetErrorString((cudaError_t)r));
+    return FX_OK;
+}
+
+// ComputePhi_Rho, ElectrostaticSolver.cpp:678-747
+int compute_phi_rho(fx_ctx* c) {
+    int r = ensure_device(c);
+    if (r) return r;
+    c->E_valid = false;
+    c->mg_last = 0;
+    if (!c->contains_sc) {
+        r = compute_rhs_p(c, true);
+        if (r) return r;
+        r = read_out(c, 2);
+        if (r) return r;
+        const double nb = c->h_out[0], nbp = c->h_out[1];
+        c->mg.set_alpha(nullptr, nullptr, false, c->s);
+        r = mg_solve(c, c->d_rhsP, nb, nbp);
+        if (r) return r;
+        c->rhs_is_newton = false;
+        c->newton_last = 1;
+        c->newton_total += 1;
+        c->phi_err_last = 0.0;
+        return FX_OK;
+    }
+    r = compute_rhs_p(c, false);
+    if (r) return r;
+    const double tol = 1.e-5;
+    double err = 1.0;
+    int iter = 0, passes = 0;
+    while (err > tol) {
+        if (passes >= c->par.newton_max_iter) {
+            std::ostringstream o;
+            o << "Phi-rho Newton iteration did not reach 1e-5 in " << passes << " passes (err = " << err << ")";
+            return set_err(c, std::isfinite(err) ? FX_ERR_NO_CONVERGENCE : FX_ERR_NONFINITE, o.str());
+        }
+        ++passes;
+        FX_CUDA(c, cudaMemsetAsync(c->d_out, 0, 2 * sizeof(double), c->s));
+        ++g_launches;
+        c->prof.begin(PROF_NEWTON, c->s);
+        r = k_status(c, launch_newton(c->dp, c->d_code, c->d_phi, c->d_rho, c->d_rhsP, c->d_alpha, c->d_alpha32,
+                                      c->d_rhs, c->d_out, c->s));
+        c->prof.end(c->s);
+        if (r) return r;
+        r = read_out(c, 2);
+        if (r) return r;
+        const double nb = c->h_out[0], nbp = c->h_out[1];
+        c->mg.set_alpha(c->d_alpha, c->d_alpha32, true, c->s);
+        r = mg_solve(c, c->d_rhs, nb, nbp);
+        if (r) return r;
+        ++g_launches;
+        c->prof.begin(PROF_RHO, c->s);
+        r = k_status(c, launch_rho(c->dp, c->d_code, c->d_phi, c->d_phi_prev, c->d_rho, c->d_e, c->d_h, c->d_part,
+                                   c->d_counter, c->d_out, 1, c->s));
+        c->prof.end(c->s);
+        if (r) return r;
+        r = read_out(c, 2);
+        if (r) return r;
+        if (iter > 0) err = c->h_out[0] / c->h_out[1];
+        iter = iter + 1;
+        if (c->par.verbose) printf("%d iterations :: err = %g\n", iter, err);
+    }
+    c->rhs_is_newton = true;
+    c->newton_last = passes;
+    c->newton_total += passes;
+    c->phi_err_last = err;
+    return FX_OK;
+}
+
+int tdgl_update(fx_ctx* c) {
+    int r = ensure_device(c);
+    if (r) return r;
+    if (c->par.TimeIntegratorOrder != 1)
+        return set_err(c, FX_ERR_UNSUPPORTED, "TimeIntegratorOrder = 2 is not implemented in this build");
+    const double* Pin[3];
+    P_in(c, Pin);
+    double* Pout[3] = {c->scalarP ? nullptr : c->d_P[1 - c->cur][0], c->scalarP ? nullptr : c->d_P[1 - c->cur][1],
+                       c->d_P[1 - c->cur][2]};
+    ++g_launches;
+    c->prof.begin(PROF_TDGL, c->s);
+    r = k_status(c, launch_tdgl(c->dp, c->par.precision == 1, c->d_code, c->d_var, c->d_vt, Pin, Pout, c->d_phi, c->s));
+    c->prof.end(c->s);
+    if (r) return r;
+    c->cur = 1 - c->cur;
+    return FX_OK;
+}
+
+int check_steady(fx_ctx* c, int step) {
+    int r = ensure_device(c);
+    if (r) return r;
+    FX_CUDA(c, cudaMemsetAsync(c->d_out, 0, 2 * sizeof(double), c->s));
+    ++g_launches;
+    c->prof.begin(PROF_STEADY, c->s);
+    r = k_status(c, launch_steady(c->dp, c->d_phi, c->d_phi_old, c->d_dphi, c->d_out, c->s));
+    c->prof.end(c->s);
+    if (r) return r;
+    r = read_out(c, 2);
+    if (r) return r;
+    const double phi_max = c->h_out[0], dmax = c->h_out[1];
+    double max_phi_err;
+    if (phi_max > 0) max_phi_err = dmax / phi_max;
+    else max_phi_err = dmax > 0 ? INFINITY : 0.0;   // all-NaN Phidiff passes norm0 as 0
+    c->phi_max_last = phi_max;
+    if (step > 1 && max_phi_err < c->par.phi_tolerance) {
+        c->steady_state_step = step;
+        c->inc_step = step;
+    }
+    c->steady_err_last = max_phi_err;
+    if (c->par.verbose) printf("Steady state check : (phi(t) - phi(t-1)).norm0() = %g\n", max_phi_err);
+    return FX_OK;
+}
+
+// one pass of main.cpp:261-621; returns 1 when the loop breaks
+int step_once(fx_ctx* c) {
+    const int step = c->step + 1;
+    int r = compute_phi_rho(c);
+    if (r) return r;
+    r = tdgl_update(c);
+    if (r) return r;
+    r = check_steady(c, step);
+    if (r) return r;
+    c->E_valid = false;
+    c->time = c->time + c->par.dt;
+    c->step = step;
+    const Params& p = c->par;
+    const double tiny = 1.e-6;
+    bool inc = false;
+    if (p.voltage_sweep == 1) {
+        if (p.sweep_mode == 1) inc = p.steps_per_voltage > 0 && step % p.steps_per_voltage == 0;
+        else inc = c->inc_step > 0 && step == c->inc_step;
+    }
+    if (inc) {
+        c->Phi_Bc_hi += c->sign * p.Phi_Bc_inc;
+        c->num_Vapp += 1;
+        if (std::fabs(std::fabs(c->Phi_Bc_hi) - p.Phi_Bc_hi_max) <= tiny) c->sign *= -1;
+        if (c->par.verbose)
+            printf("step = %d, Phi_Bc_hi = %g, num_Vapp = %d, sign = %d\n", step, c->Phi_Bc_hi, c->num_Vapp, c->sign);
+        electrode_values(c);
+        r = compute_phi_rho(c);
+        if (r) return r;
+    }
+    bool brk = false;
+    if (p.voltage_sweep == 0 && step == c->steady_state_step) brk = true;
+    if (p.voltage_sweep == 1 && c->Phi_Bc_hi > 0. && c->Phi_Bc_hi - p.Phi_Bc_hi_max > tiny) brk = true;
+    if (p.voltage_sweep == 1 && c->Phi_Bc_hi < 0. && -c->Phi_Bc_hi - p.Phi_Bc_hi_max > tiny) brk = true;
+    if (p.voltage_sweep == 1 && c->num_Vapp == p.num_Vapp_max) brk = true;
+    if (brk) c->finished = true;
+    c->prof.collect();
+    return brk ? 1 : 0;
+}
+
+int materialize_E(fx_ctx* c) {
+    int r = ensure_device(c);
+    if (r) return r;
+    if (c->E_valid) return FX_OK;
+    for (int d = 0; d < 3; ++d)
+        if (!c->d_E[d]) { r = dmalloc(c, &c->d_E[d], c->N); if (r) return r; }
+    ++g_launches;
+    c->prof.begin(PROF_EFIELD, c->s);
+    r = k_status(c, launch_efield(c->dp, c->d_var, c->d_vt, c->d_phi, c->d_E, c->s));
+    c->prof.end(c->s);
+    if (r) return r;
+    c->E_valid = true;
+    return FX_OK;
+}
+
+int host_field(fx_ctx* c, int f, std::vector<double>& out) {
+    const size_t N = c->N;
+    out.assign(N, 0.0);
+    switch (f) {
+    case FX_FIELD_EPSILON:
+        for (size_t q = 0; q < N; ++q) out[q] = eps_of_code(c->par, c->code[q + c->nxy]);
+        return 1;
+    case FX_FIELD_MASK:
+        for (size_t q = 0; q < N; ++q) out[q] = (double)(c->code[q + c->nxy] & 3);
+        return 1;
+    case FX_FIELD_TPHASE: out = c->tphase; return 1;
+    case FX_FIELD_ANGLE_ALPHA: out = c->ang[0]; return 1;
+    case FX_FIELD_ANGLE_BETA: out = c->ang[1]; return 1;
+    case FX_FIELD_ANGLE_THETA: out = c->ang[2]; return 1;
+    case FX_FIELD_GAMMA:
+        for (size_t q = 0; q < N; ++q) out[q] = (c->code[q + c->nxy] & 3) == 0 ? c->par.BigGamma : 0.0;
+        return 1;
+    }
+    return 0;
+}
+
+int get_field(fx_ctx* c, int f, double* out) {
+    std::vector<double> h;
+    if (host_field(c, f, h)) {
+        std::memcpy(out, h.data(), c->N * 8);
+        return FX_OK;
+    }
+    if (!c->dev && (f == FX_FIELD_PX || f == FX_FIELD_PY || f == FX_FIELD_PZ)) {
+        std::memcpy(out, c->P0[f].data(), c->N * 8);
+        return FX_OK;
+    }
+    int r = ensure_device(c);
+    if (r) return r;
+    const double* src = nullptr;
+    switch (f) {
+    case FX_FIELD_PX: case FX_FIELD_PY: case FX_FIELD_PZ: src = c->d_P[c->cur][f]; break;
+    case FX_FIELD_PHI: src = c->d_phi; break;
+    case FX_FIELD_POISSON_RHS: src = c->rhs_is_newton ? c->d_rhs : c->d_rhsP; break;
+    case FX_FIELD_EX: case FX_FIELD_EY: case FX_FIELD_EZ:
+        r = materialize_E(c);
+        if (r) return r;
+        src = c->d_E[f - FX_FIELD_EX];
+        break;
+    case FX_FIELD_HOLES: src = c->d_h; break;
+    case FX_FIELD_ELECTRONS: src = c->d_e; break;
+    case FX_FIELD_CHARGE: src = c->d_rho; break;
+    case FX_FIELD_PHIDIFF: src = c->d_dphi; break;
+    case FX_FIELD_ALPHA_CC: src = c->d_alpha; break;
+    default: return set_err(c, FX_ERR_INVALID_ARGUMENT, "unknown field id");
+    }
+    FX_CUDA(c, cudaMemcpyAsync(out, src, c->N * 8, cudaMemcpyDeviceToHost, c->s));
+    FX_CUDA(c, cudaStreamSynchronize(c->s));
+    if (f == FX_FIELD_PHIDIFF) {
+        // Phidiff = |phi - phi_old| / max|phi| (ElectrostaticSolver.cpp:542)
+        const double m = c->phi_max_last;
+        for (size_t q = 0; q < c->N; ++q) out[q] = out[q] / m;
+    }
+    return FX_OK;
+}
+
+void read_inputs(const char* inputs, int is_text, std::string& text) {
+    if (is_text) { text = inputs; return; }
+    std::ifstream f(inputs);
+    if (!f) throw FxError{FX_ERR_IO, std::string("cannot open inputs file ") + inputs};
+    std::stringstream ss;
+    ss << f.rdbuf();
+    text = ss.str();
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* fx_version(void) { return "ferrox_b200 0.1 (sm_100a)"; }
+
+const char* fx_create_error(void) { return t_create_error.c_str(); }
+
+int fx_create(const char* inputs, int is_text, fx_ctx** out) {
+    if (!out) return FX_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    t_create_error.clear();
+    if (!inputs) { t_create_error = "inputs is NULL"; return FX_ERR_INVALID_ARGUMENT; }
+    std::unique_ptr<fx_ctx> c(new fx_ctx());
+    try {
+        std::string text;
+        read_inputs(inputs, is_text, text);
+        c->in = parse_inputs(text);
+        c->par = make_params(c->in);
+        Params& p = c->par;
+        if (!p.is_periodic[0] || !p.is_periodic[1] || p.is_periodic[2])
+            throw FxError{FX_ERR_UNSUPPORTED, "only domain.is_periodic = 1 1 0 (periodic x/y, electrodes in z) is supported"};
+        for (int d = 0; d < 2; ++d)
+            if ((!p.bc_lo[d].empty() && p.bc_lo[d].substr(0, 3) != "per") || (!p.bc_hi[d].empty() && p.bc_hi[d].substr(0, 3) != "per"))
+                throw FxError{FX_ERR_INPUTS, "boundary.lo/hi must be 'per' in periodic directions (BoundaryConditions.cpp:196)"};
+        if ((!p.bc_lo[2].empty() && p.bc_lo[2].substr(0, 3) != "dir") || (!p.bc_hi[2].empty() && p.bc_hi[2].substr(0, 3) != "dir"))
+            throw FxError{FX_ERR_UNSUPPORTED, "z boundaries must be Dirichlet electrodes (dir)"};
+        c->nx = p.n_cell[0]; c->ny = p.n_cell[1]; c->nz = p.n_cell[2];
+        for (int d = 0; d < 2; ++d)
+            if (p.n_cell[d] != 1 && p.n_cell[d] % 2 != 0)
+                throw FxError{FX_ERR_UNSUPPORTED, "periodic x/y cell counts must be even (red-black ordering) or 1"};
+        c->nxy = (size_t)c->nx * c->ny;
+        c->N = c->nxy * c->nz;
+        for (int d = 0; d < 3; ++d) c->dx[d] = (p.prob_hi[d] - p.prob_lo[d]) / p.n_cell[d];
+        // DphiDz decides the electrode layers from cell-face positions
+        // (ElectrostaticSolver.cpp:162-163); the device uses k == 0 / nz-1
+        for (int k = 0; k < c->nz; ++k) {
+            const double z_hi = p.prob_lo[2] + (k + 1.5) * c->dx[2];
+            const double z_lo = p.prob_lo[2] + (k - 0.5) * c->dx[2];
+            const bool bot = z_lo < p.prob_lo[2], top = !bot && z_hi > p.prob_hi[2];
+            if (bot != (k == 0) || top != (k == c->nz - 1 && c->nz > 1))
+                throw FxError{FX_ERR_UNSUPPORTED, "electrode-layer test of DphiDz does not select k = 0 / nz-1 for this grid"};
+        }
+        // t-phase mask and Euler angles (main.cpp:178-181)
+        c->tphase.assign(c->N, 0.0);
+        for (int d = 0; d < 3; ++d) c->ang[d].assign(c->N, 0.0);
+        if (p.Coordinate_Transformation == 1) {
+            const char* keys[4] = {"tphase_geom.tphase_geom_function(x,y,z)", "angle_alpha.alpha_function(x,y,z)",
+                                   "angle_beta.beta_function(x,y,z)", "angle_theta.theta_function(x,y,z)"};
+            std::vector<double>* dst[4] = {&c->tphase, &c->ang[0], &c->ang[1], &c->ang[2]};
+            for (int f = 0; f < 4; ++f) {
+                auto it = c->in.table.find(keys[f]);
+                if (it == c->in.table.end() || it->second.empty()) continue;   // set later by fx_set_grains
+                std::string ex;
+                for (auto& s : it->second) ex += (ex.empty() ? "" : " ") + s;
+                auto e = compile_expr(ex, c->in.constants);
+                for (int k = 0; k < c->nz; ++k)
+                    for (int j = 0; j < c->ny; ++j)
+                        for (int i = 0; i < c->nx; ++i)
+                            (*dst[f])[(size_t)i + c->nx * ((size_t)j + (size_t)c->ny * k)] =
+                                e->eval(p.prob_lo[0] + (i + 0.5) * c->dx[0], p.prob_lo[1] + (j + 0.5) * c->dx[1],
+                                        p.prob_lo[2] + (k + 0.5) * c->dx[2]);
+            }
+        }
+        build_codes(c.get());
+        std::string w = check_wrapped_mask(c.get());
+        if (!w.empty()) throw FxError{FX_ERR_UNSUPPORTED, w};
+        build_variants(c.get(), nullptr, nullptr);
+        build_P0(c.get());
+        c->Phi_Bc_hi = p.Phi_Bc_hi;
+        c->inc_step = p.inc_step;
+        fill_devparams(c.get());
+    } catch (FxError& e) {
+        t_create_error = e.msg;
+        return e.code;
+    } catch (std::exception& e) {
+        t_create_error = e.what();
+        return FX_ERR_INPUTS;
+    }
+    *out = c.release();
+    return FX_OK;
+}
+
+void fx_destroy(fx_ctx* c) {
+    if (!c) return;
+    if (c->dev) {
+        cudaStreamSynchronize(c->s);
+        cudaFree(c->d_code); cudaFree(c->d_var); cudaFree(c->d_vt);
+        for (int b = 0; b < 2; ++b)
+            for (int d = 0; d < 3; ++d) cudaFree(c->d_P[b][d]);
+        for (double* a : {c->d_phi, c->d_phi_old, c->d_phi_prev, c->d_rho, c->d_e, c->d_h, c->d_alpha, c->d_rhs,
+                          c->d_rhsP, c->d_dphi, c->d_E[0], c->d_E[1], c->d_E[2], c->d_part, c->d_out})
+            cudaFree(a);
+        cudaFree(c->d_alpha32);
+        cudaFree(c->d_counter);
+        if (c->h_out) cudaFreeHost(c->h_out);
+        c->prof.collect();
+        if (c->own_stream) cudaStreamDestroy(c->s);
+    }
+    delete c;
+}
+
+const char* fx_last_error(const fx_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int fx_get_dims(const fx_ctx* c, int n[3], double dx[3]) {
+    if (!c) return FX_ERR_INVALID_ARGUMENT;
+    if (n) { n[0] = c->nx; n[1] = c->ny; n[2] = c->nz; }
+    if (dx) for (int d = 0; d < 3; ++d) dx[d] = c->dx[d];
+    return FX_OK;
+}
+
+int fx_get_param(const fx_ctx* c, const char* key, double* v) {
+    if (!c || !key || !v) return FX_ERR_INVALID_ARGUMENT;
+    const Params& p = c->par;
+    const std::string k(key);
+    static const char* arr3[] = {"FE_lo", "FE_hi", "DE_lo", "DE_hi", "SC_lo", "SC_hi", "Channel_lo", "Channel_hi", "Remnant_P",
+                                 "domain.prob_lo", "domain.prob_hi"};
+    const std::map<std::string, double> m = {
+        {"dt", p.dt}, {"lambda", p.lambda}, {"epsilon_0", p.epsilon_0}, {"epsilonX_fe", p.epsilonX_fe},
+        {"epsilonX_fe_tphase", p.epsilonX_fe_tphase}, {"epsilonZ_fe", p.epsilonZ_fe}, {"epsilon_de", p.epsilon_de},
+        {"epsilon_si", p.epsilon_si}, {"alpha", p.alpha}, {"beta", p.beta}, {"gamma", p.gamma}, {"alpha_12", p.alpha_12},
+        {"alpha_112", p.alpha_112}, {"alpha_123", p.alpha_123}, {"BigGamma", p.BigGamma}, {"g11", p.g11}, {"g44", p.g44},
+        {"g12", p.g12}, {"g44_p", p.g44_p}, {"acceptor_doping", p.acceptor_doping}, {"donor_doping", p.donor_doping},
+        {"use_Fermi_Dirac", p.use_Fermi_Dirac}, {"use_work_function", p.use_work_function},
+        {"metal_work_function", p.metal_work_function}, {"is_polarization_scalar", p.is_polarization_scalar},
+        {"delta", p.delta}, {"voltage_sweep", p.voltage_sweep}, {"inc_step", c->inc_step}, {"Phi_Bc_lo", p.Phi_Bc_lo},
+        {"Phi_Bc_hi", c->Phi_Bc_hi}, {"Phi_Bc_inc", p.Phi_Bc_inc}, {"Phi_Bc_hi_max", p.Phi_Bc_hi_max},
+        {"phi_tolerance", p.phi_tolerance}, {"num_Vapp_max", p.num_Vapp_max}, {"random_seed", p.random_seed},
+        {"include_Landau", p.include_Landau}, {"include_Grad", p.include_Grad}, {"include_Elec", p.include_Elec},
+        {"Coordinate_Transformation", p.Coordinate_Transformation}, {"use_Euler_angles", p.use_Euler_angles},
+        {"prob_type", p.prob_type}, {"TimeIntegratorOrder", p.TimeIntegratorOrder}, {"nsteps", p.nsteps},
+        {"plot_int", p.plot_int}, {"fx.mg_rtol", p.mg_rtol}, {"fx.phi_ghost_mode", p.phi_ghost_mode},
+        {"fx.sweep_mode", p.sweep_mode}, {"fx.steps_per_voltage", p.steps_per_voltage},
+        {"fx.newton_max_iter", p.newton_max_iter}, {"fx.mg_max_iter", p.mg_max_iter}, {"fx.precision", p.precision},
+        {"fx.warm_start", p.warm_start}, {"contains_sc", c->contains_sc ? 1.0 : 0.0},
+        {"V_lo", c->dp.V_lo}, {"V_hi", c->dp.V_hi}, {"phi_ref", phi_ref()},
+        {"intrinsic_carrier_concentration", std::sqrt(kNc * kNv) * exp(-0.5 * kQ * kEg / (kKb * kT))},
+        {"num_variants", (double)c->variants.size()}};
+    auto it = m.find(k);
+    if (it != m.end()) { *v = it->second; return FX_OK; }
+    // "FE_lo[2]" style access to the 3-vectors
+    for (const char* a : arr3) {
+        const std::string s(a);
+        if (k.size() == s.size() + 3 && k.compare(0, s.size(), s) == 0 && k[s.size()] == '[' && k.back() == ']') {
+            const int d = k[s.size() + 1] - '0';
+            if (d < 0 || d > 2) break;
+            const double* arr = s == "FE_lo" ? p.FE_lo : s == "FE_hi" ? p.FE_hi : s == "DE_lo" ? p.DE_lo : s == "DE_hi" ? p.DE_hi
+                              : s == "SC_lo" ? p.SC_lo : s == "SC_hi" ? p.SC_hi : s == "Channel_lo" ? p.Channel_lo
+                              : s == "Channel_hi" ? p.Channel_hi : s == "Remnant_P" ? p.Remnant_P
+                              : s == "domain.prob_lo" ? p.prob_lo : p.prob_hi;
+            *v = arr[d];
+            return FX_OK;
+        }
+    }
+    for (const char* a : {"P_BC_flag_lo", "P_BC_flag_hi", "domain.n_cell", "domain.is_periodic"}) {
+        const std::string s(a);
+        if (k.size() == s.size() + 3 && k.compare(0, s.size(), s) == 0 && k[s.size()] == '[') {
+            const int d = k[s.size() + 1] - '0';
+            if (d < 0 || d > 2) break;
+            const int* arr = s == "P_BC_flag_lo" ? p.P_BC_flag_lo : s == "P_BC_flag_hi" ? p.P_BC_flag_hi
+                           : s == "domain.n_cell" ? p.n_cell : p.is_periodic;
+            *v = arr[d];
+            return FX_OK;
+        }
+    }
+    return FX_ERR_INVALID_ARGUMENT;
+}
+
+int fx_set_param(fx_ctx* c, const char* key, double v) {
+    if (!c || !key) return FX_ERR_INVALID_ARGUMENT;
+    const std::string k(key);
+    Params& p = c->par;
+    if (k == "Phi_Bc_hi") { c->Phi_Bc_hi = v; electrode_values(c); c->E_valid = false; return FX_OK; }
+    if (k == "Phi_Bc_lo") { p.Phi_Bc_lo = v; electrode_values(c); c->E_valid = false; return FX_OK; }
+    if (k == "fx.mg_rtol") { p.mg_rtol = v; return FX_OK; }
+    if (k == "fx.mg_max_iter") { p.mg_max_iter = (int)v; return FX_OK; }
+    if (k == "fx.newton_max_iter") { p.newton_max_iter = (int)v; return FX_OK; }
+    if (k == "fx.warm_start") { p.warm_start = (int)v; return FX_OK; }
+    if (k == "fx.verbose") { p.verbose = (int)v; c->mg.verbose = (int)v; return FX_OK; }
+    if (k == "fx.profile") { c->prof.collect(); c->prof.on = v != 0.0; return FX_OK; }
+    if (k == "fx.mg_nu1") { c->mg.nu1 = (int)v; return FX_OK; }
+    if (k == "fx.mg_nu2") { c->mg.nu2 = (int)v; return FX_OK; }
+    if (k == "fx.phi_ghost_mode") { p.phi_ghost_mode = (int)v; c->dp.ghost_mode = (int)v; c->E_valid = false; return FX_OK; }
+    if (k == "dt") { p.dt = v; c->dp.dt = v; return FX_OK; }
+    if (k == "alpha") { p.alpha = v; c->dp.alpha = v; return FX_OK; }
+    if (k == "beta") { p.beta = v; c->dp.beta = v; return FX_OK; }
+    if (k == "gamma") { p.gamma = v; c->dp.gamma = v; return FX_OK; }
+    if (k == "g11") { p.g11 = v; c->dp.g11 = v; return FX_OK; }
+    if (k == "g44") { p.g44 = v; c->dp.g44 = v; return FX_OK; }
+    if (k == "BigGamma") { p.BigGamma = v; c->dp.BigGamma = v; return FX_OK; }
+    if (k == "inc_step") { c->inc_step = (int)v; return FX_OK; }
+    return set_err(c, FX_ERR_INVALID_ARGUMENT, "parameter '" + k + "' cannot be set after creation");
+}
+
+int fx_set_precision(fx_ctx* c, int mode) {
+    if (!c || (mode != 0 && mode != 1)) return FX_ERR_INVALID_ARGUMENT;
+    if (c->dev && mode != c->par.precision)
+        return set_err(c, FX_ERR_INVALID_ARGUMENT, "precision must be chosen before the first device call");
+    c->par.precision = mode;
+    return FX_OK;
+}
+
+int fx_set_initial_P(fx_ctx* c, const double* Px, const double* Py, const double* Pz, size_t n) {
+    if (!c || !Pz || n != c->N) return c ? set_err(c, FX_ERR_INVALID_ARGUMENT, "P arrays must hold nx*ny*nz values") : FX_ERR_INVALID_ARGUMENT;
+    const double* src[3] = {Px, Py, Pz};
+    bool zero_xy = true;
+    for (int d = 0; d < 2; ++d)
+        if (src[d]) for (size_t q = 0; q < n; ++q) if (src[d][q] != 0.0) { zero_xy = false; break; }
+    for (int d = 0; d < 3; ++d) {
+        if (src[d]) c->P0[d].assign(src[d], src[d] + n);
+        else c->P0[d].assign(n, 0.0);
+    }
+    c->user_P = true;
+    c->scalarP = c->par.is_polarization_scalar == 1 && zero_xy;
+    if (c->dev) {
+        for (int b = 0; b < 2; ++b)
+            for (int d = 0; d < 3; ++d)
+                FX_CUDA(c, cudaMemcpyAsync(c->d_P[b][d], c->P0[d].data(), n * 8, cudaMemcpyHostToDevice, c->s));
+        FX_CUDA(c, cudaStreamSynchronize(c->s));
+    }
+    return FX_OK;
+}
+
+int fx_set_grains(fx_ctx* c, const uint8_t* gid, size_t n, const double* ang, const uint8_t* gtph, int ng) {
+    if (!c) return FX_ERR_INVALID_ARGUMENT;
+    if (!gid || !ang || !gtph || n != c->N || ng <= 0 || ng > 255)
+        return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx_set_grains: bad arguments");
+    if (c->dev) return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx_set_grains must precede the first device call");
+    std::vector<uint8_t> g(gid, gid + n);
+    for (size_t q = 0; q < n; ++q) {
+        if (g[q] != 255 && g[q] >= ng) return set_err(c, FX_ERR_INVALID_ARGUMENT, "grain id out of range");
+        const bool in = g[q] != 255;
+        c->tphase[q] = in ? (gtph[g[q]] ? 1.0 : 0.0) : 0.0;
+        for (int d = 0; d < 3; ++d) c->ang[d][q] = in ? ang[3 * g[q] + d] : 0.0;
+    }
+    try {
+        build_codes(c);
+        std::string w = check_wrapped_mask(c);
+        if (!w.empty()) return set_err(c, FX_ERR_UNSUPPORTED, w);
+        c->gid = g;
+        build_variants(c, &c->gid, c->galpha.empty() ? nullptr : &c->galpha);
+    } catch (FxError& e) {
+        return set_err(c, e.code, e.msg);
+    }
+    c->grains_set = true;
+    if (!c->user_P) build_P0(c);
+    else for (size_t q = 0; q < n; ++q) if (c->tphase[q] == 1.0) c->P0[2][q] = 0.0;
+    return FX_OK;
+}
+
+int fx_set_grain_alpha(fx_ctx* c, const double* alpha, int ng) {
+    if (!c || !alpha || ng <= 0) return FX_ERR_INVALID_ARGUMENT;
+    if (!c->grains_set) return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx_set_grains must come first");
+    c->galpha.assign(alpha, alpha + ng);
+    try {
+        build_variants(c, &c->gid, &c->galpha);
+    } catch (FxError& e) {
+        return set_err(c, e.code, e.msg);
+    }
+    if (c->dev) {
+        cudaFree(c->d_vt);
+        c->d_vt = nullptr;
+        int r = dmalloc(c, &c->d_vt, c->variants.size());
+        if (r) return r;
+        FX_CUDA(c, cudaMemcpy(c->d_var, c->var.data(), c->N, cudaMemcpyHostToDevice));
+        FX_CUDA(c, cudaMemcpy(c->d_vt, c->variants.data(), c->variants.size() * sizeof(Variant), cudaMemcpyHostToDevice));
+    }
+    return FX_OK;
+}
+
+int fx_get_field(fx_ctx* c, int f, double* out, size_t n) {
+    if (!c || !out) return FX_ERR_INVALID_ARGUMENT;
+    if (f < 0 || f >= FX_NFIELDS) return set_err(c, FX_ERR_INVALID_ARGUMENT, "unknown field id");
+    if (n != c->N) return set_err(c, FX_ERR_INVALID_ARGUMENT, "field buffers hold nx*ny*nz values");
+    return get_field(c, f, out);
+}
+
+int fx_set_field(fx_ctx* c, int f, const double* in, size_t n) {
+    if (!c || !in) return FX_ERR_INVALID_ARGUMENT;
+    if (n != c->N) return set_err(c, FX_ERR_INVALID_ARGUMENT, "field buffers hold nx*ny*nz values");
+    if (f == FX_FIELD_PX || f == FX_FIELD_PY || f == FX_FIELD_PZ) {
+        if (f != FX_FIELD_PZ && c->scalarP) {
+            bool nz = false;
+            for (size_t q = 0; q < n; ++q) if (in[q] != 0.0) { nz = true; break; }
+            if (nz) {
+                if (c->dev) return set_err(c, FX_ERR_INVALID_ARGUMENT, "nonzero Px/Py must be set before the first device call");
+                c->scalarP = false;
+            }
+        }
+        if (!c->dev) { c->P0[f].assign(in, in + n); c->user_P = true; return FX_OK; }
+        FX_CUDA(c, cudaMemcpyAsync(c->d_P[c->cur][f], in, n * 8, cudaMemcpyHostToDevice, c->s));
+        FX_CUDA(c, cudaStreamSynchronize(c->s));
+        c->E_valid = false;
+        return FX_OK;
+    }
+    if (f == FX_FIELD_PHI) {
+        int r = ensure_device(c);
+        if (r) return r;
+        FX_CUDA(c, cudaMemcpyAsync(c->d_phi, in, n * 8, cudaMemcpyHostToDevice, c->s));
+        FX_CUDA(c, cudaStreamSynchronize(c->s));
+        c->E_valid = false;
+        return FX_OK;
+    }
+    return set_err(c, FX_ERR_INVALID_ARGUMENT, "only Px, Py, Pz and Phi can be set");
+}
+
+int fx_compute_poisson_rhs(fx_ctx* c) {
+    if (!c) return FX_ERR_INVALID_ARGUMENT;
+    int r = ensure_device(c);
+    if (r) return r;
+    r = compute_rhs_p(c, false);
+    if (r) return r;
+    if (c->contains_sc) {
+        // SC cells take rho (ElectrostaticSolver.cpp:65-67): the Newton kernel
+        // with alpha forced to zero is not the reference's RHS, so combine here
+        FX_CUDA(c, cudaMemsetAsync(c->d_out, 0, 2 * sizeof(double), c->s));
+        DevParams q = c->dp;
+        q.delta = 0.0; q.inv_delta = 0.0; q.neg_inv_delta = 0.0;
+        ++g_launches;
+        r = k_status(c, launch_newton(q, c->d_code, c->d_phi, c->d_rho, c->d_rhsP, c->d_alpha, c->d_alpha32, c->d_rhs,
+                                      c->d_out, c->s));
+        if (r) return r;
+        c->rhs_is_newton = true;
+    } else {
+        c->rhs_is_newton = false;
+    }
+    FX_CUDA(c, cudaStreamSynchronize(c->s));
+    return FX_OK;
+}
+
+int fx_compute_rho(fx_ctx* c) {
+    if (!c) return FX_ERR_INVALID_ARGUMENT;
+    int r = ensure_device(c);
+    if (r) return r;
+    ++g_launches;
+    r = k_status(c, launch_rho(c->dp, c->d_code, c->d_phi, c->d_phi_prev, c->d_rho, c->d_e, c->d_h, c->d_part,
+                               c->d_counter, c->d_out, 0, c->s));
+    if (r) return r;
+    FX_CUDA(c, cudaStreamSynchronize(c->s));
+    return FX_OK;
+}
+
+int fx_compute_phi_rho(fx_ctx* c) {
+    if (!c) return FX_ERR_INVALID_ARGUMENT;
+    return compute_phi_rho(c);
+}
+
+int fx_compute_E(fx_ctx* c) {
+    if (!c) return FX_ERR_INVALID_ARGUMENT;
+    c->E_valid = false;
+    int r = materialize_E(c);
+    if (r) return r;
+    FX_CUDA(c, cudaStreamSynchronize(c->s));
+    return FX_OK;
+}
+
+int fx_tdgl_euler(fx_ctx* c) {
+    if (!c) return FX_ERR_INVALID_ARGUMENT;
+    int r = tdgl_update(c);
+    if (r) return r;
+    FX_CUDA(c, cudaStreamSynchronize(c->s));
+    return FX_OK;
+}
+
+int fx_set_phi_bc(fx_ctx* c) {
+    if (!c) return FX_ERR_INVALID_ARGUMENT;
+    electrode_values(c);
+    c->E_valid = false;
+    return FX_OK;
+}
+
+int fx_check_steady_state(fx_ctx* c, int step) {
+    if (!c) return FX_ERR_INVALID_ARGUMENT;
+    return check_steady(c, step);
+}
+
+int fx_step(fx_ctx* c, int nsteps, int* done) {
+    if (!c || nsteps < 0) return FX_ERR_INVALID_ARGUMENT;
+    int k = 0;
+    if (done) *done = 0;
+    for (; k < nsteps && !c->finished; ++k) {
+        int r = step_once(c);
+        if (r < 0) { if (done) *done = k; return r; }
+        if (done) *done = k + 1;
+        if (r == 1) break;
+    }
+    return FX_OK;
+}
+
+int fx_write_plotfile(fx_ctx* c, int step, const char* dir) {
+    if (!c) return FX_ERR_INVALID_ARGUMENT;
+    const Params& p = c->par;
+    std::vector<std::string> names = {"Px", "Py", "Pz"};
+    std::vector<int> ids = {FX_FIELD_PX, FX_FIELD_PY, FX_FIELD_PZ};
+    auto add = [&](int flag, const char* nm, int id) { if (flag) { names.push_back(nm); ids.push_back(id); } };
+    add(p.plot_Phi, "Phi", FX_FIELD_PHI);
+    add(p.plot_PoissonRHS, "PoissonRHS", FX_FIELD_POISSON_RHS);
+    if (p.plot_E) { names.insert(names.end(), {"Ex", "Ey", "Ez"}); ids.insert(ids.end(), {FX_FIELD_EX, FX_FIELD_EY, FX_FIELD_EZ}); }
+    add(p.plot_holes, "holes", FX_FIELD_HOLES);
+    add(p.plot_electrons, "electrons", FX_FIELD_ELECTRONS);
+    add(p.plot_charge, "charge", FX_FIELD_CHARGE);
+    add(p.plot_epsilon, "epsilon", FX_FIELD_EPSILON);
+    add(p.plot_mask, "mask", FX_FIELD_MASK);
+    add(p.plot_tphase, "tphase", FX_FIELD_TPHASE);
+    add(p.plot_alpha, "alpha", FX_FIELD_ANGLE_ALPHA);
+    add(p.plot_beta, "beta", FX_FIELD_ANGLE_BETA);
+    add(p.plot_theta, "theta", FX_FIELD_ANGLE_THETA);
+    add(p.plot_PhiDiff, "PhiDiff", FX_FIELD_PHIDIFF);
+    std::vector<std::vector<double>> data(ids.size(), std::vector<double>(c->N));
+    std::vector<const double*> ptr;
+    for (size_t q = 0; q < ids.size(); ++q) {
+        int r = get_field(c, ids[q], data[q].data());
+        if (r) return r;
+        ptr.push_back(data[q].data());
+    }
+    PlotGeom g;
+    for (int d = 0; d < 3; ++d) { g.n[d] = p.n_cell[d]; g.prob_lo[d] = p.prob_lo[d]; g.prob_hi[d] = p.prob_hi[d]; g.dx[d] = c->dx[d]; }
+    g.time = c->time;
+    g.step = step;
+    std::string base = dir ? dir : p.plot_dir;
+    std::string e;
+    if (write_plotfile(base + "/" + plotfile_name(step), g, names, ptr, &e)) return set_err(c, FX_ERR_IO, e);
+    return FX_OK;
+}
+
+int fx_run(fx_ctx* c, int* done) {
+    if (!c) return FX_ERR_INVALID_ARGUMENT;
+    const Params& p = c->par;
+    if (done) *done = 0;
+    if (p.plot_int > 0 && c->step == 0) {
+        int r = fx_write_plotfile(c, 0, nullptr);
+        if (r) return r;
+    }
+    while (c->step < p.nsteps && !c->finished) {
+        auto t0 = std::chrono::steady_clock::now();
+        int r = step_once(c);
+        if (r < 0) return r;
+        if (p.verbose) {
+            FX_CUDA(c, cudaStreamSynchronize(c->s));
+            double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            printf("Advanced step %d in %g seconds\n \n", c->step, sec);
+        }
+        if (done) *done = c->step;
+        if (p.plot_int > 0 && (c->step % p.plot_int == 0 || c->step == c->steady_state_step)) {
+            int w = fx_write_plotfile(c, c->step, nullptr);
+            if (w) return w;
+        }
+        if (r == 1) break;
+    }
+    return FX_OK;
+}
+
+int fx_get_stats(const fx_ctx* c, fx_stats* o) {
+    if (!c || !o) return FX_ERR_INVALID_ARGUMENT;
+    o->step = c->step;
+    o->finished = c->finished;
+    o->newton_iters_last = c->newton_last;
+    o->mg_cycles_last = c->mg_last;
+    o->newton_iters_total = c->newton_total;
+    o->mg_cycles_total = c->mg_total;
+    o->kernel_launches = g_launches.load();
+    o->mg_resid_last = c->mg_resid_last;
+    o->mg_target_last = c->mg_target_last;
+    o->phi_err_last = c->phi_err_last;
+    o->steady_err_last = c->steady_err_last;
+    o->Phi_Bc_hi = c->Phi_Bc_hi;
+    o->time = c->time;
+    o->steady_state_step = c->steady_state_step;
+    o->inc_step = c->inc_step;
+    o->num_Vapp = c->num_Vapp;
+    o->sign = c->sign;
+    o->device_bytes = (double)c->dev_bytes;
+    return FX_OK;
+}
+
+int fx_mean_P(fx_ctx* c, double out[3]) {
+    if (!c || !out) return FX_ERR_INVALID_ARGUMENT;
+    int r = ensure_device(c);
+    if (r) return r;
+    const double* P[3];
+    P_in(c, P);
+    ++g_launches;
+    r = k_status(c, launch_mean_p(c->dp, c->d_code, P, c->d_part, c->d_counter, c->d_out, c->s));
+    if (r) return r;
+    r = read_out(c, 3);
+    if (r) return r;
+    for (int q = 0; q < 3; ++q) out[q] = c->h_out[q];
+    return FX_OK;
+}
+
+int fx_set_stream(fx_ctx* c, void* stream) {
+    if (!c) return FX_ERR_INVALID_ARGUMENT;
+    if (c->dev) {
+        FX_CUDA(c, cudaStreamSynchronize(c->s));
+        if (c->own_stream) cudaStreamDestroy(c->s);
+    }
+    c->s = (cudaStream_t)stream;
+    c->own_stream = false;
+    return FX_OK;
+}
+
+int fx_get_kernel_times(fx_ctx* c, double* ms, long long* counts, int n) {
+    if (!c || !ms || !counts || n <= 0) return FX_ERR_INVALID_ARGUMENT;
+    if (c->dev) FX_CUDA(c, cudaStreamSynchronize(c->s));
+    c->prof.collect();
+    for (int q = 0; q < n && q < PROF_NCAT; ++q) { ms[q] = c->prof.ms[q]; counts[q] = c->prof.cnt[q]; }
+    for (int q = PROF_NCAT; q < n; ++q) { ms[q] = 0; counts[q] = 0; }
+    return PROF_NCAT;
+}
+
+int fx_reset_kernel_times(fx_ctx* c) {
+    if (!c) return FX_ERR_INVALID_ARGUMENT;
+    if (c->dev) FX_CUDA(c, cudaStreamSynchronize(c->s));
+    c->prof.collect();
+    c->prof.reset();
+    return FX_OK;
+}
+
+int fx_sync(fx_ctx* c) {
+    if (!c) return FX_ERR_INVALID_ARGUMENT;
+    if (!c->dev) return FX_OK;
+    FX_CUDA(c, cudaStreamSynchronize(c->s));
+    return FX_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,226 @@
+// fx_device.cuh -- device data layout and the restated FerroX stencils.
+//
+// HBM layout (one GPU, one box covering the domain):
+//   * every cell field is a flat array, x fastest: c = i + nx*(j + ny*k);
+//     periodic x/y neighbours are wrapped in the index, no ghost storage;
+//   * P components stay FP64 (the accumulated state); outside the z range a P
+//     read returns 0, which is what the reference's never-filled z ghost cells
+//     of P_old hold (main.cpp:157, :302-306);
+//   * the material code is one byte per cell, code = mask | tphase << 2, with
+//     one extra z layer below and above (nx*ny*(nz+2) bytes) so the stencils
+//     can read the mask of the z ghost cells that InitializeMaterialMask fills
+//     with the cell-centre rule (Initialization.cpp:177-202);
+//   * an optional second byte per cell indexes a small table of rotation
+//     matrices (per grain / per Euler-angle triple) and per-grain Landau alpha;
+//   * phi has no ghost storage: its z ghost value follows from the electrode
+//     value and the ghost mode (see phi_ghost()).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace fx {
+
+struct Variant {
+    double R[9];
+    double alpha;
+    double pad[2];
+};
+
+struct DevParams {
+    int nx, ny, nz;
+    int ngrid_red;             // blocks of the reduction kernels
+    long long nxy, N;
+    double dx[3];
+    double ih2[3];             // 1/dx^2
+    double dt;
+    double alpha, beta, gamma, a12, a112, a123;
+    double BigGamma, g11, g44, g44p, g12, lambda;
+    int flo[3], fhi[3];
+    int incl_L, incl_G, incl_E;
+    int scalar;
+    double eps[8];             // eps_r * eps_0 by material code
+    // semiconductor (ChargeDensity.cpp, FerroX.cpp:534-554)
+    double q, kb, T, Nc, Nv, Eg, Chi, Ea, Ed, NA, ND, phi_ref;
+    int use_FD;
+    double delta, inv_delta, neg_inv_delta;
+    // z Dirichlet values of phi held by the solver and the ghost mode
+    double V_lo, V_hi;
+    int ghost_mode;
+};
+
+__device__ __forceinline__ int wrap(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+
+__device__ __forceinline__ size_t cidx(const DevParams& p, int i, int j, int k) {
+    return (size_t)i + (size_t)p.nx * ((size_t)j + (size_t)p.ny * (size_t)k);
+}
+
+// material code at (i, j, k); i, j may be one or two cells outside (periodic),
+// k in [-1, nz]
+__device__ __forceinline__ int mcode(const uint8_t* __restrict__ code, const DevParams& p, int i, int j, int k) {
+    i = wrap(i, p.nx);
+    j = wrap(j, p.ny);
+    return __ldg(code + (size_t)i + (size_t)p.nx * ((size_t)j + (size_t)p.ny * (size_t)(k + 1)));
+}
+
+template <typename T>
+struct PView {
+    const double* __restrict__ a;
+    const DevParams* p;
+    __device__ __forceinline__ T operator()(int i, int j, int k) const {
+        if (k < 0 || k >= p->nz) return T(0);
+        return T(__ldg(a + cidx(*p, wrap(i, p->nx), wrap(j, p->ny), k)));
+    }
+};
+
+struct MView {
+    const uint8_t* __restrict__ code;
+    const DevParams* p;
+    __device__ __forceinline__ int operator()(int i, int j, int k) const { return mcode(code, *p, i, j, k) & 3; }
+};
+
+// DPDx / DPDy / DPDz, DerivativeAlgorithm.H:45-252 (direction D)
+template <int D, typename T>
+__device__ __forceinline__ T dpd(const PView<T>& F, const MView& M, int i, int j, int k) {
+    constexpr int ox = D == 0, oy = D == 1, oz = D == 2;
+    const DevParams& p = *F.p;
+    const T h = T(p.dx[D]);
+    const T lam = T(p.lambda);
+    const int mc = M(i, j, k);
+    if (mc != 0) return T(0);
+    if (M(i - ox, j - oy, k - oz) != 0) {
+        const int f = p.flo[D];
+        const T F0 = F(i, j, k), F1 = F(i + ox, j + oy, k + oz);
+        if (f == 0) { T F_lo = T(0); return (T(-4.) * F_lo + T(3.) * F0 + F1) / (T(3.) * h); }
+        if (f == 1) { T F_lo = F0 / (T(1) + h / T(2) / lam); return (h * F_lo / lam - F0 + F1) / (T(2.) * h); }
+        if (f == 2) return (-F0 + F1) / (T(2.) * h);
+        if (f == 3) return (-F(i - ox, j - oy, k - oz) + F1) / (T(2.) * h);
+        return (-F0 + F1) / h;
+    }
+    if (M(i + ox, j + oy, k + oz) != 0) {
+        const int f = p.fhi[D];
+        const T F0 = F(i, j, k), Fm = F(i - ox, j - oy, k - oz);
+        if (f == 0) { T F_hi = T(0); return (T(4.) * F_hi - T(3.) * F0 - Fm) / (T(3.) * h); }
+        if (f == 1) { T F_hi = F0 / (T(1) - h / T(2) / lam); return (h * F_hi / lam + F0 - Fm) / (T(2.) * h); }
+        if (f == 2) return (F0 - Fm) / (T(2.) * h);
+        if (f == 3) return (F(i + ox, j + oy, k + oz) - Fm) / (T(2.) * h);
+        return (F0 - Fm) / h;
+    }
+    return (F(i + ox, j + oy, k + oz) - F(i - ox, j - oy, k - oz)) / (T(2.) * h);
+}
+
+// DoubleDPDx / y / z, DerivativeAlgorithm.H:256-467 (direction D)
+template <int D, typename T>
+__device__ __forceinline__ T ddpd(const PView<T>& F, const MView& M, int i, int j, int k) {
+    constexpr int ox = D == 0, oy = D == 1, oz = D == 2;
+    const DevParams& p = *F.p;
+    const T h = T(p.dx[D]);
+    const T lam = T(p.lambda);
+    if (M(i, j, k) != 0) return T(0);
+    const T F0 = F(i, j, k);
+    if (M(i - ox, j - oy, k - oz) != 0) {
+        const int f = p.flo[D];
+        const T F1 = F(i + ox, j + oy, k + oz);
+        if (f == 0) { T F_lo = T(0); return T(4.) * (T(2.) * F_lo - T(3.) * F0 + F1) / T(3.) / h / h; }
+        if (f == 1) { T F_lo = F0 / (T(1) + h / T(2) / lam); return (-h * F_lo / lam - F0 + F1) / h / h; }
+        if (f == 2) return (-F0 + F1) / h / h;
+        if (f == 3) {
+            const T Fm = F(i - ox, j - oy, k - oz);
+            if (D == 2) return (Fm - T(2.) * F0 + F1) / h / h;
+            return (F1 - T(2.) * F0 + Fm) / h / h;
+        }
+        const T F2 = F(i + 2 * ox, j + 2 * oy, k + 2 * oz);
+        if (D == 2) return (F0 - T(2.) * F1 + F2) / h / h;
+        return (F2 - T(2.) * F1 + F0) / h / h;
+    }
+    if (M(i + ox, j + oy, k + oz) != 0) {
+        const int f = p.fhi[D];
+        const T Fm = F(i - ox, j - oy, k - oz);
+        if (f == 0) { T F_hi = T(0); return T(4.) * (T(2.) * F_hi - T(3.) * F0 + Fm) / T(3.) / h / h; }
+        if (f == 1) { T F_hi = F0 / (T(1) - h / T(2) / lam); return (h * F_hi / lam - F0 + Fm) / h / h; }
+        if (f == 2) return (-F0 + Fm) / h / h;
+        if (f == 3) return (F(i + ox, j + oy, k + oz) - T(2.) * F0 + Fm) / h / h;
+        return (F0 - T(2.) * Fm + F(i - 2 * ox, j - 2 * oy, k - 2 * oz)) / h / h;
+    }
+    return (F(i + ox, j + oy, k + oz) - T(2.) * F0 + F(i - ox, j - oy, k - oz)) / (h * h);
+}
+
+// DoubleDPDxDy / DxDz / DyDz, DerivativeAlgorithm.H:471-497
+template <typename T>
+__device__ __forceinline__ T dxdy(const PView<T>& F, const MView& M, int i, int j, int k) {
+    return (dpd<1>(F, M, i + 1, j, k) - dpd<1>(F, M, i - 1, j, k)) / T(2.) / T(F.p->dx[0]);
+}
+template <typename T>
+__device__ __forceinline__ T dxdz(const PView<T>& F, const MView& M, int i, int j, int k) {
+    return (dpd<2>(F, M, i + 1, j, k) - dpd<2>(F, M, i - 1, j, k)) / T(2.) / T(F.p->dx[0]);
+}
+template <typename T>
+__device__ __forceinline__ T dydz(const PView<T>& F, const MView& M, int i, int j, int k) {
+    return (dpd<2>(F, M, i, j + 1, k) - dpd<2>(F, M, i, j - 1, k)) / T(2.) / T(F.p->dx[1]);
+}
+
+// phi with its z ghost values: after the MLMG solve the ghost holds the
+// maxorder-2 Dirichlet extrapolation 2 V - phi_0 (mode 0), or the face value V
+// (mode 1), or 0 (mode 2)
+__device__ __forceinline__ double phi_at(const double* __restrict__ phi, const DevParams& p, int i, int j, int k) {
+    i = wrap(i, p.nx);
+    j = wrap(j, p.ny);
+    if (k < 0) {
+        if (p.ghost_mode == 0) return 2.0 * p.V_lo + (-1.0) * __ldg(phi + cidx(p, i, j, 0));
+        return p.ghost_mode == 1 ? p.V_lo : 0.0;
+    }
+    if (k >= p.nz) {
+        if (p.ghost_mode == 0) return 2.0 * p.V_hi + (-1.0) * __ldg(phi + cidx(p, i, j, p.nz - 1));
+        return p.ghost_mode == 1 ? p.V_hi : 0.0;
+    }
+    return __ldg(phi + cidx(p, i, j, k));
+}
+
+// grad phi as used by ComputeEfromPhi (ElectrostaticSolver.cpp:195-197):
+// central in x / y, DphiDz (DerivativeAlgorithm.H:8-22) in z with the
+// one-sided forms in the electrode-adjacent layers
+template <typename T>
+__device__ __forceinline__ void grad_phi(const double* __restrict__ phi, const DevParams& p, int i, int j, int k,
+                                         T& gx, T& gy, T& gz) {
+    // differences are taken in FP64 (phi is O(1 V) and its differences small)
+    gx = T((phi_at(phi, p, i + 1, j, k) - phi_at(phi, p, i - 1, j, k)) / (2. * p.dx[0]));
+    gy = T((phi_at(phi, p, i, j + 1, k) - phi_at(phi, p, i, j - 1, k)) / (2. * p.dx[1]));
+    const double dz = p.dx[2];
+    if (k == 0) {
+        gz = T((-4. * phi_at(phi, p, i, j, k - 1) + 3. * phi_at(phi, p, i, j, k) + phi_at(phi, p, i, j, k + 1)) / (3. * dz));
+    } else if (k == p.nz - 1) {
+        gz = T((4. * phi_at(phi, p, i, j, k + 1) - 3. * phi_at(phi, p, i, j, k) - phi_at(phi, p, i, j, k - 1)) / (3. * dz));
+    } else {
+        gz = T((phi_at(phi, p, i, j, k + 1) - phi_at(phi, p, i, j, k - 1)) / (2. * dz));
+    }
+}
+
+// ChargeDensity.cpp:4-11
+__device__ __forceinline__ double fd_half(double eta) {
+    double nu = pow(eta, 4.0) + 50.0 + 33.6 * eta * (1.0 - 0.68 * exp(-0.17 * pow((eta + 1.0), 2.0)));
+    double xi = 3.0 * sqrt(3.14) / (4.0 * pow(nu, 3. / 8.));
+    return pow(exp(-eta) + xi, -1.0);
+}
+
+// ChargeDensity.cpp:46-93: carrier densities and charge at potential phi
+__device__ __forceinline__ double sc_charge(const DevParams& p, double phi, double& e_den, double& h_den) {
+    const double Ef = 0.0;
+    const double q = p.q, kb = p.kb, T = p.T, Chi = p.Chi, Eg = p.Eg, phi_ref = p.phi_ref;
+    double Ec_corr = -q * (phi - phi_ref) - Chi * q;
+    double Ev_corr = Ec_corr - q * Eg;
+    const double g_A = 4.0, g_D = 2.0;
+    if (p.use_FD == 1) {
+        double eta_n = -(Ec_corr - q * Ef) / (kb * T);
+        double eta_p = -(q * Ef - Ev_corr) / (kb * T);
+        e_den = p.Nc * fd_half(eta_n);
+        h_den = p.Nv * fd_half(eta_p);
+    } else {
+        e_den = p.Nc * exp(-(Ec_corr - q * Ef) / (kb * T));
+        h_den = p.Nv * exp(-(q * Ef - Ev_corr) / (kb * T));
+    }
+    double acc = p.NA / (1.0 + g_A * exp((-q * Ef + q * p.Ea + q * phi_ref - q * Chi - q * Eg - q * phi) / (kb * T)));
+    double don = p.ND / (1.0 + g_D * exp((q * Ef + q * p.Ed - q * phi_ref + q * Chi + q * phi) / (kb * T)));
+    return q * (h_den - e_den - acc + don);
+}
+
+}  // namespace fx

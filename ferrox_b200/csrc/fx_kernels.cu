@@ -1,0 +1,514 @@
+// fx_kernels.cu -- the coupled-step kernels other than the Poisson multigrid.
+//
+//   k_tdgl      Calculate_Landau + Calculate_Grad + Calculate_Elec +
+//               CalculateTDGL_RHS + the forward-Euler LinComb in one pass
+//               (TotalEnergyDensity.cpp:6-294, main.cpp:280-306); E is taken
+//               on the fly from phi (ElectrostaticSolver.cpp:134-203)
+//   k_rhs_p     the FE branch of ComputePoissonRHS (ElectrostaticSolver.cpp:
+//               73-77) -- P does not change inside the Newton loop
+//   k_newton    ComputeRho(phi+delta) + dF_dPhi + ComputePoissonRHS_Newton
+//               (ElectrostaticSolver.cpp:85-132, ChargeDensity.cpp:15-102)
+//   k_rho       ComputeRho(phi) after the solve, with the L1 norms of the
+//               Newton error (ElectrostaticSolver.cpp:723-738)
+//   k_steady    CheckSteadyState's two norm0 reductions and the copy
+//               (ElectrostaticSolver.cpp:526-560)
+//   k_efield    ComputeEfromPhi, materialised for output only
+#include "fx_kernels.h"
+
+#include <cmath>
+
+namespace fx {
+
+namespace {
+
+constexpr int RED_THREADS = 256;
+
+__device__ __forceinline__ void atomic_max_nonneg(double* addr, double v) {
+    if (!(v == v)) return;  // NaN never wins a std::max
+    atomicMax(reinterpret_cast<unsigned long long*>(addr), (unsigned long long)__double_as_longlong(v));
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// block sum in a fixed order (deterministic for a fixed launch shape)
+__device__ double block_sum(double v, double* sh) {
+    v = warp_sum(v);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (w == 0) {
+        r = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
+        r = warp_sum(r);
+    }
+    __syncthreads();
+    return r;
+}
+__device__ double block_max(double v, double* sh) {
+    v = warp_max(v);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (w == 0) {
+        r = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
+        r = warp_max(r);
+    }
+    __syncthreads();
+    return r;
+}
+
+// Landau derivative dF/dP_a (TotalEnergyDensity.cpp:88-110) for component a
+// with the other two components b, c
+template <typename T>
+__device__ __forceinline__ T landau(const DevParams& p, T alpha, T a, T b, T c) {
+    const T a2 = a * a, b2 = b * b, c2 = c * c;
+    return alpha * a + T(p.beta) * (a2 * a) + T(p.gamma) * (a2 * a2 * a)
+        + T(2.) * T(p.a12) * a * b2
+        + T(2.) * T(p.a12) * a * c2
+        + T(4.) * T(p.a112) * (a2 * a) * (b2 + c2)
+        + T(2.) * T(p.a112) * a * (b2 * b2)
+        + T(2.) * T(p.a112) * a * (c2 * c2)
+        + T(2.) * T(p.a123) * a * b2 * c2;
+}
+
+// the six second derivatives of one component, for the rotated Pr term
+template <typename T>
+struct Hess { T xx, yy, zz, xy, yz, xz; };
+
+template <typename T, bool ROT>
+__device__ __forceinline__ Hess<T> hess(const PView<T>& F, const MView& M, int i, int j, int k) {
+    Hess<T> h;
+    h.xx = ddpd<0>(F, M, i, j, k);
+    h.yy = ddpd<1>(F, M, i, j, k);
+    h.zz = ddpd<2>(F, M, i, j, k);
+    if (ROT) {
+        h.xy = dxdy(F, M, i, j, k);
+        h.yz = dydz(F, M, i, j, k);
+        h.xz = dxdz(F, M, i, j, k);
+    } else {
+        h.xy = h.yz = h.xz = T(0);
+    }
+    return h;
+}
+
+// R_a1 R_a1 Dxx + ... + 2 R_a3 R_a1 Dxz, TotalEnergyDensity.cpp:209-228
+template <typename T>
+__device__ __forceinline__ T rot_quad(const T* R, int a, const Hess<T>& H) {
+    const T r1 = R[3 * a], r2 = R[3 * a + 1], r3 = R[3 * a + 2];
+    return r1 * r1 * H.xx + r2 * r2 * H.yy + r3 * r3 * H.zz + T(2.) * r1 * r2 * H.xy + T(2.) * r2 * r3 * H.yz +
+           T(2.) * r3 * r1 * H.xz;
+}
+
+// One forward-Euler TDGL update.  T is the stencil arithmetic (double for the
+// FP64 path, float for the mixed path); the P state is read and written in
+// FP64.  SCALAR: is_polarization_scalar == 1 with Px = Py = 0, so only Pz is
+// read and updated.  ROT: a rotation table is present (else R = identity,
+// whose zero entries contribute exact zeros in the reference's sums).
+template <typename T, bool SCALAR, bool ROT>
+__global__ void __launch_bounds__(256) k_tdgl(DevParams p, const uint8_t* __restrict__ code,
+                                              const uint8_t* __restrict__ var, const Variant* __restrict__ vt,
+                                              const double* __restrict__ Pp, const double* __restrict__ Pq,
+                                              const double* __restrict__ Pr, const double* __restrict__ phi,
+                                              double* __restrict__ Pp_out, double* __restrict__ Pq_out,
+                                              double* __restrict__ Pr_out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (i >= p.nx || j >= p.ny) return;
+    const size_t c = cidx(p, i, j, k);
+    const int m = mcode(code, p, i, j, k);
+    const double pr0 = Pr[c];
+    const double pp0 = SCALAR ? 0.0 : Pp[c];
+    const double pq0 = SCALAR ? 0.0 : Pq[c];
+    // Gamma = 0 outside FE (Initialization.cpp:113, :125) and the t-phase
+    // zeroing (TotalEnergyDensity.cpp:123-127) leave P unchanged there
+    if ((m & 3) != 0 || (m & 4) != 0) {
+        Pr_out[c] = pr0;
+        if (!SCALAR) { Pp_out[c] = pp0; Pq_out[c] = pq0; }
+        return;
+    }
+    T R[9] = {T(1), T(0), T(0), T(0), T(1), T(0), T(0), T(0), T(1)};
+    T alpha = T(p.alpha);
+    if (ROT) {
+        const Variant& v = vt[__ldg(var + c)];
+        for (int q = 0; q < 9; ++q) R[q] = T(v.R[q]);
+        alpha = T(v.alpha);
+    }
+    const T Gam = T(p.BigGamma);
+    MView M{code, &p};
+    PView<T> Fr{Pr, &p};
+    const T g11 = T(p.g11), g44 = T(p.g44), g44p = T(p.g44p), g12 = T(p.g12);
+
+    // electric field from phi, ElectrostaticSolver.cpp:195-197
+    T gx = T(0), gy = T(0), gz = T(0);
+    if (p.incl_E) grad_phi<T>(phi, p, i, j, k, gx, gy, gz);
+
+    // ---- r component
+    const T r = T(pr0), pp = T(pp0), pq = T(pq0);
+    T fr = T(0);
+    if (p.incl_L) fr += T(-1.0) * Gam * landau<T>(p, alpha, r, pp, pq);
+    if (p.incl_G) {
+        Hess<T> H = hess<T, ROT>(Fr, M, i, j, k);
+        T g;
+        if (ROT) {
+            g = -g11 * rot_quad(R, 2, H) - (g44 - g44p) * rot_quad(R, 0, H) - (g44 - g44p) * rot_quad(R, 1, H);
+        } else {
+            g = -g11 * H.zz - (g44 - g44p) * H.xx - (g44 - g44p) * H.yy;
+        }
+        if (!SCALAR) {
+            PView<T> Fp{Pp, &p}, Fq{Pq, &p};
+            g = g - (g44 + g44p + g12) * dydz(Fq, M, i, j, k) - (g44 + g44p + g12) * dxdz(Fp, M, i, j, k);
+        }
+        fr += T(-1.0) * Gam * g;
+    }
+    if (p.incl_E) {
+        const T Er = -(R[6] * gx + R[7] * gy + R[8] * gz);
+        fr += T(-1.0) * Gam * (-Er);
+    }
+    Pr_out[c] = 1.0 * pr0 + p.dt * (double)fr;
+
+    if (!SCALAR) {
+        PView<T> Fp{Pp, &p}, Fq{Pq, &p};
+        T fp = T(0), fq = T(0);
+        if (p.incl_L) {
+            fp += T(-1.0) * Gam * landau<T>(p, alpha, pp, pq, r);
+            fq += T(-1.0) * Gam * landau<T>(p, alpha, pq, pp, r);
+        }
+        if (p.incl_G) {
+            T gp = -g11 * ddpd<0>(Fp, M, i, j, k) - (g44 + g44p) * ddpd<1>(Fp, M, i, j, k) -
+                   (g44 + g44p) * ddpd<2>(Fp, M, i, j, k) - (g12 + g44 - g44p) * dxdy(Fq, M, i, j, k) -
+                   (g12 + g44 - g44p) * dxdz(Fr, M, i, j, k);
+            T gq = -g11 * ddpd<1>(Fq, M, i, j, k) - (g44 - g44p) * ddpd<0>(Fq, M, i, j, k) -
+                   (g44 - g44p) * ddpd<2>(Fq, M, i, j, k) - (g12 + g44 + g44p) * dxdy(Fp, M, i, j, k) -
+                   (g12 + g44 - g44p) * dydz(Fr, M, i, j, k);
+            fp += T(-1.0) * Gam * gp;
+            fq += T(-1.0) * Gam * gq;
+        }
+        if (p.incl_E) {
+            const T Ep = -(R[0] * gx + R[1] * gy + R[2] * gz);
+            const T Eq = -(R[3] * gx + R[4] * gy + R[5] * gz);
+            fp += T(-1.0) * Gam * (-Ep);
+            fq += T(-1.0) * Gam * (-Eq);
+        }
+        if (p.scalar) { fp = T(0); fq = T(0); }
+        Pp_out[c] = 1.0 * pp0 + p.dt * (double)fp;
+        Pq_out[c] = 1.0 * pq0 + p.dt * (double)fq;
+    }
+}
+
+// FE branch of ComputePoissonRHS, ElectrostaticSolver.cpp:65-77 (DE -> 0; the
+// SC value rho is supplied by k_newton).  Also reduces max|rhs| and max|b'|
+// where b' adds the Dirichlet electrode terms (the MLMG stopping rule's norms)
+template <bool SCALAR, bool ROT>
+__global__ void __launch_bounds__(256) k_rhs_p(DevParams p, const uint8_t* __restrict__ code,
+                                               const uint8_t* __restrict__ var, const Variant* __restrict__ vt,
+                                               const double* __restrict__ Pp, const double* __restrict__ Pq,
+                                               const double* __restrict__ Pr, double* __restrict__ rhs,
+                                               double* __restrict__ norms) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    __shared__ double sh[32];
+    double nb = 0.0, nbp = 0.0;
+    if (i < p.nx && j < p.ny) {
+        const size_t c = cidx(p, i, j, k);
+        const int m = mcode(code, p, i, j, k);
+        double v = 0.0;
+        if ((m & 3) == 0) {
+            double R[9] = {1, 0, 0, 0, 1, 0, -0.0, 0, 1};
+            if (ROT) {
+                const Variant& vv = vt[__ldg(var + c)];
+                for (int q = 0; q < 9; ++q) R[q] = vv.R[q];
+            }
+            MView M{code, &p};
+            PView<double> Fr{Pr, &p};
+            const double r3 = R[6] * dpd<0>(Fr, M, i, j, k) + R[7] * dpd<1>(Fr, M, i, j, k) + R[8] * dpd<2>(Fr, M, i, j, k);
+            if (SCALAR) {
+                v = -r3;
+            } else {
+                PView<double> Fp{Pp, &p}, Fq{Pq, &p};
+                const double r1 = R[0] * dpd<0>(Fp, M, i, j, k) + R[1] * dpd<1>(Fp, M, i, j, k) + R[2] * dpd<2>(Fp, M, i, j, k);
+                const double r2 = R[3] * dpd<0>(Fq, M, i, j, k) + R[4] * dpd<1>(Fq, M, i, j, k) + R[5] * dpd<2>(Fq, M, i, j, k);
+                v = -(r1) - (r2) - (r3);
+            }
+        }
+        rhs[c] = v;
+        nb = fabs(v);
+        double bp = v;
+        const double e = p.eps[m & 7];
+        if (k == 0) bp += 2.0 * e * p.ih2[2] * p.V_lo;
+        if (k == p.nz - 1) bp += 2.0 * e * p.ih2[2] * p.V_hi;
+        nbp = fabs(bp);
+    }
+    if (norms) {
+        const double a = block_max(nb, sh);
+        const double b = block_max(nbp, sh);
+        if (threadIdx.x == 0 && threadIdx.y == 0) {
+            atomic_max_nonneg(norms, a);
+            atomic_max_nonneg(norms + 1, b);
+        }
+    }
+}
+
+// one Newton linearisation pass (FP64): alpha = (rho(phi+delta) - rho)/delta
+// by the reference's LinComb, rhs = RHS - alpha phi; alpha is also written in
+// FP32 for the mixed-precision multigrid
+__global__ void __launch_bounds__(256) k_newton(DevParams p, const uint8_t* __restrict__ code,
+                                                const double* __restrict__ phi, const double* __restrict__ rho,
+                                                const double* __restrict__ rhs_p, double* __restrict__ alpha,
+                                                float* __restrict__ alpha32, double* __restrict__ rhs,
+                                                double* __restrict__ norms) {
+    __shared__ double sh[32];
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+    double nb = 0.0, nbp = 0.0;
+    for (long long c = (long long)blockIdx.x * 256 + tid; c < p.N; c += (long long)gridDim.x * 256) {
+        const int i = (int)(c % p.nx);
+        const int j = (int)((c / p.nx) % p.ny);
+        const int k = (int)(c / p.nxy);
+        const int m = mcode(code, p, i, j, k);
+        const int mask = m & 3;
+        double a = 0.0, v;
+        if (mask >= 2) {
+            double e, h;
+            const double rho_pd = sc_charge(p, phi[c] + p.delta, e, h);
+            const double r0 = rho[c];
+            a = p.inv_delta * rho_pd + p.neg_inv_delta * r0;
+            v = r0 - a * phi[c];
+        } else if (mask == 1) {
+            v = 0.0;
+        } else {
+            v = rhs_p[c];
+        }
+        alpha[c] = a;
+        alpha32[c] = (float)a;
+        rhs[c] = v;
+        nb = fmax(nb, fabs(v));
+        double bp = v;
+        const double eps = p.eps[m & 7];
+        if (k == 0) bp += 2.0 * eps * p.ih2[2] * p.V_lo;
+        if (k == p.nz - 1) bp += 2.0 * eps * p.ih2[2] * p.V_hi;
+        nbp = fmax(nbp, fabs(bp));
+    }
+    const double x = block_max(nb, sh);
+    const double y = block_max(nbp, sh);
+    if (tid == 0) {
+        atomic_max_nonneg(norms, x);
+        atomic_max_nonneg(norms + 1, y);
+    }
+}
+
+// ComputeRho at the new phi + the Newton error norms; partial sums go to
+// part[2*block], the last block folds them in block order (deterministic)
+__global__ void __launch_bounds__(256) k_rho(DevParams p, const uint8_t* __restrict__ code,
+                                             const double* __restrict__ phi, double* __restrict__ phi_prev,
+                                             double* __restrict__ rho, double* __restrict__ e_den,
+                                             double* __restrict__ h_den, double* __restrict__ part,
+                                             unsigned int* __restrict__ counter, double* __restrict__ out,
+                                             int track) {
+    __shared__ double sh[32];
+    __shared__ bool last;
+    double s1 = 0.0, s2 = 0.0;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < p.N; c += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(c % p.nx);
+        const int j = (int)((c / p.nx) % p.ny);
+        const int k = (int)(c / p.nxy);
+        const int m = mcode(code, p, i, j, k) & 3;
+        const double ph = phi[c];
+        if (m >= 2) {
+            double e, h;
+            rho[c] = sc_charge(p, ph, e, h);
+            e_den[c] = e;
+            h_den[c] = h;
+        } else {
+            rho[c] = 0.0;
+        }
+        if (track) {
+            s1 += fabs(ph - phi_prev[c]);
+            s2 += fabs(ph);
+            phi_prev[c] = ph;
+        }
+    }
+    if (!track) return;
+    const double b1 = block_sum(s1, sh);
+    const double b2 = block_sum(s2, sh);
+    if (threadIdx.x == 0) {
+        part[2 * blockIdx.x] = b1;
+        part[2 * blockIdx.x + 1] = b2;
+        __threadfence();
+        last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        double t1 = 0.0, t2 = 0.0;
+        for (unsigned b = 0; b < gridDim.x; ++b) {
+            t1 += ((volatile double*)part)[2 * b];
+            t2 += ((volatile double*)part)[2 * b + 1];
+        }
+        out[0] = t1;
+        out[1] = t2;
+        *counter = 0;
+    }
+}
+
+// CheckSteadyState: max|phi|, max|phi - phi_old| over valid cells, then
+// phi_old := phi; optionally keeps |phi - phi_old| for the PhiDiff output
+__global__ void __launch_bounds__(256) k_steady(DevParams p, const double* __restrict__ phi,
+                                                double* __restrict__ phi_old, double* __restrict__ dphi,
+                                                double* __restrict__ out) {
+    __shared__ double sh[32];
+    double m1 = 0.0, m2 = 0.0;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < p.N; c += (long long)gridDim.x * blockDim.x) {
+        const double a = phi[c];
+        const double d = fabs(a - phi_old[c]);
+        if (dphi) dphi[c] = d;
+        phi_old[c] = a;
+        const double fa = fabs(a);
+        if (fa == fa) m1 = fmax(m1, fa);
+        if (d == d) m2 = fmax(m2, d);
+    }
+    const double x = block_max(m1, sh);
+    const double y = block_max(m2, sh);
+    if (threadIdx.x == 0) {
+        atomic_max_nonneg(out, x);
+        atomic_max_nonneg(out + 1, y);
+    }
+}
+
+// mean of Px, Py, Pz over the ferroelectric cells (mask 0): the hysteresis
+// observable; partial sums per block, folded in block order by the last block
+__global__ void __launch_bounds__(256) k_mean_p(DevParams p, const uint8_t* __restrict__ code,
+                                                const double* __restrict__ Px, const double* __restrict__ Py,
+                                                const double* __restrict__ Pz, double* __restrict__ part,
+                                                unsigned int* __restrict__ counter, double* __restrict__ out) {
+    __shared__ double sh[32];
+    __shared__ bool last;
+    double s[4] = {0.0, 0.0, 0.0, 0.0};
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < p.N; c += (long long)gridDim.x * blockDim.x) {
+        if ((__ldg(code + c + p.nxy) & 3) == 0) {
+            if (Px) s[0] += Px[c];
+            if (Py) s[1] += Py[c];
+            s[2] += Pz[c];
+            s[3] += 1.0;
+        }
+    }
+    double b[4];
+    for (int q = 0; q < 4; ++q) b[q] = block_sum(s[q], sh);
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < 4; ++q) part[4 * blockIdx.x + q] = b[q];
+        __threadfence();
+        last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        double t[4] = {0.0, 0.0, 0.0, 0.0};
+        for (unsigned blk = 0; blk < gridDim.x; ++blk)
+            for (int q = 0; q < 4; ++q) t[q] += ((volatile double*)part)[4 * blk + q];
+        for (int q = 0; q < 3; ++q) out[q] = t[3] > 0 ? t[q] / t[3] : 0.0;
+        *counter = 0;
+    }
+}
+
+template <bool ROT>
+__global__ void __launch_bounds__(256) k_efield(DevParams p, const uint8_t* __restrict__ var,
+                                                const Variant* __restrict__ vt, const double* __restrict__ phi,
+                                                double* __restrict__ Ex, double* __restrict__ Ey,
+                                                double* __restrict__ Ez) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (i >= p.nx || j >= p.ny) return;
+    const size_t c = cidx(p, i, j, k);
+    double R[9] = {1, 0, 0, 0, 1, 0, -0.0, 0, 1};
+    if (ROT) {
+        const Variant& v = vt[__ldg(var + c)];
+        for (int q = 0; q < 9; ++q) R[q] = v.R[q];
+    }
+    double gx, gy, gz;
+    grad_phi<double>(phi, p, i, j, k, gx, gy, gz);
+    Ex[c] = -(R[0] * gx + R[1] * gy + R[2] * gz);
+    Ey[c] = -(R[3] * gx + R[4] * gy + R[5] * gz);
+    Ez[c] = -(R[6] * gx + R[7] * gy + R[8] * gz);
+}
+
+dim3 cell_grid(const DevParams& p) { return dim3((p.nx + 31) / 32, (p.ny + 7) / 8, p.nz); }
+
+}  // namespace
+
+// ------------------------------------------------------------ launchers --
+int launch_tdgl(const DevParams& p, int mixed, const uint8_t* code, const uint8_t* var, const Variant* vt,
+                const double* const Pin[3], double* const Pout[3], const double* phi, cudaStream_t s) {
+    const dim3 g = cell_grid(p), b(32, 8);
+    const bool scal = p.scalar && Pin[0] == nullptr;
+    const bool rot = var != nullptr;
+#define FX_TDGL(T, S, R) k_tdgl<T, S, R><<<g, b, 0, s>>>(p, code, var, vt, Pin[0], Pin[1], Pin[2], phi, Pout[0], Pout[1], Pout[2])
+    if (!mixed) {
+        if (scal) { if (rot) FX_TDGL(double, true, true); else FX_TDGL(double, true, false); }
+        else { if (rot) FX_TDGL(double, false, true); else FX_TDGL(double, false, false); }
+    } else {
+        if (scal) { if (rot) FX_TDGL(float, true, true); else FX_TDGL(float, true, false); }
+        else { if (rot) FX_TDGL(float, false, true); else FX_TDGL(float, false, false); }
+    }
+#undef FX_TDGL
+    return (int)cudaGetLastError();
+}
+
+int launch_rhs_p(const DevParams& p, const uint8_t* code, const uint8_t* var, const Variant* vt,
+                 const double* const P[3], double* rhs, double* norms, cudaStream_t s) {
+    const dim3 g = cell_grid(p), b(32, 8);
+    const bool scal = p.scalar && P[0] == nullptr;
+    const bool rot = var != nullptr;
+    if (scal) {
+        if (rot) k_rhs_p<true, true><<<g, b, 0, s>>>(p, code, var, vt, P[0], P[1], P[2], rhs, norms);
+        else k_rhs_p<true, false><<<g, b, 0, s>>>(p, code, var, vt, P[0], P[1], P[2], rhs, norms);
+    } else {
+        if (rot) k_rhs_p<false, true><<<g, b, 0, s>>>(p, code, var, vt, P[0], P[1], P[2], rhs, norms);
+        else k_rhs_p<false, false><<<g, b, 0, s>>>(p, code, var, vt, P[0], P[1], P[2], rhs, norms);
+    }
+    return (int)cudaGetLastError();
+}
+
+int launch_newton(const DevParams& p, const uint8_t* code, const double* phi, const double* rho,
+                  const double* rhs_p, double* alpha, float* alpha32, double* rhs, double* norms, cudaStream_t s) {
+    k_newton<<<p.ngrid_red, dim3(256), 0, s>>>(p, code, phi, rho, rhs_p, alpha, alpha32, rhs, norms);
+    return (int)cudaGetLastError();
+}
+
+int launch_rho(const DevParams& p, const uint8_t* code, const double* phi, double* phi_prev, double* rho,
+               double* e_den, double* h_den, double* part, unsigned int* counter, double* out, int track,
+               cudaStream_t s) {
+    k_rho<<<p.ngrid_red, RED_THREADS, 0, s>>>(p, code, phi, phi_prev, rho, e_den, h_den, part, counter, out, track);
+    return (int)cudaGetLastError();
+}
+
+int launch_steady(const DevParams& p, const double* phi, double* phi_old, double* dphi, double* out,
+                  cudaStream_t s) {
+    k_steady<<<p.ngrid_red, RED_THREADS, 0, s>>>(p, phi, phi_old, dphi, out);
+    return (int)cudaGetLastError();
+}
+
+int launch_mean_p(const DevParams& p, const uint8_t* code, const double* const P[3], double* part,
+                  unsigned int* counter, double* out, cudaStream_t s) {
+    k_mean_p<<<p.ngrid_red, RED_THREADS, 0, s>>>(p, code, P[0], P[1], P[2], part, counter, out);
+    return (int)cudaGetLastError();
+}
+
+int launch_efield(const DevParams& p, const uint8_t* var, const Variant* vt, const double* phi, double* E[3],
+                  cudaStream_t s) {
+    const dim3 g = cell_grid(p), b(32, 8);
+    if (var) k_efield<true><<<g, b, 0, s>>>(p, var, vt, phi, E[0], E[1], E[2]);
+    else k_efield<false><<<g, b, 0, s>>>(p, var, vt, phi, E[0], E[1], E[2]);
+    return (int)cudaGetLastError();
+}
+
+}  // namespace fx

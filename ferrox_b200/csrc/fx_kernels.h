@@ -1,0 +1,28 @@
+// fx_kernels.h -- launchers of the coupled-step kernels (fx_kernels.cu) and
+// of the Poisson multigrid (fx_mg.cu).  All launches go to the given stream.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "fx_device.cuh"
+
+namespace fx {
+
+// Pin/Pout: {Px, Py, Pz}; Px = Py = nullptr selects the scalar-P kernel
+int launch_tdgl(const DevParams& p, int mixed, const uint8_t* code, const uint8_t* var, const Variant* vt,
+                const double* const Pin[3], double* const Pout[3], const double* phi, cudaStream_t s);
+int launch_rhs_p(const DevParams& p, const uint8_t* code, const uint8_t* var, const Variant* vt,
+                 const double* const P[3], double* rhs, double* norms, cudaStream_t s);
+int launch_newton(const DevParams& p, const uint8_t* code, const double* phi, const double* rho,
+                  const double* rhs_p, double* alpha, float* alpha32, double* rhs, double* norms, cudaStream_t s);
+int launch_rho(const DevParams& p, const uint8_t* code, const double* phi, double* phi_prev, double* rho,
+               double* e_den, double* h_den, double* part, unsigned int* counter, double* out, int track,
+               cudaStream_t s);
+int launch_steady(const DevParams& p, const double* phi, double* phi_old, double* dphi, double* out,
+                  cudaStream_t s);
+int launch_mean_p(const DevParams& p, const uint8_t* code, const double* const P[3], double* part,
+                  unsigned int* counter, double* out, cudaStream_t s);
+int launch_efield(const DevParams& p, const uint8_t* var, const Variant* vt, const double* phi, double* E[3],
+                  cudaStream_t s);
+
+}  // namespace fx

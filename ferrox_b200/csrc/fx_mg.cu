@@ -1,0 +1,683 @@
+// fx_mg.cu -- geometric multigrid for (-alpha - div beta grad) phi = rhs.
+// See fx_mg.h for the hierarchy.  Level 0 reads the one-byte material code of
+// each cell and forms beta_face = 0.5 (eps_L + eps_R) on the fly (the face
+// average of eXstaticUtil.cpp:128-136 with the eps of
+// ElectrostaticSolver.cpp:238-251); coarse levels store face beta and alpha.
+#include "fx_mg.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <atomic>
+
+namespace fx {
+
+extern std::atomic<long long> g_launches;
+
+namespace {
+
+template <typename T>
+struct Op {
+    int nx, ny, nz;
+    long long nxy;
+    T ih2x, ih2y, ih2z;
+    const uint8_t* code;   // level 0: material codes (with z ghost layers)
+    T eps[8];
+    const T* bw;           // coarse: beta on the low-x / low-y / low-z faces
+    const T* bs;
+    const T* bb;           // nz + 1 layers
+    const T* a;            // alpha (may be null)
+    T vlo, vhi;            // electrode values (inhomogeneous level-0 operator only)
+};
+
+// couplings of cell (i,j,k) to its six neighbours (already divided by h^2),
+// the diagonal and the electrode contribution to the right-hand side
+template <typename T, bool FINE>
+__device__ __forceinline__ void coeffs(const Op<T>& o, int i, int j, int k, size_t c, int im, int ip, int jm, int jp,
+                                       T& cw, T& ce, T& cs, T& cn, T& cb, T& ct, T& diag, T& bcv) {
+    T extra = T(0);
+    bcv = T(0);
+    if (FINE) {
+        const uint8_t* cd = o.code + o.nxy;   // skip the k = -1 ghost layer
+        const size_t row = c - i;
+        const T ec = o.eps[__ldg(cd + c) & 7];
+        cw = T(0.5) * (ec + o.eps[__ldg(cd + row + im) & 7]) * o.ih2x;
+        ce = T(0.5) * (o.eps[__ldg(cd + row + ip) & 7] + ec) * o.ih2x;
+        cs = T(0.5) * (ec + o.eps[__ldg(cd + c + (size_t)(jm - j) * o.nx) & 7]) * o.ih2y;
+        cn = T(0.5) * (o.eps[__ldg(cd + c + (size_t)(jp - j) * o.nx) & 7] + ec) * o.ih2y;
+        if (k > 0) cb = T(0.5) * (ec + o.eps[__ldg(cd + c - o.nxy) & 7]) * o.ih2z;
+        else { cb = T(0); extra += T(2) * ec * o.ih2z; bcv += T(2) * ec * o.ih2z * o.vlo; }
+        if (k < o.nz - 1) ct = T(0.5) * (o.eps[__ldg(cd + c + o.nxy) & 7] + ec) * o.ih2z;
+        else { ct = T(0); extra += T(2) * ec * o.ih2z; bcv += T(2) * ec * o.ih2z * o.vhi; }
+    } else {
+        const size_t row = c - i;
+        cw = __ldg(o.bw + c) * o.ih2x;
+        ce = __ldg(o.bw + row + ip) * o.ih2x;
+        cs = __ldg(o.bs + c) * o.ih2y;
+        cn = __ldg(o.bs + c + (size_t)(jp - j) * o.nx) * o.ih2y;
+        const T fb = __ldg(o.bb + c), ft = __ldg(o.bb + c + o.nxy);
+        if (k > 0) cb = fb * o.ih2z;
+        else { cb = T(0); extra += T(2) * fb * o.ih2z; }
+        if (k < o.nz - 1) ct = ft * o.ih2z;
+        else { ct = T(0); extra += T(2) * ft * o.ih2z; }
+    }
+    if (o.nx == 1) { cw = T(0); ce = T(0); }
+    if (o.ny == 1) { cs = T(0); cn = T(0); }
+    const T a = o.a ? o.a[c] : T(0);
+    diag = -a + cw + ce + cs + cn + cb + ct + extra;
+}
+
+__device__ __forceinline__ void nbr(int i, int n, int& m, int& p) {
+    m = i == 0 ? n - 1 : i - 1;
+    p = i == n - 1 ? 0 : i + 1;
+}
+
+__device__ __forceinline__ void atomic_max_nonneg(double* addr, double v) {
+    if (!(v == v)) v = __longlong_as_double(0x7ff0000000000000LL);  // a NaN residual never converges
+    atomicMax(reinterpret_cast<unsigned long long*>(addr), (unsigned long long)__double_as_longlong(v));
+}
+
+__device__ double block_max_all(double v) {
+    __shared__ double sh[32];
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    const int t = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int nt = blockDim.x * blockDim.y * blockDim.z;
+    if ((t & 31) == 0) sh[t >> 5] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (t < 32) {
+        r = t < (nt + 31) / 32 ? sh[t] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) r = fmax(r, __shfl_down_sync(0xffffffffu, r, o));
+    }
+    return r;
+}
+
+// red-black point Gauss-Seidel half sweep: color = parity of i + j + k
+template <typename T, bool FINE>
+__global__ void __launch_bounds__(256) k_rbgs(Op<T> o, T* __restrict__ x, const T* __restrict__ b, int color) {
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((j + k + color) & 1);
+    if (j >= o.ny || i >= o.nx) return;
+    const size_t c = (size_t)i + (size_t)o.nx * ((size_t)j + (size_t)o.ny * k);
+    int im, ip, jm, jp;
+    nbr(i, o.nx, im, ip);
+    nbr(j, o.ny, jm, jp);
+    T cw, ce, cs, cn, cb, ct, diag, bcv;
+    coeffs<T, FINE>(o, i, j, k, c, im, ip, jm, jp, cw, ce, cs, cn, cb, ct, diag, bcv);
+    const size_t row = c - i;
+    T s = b[c] + bcv + cw * x[row + im] + ce * x[row + ip] + cs * x[c + (size_t)(jm - j) * o.nx] +
+          cn * x[c + (size_t)(jp - j) * o.nx];
+    if (k > 0) s += cb * x[c - o.nxy];
+    if (k < o.nz - 1) s += ct * x[c + o.nxy];
+    x[c] = s / diag;
+}
+
+// red-black z-line Gauss-Seidel half sweep: color = parity of i + j; each
+// thread solves the tridiagonal system of one column (Thomas), q holds the
+// forward-elimination ratios
+template <typename T, bool FINE>
+__global__ void __launch_bounds__(128) k_line(Op<T> o, T* __restrict__ x, const T* __restrict__ b, T* __restrict__ q,
+                                              int color) {
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((j + color) & 1);
+    if (j >= o.ny || i >= o.nx) return;
+    int im, ip, jm, jp;
+    nbr(i, o.nx, im, ip);
+    nbr(j, o.ny, jm, jp);
+    T qprev = T(0), dprev = T(0);
+    size_t c = (size_t)i + (size_t)o.nx * (size_t)j;
+    for (int k = 0; k < o.nz; ++k, c += o.nxy) {
+        T cw, ce, cs, cn, cb, ct, diag, bcv;
+        coeffs<T, FINE>(o, i, j, k, c, im, ip, jm, jp, cw, ce, cs, cn, cb, ct, diag, bcv);
+        const size_t row = c - i;
+        const T r = b[c] + bcv + cw * x[row + im] + ce * x[row + ip] + cs * x[c + (size_t)(jm - j) * o.nx] +
+                    cn * x[c + (size_t)(jp - j) * o.nx];
+        const T den = diag - cb * qprev;
+        const T qk = ct / den;
+        const T dk = (r + cb * dprev) / den;
+        q[c] = qk;
+        x[c] = dk;
+        qprev = qk;
+        dprev = dk;
+    }
+    c -= o.nxy;   // top cell
+    T xn = x[c];
+    for (int k = o.nz - 2; k >= 0; --k) {
+        c -= o.nxy;
+        xn = x[c] + q[c] * xn;
+        x[c] = xn;
+    }
+}
+
+// residual b - A x at the children of each coarse cell, averaged into the
+// coarse right-hand side; optionally the |r|_inf of the level
+template <typename T, bool FINE>
+__global__ void __launch_bounds__(256) k_resid_restrict(Op<T> o, const T* __restrict__ x, const T* __restrict__ b,
+                                                        T* __restrict__ bc, int ncx, int ncy, int ncz, int rx, int ry,
+                                                        int rz, double* __restrict__ norm) {
+    const int I = blockIdx.x * blockDim.x + threadIdx.x;
+    const int J = blockIdx.y * blockDim.y + threadIdx.y;
+    const int K = blockIdx.z;
+    double mx = 0.0;
+    if (I < ncx && J < ncy) {
+        T s = T(0);
+        for (int dk = 0; dk < rz; ++dk)
+            for (int dj = 0; dj < ry; ++dj)
+                for (int di = 0; di < rx; ++di) {
+                    const int i = rx * I + di, j = ry * J + dj, k = rz * K + dk;
+                    const size_t c = (size_t)i + (size_t)o.nx * ((size_t)j + (size_t)o.ny * k);
+                    int im, ip, jm, jp;
+                    nbr(i, o.nx, im, ip);
+                    nbr(j, o.ny, jm, jp);
+                    T cw, ce, cs, cn, cb, ct, diag, bcv;
+                    coeffs<T, FINE>(o, i, j, k, c, im, ip, jm, jp, cw, ce, cs, cn, cb, ct, diag, bcv);
+                    const size_t row = c - i;
+                    T off = cw * x[row + im] + ce * x[row + ip] + cs * x[c + (size_t)(jm - j) * o.nx] +
+                            cn * x[c + (size_t)(jp - j) * o.nx];
+                    if (k > 0) off += cb * x[c - o.nxy];
+                    if (k < o.nz - 1) off += ct * x[c + o.nxy];
+                    const T r = (b[c] + bcv) - (diag * x[c] - off);
+                    s += r;
+                    mx = fmax(mx, fabs((double)r));
+                }
+        bc[(size_t)I + (size_t)ncx * ((size_t)J + (size_t)ncy * K)] = s / T(rx * ry * rz);
+    }
+    if (norm) {
+        const double m = block_max_all(mx);
+        if (threadIdx.x == 0 && threadIdx.y == 0) atomic_max_nonneg(norm, m);
+    }
+}
+
+// FP64 residual of the level-0 operator with electrode terms; optional FP32
+// copy for the mixed-precision correction solve
+__global__ void __launch_bounds__(256) k_resid64(Op<double> o, const double* __restrict__ x, const double* __restrict__ b,
+                                                 float* __restrict__ r32, double* __restrict__ norm) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    double mx = 0.0;
+    if (i < o.nx && j < o.ny) {
+        const size_t c = (size_t)i + (size_t)o.nx * ((size_t)j + (size_t)o.ny * k);
+        int im, ip, jm, jp;
+        nbr(i, o.nx, im, ip);
+        nbr(j, o.ny, jm, jp);
+        double cw, ce, cs, cn, cb, ct, diag, bcv;
+        coeffs<double, true>(o, i, j, k, c, im, ip, jm, jp, cw, ce, cs, cn, cb, ct, diag, bcv);
+        const size_t row = c - i;
+        double off = cw * x[row + im] + ce * x[row + ip] + cs * x[c + (size_t)(jm - j) * o.nx] +
+                     cn * x[c + (size_t)(jp - j) * o.nx];
+        if (k > 0) off += cb * x[c - o.nxy];
+        if (k < o.nz - 1) off += ct * x[c + o.nxy];
+        const double r = (b[c] + bcv) - (diag * x[c] - off);
+        if (r32) r32[c] = (float)r;
+        mx = fabs(r);
+    }
+    const double m = block_max_all(mx);
+    if (threadIdx.x == 0 && threadIdx.y == 0) atomic_max_nonneg(norm, m);
+}
+
+// prolongation in the coarsened directions with the per-cell resistor-chain
+// weights (near parent, far neighbour), added to x; beyond an electrode the
+// far neighbour is the homogeneous Dirichlet value 0
+template <typename T>
+__global__ void __launch_bounds__(256) k_prolong(T* __restrict__ xf, const T* __restrict__ xc, const float* __restrict__ wx,
+                                                 const float* __restrict__ wy, const float* __restrict__ wz, int nx, int ny,
+                                                 int nz, int ncx, int ncy, int ncz, int rx, int ry, int rz) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (i >= nx || j >= ny) return;
+    const size_t fc = (size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * k);
+    int I[2], J[2], K[2];
+    T wi[2], wj[2], wk[2];
+    int ni = 1, nj = 1, nk = 1;
+    I[0] = i / rx; wi[0] = T(1);
+    if (rx == 2) { ni = 2; wi[1] = T(__ldg(wx + fc)); wi[0] = T(1) - wi[1]; I[1] = (i & 1) ? I[0] + 1 : I[0] - 1; I[1] = (I[1] + ncx) % ncx; }
+    J[0] = j / ry; wj[0] = T(1);
+    if (ry == 2) { nj = 2; wj[1] = T(__ldg(wy + fc)); wj[0] = T(1) - wj[1]; J[1] = (j & 1) ? J[0] + 1 : J[0] - 1; J[1] = (J[1] + ncy) % ncy; }
+    K[0] = k / rz; wk[0] = T(1);
+    if (rz == 2) {
+        nk = 2; wk[1] = T(__ldg(wz + fc)); wk[0] = T(1) - wk[1]; K[1] = (k & 1) ? K[0] + 1 : K[0] - 1;
+        if (K[1] < 0 || K[1] >= ncz) { K[1] = K[0]; wk[1] = T(0); }
+    }
+    T s = T(0);
+    for (int a = 0; a < nk; ++a)
+        for (int bb = 0; bb < nj; ++bb)
+            for (int d = 0; d < ni; ++d)
+                s += wk[a] * wj[bb] * wi[d] * xc[(size_t)I[d] + (size_t)ncx * ((size_t)J[bb] + (size_t)ncy * K[a])];
+    xf[fc] += s;
+}
+
+template <typename Tin, typename T>
+__global__ void __launch_bounds__(256) k_avg_alpha(const Tin* __restrict__ af, T* __restrict__ ac, int nx, int ny,
+                                                   int ncx, int ncy, int ncz, int rx, int ry, int rz) {
+    const int I = blockIdx.x * blockDim.x + threadIdx.x;
+    const int J = blockIdx.y * blockDim.y + threadIdx.y;
+    const int K = blockIdx.z;
+    if (I >= ncx || J >= ncy) return;
+    double s = 0.0;
+    for (int dk = 0; dk < rz; ++dk)
+        for (int dj = 0; dj < ry; ++dj)
+            for (int di = 0; di < rx; ++di)
+                s += (double)af[(size_t)(rx * I + di) + (size_t)nx * ((size_t)(ry * J + dj) + (size_t)ny * (rz * K + dk))];
+    ac[(size_t)I + (size_t)ncx * ((size_t)J + (size_t)ncy * K)] = (T)(s / (rx * ry * rz));
+}
+
+__global__ void __launch_bounds__(256) k_add_corr(double* __restrict__ phi, const float* __restrict__ e, long long n) {
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x)
+        phi[c] += (double)e[c];
+}
+
+template <typename T>
+T* dalloc(size_t n, size_t& bytes) {
+    T* p = nullptr;
+    if (n == 0) return nullptr;
+    if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) return nullptr;
+    bytes += n * sizeof(T);
+    return p;
+}
+
+template <typename T>
+Op<T> make_op(const MGLevel& L, int l, const uint8_t* code, const double* eps, const T* a, bool inhom,
+              const DevParams& p) {
+    Op<T> o;
+    o.nx = L.n[0]; o.ny = L.n[1]; o.nz = L.n[2];
+    o.nxy = (long long)L.n[0] * L.n[1];
+    o.ih2x = T(1.0 / (L.h[0] * L.h[0]));
+    o.ih2y = T(1.0 / (L.h[1] * L.h[1]));
+    o.ih2z = T(1.0 / (L.h[2] * L.h[2]));
+    o.code = code;
+    for (int q = 0; q < 8; ++q) o.eps[q] = T(eps[q]);
+    if constexpr (sizeof(T) == 8) { o.bw = (const T*)L.bw64; o.bs = (const T*)L.bs64; o.bb = (const T*)L.bb64; }
+    else { o.bw = (const T*)L.bw32; o.bs = (const T*)L.bs32; o.bb = (const T*)L.bb32; }
+    o.a = a;
+    o.vlo = inhom ? T(p.V_lo) : T(0);
+    o.vhi = inhom ? T(p.V_hi) : T(0);
+    (void)l;
+    return o;
+}
+
+template <typename T> T* lx(MGLevel& L);
+template <> double* lx<double>(MGLevel& L) { return L.x64; }
+template <> float* lx<float>(MGLevel& L) { return L.x32; }
+template <typename T> T* lb(MGLevel& L);
+template <> double* lb<double>(MGLevel& L) { return L.b64; }
+template <> float* lb<float>(MGLevel& L) { return L.b32; }
+template <typename T> T* la(MGLevel& L);
+template <> double* la<double>(MGLevel& L) { return L.a64; }
+template <> float* la<float>(MGLevel& L) { return L.a32; }
+template <typename T> T* lq(MGLevel& L);
+template <> double* lq<double>(MGLevel& L) { return L.cp64; }
+template <> float* lq<float>(MGLevel& L) { return L.cp32; }
+
+}  // namespace
+
+Multigrid::~Multigrid() {
+    for (size_t l = 0; l < lev_.size(); ++l) {
+        MGLevel& L = lev_[l];
+        // level 0 borrows phi / rhs (FP64) and e32_ / r32_ (FP32), freed below
+        if (l > 0) { cudaFree(L.x64); cudaFree(L.b64); cudaFree(L.x32); cudaFree(L.b32); }
+        cudaFree(L.bw64); cudaFree(L.bs64); cudaFree(L.bb64); cudaFree(L.a64); cudaFree(L.cp64);
+        cudaFree(L.bw32); cudaFree(L.bs32); cudaFree(L.bb32); cudaFree(L.a32); cudaFree(L.cp32);
+        for (int d = 0; d < 3; ++d) cudaFree(L.wf[d]);
+    }
+    cudaFree(d_norm_);
+    if (h_norm_) cudaFreeHost(h_norm_);
+    cudaFree(e32_);
+    cudaFree(r32_);
+}
+
+int Multigrid::setup(const DevParams& p, const std::vector<uint8_t>& code, bool want64, bool want32) {
+    for (int q = 0; q < 8; ++q) eps_[q] = p.eps[q];
+    lev_.clear();
+    MGLevel L0{};
+    L0.n[0] = p.nx; L0.n[1] = p.ny; L0.n[2] = p.nz;
+    for (int d = 0; d < 3; ++d) { L0.h[d] = p.dx[d]; L0.cr[d] = 1; }
+    L0.N = (size_t)p.N;
+    L0.line = false;
+    lev_.push_back(L0);
+    auto coarsenable_xy = [](int n) { return n % 2 == 0 && (n / 2 == 1 || (n / 2) % 2 == 0); };
+    while (true) {
+        MGLevel& f = lev_.back();
+        const double hmin = std::min(f.h[0], std::min(f.h[1], f.h[2]));
+        const bool cz = f.n[2] % 2 == 0 && f.h[2] <= 1.5 * hmin;
+        int cr[3] = {1, 1, 1};
+        if (cz) {
+            cr[2] = 2;
+            for (int d = 0; d < 2; ++d)
+                if (coarsenable_xy(f.n[d]) && f.h[d] <= 1.5 * hmin) cr[d] = 2;
+            f.line = false;
+        } else {
+            for (int d = 0; d < 2; ++d)
+                if (coarsenable_xy(f.n[d])) cr[d] = 2;
+            f.line = true;
+            if (cr[0] == 1 && cr[1] == 1) break;   // bottom
+        }
+        MGLevel c{};
+        for (int d = 0; d < 3; ++d) { c.n[d] = f.n[d] / cr[d]; c.h[d] = f.h[d] * cr[d]; c.cr[d] = cr[d]; }
+        c.N = (size_t)c.n[0] * c.n[1] * c.n[2];
+        c.line = true;
+        lev_.push_back(c);
+        if (lev_.size() > 64) return -1;
+    }
+
+    // level-0 face beta on the host, then face averages down the hierarchy
+    const int nx = p.nx, ny = p.ny, nz = p.nz;
+    const size_t nxy = (size_t)nx * ny;
+    auto ecode = [&](int i, int j, int k) { return eps_[code[(size_t)i + nx * ((size_t)j + (size_t)ny * (k + 1))] & 7]; };
+    std::vector<double> fw(L0.N), fs(L0.N), fb(L0.N + nxy);
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                const size_t c = (size_t)i + nx * ((size_t)j + (size_t)ny * k);
+                const double ec = ecode(i, j, k);
+                fw[c] = 0.5 * (ec + ecode((i + nx - 1) % nx, j, k));
+                fs[c] = 0.5 * (ec + ecode(i, (j + ny - 1) % ny, k));
+                fb[c] = k == 0 ? ec : 0.5 * (ec + ecode(i, j, k - 1));
+            }
+    for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) fb[nz * nxy + (size_t)i + nx * (size_t)j] = ecode(i, j, nz - 1);
+
+    bytes_ = 0;
+    for (size_t l = 0; l < lev_.size(); ++l) {
+        MGLevel& L = lev_[l];
+        const size_t N = L.N, lnxy = (size_t)L.n[0] * L.n[1];
+        if (l > 0) {
+            const MGLevel& F = lev_[l - 1];
+            const int rx = L.cr[0], ry = L.cr[1], rz = L.cr[2];
+            const int fnx = F.n[0], fny = F.n[1];
+            // Face beta of the coarse level.  Along a coarsened direction the
+            // coarse face joins the fine links between the two coarse centres
+            // in series (half link, full link, half link: beta_c =
+            // 4 / (1/b_{2I-1} + 2/b_{2I} + 1/b_{2I+1})), so thin low-eps layers
+            // keep their resistance; across the transverse children the links
+            // are in parallel (arithmetic mean).  At a Dirichlet face the path
+            // runs from the coarse centre to the electrode: half of the first
+            // interior link and the fine boundary link, beta_c = 2/(1/b_0 + 1/b_1).
+            const int fnz = F.n[2];
+            // prolongation weights: a fine cell between its parent's centre
+            // (h/2 away) and the neighbouring coarse centre (3h/2 away) takes
+            // the weights of a 1-D resistor chain built from the fine face
+            // beta (3/4, 1/4 for uniform beta; the neighbour beyond an
+            // electrode is the homogeneous Dirichlet value)
+            for (int d = 0; d < 3; ++d) {
+                if (L.cr[d] != 2) continue;
+                std::vector<float> w(F.N);
+                const double h = F.h[d];
+                const int nd = F.n[d];
+                for (int k = 0; k < fnz; ++k)
+                    for (int j = 0; j < fny; ++j)
+                        for (int i = 0; i < fnx; ++i) {
+                            const int q = d == 0 ? i : d == 1 ? j : k;
+                            auto B = [&](int t) {
+                                if (d == 0) return fw[(size_t)(((t % nd) + nd) % nd) + fnx * ((size_t)j + (size_t)fny * k)];
+                                if (d == 1) return fs[(size_t)i + fnx * ((size_t)(((t % nd) + nd) % nd) + (size_t)fny * k)];
+                                return fb[(size_t)i + fnx * ((size_t)j + (size_t)fny * t)];
+                            };
+                            double gn, gf;
+                            if ((q & 1) == 0) {
+                                gn = 2.0 * B(q + 1) / h;
+                                gf = (d == 2 && q == 0) ? 2.0 * B(0) / h : 1.0 / (h / B(q) + h / (2.0 * B(q - 1)));
+                            } else {
+                                gn = 2.0 * B(q) / h;
+                                gf = (d == 2 && q == nd - 1) ? 2.0 * B(nd) / h : 1.0 / (h / B(q + 1) + h / (2.0 * B(q + 2)));
+                            }
+                            w[(size_t)i + fnx * ((size_t)j + (size_t)fny * k)] = (float)(gf / (gn + gf));
+                        }
+                L.wf[d] = dalloc<float>(F.N, bytes_);
+                if (!L.wf[d]) return -2;
+                if (cudaMemcpy(L.wf[d], w.data(), F.N * 4, cudaMemcpyHostToDevice) != cudaSuccess) return -1;
+            }
+            auto FW = [&](int i, int j, int k) { return fw[(size_t)((i % fnx + fnx) % fnx) + fnx * ((size_t)j + (size_t)fny * k)]; };
+            auto FS = [&](int i, int j, int k) { return fs[(size_t)i + fnx * ((size_t)((j % fny + fny) % fny) + (size_t)fny * k)]; };
+            auto FB = [&](int i, int j, int k) { return fb[(size_t)i + fnx * ((size_t)j + (size_t)fny * k)]; };
+            auto ser = [](double a, double b, double c) { return 4.0 / (1.0 / a + 2.0 / b + 1.0 / c); };
+            std::vector<double> cw(N), cs(N), cb(N + lnxy);
+            for (int k = 0; k < L.n[2]; ++k)
+                for (int j = 0; j < L.n[1]; ++j)
+                    for (int i = 0; i < L.n[0]; ++i) {
+                        const size_t c = (size_t)i + L.n[0] * ((size_t)j + (size_t)L.n[1] * k);
+                        double s = 0;
+                        for (int dk = 0; dk < rz; ++dk)
+                            for (int dj = 0; dj < ry; ++dj) {
+                                const int fj = ry * j + dj, fk = rz * k + dk;
+                                s += rx == 2 ? ser(FW(2 * i - 1, fj, fk), FW(2 * i, fj, fk), FW(2 * i + 1, fj, fk)) : FW(i, fj, fk);
+                            }
+                        cw[c] = s / (ry * rz);
+                        s = 0;
+                        for (int dk = 0; dk < rz; ++dk)
+                            for (int di = 0; di < rx; ++di) {
+                                const int fi = rx * i + di, fk = rz * k + dk;
+                                s += ry == 2 ? ser(FS(fi, 2 * j - 1, fk), FS(fi, 2 * j, fk), FS(fi, 2 * j + 1, fk)) : FS(fi, j, fk);
+                            }
+                        cs[c] = s / (rx * rz);
+                    }
+            for (int k = 0; k <= L.n[2]; ++k)
+                for (int j = 0; j < L.n[1]; ++j)
+                    for (int i = 0; i < L.n[0]; ++i) {
+                        double s = 0;
+                        for (int dj = 0; dj < ry; ++dj)
+                            for (int di = 0; di < rx; ++di) {
+                                const int fi = rx * i + di, fj = ry * j + dj;
+                                double v;
+                                if (rz == 1) v = FB(fi, fj, k);
+                                else if (k == 0) v = 2.0 / (1.0 / FB(fi, fj, 0) + 1.0 / FB(fi, fj, 1));
+                                else if (k == L.n[2]) v = 2.0 / (1.0 / FB(fi, fj, fnz) + 1.0 / FB(fi, fj, fnz - 1));
+                                else v = ser(FB(fi, fj, 2 * k - 1), FB(fi, fj, 2 * k), FB(fi, fj, 2 * k + 1));
+                                s += v;
+                            }
+                        cb[(size_t)i + L.n[0] * ((size_t)j + (size_t)L.n[1] * k)] = s / (rx * ry);
+                    }
+            fw.swap(cw); fs.swap(cs); fb.swap(cb);
+            if (want64) {
+                L.x64 = dalloc<double>(N, bytes_); L.b64 = dalloc<double>(N, bytes_); L.a64 = dalloc<double>(N, bytes_);
+                L.bw64 = dalloc<double>(N, bytes_); L.bs64 = dalloc<double>(N, bytes_); L.bb64 = dalloc<double>(N + lnxy, bytes_);
+                if (!L.x64 || !L.b64 || !L.a64 || !L.bw64 || !L.bs64 || !L.bb64) return -2;
+                if (cudaMemcpy(L.bw64, fw.data(), N * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+                    cudaMemcpy(L.bs64, fs.data(), N * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+                    cudaMemcpy(L.bb64, fb.data(), (N + lnxy) * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+                    cudaMemset(L.a64, 0, N * 8) != cudaSuccess)
+                    return -1;
+            }
+            if (want32) {
+                L.x32 = dalloc<float>(N, bytes_); L.b32 = dalloc<float>(N, bytes_); L.a32 = dalloc<float>(N, bytes_);
+                L.bw32 = dalloc<float>(N, bytes_); L.bs32 = dalloc<float>(N, bytes_); L.bb32 = dalloc<float>(N + lnxy, bytes_);
+                if (!L.x32 || !L.b32 || !L.a32 || !L.bw32 || !L.bs32 || !L.bb32) return -2;
+                std::vector<float> t(N + lnxy);
+                for (size_t q = 0; q < N; ++q) t[q] = (float)fw[q];
+                if (cudaMemcpy(L.bw32, t.data(), N * 4, cudaMemcpyHostToDevice) != cudaSuccess) return -1;
+                for (size_t q = 0; q < N; ++q) t[q] = (float)fs[q];
+                if (cudaMemcpy(L.bs32, t.data(), N * 4, cudaMemcpyHostToDevice) != cudaSuccess) return -1;
+                for (size_t q = 0; q < N + lnxy; ++q) t[q] = (float)fb[q];
+                if (cudaMemcpy(L.bb32, t.data(), (N + lnxy) * 4, cudaMemcpyHostToDevice) != cudaSuccess) return -1;
+                if (cudaMemset(L.a32, 0, N * 4) != cudaSuccess) return -1;
+            }
+        }
+        if (L.line) {
+            if (want64) { L.cp64 = dalloc<double>(N, bytes_); if (!L.cp64) return -2; }
+            if (want32) { L.cp32 = dalloc<float>(N, bytes_); if (!L.cp32) return -2; }
+        }
+    }
+    if (cudaMalloc(&d_norm_, 64) != cudaSuccess) return -2;
+    if (cudaMallocHost(&h_norm_, 64) != cudaSuccess) return -2;
+    if (want32) {
+        e32_ = dalloc<float>(L0.N, bytes_);
+        r32_ = dalloc<float>(L0.N, bytes_);
+        if (!e32_ || !r32_) return -2;
+        lev_[0].x32 = e32_;
+        lev_[0].b32 = r32_;
+    }
+    if (verbose) {
+        for (size_t l = 0; l < lev_.size(); ++l)
+            printf("  mg level %zu: %d x %d x %d  h = %.4g %.4g %.4g nm  %s\n", l, lev_[l].n[0], lev_[l].n[1], lev_[l].n[2],
+                   lev_[l].h[0] * 1e9, lev_[l].h[1] * 1e9, lev_[l].h[2] * 1e9, lev_[l].line ? "z-line GS" : "point RB-GS");
+    }
+    return 0;
+}
+
+int Multigrid::set_alpha(const double* a64, const float* a32, bool has_alpha, cudaStream_t s) {
+    a0_64 = a64;
+    a0_32 = a32;
+    has_alpha_ = has_alpha;
+    if (!has_alpha) return 0;
+    for (size_t l = 1; l < lev_.size(); ++l) {
+        MGLevel& L = lev_[l];
+        const MGLevel& F = lev_[l - 1];
+        dim3 b(32, 8), g((L.n[0] + 31) / 32, (L.n[1] + 7) / 8, L.n[2]);
+        if (L.a64) {
+            if (l == 1) { ++g_launches; k_avg_alpha<double, double><<<g, b, 0, s>>>(a64, L.a64, F.n[0], F.n[1], L.n[0], L.n[1], L.n[2], L.cr[0], L.cr[1], L.cr[2]); }
+            else { ++g_launches; k_avg_alpha<double, double><<<g, b, 0, s>>>(F.a64, L.a64, F.n[0], F.n[1], L.n[0], L.n[1], L.n[2], L.cr[0], L.cr[1], L.cr[2]); }
+        }
+        if (L.a32) {
+            if (l == 1) { ++g_launches; k_avg_alpha<double, float><<<g, b, 0, s>>>(a64, L.a32, F.n[0], F.n[1], L.n[0], L.n[1], L.n[2], L.cr[0], L.cr[1], L.cr[2]); }
+            else { ++g_launches; k_avg_alpha<float, float><<<g, b, 0, s>>>(F.a32, L.a32, F.n[0], F.n[1], L.n[0], L.n[1], L.n[2], L.cr[0], L.cr[1], L.cr[2]); }
+        }
+    }
+    return (int)cudaGetLastError();
+}
+
+template <typename T>
+void Multigrid::smooth(const DevParams& p, const uint8_t* code, int l, T* x, const T* b, bool inhom, int sweeps,
+                       cudaStream_t s) {
+    MGLevel& L = lev_[l];
+    const T* a = nullptr;
+    if (has_alpha_) {
+        if (l == 0) { if constexpr (sizeof(T) == 8) a = (const T*)a0_64; else a = (const T*)a0_32; }
+        else a = la<T>(L);
+    }
+    Op<T> o = make_op<T>(L, l, code, eps_, a, inhom, p);
+    if (L.line) {
+        T* q = lq<T>(L);
+        dim3 b2(32, 4), g2(((L.n[0] + 1) / 2 + 31) / 32, (L.n[1] + 3) / 4, 1);
+        for (int it = 0; it < sweeps; ++it)
+            for (int color = 0; color < 2; ++color) {
+                if (prof) prof->begin(l == 0 ? PROF_SMOOTH_L0 : PROF_MG_COARSE, s);
+                if (l == 0) { ++g_launches; k_line<T, true><<<g2, b2, 0, s>>>(o, x, b, q, color); }
+                else { ++g_launches; k_line<T, false><<<g2, b2, 0, s>>>(o, x, b, q, color); }
+                if (prof) prof->end(s);
+            }
+    } else {
+        dim3 b2(32, 8), g2(((L.n[0] + 1) / 2 + 31) / 32, (L.n[1] + 7) / 8, L.n[2]);
+        for (int it = 0; it < sweeps; ++it)
+            for (int color = 0; color < 2; ++color) {
+                if (prof) prof->begin(l == 0 ? PROF_SMOOTH_L0 : PROF_MG_COARSE, s);
+                if (l == 0) { ++g_launches; k_rbgs<T, true><<<g2, b2, 0, s>>>(o, x, b, color); }
+                else { ++g_launches; k_rbgs<T, false><<<g2, b2, 0, s>>>(o, x, b, color); }
+                if (prof) prof->end(s);
+            }
+    }
+}
+
+template <typename T>
+void Multigrid::vcycle(const DevParams& p, const uint8_t* code, int l, T* x, const T* b, bool inhom, cudaStream_t s) {
+    MGLevel& L = lev_[l];
+    const int last = (int)lev_.size() - 1;
+    if (l == last) {
+        const bool exact = L.line && L.n[0] * L.n[1] == 1;
+        smooth<T>(p, code, l, x, b, inhom, exact ? 1 : nu_bottom, s);
+        return;
+    }
+    smooth<T>(p, code, l, x, b, inhom, nu1, s);
+    MGLevel& C = lev_[l + 1];
+    const T* a = nullptr;
+    if (has_alpha_) {
+        if (l == 0) { if constexpr (sizeof(T) == 8) a = (const T*)a0_64; else a = (const T*)a0_32; }
+        else a = la<T>(L);
+    }
+    Op<T> o = make_op<T>(L, l, code, eps_, a, inhom, p);
+    dim3 b2(32, 8), g2((C.n[0] + 31) / 32, (C.n[1] + 7) / 8, C.n[2]);
+    double* norm = (l == 0) ? d_norm_ : nullptr;
+    if (prof) prof->begin(l == 0 ? PROF_RESTRICT_L0 : PROF_MG_COARSE, s);
+    if (l == 0) { ++g_launches; k_resid_restrict<T, true><<<g2, b2, 0, s>>>(o, x, b, lb<T>(C), C.n[0], C.n[1], C.n[2], C.cr[0], C.cr[1], C.cr[2], norm); }
+    else { ++g_launches; k_resid_restrict<T, false><<<g2, b2, 0, s>>>(o, x, b, lb<T>(C), C.n[0], C.n[1], C.n[2], C.cr[0], C.cr[1], C.cr[2], norm); }
+    if (prof) prof->end(s);
+    cudaMemsetAsync(lx<T>(C), 0, C.N * sizeof(T), s);
+    vcycle<T>(p, code, l + 1, lx<T>(C), lb<T>(C), false, s);
+    dim3 g3((L.n[0] + 31) / 32, (L.n[1] + 7) / 8, L.n[2]);
+    if (prof) prof->begin(l == 0 ? PROF_PROLONG_L0 : PROF_MG_COARSE, s);
+    { ++g_launches; k_prolong<T><<<g3, b2, 0, s>>>(x, lx<T>(C), C.wf[0], C.wf[1], C.wf[2], L.n[0], L.n[1], L.n[2], C.n[0], C.n[1], C.n[2], C.cr[0], C.cr[1], C.cr[2]); }
+    if (prof) prof->end(s);
+    smooth<T>(p, code, l, x, b, inhom, nu2, s);
+}
+
+int Multigrid::residual64(const DevParams& p, const uint8_t* code, const double* phi, const double* rhs, double* r,
+                          cudaStream_t s, double* norm_out) {
+    MGLevel& L = lev_[0];
+    Op<double> o = make_op<double>(L, 0, code, eps_, has_alpha_ ? a0_64 : nullptr, true, p);
+    cudaMemsetAsync(d_norm_, 0, 8, s);
+    dim3 b2(32, 8), g2((L.n[0] + 31) / 32, (L.n[1] + 7) / 8, L.n[2]);
+    (void)r;
+    if (prof) prof->begin(PROF_RESID64, s);
+    { ++g_launches; k_resid64<<<g2, b2, 0, s>>>(o, phi, rhs, nullptr, d_norm_); }
+    if (prof) prof->end(s);
+    cudaMemcpyAsync(h_norm_, d_norm_, 8, cudaMemcpyDeviceToHost, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (norm_out) *norm_out = h_norm_[0];
+    return (int)e;
+}
+
+int Multigrid::solve64(const DevParams& p, const uint8_t* code, double* phi, const double* rhs, double target,
+                       int maxit, cudaStream_t s, MGStats* st) {
+    int it = 0;
+    double rn = 0.0;
+    int e = residual64(p, code, phi, rhs, nullptr, s, &rn);
+    if (e) return e;
+    while (!(rn <= target) && it < maxit) {
+        // one V-cycle; the level-0 residual norm after pre-smoothing bounds
+        // the residual after the cycle, so it is the loop test; the exact
+        // final residual is checked before returning
+        cudaMemsetAsync(d_norm_, 0, 8, s);
+        vcycle<double>(p, code, 0, phi, rhs, true, s);
+        cudaMemcpyAsync(h_norm_, d_norm_, 8, cudaMemcpyDeviceToHost, s);
+        e = (int)cudaStreamSynchronize(s);
+        if (e) return e;
+        ++it;
+        const double mid = h_norm_[0];
+        if (verbose > 1) printf("  mg cycle %d: |r|/target after pre-smoothing = %.3e\n", it, mid / target);
+        if (lev_.size() == 1) { e = residual64(p, code, phi, rhs, nullptr, s, &rn); if (e) return e; continue; }
+        if (mid <= target) {
+            e = residual64(p, code, phi, rhs, nullptr, s, &rn);
+            if (e) return e;
+        } else {
+            rn = mid;
+        }
+    }
+    if (st) { st->cycles = it; st->resid = rn; }
+    return rn <= target ? 0 : -3;
+}
+
+int Multigrid::solve_mixed(const DevParams& p, const uint8_t* code, double* phi, const double* rhs, double target,
+                           int maxit, cudaStream_t s, MGStats* st) {
+    MGLevel& L = lev_[0];
+    Op<double> o64 = make_op<double>(L, 0, code, eps_, has_alpha_ ? a0_64 : nullptr, true, p);
+    dim3 b2(32, 8), g2((L.n[0] + 31) / 32, (L.n[1] + 7) / 8, L.n[2]);
+    int it = 0;
+    double rn = 0.0;
+    while (true) {
+        cudaMemsetAsync(d_norm_, 0, 8, s);
+        if (prof) prof->begin(PROF_RESID64, s);
+        { ++g_launches; k_resid64<<<g2, b2, 0, s>>>(o64, phi, rhs, r32_, d_norm_); }
+        if (prof) prof->end(s);
+        cudaMemcpyAsync(h_norm_, d_norm_, 8, cudaMemcpyDeviceToHost, s);
+        int e = (int)cudaStreamSynchronize(s);
+        if (e) return e;
+        rn = h_norm_[0];
+        if (verbose > 1) printf("  refinement %d: |r|/target = %.3e\n", it, rn / target);
+        if (rn <= target || it >= maxit) break;
+        cudaMemsetAsync(e32_, 0, L.N * sizeof(float), s);
+        vcycle<float>(p, code, 0, e32_, r32_, false, s);
+        if (prof) prof->begin(PROF_RESID64, s);
+        { ++g_launches; k_add_corr<<<592, 256, 0, s>>>(phi, e32_, (long long)L.N); }
+        if (prof) prof->end(s);
+        ++it;
+    }
+    if (st) { st->cycles = it; st->resid = rn; }
+    return rn <= target ? 0 : -3;
+}
+
+template void Multigrid::vcycle<double>(const DevParams&, const uint8_t*, int, double*, const double*, bool, cudaStream_t);
+template void Multigrid::vcycle<float>(const DevParams&, const uint8_t*, int, float*, const float*, bool, cudaStream_t);
+
+}  // namespace fx

@@ -1,0 +1,125 @@
+// fx_mg.h -- geometric multigrid for the variable-permittivity Poisson
+// operator that replaces AMReX MLABecLaplacian + MLMG
+// (ElectrostaticSolver.cpp:562-611, solve at :719):
+//
+//   (-alpha - div beta grad) phi = rhs,   beta on faces = 0.5 (eps_L + eps_R),
+//   x / y periodic, z Dirichlet through the maxorder-2 ghost 2 V - phi_0.
+//
+// Hierarchy: a direction is halved while its cell count is even and its
+// spacing is within 1.5x of the finest spacing; while z is being coarsened a
+// level uses red-black point Gauss-Seidel, once only x / y are coarsened it
+// uses red-black z-line Gauss-Seidel (a tridiagonal solve per column), so the
+// 1 x 1 x nz bottom level is solved exactly.  Prolongation is linear in the
+// coarsened directions, restriction averages, coarse coefficients are face
+// averages (beta) and cell averages (alpha).
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "fx_device.cuh"
+
+namespace fx {
+
+struct MGLevel {
+    int n[3];
+    double h[3];
+    int cr[3];          // coarsening ratio from the finer level
+    bool line;          // z-line smoother
+    float* wf[3] = {nullptr, nullptr, nullptr};  // prolongation far-neighbour weight per finer cell
+    size_t N;
+    // device storage, FP64 and FP32 copies
+    double *x64 = nullptr, *b64 = nullptr, *bw64 = nullptr, *bs64 = nullptr, *bb64 = nullptr, *a64 = nullptr, *cp64 = nullptr;
+    float *x32 = nullptr, *b32 = nullptr, *bw32 = nullptr, *bs32 = nullptr, *bb32 = nullptr, *a32 = nullptr, *cp32 = nullptr;
+};
+
+// Optional per-launch timing: CUDA events around each launch of a kernel
+// class, on the launching stream, summed after the stream has synchronised.
+enum ProfCat {
+    PROF_TDGL = 0, PROF_RHS_P, PROF_NEWTON, PROF_RHO, PROF_STEADY, PROF_SMOOTH_L0, PROF_RESTRICT_L0,
+    PROF_PROLONG_L0, PROF_MG_COARSE, PROF_RESID64, PROF_EFIELD, PROF_NCAT
+};
+
+struct Prof {
+    bool on = false;
+    std::vector<cudaEvent_t> pool;
+    std::vector<int> cats;     // category of pending pair q: events 2q, 2q+1
+    double ms[PROF_NCAT] = {0};
+    long long cnt[PROF_NCAT] = {0};
+    void begin(int cat, cudaStream_t s) {
+        if (!on) return;
+        const size_t q = cats.size();
+        while (pool.size() < 2 * q + 2) {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            pool.push_back(e);
+        }
+        cats.push_back(cat);
+        cudaEventRecord(pool[2 * q], s);
+    }
+    void end(cudaStream_t s) {
+        if (!on || cats.empty()) return;
+        cudaEventRecord(pool[2 * (cats.size() - 1) + 1], s);
+    }
+    void collect() {
+        for (size_t q = 0; q < cats.size(); ++q) {
+            float t = 0.f;
+            cudaEventSynchronize(pool[2 * q + 1]);
+            if (cudaEventElapsedTime(&t, pool[2 * q], pool[2 * q + 1]) == cudaSuccess) {
+                ms[cats[q]] += t;
+                cnt[cats[q]] += 1;
+            }
+        }
+        cats.clear();
+    }
+    void reset() { for (int c = 0; c < PROF_NCAT; ++c) { ms[c] = 0; cnt[c] = 0; } cats.clear(); }
+    ~Prof() { for (auto e : pool) cudaEventDestroy(e); }
+};
+
+struct MGStats {
+    int cycles = 0;
+    double resid = 0.0;       // final |r|_inf
+};
+
+class Multigrid {
+public:
+    ~Multigrid();
+    // builds the hierarchy and uploads the coarse face coefficients
+    int setup(const DevParams& p, const std::vector<uint8_t>& code_host, bool want64, bool want32);
+    // alpha changed on level 0 (device, FP64 and FP32 copies): average down
+    int set_alpha(const double* a64, const float* a32, bool has_alpha, cudaStream_t s);
+    // FP64 solve of A phi = rhs (+ electrode terms) to |r|_inf <= target
+    int solve64(const DevParams& p, const uint8_t* code, double* phi, const double* rhs, double target, int maxit,
+                cudaStream_t s, MGStats* st);
+    // FP64 iterative refinement around FP32 V-cycles
+    int solve_mixed(const DevParams& p, const uint8_t* code, double* phi, const double* rhs, double target,
+                    int maxit, cudaStream_t s, MGStats* st);
+    // |b' - A phi|_inf with the electrode terms (FP64); r may be null
+    int residual64(const DevParams& p, const uint8_t* code, const double* phi, const double* rhs, double* r,
+                   cudaStream_t s, double* norm_out);
+    size_t bytes() const { return bytes_; }
+    const std::vector<MGLevel>& levels() const { return lev_; }
+    int nu1 = 2, nu2 = 2, nu_bottom = 40;
+    Prof* prof = nullptr;
+    int verbose = 0;
+
+private:
+    std::vector<MGLevel> lev_;
+    double eps_[8];
+    const double* a0_64 = nullptr;
+    const float* a0_32 = nullptr;
+    bool has_alpha_ = false;
+    double* d_norm_ = nullptr;       // device scalar
+    double* h_norm_ = nullptr;       // pinned host
+    float* e32_ = nullptr;           // level-0 FP32 correction
+    float* r32_ = nullptr;           // level-0 FP32 residual
+    double* cp0_64_ = nullptr;       // level-0 line scratch
+    float* cp0_32_ = nullptr;
+    size_t bytes_ = 0;
+    template <typename T> void vcycle(const DevParams& p, const uint8_t* code, int l, T* x0, const T* b0, bool inhom, cudaStream_t s);
+    template <typename T> void smooth(const DevParams& p, const uint8_t* code, int l, T* x, const T* b, bool inhom, int sweeps, cudaStream_t s);
+};
+
+}  // namespace fx

@@ -126,7 +126,7 @@ def eval_expr(expr: str, consts: dict[str, float], x=None, y=None, z=None):
     env.update(consts)
     if x is not None:
         env.update(x=x, y=y, z=z)
-    code = _to_python(expr)
+    code = _to_python(" ".join(expr.split()))
     # comparisons yield booleans; arithmetic on them gives 0/1 as in AMReX Parser
     val = eval(code, {"__builtins__": {}}, env)  # noqa: S307 - trusted test decks
     return np.asarray(val, dtype=np.float64) * 1.0

@@ -85,6 +85,7 @@ struct MGLevel {
     int n[3];
     double h[3];
     int cr[3] = {1, 1, 1};           // coarsening ratio from the finer level
+    std::vector<double> wfar[3];     // prolongation weight of the far coarse cell, per fine cell of the finer level
     std::vector<double> a;           // alpha_cc (A = -1 multiplies it)
     std::vector<double> bx, by, bz;  // face coefficients (nx+1)*ny*nz etc.
     std::vector<double> x, r, t;     // correction, rhs, scratch
@@ -476,12 +477,24 @@ void mg_average_coeffs(std::vector<MGLevel>& mg) {
                             for (int di = 0; di < rx; ++di) s += f.a[L3(f, rx * i + di, ry * j + dj, rz * k + dk)];
                     c.a[L3(c, i, j, k)] = s / (rx * ry * rz);
                 }
+        // along a coarsened direction the fine links between two coarse
+        // centres act in series (half, full, half link), across the
+        // transverse children in parallel; at a Dirichlet face the path runs
+        // from the coarse centre to the electrode
+        auto ser = [](double a, double b, double c2) { return 4.0 / (1.0 / a + 2.0 / b + 1.0 / c2); };
+        const int fnx = f.n[0], fny = f.n[1], fnz = f.n[2];
+        auto BX = [&](int i, int j, int k) { return f.bx[FX(f, ((i % fnx) + fnx) % fnx, j, k)]; };
+        auto BY = [&](int i, int j, int k) { return f.by[FY(f, i, ((j % fny) + fny) % fny, k)]; };
+        auto BZ = [&](int i, int j, int k) { return f.bz[FZ(f, i, j, k)]; };
         for (int k = 0; k < c.n[2]; ++k)
             for (int j = 0; j < c.n[1]; ++j)
                 for (int i = 0; i <= c.n[0]; ++i) {
                     double s = 0.0;
                     for (int dk = 0; dk < rz; ++dk)
-                        for (int dj = 0; dj < ry; ++dj) s += f.bx[FX(f, rx * i, ry * j + dj, rz * k + dk)];
+                        for (int dj = 0; dj < ry; ++dj) {
+                            const int fj = ry * j + dj, fk = rz * k + dk;
+                            s += rx == 2 ? ser(BX(2 * i - 1, fj, fk), BX(2 * i, fj, fk), BX(2 * i + 1, fj, fk)) : BX(i, fj, fk);
+                        }
                     c.bx[FX(c, i, j, k)] = s / (ry * rz);
                 }
         for (int k = 0; k < c.n[2]; ++k)
@@ -489,7 +502,10 @@ void mg_average_coeffs(std::vector<MGLevel>& mg) {
                 for (int i = 0; i < c.n[0]; ++i) {
                     double s = 0.0;
                     for (int dk = 0; dk < rz; ++dk)
-                        for (int di = 0; di < rx; ++di) s += f.by[FY(f, rx * i + di, ry * j, rz * k + dk)];
+                        for (int di = 0; di < rx; ++di) {
+                            const int fi = rx * i + di, fk = rz * k + dk;
+                            s += ry == 2 ? ser(BY(fi, 2 * j - 1, fk), BY(fi, 2 * j, fk), BY(fi, 2 * j + 1, fk)) : BY(fi, j, fk);
+                        }
                     c.by[FY(c, i, j, k)] = s / (rx * rz);
                 }
         for (int k = 0; k <= c.n[2]; ++k)
@@ -497,9 +513,59 @@ void mg_average_coeffs(std::vector<MGLevel>& mg) {
                 for (int i = 0; i < c.n[0]; ++i) {
                     double s = 0.0;
                     for (int dj = 0; dj < ry; ++dj)
-                        for (int di = 0; di < rx; ++di) s += f.bz[FZ(f, rx * i + di, ry * j + dj, rz * k)];
+                        for (int di = 0; di < rx; ++di) {
+                            const int fi = rx * i + di, fj = ry * j + dj;
+                            double v;
+                            if (rz == 1) v = BZ(fi, fj, k);
+                            else if (k == 0) v = 2.0 / (1.0 / BZ(fi, fj, 0) + 1.0 / BZ(fi, fj, 1));
+                            else if (k == c.n[2]) v = 2.0 / (1.0 / BZ(fi, fj, fnz) + 1.0 / BZ(fi, fj, fnz - 1));
+                            else v = ser(BZ(fi, fj, 2 * k - 1), BZ(fi, fj, 2 * k), BZ(fi, fj, 2 * k + 1));
+                            s += v;
+                        }
                     c.bz[FZ(c, i, j, k)] = s / (rx * ry);
                 }
+    }
+}
+
+// Prolongation weights from the fine face coefficients: along a coarsened
+// direction a fine cell lies between its parent's centre (near, h/2 away) and
+// the neighbouring coarse centre (far, 3h/2 away); the weights are those of a
+// 1-D resistor chain, G_near / G_far, so a thin low-eps layer between the two
+// centres shifts the interpolated correction as the flux continuity demands.
+// Uniform coefficients give the linear weights 3/4, 1/4 (1/2 at an electrode).
+void mg_interp_weights(std::vector<MGLevel>& mg) {
+    for (size_t l = 1; l < mg.size(); ++l) {
+        const MGLevel& f = mg[l - 1];
+        MGLevel& c = mg[l];
+        const int nx = f.n[0], ny = f.n[1], nz = f.n[2];
+        for (int d = 0; d < 3; ++d) {
+            c.wfar[d].assign(f.N(), 0.25);
+            if (c.cr[d] != 2) continue;
+            const double h = f.h[d];
+            for (int k = 0; k < nz; ++k)
+                for (int j = 0; j < ny; ++j)
+                    for (int i = 0; i < nx; ++i) {
+                        const int q = d == 0 ? i : d == 1 ? j : k;
+                        const int n = f.n[d];
+                        // face beta at fine face index t (between cells t-1 and t)
+                        auto B = [&](int t) {
+                            if (d == 0) return f.bx[FX(f, ((t % n) + n) % n, j, k)];
+                            if (d == 1) return f.by[FY(f, i, ((t % n) + n) % n, k)];
+                            return f.bz[FZ(f, i, j, t)];
+                        };
+                        double gn, gf;
+                        if ((q & 1) == 0) {
+                            gn = 2.0 * B(q + 1) / h;
+                            if (d == 2 && q == 0) gf = 2.0 * B(0) / h;
+                            else gf = 1.0 / (h / B(q) + h / (2.0 * B(q - 1)));
+                        } else {
+                            gn = 2.0 * B(q) / h;
+                            if (d == 2 && q == n - 1) gf = 2.0 * B(n) / h;
+                            else gf = 1.0 / (h / B(q + 1) + h / (2.0 * B(q + 2)));
+                        }
+                        c.wfar[d][L3(f, i, j, k)] = gf / (gn + gf);
+                    }
+        }
     }
 }
 
@@ -547,34 +613,31 @@ void mg_vcycle(std::vector<MGLevel>& mg, size_t lev) {
                 c.r[L3(c, i, j, k)] = s * inv;
             }
     mg_vcycle(mg, lev + 1);
-    // linear cell-centred prolongation in the coarsened directions: weights
-    // 3/4 (parent) and 1/4 (the coarse neighbour on the child's side);
-    // periodic in x/y, homogeneous Dirichlet ghost -e0 in z
+    // prolongation in the coarsened directions with the resistor-chain
+    // weights (near parent / far neighbour); the far neighbour beyond an
+    // electrode is the homogeneous Dirichlet value 0
 #pragma omp parallel for schedule(static)
     for (int k = 0; k < l.n[2]; ++k)
         for (int j = 0; j < l.n[1]; ++j)
             for (int i = 0; i < l.n[0]; ++i) {
+                const size_t fc = L3(l, i, j, k);
                 int I[2], J[2], K[2];
                 double wi[2], wj[2], wk[2];
                 int ni = 1, nj = 1, nk = 1;
                 I[0] = i / rx; wi[0] = 1.0;
-                if (rx == 2) { ni = 2; wi[0] = 0.75; wi[1] = 0.25; I[1] = (i & 1) ? I[0] + 1 : I[0] - 1; I[1] = (I[1] + c.n[0]) % c.n[0]; }
+                if (rx == 2) { ni = 2; wi[1] = c.wfar[0][fc]; wi[0] = 1.0 - wi[1]; I[1] = (i & 1) ? I[0] + 1 : I[0] - 1; I[1] = (I[1] + c.n[0]) % c.n[0]; }
                 J[0] = j / ry; wj[0] = 1.0;
-                if (ry == 2) { nj = 2; wj[0] = 0.75; wj[1] = 0.25; J[1] = (j & 1) ? J[0] + 1 : J[0] - 1; J[1] = (J[1] + c.n[1]) % c.n[1]; }
+                if (ry == 2) { nj = 2; wj[1] = c.wfar[1][fc]; wj[0] = 1.0 - wj[1]; J[1] = (j & 1) ? J[0] + 1 : J[0] - 1; J[1] = (J[1] + c.n[1]) % c.n[1]; }
                 K[0] = k / rz; wk[0] = 1.0;
-                double zsign = 1.0;
                 if (rz == 2) {
-                    nk = 2; wk[0] = 0.75; wk[1] = 0.25; K[1] = (k & 1) ? K[0] + 1 : K[0] - 1;
-                    if (K[1] < 0 || K[1] >= c.n[2]) { K[1] = K[0]; zsign = -1.0; }
+                    nk = 2; wk[1] = c.wfar[2][fc]; wk[0] = 1.0 - wk[1]; K[1] = (k & 1) ? K[0] + 1 : K[0] - 1;
+                    if (K[1] < 0 || K[1] >= c.n[2]) { K[1] = K[0]; wk[1] = 0.0; }
                 }
                 double s = 0.0;
                 for (int a = 0; a < nk; ++a)
                     for (int b = 0; b < nj; ++b)
-                        for (int d = 0; d < ni; ++d) {
-                            double w = wk[a] * wj[b] * wi[d] * (a == 1 ? zsign : 1.0);
-                            s += w * c.x[L3(c, I[d], J[b], K[a])];
-                        }
-                l.x[L3(l, i, j, k)] += s;
+                        for (int d = 0; d < ni; ++d) s += wk[a] * wj[b] * wi[d] * c.x[L3(c, I[d], J[b], K[a])];
+                l.x[fc] += s;
             }
     gsrb(l, 2);
 }
@@ -593,6 +656,7 @@ void mg_setup(ofx_ctx* c, const double* alpha_cc_valid) {
     MGLevel& l0 = c->mg[0];
     for (size_t q = 0; q < l0.N(); ++q) l0.a[q] = alpha_cc_valid ? alpha_cc_valid[q] : 0.0;
     mg_average_coeffs(c->mg);
+    mg_interp_weights(c->mg);
 }
 
 // returns 0 on convergence, -3 when the iteration cap is hit
@@ -1190,7 +1254,8 @@ int ofx_set_field(ofx_ctx* c, int id, const double* in) {
     Fab* f = field_ptr(c, id);
     if (!f) return -1;
     valid_to_fab(in, *f);
-    if (id <= OFX_PZ || id == OFX_PHI || id == OFX_MASK || id == OFX_TPHASE) fill_boundary(*f, c->p.is_periodic);
+    if (id == OFX_PHI) phi_ghosts_after_solve(c);   // phi as left by a solve
+    else if (id <= OFX_PZ || id == OFX_MASK || id == OFX_TPHASE) fill_boundary(*f, c->p.is_periodic);
     return 0;
 }
 

@@ -1,0 +1,146 @@
+"""The C ABI without a GPU: the library loads, exports every declared entry
+point, parses inputs like the reference (checked against the oracle's reader),
+sets up masks / permittivity / initial P bit-exactly, and refuses to compute
+without a device instead of falling back to the CPU."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from ferrox_b200 import api, decks
+from oracle import inputs as I
+from oracle import oracle as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF_DECK = """
+domain.prob_lo = -8.e-9 -8.e-9 0.e-9
+domain.prob_hi =  8.e-9  8.e-9 9.e-9
+domain.n_cell = 16 16 18
+domain.is_periodic = 1 1 0
+boundary.hi = per per dir(Zmax)
+boundary.lo = per per dir(Zmin)
+prob_type = 2
+TimeIntegratorOrder = 1
+dt = 2.0e-13
+P_BC_flag_lo = 3 3 0
+P_BC_flag_hi = 3 3 1
+lambda = 3.0e-9
+my_constants.tlo = 5.0e-9
+my_constants.w = 2*tlo
+Coordinate_Transformation = 1
+tphase_geom.tphase_geom_function(x,y,z) = "1.*(x >= -3.e-9)*(x <= 3.e-9)*(z >= tlo)
+                                         + 0.*(y > 0)"
+angle_alpha.alpha_function(x,y,z) = "if(x > 0, 30.0, -15.0)"
+angle_beta.beta_function(x,y,z) = "10.0 + 20.0*(y > 1e-9)"
+angle_theta.theta_function(x,y,z) = "5.0 * (z > w/3)"
+SC_lo = -1.0 -1.0 -1.0
+SC_hi = -1.0 -1.0 -1.0
+DE_lo = -8.e-9 -8.e-9 0.0e-9
+DE_hi =  8.e-9  8.e-9 4.0e-9
+FE_lo = -8.e-9 -8.e-9 4.0e-9
+FE_hi =  8.e-9  8.e-9 9.0e-9
+epsilon_0 = 8.85e-12
+epsilonX_fe = 24.0
+epsilonX_fe_tphase = 40.0
+epsilonZ_fe = 24.0
+epsilon_de = 10.0
+epsilon_si = 11.7
+alpha = -2.5e9
+beta = 6.0e10
+gamma = 1.5e11
+BigGamma = 100
+g11 = 1.0e-9
+g44 = 1.0e-9
+g44_p = 0.0
+g12 = 0.0
+alpha_12 = 0.0
+alpha_112 = 0.0
+alpha_123 = 0.0
+"""
+
+
+def test_library_exports_every_declared_symbol():
+    L = api.lib()
+    with open(os.path.join(ROOT, "include", "ferrox_b200.h")) as f:
+        hdr = f.read()
+    declared = set(re.findall(r"\b(fx_\w+)\s*\(", hdr))
+    assert declared == set(api.EXPORTS), declared ^ set(api.EXPORTS)
+    for name in declared:
+        assert hasattr(L, name), name
+    assert b"sm_100a" in L.fx_version()
+
+
+@pytest.mark.parametrize("text", [decks.mfim(16, 16, 12), decks.mfism(16, 16, 48), REF_DECK])
+def test_setup_matches_oracle(text):
+    f = api.FerroX(text)
+    table = I.parse_table(text)
+    p = I.ferrox_params(table)
+    tph, a, b, t = I.function_fields(table, p)
+    o = O.Oracle(p, tph, (a, b, t))
+    for name in ["mask", "epsilon", "Gamma", "tphase", "alpha", "beta", "theta", "Px", "Py", "Pz"]:
+        assert np.array_equal(f.field(name), o.field(name)), name
+    for key in ["dt", "lambda", "alpha", "beta", "gamma", "g11", "g44", "BigGamma", "epsilon_de", "delta",
+                "phi_tolerance", "inc_step", "num_Vapp_max", "use_Fermi_Dirac", "prob_type"]:
+        assert f.param(key) == pytest.approx(p[key], rel=0, abs=0), key
+    for d in range(3):
+        assert f.param(f"DE_lo[{d}]") == p["DE_lo"][d]
+        assert f.param(f"P_BC_flag_hi[{d}]") == p["P_BC_flag_hi"][d]
+    assert f.param("V_hi") == o.scalar("V_hi") and f.param("V_lo") == o.scalar("V_lo")
+
+
+def test_grains_setup_matches_oracle():
+    text, g = decks.polycrystal(16, 16, 24, ngrains=6, seed=3)
+    f = api.FerroX(text)
+    f.set_grains(g["id"], g["angles"], g["tphase"])
+    tph, ang = decks.grain_fields(g)
+    o = O.Oracle(I.ferrox_params(I.parse_table(text)), tph, tuple(ang))
+    for name in ["mask", "epsilon", "tphase", "alpha", "beta", "theta", "Pz"]:
+        assert np.array_equal(f.field(name), o.field(name)), name
+    assert f.param("num_variants") >= 2
+
+
+@pytest.mark.parametrize("bad,code", [
+    ("FE_lo = -1 -1 -1\n", -3),
+    ("P_BC_flag_lo = 3 3 7\n", -2),
+    ("prob_type = 9\n", -2),
+    ("domain.is_periodic = 0 1 0\n", -3),
+    ("fx.phi_ghost_mode = sideways\n", -2),
+    ("tphase_geom.tphase_geom_function(x,y,z) = \"x +* 2\"\nCoordinate_Transformation = 1\n", -2),
+])
+def test_bad_inputs_are_rejected_with_a_message(bad, code):
+    text = decks.mfim(8, 8, 12) + bad
+    if code is None:
+        api.FerroX(text).close()
+        return
+    with pytest.raises(api.FxError) as e:
+        api.FerroX(text)
+    assert e.value.code == code
+    assert len(str(e.value)) > 20
+
+
+def test_missing_required_key():
+    text = "\n".join(l for l in decks.mfim(8, 8, 12).splitlines() if not l.startswith("BigGamma"))
+    with pytest.raises(api.FxError) as e:
+        api.FerroX(text)
+    assert "BigGamma" in str(e.value)
+
+
+def test_no_cpu_fallback_without_a_device():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    f = api.FerroX(decks.mfim(8, 8, 12))
+    for call in [f.compute_phi_rho, f.tdgl_euler, lambda: f.step(1), f.compute_E, f.compute_rho]:
+        with pytest.raises(api.FxError) as e:
+            call()
+        assert e.value.code == -4
+    with pytest.raises(api.FxError):
+        f.field("Phi")
+
+
+def test_odd_periodic_count_is_rejected():
+    with pytest.raises(api.FxError) as e:
+        api.FerroX(decks.mfim(9, 8, 12))
+    assert e.value.code == -3
