@@ -32,7 +32,7 @@ EXPORTS = ["fx_version", "fx_create", "fx_create_error", "fx_destroy", "fx_last_
            "fx_get_kernel_times", "fx_reset_kernel_times"]
 
 KERNEL_CLASSES = ["tdgl", "rhs_p", "newton", "rho", "steady", "smooth_l0", "restrict_l0", "prolong_l0",
-                  "mg_coarse", "resid64", "efield"]
+                  "mg_coarse", "resid64", "efield", "mg_l1", "mg_l2", "coarse_cta"]
 
 
 class FxError(RuntimeError):

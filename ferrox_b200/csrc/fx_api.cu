@@ -865,6 +865,7 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
     if (k == "fx.verbose") { p.verbose = (int)v; c->mg.verbose = (int)v; return FX_OK; }
     if (k == "fx.profile") { c->prof.collect(); c->prof.on = v != 0.0; return FX_OK; }
     if (k == "fx.mg_nu1") { c->mg.nu1 = (int)v; return FX_OK; }
+    if (k == "fx.graphs") { c->mg.set_graphs(v != 0.0); return FX_OK; }
     if (k == "fx.mg_nu2") { c->mg.nu2 = (int)v; return FX_OK; }
     if (k == "fx.phi_ghost_mode") { p.phi_ghost_mode = (int)v; c->dp.ghost_mode = (int)v; c->E_valid = false; return FX_OK; }
     if (k == "dt") { p.dt = v; c->dp.dt = v; return FX_OK; }
@@ -1182,6 +1183,8 @@ int fx_set_stream(fx_ctx* c, void* stream) {
     }
     c->s = (cudaStream_t)stream;
     c->own_stream = false;
+    // stream capture is not permitted on the legacy default stream
+    if (stream == nullptr || stream == (void*)cudaStreamLegacy) c->mg.set_graphs(false);
     return FX_OK;
 }
 

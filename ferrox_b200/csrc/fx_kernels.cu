@@ -347,16 +347,21 @@ __global__ void __launch_bounds__(256) k_rho(DevParams p, const uint8_t* __restr
         last = atomicAdd(counter, 1u) == gridDim.x - 1;
     }
     __syncthreads();
-    if (last && threadIdx.x == 0) {
+    if (last) {
+        // fold the block partials with the whole block, in a fixed order
         __threadfence();
         double t1 = 0.0, t2 = 0.0;
-        for (unsigned b = 0; b < gridDim.x; ++b) {
+        for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
             t1 += ((volatile double*)part)[2 * b];
             t2 += ((volatile double*)part)[2 * b + 1];
         }
-        out[0] = t1;
-        out[1] = t2;
-        *counter = 0;
+        t1 = block_sum(t1, sh);
+        t2 = block_sum(t2, sh);
+        if (threadIdx.x == 0) {
+            out[0] = t1;
+            out[1] = t2;
+            *counter = 0;
+        }
     }
 }
 
@@ -409,13 +414,16 @@ __global__ void __launch_bounds__(256) k_mean_p(DevParams p, const uint8_t* __re
         last = atomicAdd(counter, 1u) == gridDim.x - 1;
     }
     __syncthreads();
-    if (last && threadIdx.x == 0) {
+    if (last) {
         __threadfence();
         double t[4] = {0.0, 0.0, 0.0, 0.0};
-        for (unsigned blk = 0; blk < gridDim.x; ++blk)
+        for (unsigned blk = threadIdx.x; blk < gridDim.x; blk += blockDim.x)
             for (int q = 0; q < 4; ++q) t[q] += ((volatile double*)part)[4 * blk + q];
-        for (int q = 0; q < 3; ++q) out[q] = t[3] > 0 ? t[q] / t[3] : 0.0;
-        *counter = 0;
+        for (int q = 0; q < 4; ++q) t[q] = block_sum(t[q], sh);
+        if (threadIdx.x == 0) {
+            for (int q = 0; q < 3; ++q) out[q] = t[3] > 0 ? t[q] / t[3] : 0.0;
+            *counter = 0;
+        }
     }
 }
 

@@ -73,6 +73,10 @@ __device__ __forceinline__ void nbr(int i, int n, int& m, int& p) {
     p = i == n - 1 ? 0 : i + 1;
 }
 
+// the max-norm reductions spread their block maxima over NORM_SLOTS addresses
+// (one atomic per block, fewer collisions); the host takes the max of the slots
+constexpr int NORM_SLOTS = 64;
+
 __device__ __forceinline__ void atomic_max_nonneg(double* addr, double v) {
     if (!(v == v)) v = __longlong_as_double(0x7ff0000000000000LL);  // a NaN residual never converges
     atomicMax(reinterpret_cast<unsigned long long*>(addr), (unsigned long long)__double_as_longlong(v));
@@ -186,7 +190,8 @@ __global__ void __launch_bounds__(256) k_resid_restrict(Op<T> o, const T* __rest
     }
     if (norm) {
         const double m = block_max_all(mx);
-        if (threadIdx.x == 0 && threadIdx.y == 0) atomic_max_nonneg(norm, m);
+        const int slot = (blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)) & (NORM_SLOTS - 1);
+        if (threadIdx.x == 0 && threadIdx.y == 0) atomic_max_nonneg(norm + slot, m);
     }
 }
 
@@ -248,6 +253,264 @@ __global__ void __launch_bounds__(256) k_prolong(T* __restrict__ xf, const T* __
             for (int d = 0; d < ni; ++d)
                 s += wk[a] * wj[bb] * wi[d] * xc[(size_t)I[d] + (size_t)ncx * ((size_t)J[bb] + (size_t)ncy * K[a])];
     xf[fc] += s;
+}
+
+// ---------------------------------------------------------------------
+// The small levels of the hierarchy in one CTA: every array of the levels
+// from `top` down to the bottom lives in shared memory, and one launch runs
+// their whole V-cycle (smoothing, restriction, prolongation, exact bottom
+// line solve) with __syncthreads() between phases instead of one kernel
+// launch per phase.
+constexpr int MAXLEV = 24;
+
+struct CoarseLevelDesc {
+    int nx, ny, nz, N, rx, ry, rz, line;   // r*: ratio to the next (coarser) level
+    double ihx, ihy, ihz;
+    long long ox, ob, obw, obs, obb, oa, oq, oi;   // offsets (elements of T) in shared memory
+    long long ow[3];                            // offsets (floats) of the prolongation weights into this level
+    const void* gbw;
+    const void* gbs;
+    const void* gbb;
+    const void* ga;
+    const float* gw[3];
+};
+
+struct CoarseArgs {
+    int nlev;
+    int nu1, nu2, nu_bottom;
+    long long wbase;                 // byte offset of the float region
+    const void* b_in;                // right-hand side of the top level (global)
+    void* x_out;                     // solution of the top level (global)
+    CoarseLevelDesc L[MAXLEV];
+};
+
+template <typename T>
+struct SV {
+    int nx, ny, nz, N, nxy;
+    T ihx, ihy, ihz;
+    T *x, *b, *bw, *bs, *bb, *a, *q, *inv;
+};
+
+template <typename T>
+__device__ __forceinline__ SV<T> sview(const CoarseLevelDesc& d, T* sm) {
+    SV<T> v;
+    v.nx = d.nx; v.ny = d.ny; v.nz = d.nz; v.N = d.N; v.nxy = d.nx * d.ny;
+    v.ihx = T(d.ihx); v.ihy = T(d.ihy); v.ihz = T(d.ihz);
+    v.x = sm + d.ox; v.b = sm + d.ob; v.bw = sm + d.obw; v.bs = sm + d.obs; v.bb = sm + d.obb;
+    v.a = d.oa >= 0 ? sm + d.oa : nullptr;
+    v.q = d.oq >= 0 ? sm + d.oq : nullptr;
+    v.inv = sm + d.oi;
+    return v;
+}
+
+template <typename T>
+__device__ __forceinline__ void s_coeffs(const SV<T>& o, int i, int j, int k, int c, int ip, int jp, T& cw, T& ce,
+                                         T& cs, T& cn, T& cb, T& ct, T& diag) {
+    T extra = T(0);
+    const int row = c - i;
+    cw = o.bw[c] * o.ihx;
+    ce = o.bw[row + ip] * o.ihx;
+    cs = o.bs[c] * o.ihy;
+    cn = o.bs[c + (jp - j) * o.nx] * o.ihy;
+    const T fb = o.bb[c], ft = o.bb[c + o.nxy];
+    if (k > 0) cb = fb * o.ihz; else { cb = T(0); extra += T(2) * fb * o.ihz; }
+    if (k < o.nz - 1) ct = ft * o.ihz; else { ct = T(0); extra += T(2) * ft * o.ihz; }
+    if (o.nx == 1) { cw = T(0); ce = T(0); }
+    if (o.ny == 1) { cs = T(0); cn = T(0); }
+    const T a = o.a ? o.a[c] : T(0);
+    diag = -a + cw + ce + cs + cn + cb + ct + extra;
+}
+
+// factor each z-line once per call (q_k = ct_k / den_k, inv_k = 1 / den_k;
+// stored in q and inv), or invert the point diagonal; the sweeps then need no
+// division
+template <typename T>
+__device__ void s_factor(const SV<T>& o, bool line) {
+    if (line) {
+        for (int col = threadIdx.x; col < o.nxy; col += blockDim.x) {
+            const int i = col % o.nx, j = col / o.nx;
+            const int ip = i == o.nx - 1 ? 0 : i + 1, jp = j == o.ny - 1 ? 0 : j + 1;
+            T qprev = T(0);
+            int c = col;
+            for (int k = 0; k < o.nz; ++k, c += o.nxy) {
+                T cw, ce, cs, cn, cb, ct, diag;
+                s_coeffs(o, i, j, k, c, ip, jp, cw, ce, cs, cn, cb, ct, diag);
+                const T inv = T(1) / (diag - cb * qprev);
+                o.q[c] = ct * inv;
+                o.inv[c] = inv;
+                qprev = o.q[c];
+            }
+        }
+    } else {
+        for (int c = threadIdx.x; c < o.N; c += blockDim.x) {
+            const int i = c % o.nx, j = (c / o.nx) % o.ny, k = c / o.nxy;
+            const int ip = i == o.nx - 1 ? 0 : i + 1, jp = j == o.ny - 1 ? 0 : j + 1;
+            T cw, ce, cs, cn, cb, ct, diag;
+            s_coeffs(o, i, j, k, c, ip, jp, cw, ce, cs, cn, cb, ct, diag);
+            o.inv[c] = T(1) / diag;
+        }
+    }
+}
+
+template <typename T>
+__device__ void s_smooth(const SV<T>& o, bool line, int sweeps) {
+    const int nt = blockDim.x;
+    for (int sw = 0; sw < sweeps; ++sw)
+        for (int color = 0; color < 2; ++color) {
+            if (line) {
+                const int ncol = o.nxy;
+                for (int col = threadIdx.x; col < ncol; col += nt) {
+                    const int i = col % o.nx, j = col / o.nx;
+                    if (((i + j) & 1) != color) continue;
+                    const int im = i == 0 ? o.nx - 1 : i - 1, ip = i == o.nx - 1 ? 0 : i + 1;
+                    const int jm = j == 0 ? o.ny - 1 : j - 1, jp = j == o.ny - 1 ? 0 : j + 1;
+                    T dprev = T(0);
+                    int c = col;
+                    for (int k = 0; k < o.nz; ++k, c += o.nxy) {
+                        const int row = c - i;
+                        T cw = o.bw[c] * o.ihx, ce = o.bw[row + ip] * o.ihx;
+                        T cs = o.bs[c] * o.ihy, cn = o.bs[c + (jp - j) * o.nx] * o.ihy;
+                        if (o.nx == 1) { cw = T(0); ce = T(0); }
+                        if (o.ny == 1) { cs = T(0); cn = T(0); }
+                        const T cb = k > 0 ? o.bb[c] * o.ihz : T(0);
+                        const T r = o.b[c] + cw * o.x[row + im] + ce * o.x[row + ip] + cs * o.x[c + (jm - j) * o.nx] +
+                                    cn * o.x[c + (jp - j) * o.nx];
+                        const T dk = (r + cb * dprev) * o.inv[c];
+                        o.x[c] = dk;
+                        dprev = dk;
+                    }
+                    c -= o.nxy;
+                    T xn = o.x[c];
+                    for (int k = o.nz - 2; k >= 0; --k) {
+                        c -= o.nxy;
+                        xn = o.x[c] + o.q[c] * xn;
+                        o.x[c] = xn;
+                    }
+                }
+            } else {
+                for (int c = threadIdx.x; c < o.N; c += nt) {
+                    const int i = c % o.nx, j = (c / o.nx) % o.ny, k = c / o.nxy;
+                    if (((i + j + k) & 1) != color) continue;
+                    const int im = i == 0 ? o.nx - 1 : i - 1, ip = i == o.nx - 1 ? 0 : i + 1;
+                    const int jm = j == 0 ? o.ny - 1 : j - 1, jp = j == o.ny - 1 ? 0 : j + 1;
+                    T cw, ce, cs, cn, cb, ct, diag;
+                    s_coeffs(o, i, j, k, c, ip, jp, cw, ce, cs, cn, cb, ct, diag);
+                    const int row = c - i;
+                    T s = o.b[c] + cw * o.x[row + im] + ce * o.x[row + ip] + cs * o.x[c + (jm - j) * o.nx] +
+                          cn * o.x[c + (jp - j) * o.nx];
+                    if (k > 0) s += cb * o.x[c - o.nxy];
+                    if (k < o.nz - 1) s += ct * o.x[c + o.nxy];
+                    o.x[c] = s * o.inv[c];
+                }
+            }
+            __syncthreads();
+        }
+}
+
+template <typename T>
+__device__ void s_restrict(const SV<T>& f, const SV<T>& c, int rx, int ry, int rz) {
+    for (int cc = threadIdx.x; cc < c.N; cc += blockDim.x) {
+        const int I = cc % c.nx, J = (cc / c.nx) % c.ny, K = cc / c.nxy;
+        T s = T(0);
+        for (int dk = 0; dk < rz; ++dk)
+            for (int dj = 0; dj < ry; ++dj)
+                for (int di = 0; di < rx; ++di) {
+                    const int i = rx * I + di, j = ry * J + dj, k = rz * K + dk;
+                    const int fc = i + f.nx * (j + f.ny * k);
+                    const int im = i == 0 ? f.nx - 1 : i - 1, ip = i == f.nx - 1 ? 0 : i + 1;
+                    const int jm = j == 0 ? f.ny - 1 : j - 1, jp = j == f.ny - 1 ? 0 : j + 1;
+                    T cw, ce, cs, cn, cb, ct, diag;
+                    s_coeffs(f, i, j, k, fc, ip, jp, cw, ce, cs, cn, cb, ct, diag);
+                    const int row = fc - i;
+                    T off = cw * f.x[row + im] + ce * f.x[row + ip] + cs * f.x[fc + (jm - j) * f.nx] + cn * f.x[fc + (jp - j) * f.nx];
+                    if (k > 0) off += cb * f.x[fc - f.nxy];
+                    if (k < f.nz - 1) off += ct * f.x[fc + f.nxy];
+                    s += f.b[fc] - (diag * f.x[fc] - off);
+                }
+        c.b[cc] = s / T(rx * ry * rz);
+        c.x[cc] = T(0);
+    }
+    __syncthreads();
+}
+
+template <typename T>
+__device__ void s_prolong(const SV<T>& f, const SV<T>& c, int rx, int ry, int rz, const float* wx, const float* wy,
+                          const float* wz) {
+    for (int fc = threadIdx.x; fc < f.N; fc += blockDim.x) {
+        const int i = fc % f.nx, j = (fc / f.nx) % f.ny, k = fc / f.nxy;
+        int I[2], J[2], K[2];
+        T wi[2], wj[2], wk[2];
+        int ni = 1, nj = 1, nk = 1;
+        I[0] = i / rx; wi[0] = T(1);
+        if (rx == 2) { ni = 2; wi[1] = T(wx[fc]); wi[0] = T(1) - wi[1]; I[1] = (i & 1) ? I[0] + 1 : I[0] - 1; I[1] = (I[1] + c.nx) % c.nx; }
+        J[0] = j / ry; wj[0] = T(1);
+        if (ry == 2) { nj = 2; wj[1] = T(wy[fc]); wj[0] = T(1) - wj[1]; J[1] = (j & 1) ? J[0] + 1 : J[0] - 1; J[1] = (J[1] + c.ny) % c.ny; }
+        K[0] = k / rz; wk[0] = T(1);
+        if (rz == 2) {
+            nk = 2; wk[1] = T(wz[fc]); wk[0] = T(1) - wk[1]; K[1] = (k & 1) ? K[0] + 1 : K[0] - 1;
+            if (K[1] < 0 || K[1] >= c.nz) { K[1] = K[0]; wk[1] = T(0); }
+        }
+        T s = T(0);
+        for (int a = 0; a < nk; ++a)
+            for (int bb = 0; bb < nj; ++bb)
+                for (int d = 0; d < ni; ++d) s += wk[a] * wj[bb] * wi[d] * c.x[I[d] + c.nx * (J[bb] + c.ny * K[a])];
+        f.x[fc] += s;
+    }
+    __syncthreads();
+}
+
+template <typename T>
+__global__ void __launch_bounds__(1024) k_coarse_vcycle(CoarseArgs A) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T* sm = reinterpret_cast<T*>(smraw);
+    float* sw = reinterpret_cast<float*>(smraw + A.wbase);
+    // load coefficients and the top right-hand side
+    for (int l = 0; l < A.nlev; ++l) {
+        const CoarseLevelDesc& d = A.L[l];
+        const int nxy = d.nx * d.ny;
+        const T* gbw = (const T*)d.gbw;
+        const T* gbs = (const T*)d.gbs;
+        const T* gbb = (const T*)d.gbb;
+        const T* ga = (const T*)d.ga;
+        for (int c = threadIdx.x; c < d.N; c += blockDim.x) {
+            sm[d.obw + c] = gbw[c];
+            sm[d.obs + c] = gbs[c];
+            if (d.oa >= 0) sm[d.oa + c] = ga[c];
+            sm[d.ox + c] = T(0);
+        }
+        for (int c = threadIdx.x; c < d.N + nxy; c += blockDim.x) sm[d.obb + c] = gbb[c];
+        for (int q = 0; q < 3; ++q)
+            if (d.gw[q])
+                for (int c = threadIdx.x; c < d.N; c += blockDim.x) sw[d.ow[q] + c] = d.gw[q][c];
+    }
+    {
+        const T* b_in = (const T*)A.b_in;
+        for (int c = threadIdx.x; c < A.L[0].N; c += blockDim.x) sm[A.L[0].ob + c] = b_in[c];
+    }
+    __syncthreads();
+    for (int l = 0; l < A.nlev; ++l) s_factor(sview<T>(A.L[l], sm), A.L[l].line != 0);
+    __syncthreads();
+    // V-cycle over the shared-memory levels
+    for (int l = 0; l < A.nlev - 1; ++l) {
+        const SV<T> f = sview<T>(A.L[l], sm), c = sview<T>(A.L[l + 1], sm);
+        s_smooth(f, A.L[l].line != 0, A.nu1);
+        s_restrict(f, c, A.L[l].rx, A.L[l].ry, A.L[l].rz);
+    }
+    {
+        const CoarseLevelDesc& d = A.L[A.nlev - 1];
+        const SV<T> o = sview<T>(d, sm);
+        const bool exact = d.line && d.nx * d.ny == 1;
+        s_smooth(o, d.line != 0, exact ? 1 : A.nu_bottom);
+    }
+    for (int l = A.nlev - 2; l >= 0; --l) {
+        const SV<T> f = sview<T>(A.L[l], sm), c = sview<T>(A.L[l + 1], sm);
+        const CoarseLevelDesc& d = A.L[l];
+        s_prolong(f, c, d.rx, d.ry, d.rz, d.gw[0] ? sw + d.ow[0] : nullptr, d.gw[1] ? sw + d.ow[1] : nullptr,
+                  d.gw[2] ? sw + d.ow[2] : nullptr);
+        s_smooth(f, d.line != 0, A.nu2);
+    }
+    T* x_out = (T*)A.x_out;
+    for (int c = threadIdx.x; c < A.L[0].N; c += blockDim.x) x_out[c] = sm[A.L[0].ox + c];
 }
 
 template <typename Tin, typename T>
@@ -314,6 +577,12 @@ template <> float* lq<float>(MGLevel& L) { return L.cp32; }
 
 }  // namespace
 
+double Multigrid::slots_max() const {
+    double m = 0.0;
+    for (int q = 0; q < NORM_SLOTS; ++q) m = std::max(m, h_norm_[q]);
+    return m;
+}
+
 Multigrid::~Multigrid() {
     for (size_t l = 0; l < lev_.size(); ++l) {
         MGLevel& L = lev_[l];
@@ -323,6 +592,8 @@ Multigrid::~Multigrid() {
         cudaFree(L.bw32); cudaFree(L.bs32); cudaFree(L.bb32); cudaFree(L.a32); cudaFree(L.cp32);
         for (int d = 0; d < 3; ++d) cudaFree(L.wf[d]);
     }
+    if (g64_.exec) cudaGraphExecDestroy(g64_.exec);
+    if (g32_.exec) cudaGraphExecDestroy(g32_.exec);
     cudaFree(d_norm_);
     if (h_norm_) cudaFreeHost(h_norm_);
     cudaFree(e32_);
@@ -500,8 +771,8 @@ int Multigrid::setup(const DevParams& p, const std::vector<uint8_t>& code, bool 
             if (want32) { L.cp32 = dalloc<float>(N, bytes_); if (!L.cp32) return -2; }
         }
     }
-    if (cudaMalloc(&d_norm_, 64) != cudaSuccess) return -2;
-    if (cudaMallocHost(&h_norm_, 64) != cudaSuccess) return -2;
+    if (cudaMalloc(&d_norm_, NORM_SLOTS * 8) != cudaSuccess) return -2;
+    if (cudaMallocHost(&h_norm_, NORM_SLOTS * 8) != cudaSuccess) return -2;
     if (want32) {
         e32_ = dalloc<float>(L0.N, bytes_);
         r32_ = dalloc<float>(L0.N, bytes_);
@@ -509,7 +780,10 @@ int Multigrid::setup(const DevParams& p, const std::vector<uint8_t>& code, bool 
         lev_[0].x32 = e32_;
         lev_[0].b32 = r32_;
     }
+    plan_coarse(want64, want32);
     if (verbose) {
+        printf("  one-CTA coarse cycle from level %d (FP64, %zu B smem), %d (FP32, %zu B smem)\n", coarse_top64_,
+               coarse_smem64_, coarse_top32_, coarse_smem32_);
         for (size_t l = 0; l < lev_.size(); ++l)
             printf("  mg level %zu: %d x %d x %d  h = %.4g %.4g %.4g nm  %s\n", l, lev_[l].n[0], lev_[l].n[1], lev_[l].n[2],
                    lev_[l].h[0] * 1e9, lev_[l].h[1] * 1e9, lev_[l].h[2] * 1e9, lev_[l].line ? "z-line GS" : "point RB-GS");
@@ -538,6 +812,90 @@ int Multigrid::set_alpha(const double* a64, const float* a32, bool has_alpha, cu
     return (int)cudaGetLastError();
 }
 
+// shared-memory bytes of levels top..last for element size es (alpha and the
+// line scratch always reserved so the plan holds for any alpha)
+static size_t coarse_bytes(const std::vector<MGLevel>& lev, int top, size_t es, size_t* wbase) {
+    size_t t = 0, w = 0;
+    for (size_t l = top; l < lev.size(); ++l) {
+        const size_t N = lev[l].N, nxy = (size_t)lev[l].n[0] * lev[l].n[1];
+        t += (7 * N + nxy) * es + (lev[l].line ? N * es : 0);
+        if (l + 1 < lev.size())
+            for (int d = 0; d < 3; ++d) if (lev[l + 1].cr[d] == 2) w += N;
+    }
+    t = (t + 15) / 16 * 16;
+    if (wbase) *wbase = t;
+    return t + w * 4;
+}
+
+void Multigrid::plan_coarse(bool want64, bool want32) {
+    constexpr size_t budget = 200 * 1024;
+    coarse_top64_ = coarse_top32_ = -1;
+    for (int top = 1; top < (int)lev_.size(); ++top) {
+        if (want64 && coarse_top64_ < 0 && coarse_bytes(lev_, top, 8, nullptr) <= budget) {
+            coarse_top64_ = top;
+            coarse_smem64_ = coarse_bytes(lev_, top, 8, nullptr);
+        }
+        if (want32 && coarse_top32_ < 0 && coarse_bytes(lev_, top, 4, nullptr) <= budget) {
+            coarse_top32_ = top;
+            coarse_smem32_ = coarse_bytes(lev_, top, 4, nullptr);
+        }
+    }
+    if (coarse_top64_ > 0)
+        cudaFuncSetAttribute(k_coarse_vcycle<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coarse_smem64_);
+    if (coarse_top32_ > 0)
+        cudaFuncSetAttribute(k_coarse_vcycle<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coarse_smem32_);
+}
+
+template <> int Multigrid::coarse_top<double>() const { return coarse_top64_; }
+template <> int Multigrid::coarse_top<float>() const { return coarse_top32_; }
+
+template <typename T>
+void Multigrid::launch_coarse(int top, cudaStream_t s) {
+    CoarseArgs A;
+    std::memset(&A, 0, sizeof(A));
+    const size_t es = sizeof(T);
+    size_t wbase = 0;
+    const size_t bytes = coarse_bytes(lev_, top, es, &wbase);
+    A.nlev = (int)lev_.size() - top;
+    A.nu1 = nu1; A.nu2 = nu2; A.nu_bottom = nu_bottom;
+    A.wbase = (long long)wbase;
+    A.b_in = lb<T>(lev_[top]);
+    A.x_out = lx<T>(lev_[top]);
+    long long off = 0, woff = 0;
+    for (int q = 0; q < A.nlev; ++q) {
+        MGLevel& L = lev_[top + q];
+        CoarseLevelDesc& d = A.L[q];
+        const long long N = (long long)L.N, nxy = (long long)L.n[0] * L.n[1];
+        d.nx = L.n[0]; d.ny = L.n[1]; d.nz = L.n[2]; d.N = (int)N; d.line = L.line;
+        d.ihx = 1.0 / (L.h[0] * L.h[0]); d.ihy = 1.0 / (L.h[1] * L.h[1]); d.ihz = 1.0 / (L.h[2] * L.h[2]);
+        d.ox = off; off += N;
+        d.ob = off; off += N;
+        d.obw = off; off += N;
+        d.obs = off; off += N;
+        d.obb = off; off += N + nxy;
+        d.oa = has_alpha_ ? off : -1; off += N;
+        d.oq = L.line ? off : -1; off += L.line ? N : 0;
+        d.oi = off; off += N;
+        if constexpr (sizeof(T) == 8) { d.gbw = L.bw64; d.gbs = L.bs64; d.gbb = L.bb64; d.ga = has_alpha_ ? L.a64 : nullptr; }
+        else { d.gbw = L.bw32; d.gbs = L.bs32; d.gbb = L.bb32; d.ga = has_alpha_ ? L.a32 : nullptr; }
+        if (top + q + 1 < (int)lev_.size()) {
+            const MGLevel& C = lev_[top + q + 1];
+            d.rx = C.cr[0]; d.ry = C.cr[1]; d.rz = C.cr[2];
+            for (int k = 0; k < 3; ++k) {
+                d.gw[k] = C.cr[k] == 2 ? C.wf[k] : nullptr;
+                d.ow[k] = C.cr[k] == 2 ? woff : -1;
+                if (C.cr[k] == 2) woff += N;
+            }
+        } else {
+            d.rx = d.ry = d.rz = 1;
+        }
+    }
+    if (prof) prof->begin(PROF_COARSE_CTA, s);
+    ++g_launches;
+    k_coarse_vcycle<T><<<1, 1024, bytes, s>>>(A);
+    if (prof) prof->end(s);
+}
+
 template <typename T>
 void Multigrid::smooth(const DevParams& p, const uint8_t* code, int l, T* x, const T* b, bool inhom, int sweeps,
                        cudaStream_t s) {
@@ -553,7 +911,7 @@ void Multigrid::smooth(const DevParams& p, const uint8_t* code, int l, T* x, con
         dim3 b2(32, 4), g2(((L.n[0] + 1) / 2 + 31) / 32, (L.n[1] + 3) / 4, 1);
         for (int it = 0; it < sweeps; ++it)
             for (int color = 0; color < 2; ++color) {
-                if (prof) prof->begin(l == 0 ? PROF_SMOOTH_L0 : PROF_MG_COARSE, s);
+                if (prof) prof->begin(l == 0 ? PROF_SMOOTH_L0 : l == 1 ? PROF_MG_L1 : l == 2 ? PROF_MG_L2 : PROF_MG_COARSE, s);
                 if (l == 0) { ++g_launches; k_line<T, true><<<g2, b2, 0, s>>>(o, x, b, q, color); }
                 else { ++g_launches; k_line<T, false><<<g2, b2, 0, s>>>(o, x, b, q, color); }
                 if (prof) prof->end(s);
@@ -562,7 +920,7 @@ void Multigrid::smooth(const DevParams& p, const uint8_t* code, int l, T* x, con
         dim3 b2(32, 8), g2(((L.n[0] + 1) / 2 + 31) / 32, (L.n[1] + 7) / 8, L.n[2]);
         for (int it = 0; it < sweeps; ++it)
             for (int color = 0; color < 2; ++color) {
-                if (prof) prof->begin(l == 0 ? PROF_SMOOTH_L0 : PROF_MG_COARSE, s);
+                if (prof) prof->begin(l == 0 ? PROF_SMOOTH_L0 : l == 1 ? PROF_MG_L1 : l == 2 ? PROF_MG_L2 : PROF_MG_COARSE, s);
                 if (l == 0) { ++g_launches; k_rbgs<T, true><<<g2, b2, 0, s>>>(o, x, b, color); }
                 else { ++g_launches; k_rbgs<T, false><<<g2, b2, 0, s>>>(o, x, b, color); }
                 if (prof) prof->end(s);
@@ -574,6 +932,10 @@ template <typename T>
 void Multigrid::vcycle(const DevParams& p, const uint8_t* code, int l, T* x, const T* b, bool inhom, cudaStream_t s) {
     MGLevel& L = lev_[l];
     const int last = (int)lev_.size() - 1;
+    if (l > 0 && l == coarse_top<T>()) {
+        launch_coarse<T>(l, s);
+        return;
+    }
     if (l == last) {
         const bool exact = L.line && L.n[0] * L.n[1] == 1;
         smooth<T>(p, code, l, x, b, inhom, exact ? 1 : nu_bottom, s);
@@ -589,14 +951,14 @@ void Multigrid::vcycle(const DevParams& p, const uint8_t* code, int l, T* x, con
     Op<T> o = make_op<T>(L, l, code, eps_, a, inhom, p);
     dim3 b2(32, 8), g2((C.n[0] + 31) / 32, (C.n[1] + 7) / 8, C.n[2]);
     double* norm = (l == 0) ? d_norm_ : nullptr;
-    if (prof) prof->begin(l == 0 ? PROF_RESTRICT_L0 : PROF_MG_COARSE, s);
+    if (prof) prof->begin(l == 0 ? PROF_RESTRICT_L0 : l == 1 ? PROF_MG_L1 : l == 2 ? PROF_MG_L2 : PROF_MG_COARSE, s);
     if (l == 0) { ++g_launches; k_resid_restrict<T, true><<<g2, b2, 0, s>>>(o, x, b, lb<T>(C), C.n[0], C.n[1], C.n[2], C.cr[0], C.cr[1], C.cr[2], norm); }
     else { ++g_launches; k_resid_restrict<T, false><<<g2, b2, 0, s>>>(o, x, b, lb<T>(C), C.n[0], C.n[1], C.n[2], C.cr[0], C.cr[1], C.cr[2], norm); }
     if (prof) prof->end(s);
     cudaMemsetAsync(lx<T>(C), 0, C.N * sizeof(T), s);
     vcycle<T>(p, code, l + 1, lx<T>(C), lb<T>(C), false, s);
     dim3 g3((L.n[0] + 31) / 32, (L.n[1] + 7) / 8, L.n[2]);
-    if (prof) prof->begin(l == 0 ? PROF_PROLONG_L0 : PROF_MG_COARSE, s);
+    if (prof) prof->begin(l == 0 ? PROF_PROLONG_L0 : l == 1 ? PROF_MG_L1 : l == 2 ? PROF_MG_L2 : PROF_MG_COARSE, s);
     { ++g_launches; k_prolong<T><<<g3, b2, 0, s>>>(x, lx<T>(C), C.wf[0], C.wf[1], C.wf[2], L.n[0], L.n[1], L.n[2], C.n[0], C.n[1], C.n[2], C.cr[0], C.cr[1], C.cr[2]); }
     if (prof) prof->end(s);
     smooth<T>(p, code, l, x, b, inhom, nu2, s);
@@ -606,16 +968,44 @@ int Multigrid::residual64(const DevParams& p, const uint8_t* code, const double*
                           cudaStream_t s, double* norm_out) {
     MGLevel& L = lev_[0];
     Op<double> o = make_op<double>(L, 0, code, eps_, has_alpha_ ? a0_64 : nullptr, true, p);
-    cudaMemsetAsync(d_norm_, 0, 8, s);
+    cudaMemsetAsync(d_norm_, 0, NORM_SLOTS * 8, s);
     dim3 b2(32, 8), g2((L.n[0] + 31) / 32, (L.n[1] + 7) / 8, L.n[2]);
     (void)r;
     if (prof) prof->begin(PROF_RESID64, s);
     { ++g_launches; k_resid64<<<g2, b2, 0, s>>>(o, phi, rhs, nullptr, d_norm_); }
     if (prof) prof->end(s);
-    cudaMemcpyAsync(h_norm_, d_norm_, 8, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(h_norm_, d_norm_, NORM_SLOTS * 8, cudaMemcpyDeviceToHost, s);
     cudaError_t e = cudaStreamSynchronize(s);
-    if (norm_out) *norm_out = h_norm_[0];
+    if (norm_out) *norm_out = slots_max();
     return (int)e;
+}
+
+template <typename F>
+int Multigrid::replay(GraphCache& g, const void* x, const void* rhs, const DevParams& p, cudaStream_t s, F&& enqueue) {
+    const bool profiling = prof && prof->on;
+    if (!use_graphs_ || profiling) {
+        enqueue();
+        return (int)cudaGetLastError();
+    }
+    if (!g.exec || g.x != x || g.rhs != rhs || g.has_alpha != has_alpha_ || g.vlo != p.V_lo || g.vhi != p.V_hi ||
+        g.nu1 != nu1 || g.nu2 != nu2) {
+        if (g.exec) { cudaGraphExecDestroy(g.exec); g.exec = nullptr; }
+        cudaGraph_t graph;
+        const long long l0 = g_launches.load();
+        cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+        if (e) return (int)e;
+        enqueue();
+        e = cudaStreamEndCapture(s, &graph);
+        if (e) return (int)e;
+        g.launches = g_launches.load() - l0;
+        g_launches -= g.launches;    // counted per replay below
+        e = cudaGraphInstantiate(&g.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e) return (int)e;
+        g.x = x; g.rhs = rhs; g.has_alpha = has_alpha_; g.vlo = p.V_lo; g.vhi = p.V_hi; g.nu1 = nu1; g.nu2 = nu2;
+    }
+    g_launches += g.launches;
+    return (int)cudaGraphLaunch(g.exec, s);
 }
 
 int Multigrid::solve64(const DevParams& p, const uint8_t* code, double* phi, const double* rhs, double target,
@@ -628,13 +1018,16 @@ int Multigrid::solve64(const DevParams& p, const uint8_t* code, double* phi, con
         // one V-cycle; the level-0 residual norm after pre-smoothing bounds
         // the residual after the cycle, so it is the loop test; the exact
         // final residual is checked before returning
-        cudaMemsetAsync(d_norm_, 0, 8, s);
-        vcycle<double>(p, code, 0, phi, rhs, true, s);
-        cudaMemcpyAsync(h_norm_, d_norm_, 8, cudaMemcpyDeviceToHost, s);
+        e = replay(g64_, phi, rhs, p, s, [&]() {
+            cudaMemsetAsync(d_norm_, 0, NORM_SLOTS * 8, s);
+            vcycle<double>(p, code, 0, phi, rhs, true, s);
+            cudaMemcpyAsync(h_norm_, d_norm_, NORM_SLOTS * 8, cudaMemcpyDeviceToHost, s);
+        });
+        if (e) return e;
         e = (int)cudaStreamSynchronize(s);
         if (e) return e;
         ++it;
-        const double mid = h_norm_[0];
+        const double mid = slots_max();
         if (verbose > 1) printf("  mg cycle %d: |r|/target after pre-smoothing = %.3e\n", it, mid / target);
         if (lev_.size() == 1) { e = residual64(p, code, phi, rhs, nullptr, s, &rn); if (e) return e; continue; }
         if (mid <= target) {
@@ -653,25 +1046,38 @@ int Multigrid::solve_mixed(const DevParams& p, const uint8_t* code, double* phi,
     MGLevel& L = lev_[0];
     Op<double> o64 = make_op<double>(L, 0, code, eps_, has_alpha_ ? a0_64 : nullptr, true, p);
     dim3 b2(32, 8), g2((L.n[0] + 31) / 32, (L.n[1] + 7) / 8, L.n[2]);
+    auto resid = [&]() {
+        cudaMemsetAsync(d_norm_, 0, NORM_SLOTS * 8, s);
+        if (prof) prof->begin(PROF_RESID64, s);
+        ++g_launches;
+        k_resid64<<<g2, b2, 0, s>>>(o64, phi, rhs, r32_, d_norm_);
+        if (prof) prof->end(s);
+        cudaMemcpyAsync(h_norm_, d_norm_, NORM_SLOTS * 8, cudaMemcpyDeviceToHost, s);
+    };
+    resid();
+    int e = (int)cudaStreamSynchronize(s);
+    if (e) return e;
+    double rn = slots_max();
     int it = 0;
-    double rn = 0.0;
-    while (true) {
-        cudaMemsetAsync(d_norm_, 0, 8, s);
-        if (prof) prof->begin(PROF_RESID64, s);
-        { ++g_launches; k_resid64<<<g2, b2, 0, s>>>(o64, phi, rhs, r32_, d_norm_); }
-        if (prof) prof->end(s);
-        cudaMemcpyAsync(h_norm_, d_norm_, 8, cudaMemcpyDeviceToHost, s);
-        int e = (int)cudaStreamSynchronize(s);
+    if (verbose > 1) printf("  refinement %d: |r|/target = %.3e\n", it, rn / target);
+    while (!(rn <= target) && it < maxit) {
+        // FP32 correction cycle on the FP32 residual, FP64 update and FP64
+        // residual of the updated phi
+        e = replay(g32_, phi, rhs, p, s, [&]() {
+            cudaMemsetAsync(e32_, 0, L.N * sizeof(float), s);
+            vcycle<float>(p, code, 0, e32_, r32_, false, s);
+            if (prof) prof->begin(PROF_RESID64, s);
+            ++g_launches;
+            k_add_corr<<<592, 256, 0, s>>>(phi, e32_, (long long)L.N);
+            if (prof) prof->end(s);
+            resid();
+        });
         if (e) return e;
-        rn = h_norm_[0];
-        if (verbose > 1) printf("  refinement %d: |r|/target = %.3e\n", it, rn / target);
-        if (rn <= target || it >= maxit) break;
-        cudaMemsetAsync(e32_, 0, L.N * sizeof(float), s);
-        vcycle<float>(p, code, 0, e32_, r32_, false, s);
-        if (prof) prof->begin(PROF_RESID64, s);
-        { ++g_launches; k_add_corr<<<592, 256, 0, s>>>(phi, e32_, (long long)L.N); }
-        if (prof) prof->end(s);
+        e = (int)cudaStreamSynchronize(s);
+        if (e) return e;
         ++it;
+        rn = slots_max();
+        if (verbose > 1) printf("  refinement %d: |r|/target = %.3e\n", it, rn / target);
     }
     if (st) { st->cycles = it; st->resid = rn; }
     return rn <= target ? 0 : -3;

@@ -39,7 +39,7 @@ struct MGLevel {
 // class, on the launching stream, summed after the stream has synchronised.
 enum ProfCat {
     PROF_TDGL = 0, PROF_RHS_P, PROF_NEWTON, PROF_RHO, PROF_STEADY, PROF_SMOOTH_L0, PROF_RESTRICT_L0,
-    PROF_PROLONG_L0, PROF_MG_COARSE, PROF_RESID64, PROF_EFIELD, PROF_NCAT
+    PROF_PROLONG_L0, PROF_MG_COARSE, PROF_RESID64, PROF_EFIELD, PROF_MG_L1, PROF_MG_L2, PROF_COARSE_CTA, PROF_NCAT
 };
 
 struct Prof {
@@ -101,9 +101,10 @@ public:
                    cudaStream_t s, double* norm_out);
     size_t bytes() const { return bytes_; }
     const std::vector<MGLevel>& levels() const { return lev_; }
-    int nu1 = 2, nu2 = 2, nu_bottom = 40;
+    int nu1 = 2, nu2 = 1, nu_bottom = 40;
     Prof* prof = nullptr;
     int verbose = 0;
+    void set_graphs(bool on) { use_graphs_ = on; }
 
 private:
     std::vector<MGLevel> lev_;
@@ -118,6 +119,26 @@ private:
     double* cp0_64_ = nullptr;       // level-0 line scratch
     float* cp0_32_ = nullptr;
     size_t bytes_ = 0;
+    // one V-cycle (and its norm readback) captured as a CUDA graph, replayed
+    // per cycle; re-captured when a captured launch parameter changes
+    struct GraphCache {
+        cudaGraphExec_t exec = nullptr;
+        const void* x = nullptr;
+        const void* rhs = nullptr;
+        bool has_alpha = false;
+        double vlo = 0, vhi = 0;
+        int nu1 = 0, nu2 = 0;
+        long long launches = 0;
+    };
+    GraphCache g64_, g32_;
+    bool use_graphs_ = true;
+    template <typename F> int replay(GraphCache& g, const void* x, const void* rhs, const DevParams& p, cudaStream_t s, F&& enqueue);
+    int coarse_top64_ = -1, coarse_top32_ = -1;   // first level run by the one-CTA kernel
+    size_t coarse_smem64_ = 0, coarse_smem32_ = 0;
+    void plan_coarse(bool want64, bool want32);
+    double slots_max() const;
+    template <typename T> int coarse_top() const;
+    template <typename T> void launch_coarse(int top, cudaStream_t s);
     template <typename T> void vcycle(const DevParams& p, const uint8_t* code, int l, T* x0, const T* b0, bool inhom, cudaStream_t s);
     template <typename T> void smooth(const DevParams& p, const uint8_t* code, int l, T* x, const T* b, bool inhom, int sweeps, cudaStream_t s);
 };

@@ -142,7 +142,8 @@ int fx_set_stream(fx_ctx* ctx, void* cuda_stream);
  * Returns the number of classes (FX_KT_COUNT). */
 enum fx_kernel_class {
     FX_KT_TDGL = 0, FX_KT_RHS_P, FX_KT_NEWTON, FX_KT_RHO, FX_KT_STEADY, FX_KT_SMOOTH_L0,
-    FX_KT_RESTRICT_L0, FX_KT_PROLONG_L0, FX_KT_MG_COARSE, FX_KT_RESID64, FX_KT_EFIELD, FX_KT_COUNT
+    FX_KT_RESTRICT_L0, FX_KT_PROLONG_L0, FX_KT_MG_COARSE, FX_KT_RESID64, FX_KT_EFIELD, FX_KT_MG_L1,
+    FX_KT_MG_L2, FX_KT_COARSE_CTA, FX_KT_COUNT
 };
 int fx_get_kernel_times(fx_ctx* ctx, double* ms, long long* counts, int n);
 int fx_reset_kernel_times(fx_ctx* ctx);
