@@ -29,7 +29,7 @@ EXPORTS = ["fx_version", "fx_create", "fx_create_error", "fx_destroy", "fx_last_
            "fx_set_precision", "fx_get_field", "fx_set_field", "fx_compute_poisson_rhs", "fx_compute_rho",
            "fx_compute_phi_rho", "fx_compute_E", "fx_tdgl_euler", "fx_set_phi_bc", "fx_check_steady_state",
            "fx_step", "fx_run", "fx_write_plotfile", "fx_get_stats", "fx_mean_P", "fx_sync", "fx_set_stream",
-           "fx_get_kernel_times", "fx_reset_kernel_times"]
+           "fx_get_kernel_times", "fx_reset_kernel_times", "fx_mean_P_noalloc"]
 
 KERNEL_CLASSES = ["tdgl", "rhs_p", "newton", "rho", "steady", "smooth_l0", "restrict_l0", "prolong_l0",
                   "mg_coarse", "resid64", "efield", "mg_l1", "mg_l2", "coarse_cta"]
@@ -91,6 +91,7 @@ def lib():
         L.fx_get_stats.argtypes = [vp, C.POINTER(Stats)]
         L.fx_set_stream.argtypes = [vp, vp]
         L.fx_mean_P.argtypes = [vp, dp]
+        L.fx_mean_P_noalloc.argtypes = [vp, vp, vp, vp, C.c_size_t, vp, vp]
         L.fx_get_kernel_times.argtypes = [vp, dp, C.POINTER(C.c_longlong), C.c_int]
         L.fx_reset_kernel_times.argtypes = [vp]
         _lib = L

@@ -25,15 +25,20 @@
 #include "fx_params.h"
 #include "plotfile.h"
 
+namespace {
+thread_local std::string t_create_error;
+}
+
 namespace fx {
 std::atomic<long long> g_launches{0};
+// message of the last failed call that has no context (fx_create and the
+// context-free entry points)
+void set_free_error(const std::string& m) { t_create_error = m; }
 }
 
 using namespace fx;
 
 namespace {
-
-thread_local std::string t_create_error;
 
 // Silicon constants, Source/FerroX.cpp:534-554
 constexpr double kNc = 2.8e25, kNv = 1.83e25, kEg = 1.12, kChi = 4.05, kQ = 1.602e-19, kKb = 1.38e-23, kT = 300.0;

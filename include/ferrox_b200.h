@@ -78,6 +78,7 @@ const char* fx_version(void);
  * Device memory is allocated at the first call that needs the GPU.  On
  * failure *out is NULL and fx_create_error() holds the message. */
 int         fx_create(const char* inputs, int is_text, fx_ctx** out);
+/* message of the last failed fx_create (or fx_mean_P_noalloc) on this thread */
 const char* fx_create_error(void);
 void        fx_destroy(fx_ctx* ctx);
 const char* fx_last_error(const fx_ctx* ctx);
@@ -147,6 +148,22 @@ enum fx_kernel_class {
 };
 int fx_get_kernel_times(fx_ctx* ctx, double* ms, long long* counts, int n);
 int fx_reset_kernel_times(fx_ctx* ctx);
+
+/* No counterpart in the reference.  fx_mean_P without any device allocation,
+ * for callers that cannot call cudaMalloc where they need the number (memory
+ * owned by another allocator, or code that must not synchronise the device).
+ * Inputs are the caller's device arrays: Px and Py may be NULL, mask holds
+ * one byte per cell with 0 for ferroelectric cells; d_out receives <Px>, <Py>,
+ * <Pz> (3 doubles, device).  The work is enqueued on cuda_stream and the call
+ * returns without waiting.  Scratch is a static device array of about 32 KB
+ * that every GPU loading the library keeps until exit; n may be at most
+ * 16,777,216 cells (larger n returns FX_ERR_INVALID_ARGUMENT).  The first call
+ * on a device looks up that array's device address, so make the first call
+ * before any stream capture.  Calls that overlap on the GPU share the scratch
+ * and race: order them on one stream.  Errors are reported through the
+ * return code and fx_create_error(). */
+int fx_mean_P_noalloc(const double* d_Px, const double* d_Py, const double* d_Pz, const uint8_t* d_mask, size_t n,
+                      double* d_out, void* cuda_stream);
 
 #ifdef __cplusplus
 }
