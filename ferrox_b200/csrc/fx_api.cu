@@ -138,6 +138,7 @@ struct fx_ctx {
     int cur = 0;
     double *d_phi = nullptr, *d_phi_old = nullptr, *d_phi_prev = nullptr, *d_rho = nullptr, *d_e = nullptr, *d_h = nullptr;
     double *d_alpha = nullptr, *d_rhs = nullptr, *d_rhsP = nullptr, *d_dphi = nullptr, *d_E[3] = {nullptr, nullptr, nullptr};
+    double* d_f[3] = {nullptr, nullptr, nullptr};   // f^n of the Order-2 predictor
     float* d_alpha32 = nullptr;
     double* d_part = nullptr;
     unsigned int* d_counter = nullptr;
@@ -426,10 +427,9 @@ int read_out(fx_ctx* c, int n) {
     return FX_OK;
 }
 
-// the FE part of ComputePoissonRHS for the present P
-int compute_rhs_p(fx_ctx* c, bool norms) {
-    const double* P[3];
-    P_in(c, P);
+// the FE part of ComputePoissonRHS for P in buffer `buf`
+int compute_rhs_p(fx_ctx* c, bool norms, int buf) {
+    const double* P[3] = {c->scalarP ? nullptr : c->d_P[buf][0], c->scalarP ? nullptr : c->d_P[buf][1], c->d_P[buf][2]};
     if (norms) FX_CUDA(c, cudaMemsetAsync(c->d_out, 0, 2 * sizeof(double), c->s));
     ++g_launches;
     c->prof.begin(PROF_RHS_P, c->s);
@@ -458,14 +458,14 @@ int mg_solve(fx_ctx* c, const double* rhs, double nb, double nbp) {
     return FX_OK;
 }
 
-// ComputePhi_Rho, ElectrostaticSolver.cpp:678-747
-int compute_phi_rho(fx_ctx* c) {
+// ComputePhi_Rho, ElectrostaticSolver.cpp:678-747, for P in buffer `buf`
+int compute_phi_rho_P(fx_ctx* c, int buf) {
     int r = ensure_device(c);
     if (r) return r;
     c->E_valid = false;
     c->mg_last = 0;
     if (!c->contains_sc) {
-        r = compute_rhs_p(c, true);
+        r = compute_rhs_p(c, true, buf);
         if (r) return r;
         r = read_out(c, 2);
         if (r) return r;
@@ -479,7 +479,7 @@ int compute_phi_rho(fx_ctx* c) {
         c->phi_err_last = 0.0;
         return FX_OK;
     }
-    r = compute_rhs_p(c, false);
+    r = compute_rhs_p(c, false, buf);
     if (r) return r;
     const double tol = 1.e-5;
     double err = 1.0;
@@ -523,22 +523,48 @@ int compute_phi_rho(fx_ctx* c) {
     return FX_OK;
 }
 
+int compute_phi_rho(fx_ctx* c) { return compute_phi_rho_P(c, c->cur); }
+
+int compute_phi_rho_P(fx_ctx* c, int buf);
+
+// main.cpp:280-348: Order 1 is one fused Euler pass; Order 2 is a predictor
+// pass (f^n kept, P* into the other buffer), ComputePhi_Rho at P*, and a
+// corrector pass P^{n+1} = P^n + dt (0.5 f^n + 0.5 f*) written over P^n
 int tdgl_update(fx_ctx* c) {
     int r = ensure_device(c);
     if (r) return r;
-    if (c->par.TimeIntegratorOrder != 1)
-        return set_err(c, FX_ERR_UNSUPPORTED, "TimeIntegratorOrder = 2 is not implemented in this build");
     const double* Pin[3];
     P_in(c, Pin);
-    double* Pout[3] = {c->scalarP ? nullptr : c->d_P[1 - c->cur][0], c->scalarP ? nullptr : c->d_P[1 - c->cur][1],
-                       c->d_P[1 - c->cur][2]};
+    const int nb = 1 - c->cur;
+    double* Pout[3] = {c->scalarP ? nullptr : c->d_P[nb][0], c->scalarP ? nullptr : c->d_P[nb][1], c->d_P[nb][2]};
+    const int mixed = c->par.precision == 1;
+    if (c->par.TimeIntegratorOrder == 1) {
+        ++g_launches;
+        c->prof.begin(PROF_TDGL, c->s);
+        r = k_status(c, launch_tdgl(c->dp, mixed, 0, c->d_code, c->d_var, c->d_vt, Pin, Pout, c->d_phi, nullptr, nullptr, c->s));
+        c->prof.end(c->s);
+        if (r) return r;
+        c->cur = nb;
+        return FX_OK;
+    }
+    for (int d = 0; d < 3; ++d)
+        if (!c->d_f[d]) { r = dmalloc(c, &c->d_f[d], c->N); if (r) return r; }
+    double* fb[3] = {c->d_f[0], c->d_f[1], c->d_f[2]};
     ++g_launches;
     c->prof.begin(PROF_TDGL, c->s);
-    r = k_status(c, launch_tdgl(c->dp, c->par.precision == 1, c->d_code, c->d_var, c->d_vt, Pin, Pout, c->d_phi, c->s));
+    r = k_status(c, launch_tdgl(c->dp, mixed, 1, c->d_code, c->d_var, c->d_vt, Pin, Pout, c->d_phi, fb, nullptr, c->s));
     c->prof.end(c->s);
     if (r) return r;
-    c->cur = 1 - c->cur;
-    return FX_OK;
+    r = compute_phi_rho_P(c, nb);
+    if (r) return r;
+    const double* Ppre[3] = {Pout[0], Pout[1], Pout[2]};
+    double* Pnew[3] = {c->scalarP ? nullptr : c->d_P[c->cur][0], c->scalarP ? nullptr : c->d_P[c->cur][1], c->d_P[c->cur][2]};
+    const double* Pold[3] = {Pnew[0], Pnew[1], Pnew[2]};
+    ++g_launches;
+    c->prof.begin(PROF_TDGL, c->s);
+    r = k_status(c, launch_tdgl(c->dp, mixed, 2, c->d_code, c->d_var, c->d_vt, Ppre, Pnew, c->d_phi, fb, Pold, c->s));
+    c->prof.end(c->s);
+    return r;
 }
 
 int check_steady(fx_ctx* c, int step) {
@@ -780,7 +806,8 @@ void fx_destroy(fx_ctx* c) {
         for (int b = 0; b < 2; ++b)
             for (int d = 0; d < 3; ++d) cudaFree(c->d_P[b][d]);
         for (double* a : {c->d_phi, c->d_phi_old, c->d_phi_prev, c->d_rho, c->d_e, c->d_h, c->d_alpha, c->d_rhs,
-                          c->d_rhsP, c->d_dphi, c->d_E[0], c->d_E[1], c->d_E[2], c->d_part, c->d_out})
+                          c->d_rhsP, c->d_dphi, c->d_E[0], c->d_E[1], c->d_E[2], c->d_f[0], c->d_f[1], c->d_f[2],
+                          c->d_part, c->d_out})
             cudaFree(a);
         cudaFree(c->d_alpha32);
         cudaFree(c->d_counter);
@@ -1000,7 +1027,7 @@ int fx_compute_poisson_rhs(fx_ctx* c) {
     if (!c) return FX_ERR_INVALID_ARGUMENT;
     int r = ensure_device(c);
     if (r) return r;
-    r = compute_rhs_p(c, false);
+    r = compute_rhs_p(c, false, c->cur);
     if (r) return r;
     if (c->contains_sc) {
         // SC cells take rho (ElectrostaticSolver.cpp:65-67): the Newton kernel

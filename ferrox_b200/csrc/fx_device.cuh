@@ -73,6 +73,18 @@ struct PView {
     }
 };
 
+// unit impulse at cell (ci, cj, ck): evaluating a linear stencil on it gives
+// that row's coefficient of the impulse cell (used for transposed stencils)
+template <typename T>
+struct DeltaView {
+    int ci, cj, ck;
+    const DevParams* p;
+    __device__ __forceinline__ T operator()(int i, int j, int k) const {
+        if (k < 0 || k >= p->nz) return T(0);
+        return (wrap(i, p->nx) == ci && wrap(j, p->ny) == cj && k == ck) ? T(1) : T(0);
+    }
+};
+
 struct MView {
     const uint8_t* __restrict__ code;
     const DevParams* p;
@@ -80,8 +92,8 @@ struct MView {
 };
 
 // DPDx / DPDy / DPDz, DerivativeAlgorithm.H:45-252 (direction D)
-template <int D, typename T>
-__device__ __forceinline__ T dpd(const PView<T>& F, const MView& M, int i, int j, int k) {
+template <int D, typename T, typename FV>
+__device__ __forceinline__ T dpd(const FV& F, const MView& M, int i, int j, int k) {
     constexpr int ox = D == 0, oy = D == 1, oz = D == 2;
     const DevParams& p = *F.p;
     const T h = T(p.dx[D]);
@@ -110,8 +122,8 @@ __device__ __forceinline__ T dpd(const PView<T>& F, const MView& M, int i, int j
 }
 
 // DoubleDPDx / y / z, DerivativeAlgorithm.H:256-467 (direction D)
-template <int D, typename T>
-__device__ __forceinline__ T ddpd(const PView<T>& F, const MView& M, int i, int j, int k) {
+template <int D, typename T, typename FV>
+__device__ __forceinline__ T ddpd(const FV& F, const MView& M, int i, int j, int k) {
     constexpr int ox = D == 0, oy = D == 1, oz = D == 2;
     const DevParams& p = *F.p;
     const T h = T(p.dx[D]);
@@ -146,17 +158,17 @@ __device__ __forceinline__ T ddpd(const PView<T>& F, const MView& M, int i, int 
 }
 
 // DoubleDPDxDy / DxDz / DyDz, DerivativeAlgorithm.H:471-497
-template <typename T>
-__device__ __forceinline__ T dxdy(const PView<T>& F, const MView& M, int i, int j, int k) {
-    return (dpd<1>(F, M, i + 1, j, k) - dpd<1>(F, M, i - 1, j, k)) / T(2.) / T(F.p->dx[0]);
+template <typename T, typename FV>
+__device__ __forceinline__ T dxdy(const FV& F, const MView& M, int i, int j, int k) {
+    return (dpd<1, T>(F, M, i + 1, j, k) - dpd<1, T>(F, M, i - 1, j, k)) / T(2.) / T(F.p->dx[0]);
 }
-template <typename T>
-__device__ __forceinline__ T dxdz(const PView<T>& F, const MView& M, int i, int j, int k) {
-    return (dpd<2>(F, M, i + 1, j, k) - dpd<2>(F, M, i - 1, j, k)) / T(2.) / T(F.p->dx[0]);
+template <typename T, typename FV>
+__device__ __forceinline__ T dxdz(const FV& F, const MView& M, int i, int j, int k) {
+    return (dpd<2, T>(F, M, i + 1, j, k) - dpd<2, T>(F, M, i - 1, j, k)) / T(2.) / T(F.p->dx[0]);
 }
-template <typename T>
-__device__ __forceinline__ T dydz(const PView<T>& F, const MView& M, int i, int j, int k) {
-    return (dpd<2>(F, M, i, j + 1, k) - dpd<2>(F, M, i, j - 1, k)) / T(2.) / T(F.p->dx[1]);
+template <typename T, typename FV>
+__device__ __forceinline__ T dydz(const FV& F, const MView& M, int i, int j, int k) {
+    return (dpd<2, T>(F, M, i, j + 1, k) - dpd<2, T>(F, M, i, j - 1, k)) / T(2.) / T(F.p->dx[1]);
 }
 
 // phi with its z ghost values: after the MLMG solve the ghost holds the
@@ -179,20 +191,46 @@ __device__ __forceinline__ double phi_at(const double* __restrict__ phi, const D
 // grad phi as used by ComputeEfromPhi (ElectrostaticSolver.cpp:195-197):
 // central in x / y, DphiDz (DerivativeAlgorithm.H:8-22) in z with the
 // one-sided forms in the electrode-adjacent layers
+// phi accessor with the ghost values (see phi_at)
+struct PhiAt {
+    const double* __restrict__ phi;
+    const DevParams* p;
+    __device__ __forceinline__ double operator()(int i, int j, int k) const { return phi_at(phi, *p, i, j, k); }
+};
+
+// derivative of phi_at(i, j, k) with respect to phi at cell (ci, cj, ck):
+// the extrapolated ghost 2 V - phi_0 depends on the electrode-layer cell
+struct PhiDelta {
+    int ci, cj, ck;
+    const DevParams* p;
+    __device__ __forceinline__ double operator()(int i, int j, int k) const {
+        i = wrap(i, p->nx);
+        j = wrap(j, p->ny);
+        if (k < 0) return (p->ghost_mode == 0 && i == ci && j == cj && ck == 0) ? -1.0 : 0.0;
+        if (k >= p->nz) return (p->ghost_mode == 0 && i == ci && j == cj && ck == p->nz - 1) ? -1.0 : 0.0;
+        return (i == ci && j == cj && k == ck) ? 1.0 : 0.0;
+    }
+};
+
+template <typename T, typename A>
+__device__ __forceinline__ void grad_phi_acc(const A& f, const DevParams& p, int i, int j, int k, T& gx, T& gy, T& gz) {
+    // differences are taken in FP64 (phi is O(1 V) and its differences small)
+    gx = T((f(i + 1, j, k) - f(i - 1, j, k)) / (2. * p.dx[0]));
+    gy = T((f(i, j + 1, k) - f(i, j - 1, k)) / (2. * p.dx[1]));
+    const double dz = p.dx[2];
+    if (k == 0) {
+        gz = T((-4. * f(i, j, k - 1) + 3. * f(i, j, k) + f(i, j, k + 1)) / (3. * dz));
+    } else if (k == p.nz - 1) {
+        gz = T((4. * f(i, j, k + 1) - 3. * f(i, j, k) - f(i, j, k - 1)) / (3. * dz));
+    } else {
+        gz = T((f(i, j, k + 1) - f(i, j, k - 1)) / (2. * dz));
+    }
+}
+
 template <typename T>
 __device__ __forceinline__ void grad_phi(const double* __restrict__ phi, const DevParams& p, int i, int j, int k,
                                          T& gx, T& gy, T& gz) {
-    // differences are taken in FP64 (phi is O(1 V) and its differences small)
-    gx = T((phi_at(phi, p, i + 1, j, k) - phi_at(phi, p, i - 1, j, k)) / (2. * p.dx[0]));
-    gy = T((phi_at(phi, p, i, j + 1, k) - phi_at(phi, p, i, j - 1, k)) / (2. * p.dx[1]));
-    const double dz = p.dx[2];
-    if (k == 0) {
-        gz = T((-4. * phi_at(phi, p, i, j, k - 1) + 3. * phi_at(phi, p, i, j, k) + phi_at(phi, p, i, j, k + 1)) / (3. * dz));
-    } else if (k == p.nz - 1) {
-        gz = T((4. * phi_at(phi, p, i, j, k + 1) - 3. * phi_at(phi, p, i, j, k) - phi_at(phi, p, i, j, k - 1)) / (3. * dz));
-    } else {
-        gz = T((phi_at(phi, p, i, j, k + 1) - phi_at(phi, p, i, j, k - 1)) / (2. * dz));
-    }
+    grad_phi_acc<T>(PhiAt{phi, &p}, p, i, j, k, gx, gy, gz);
 }
 
 // ChargeDensity.cpp:4-11

@@ -84,16 +84,16 @@ __device__ __forceinline__ T landau(const DevParams& p, T alpha, T a, T b, T c) 
 template <typename T>
 struct Hess { T xx, yy, zz, xy, yz, xz; };
 
-template <typename T, bool ROT>
-__device__ __forceinline__ Hess<T> hess(const PView<T>& F, const MView& M, int i, int j, int k) {
+template <typename T, bool ROT, typename FV>
+__device__ __forceinline__ Hess<T> hess(const FV& F, const MView& M, int i, int j, int k) {
     Hess<T> h;
-    h.xx = ddpd<0>(F, M, i, j, k);
-    h.yy = ddpd<1>(F, M, i, j, k);
-    h.zz = ddpd<2>(F, M, i, j, k);
+    h.xx = ddpd<0, T>(F, M, i, j, k);
+    h.yy = ddpd<1, T>(F, M, i, j, k);
+    h.zz = ddpd<2, T>(F, M, i, j, k);
     if (ROT) {
-        h.xy = dxdy(F, M, i, j, k);
-        h.yz = dydz(F, M, i, j, k);
-        h.xz = dxdz(F, M, i, j, k);
+        h.xy = dxdy<T>(F, M, i, j, k);
+        h.yz = dydz<T>(F, M, i, j, k);
+        h.xz = dxdz<T>(F, M, i, j, k);
     } else {
         h.xy = h.yz = h.xz = T(0);
     }
@@ -113,13 +113,20 @@ __device__ __forceinline__ T rot_quad(const T* R, int a, const Hess<T>& H) {
 // FP64.  SCALAR: is_polarization_scalar == 1 with Px = Py = 0, so only Pz is
 // read and updated.  ROT: a rotation table is present (else R = identity,
 // whose zero entries contribute exact zeros in the reference's sums).
-template <typename T, bool SCALAR, bool ROT>
+//
+// MODE 0: forward Euler, P_out = P + dt f(P, phi)           (main.cpp:294-306)
+// MODE 1: predictor, f_buf = f(P, phi), P_out = P + dt f     (main.cpp:291-297)
+// MODE 2: corrector, f* = f(P, phi) with P the predictor state,
+//         P_out = P_old + dt (0.5 f_buf + 0.5 f*)             (main.cpp:323-340)
+// In MODE 2 P_out may alias P_old (each cell reads its own P_old first).
+template <typename T, bool SCALAR, bool ROT, int MODE>
 __global__ void __launch_bounds__(256) k_tdgl(DevParams p, const uint8_t* __restrict__ code,
                                               const uint8_t* __restrict__ var, const Variant* __restrict__ vt,
                                               const double* __restrict__ Pp, const double* __restrict__ Pq,
                                               const double* __restrict__ Pr, const double* __restrict__ phi,
-                                              double* __restrict__ Pp_out, double* __restrict__ Pq_out,
-                                              double* __restrict__ Pr_out) {
+                                              double* Pp_out, double* Pq_out, double* Pr_out,
+                                              double* fbp, double* fbq, double* fbr,
+                                              const double* Pp_old, const double* Pq_old, const double* Pr_old) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int k = blockIdx.z;
@@ -132,6 +139,15 @@ __global__ void __launch_bounds__(256) k_tdgl(DevParams p, const uint8_t* __rest
     // Gamma = 0 outside FE (Initialization.cpp:113, :125) and the t-phase
     // zeroing (TotalEnergyDensity.cpp:123-127) leave P unchanged there
     if ((m & 3) != 0 || (m & 4) != 0) {
+        if (MODE == 2) {
+            Pr_out[c] = Pr_old[c];
+            if (!SCALAR) { Pp_out[c] = Pp_old[c]; Pq_out[c] = Pq_old[c]; }
+            return;
+        }
+        if (MODE == 1) {
+            fbr[c] = 0.0;
+            if (!SCALAR) { fbp[c] = 0.0; fbq[c] = 0.0; }
+        }
         Pr_out[c] = pr0;
         if (!SCALAR) { Pp_out[c] = pp0; Pq_out[c] = pq0; }
         return;
@@ -166,7 +182,7 @@ __global__ void __launch_bounds__(256) k_tdgl(DevParams p, const uint8_t* __rest
         }
         if (!SCALAR) {
             PView<T> Fp{Pp, &p}, Fq{Pq, &p};
-            g = g - (g44 + g44p + g12) * dydz(Fq, M, i, j, k) - (g44 + g44p + g12) * dxdz(Fp, M, i, j, k);
+            g = g - (g44 + g44p + g12) * dydz<T>(Fq, M, i, j, k) - (g44 + g44p + g12) * dxdz<T>(Fp, M, i, j, k);
         }
         fr += T(-1.0) * Gam * g;
     }
@@ -174,7 +190,9 @@ __global__ void __launch_bounds__(256) k_tdgl(DevParams p, const uint8_t* __rest
         const T Er = -(R[6] * gx + R[7] * gy + R[8] * gz);
         fr += T(-1.0) * Gam * (-Er);
     }
-    Pr_out[c] = 1.0 * pr0 + p.dt * (double)fr;
+    if (MODE == 0) Pr_out[c] = 1.0 * pr0 + p.dt * (double)fr;
+    if (MODE == 1) { fbr[c] = (double)fr; Pr_out[c] = 1.0 * pr0 + p.dt * (double)fr; }
+    if (MODE == 2) Pr_out[c] = 1.0 * Pr_old[c] + p.dt * (0.5 * fbr[c] + 0.5 * (double)fr);
 
     if (!SCALAR) {
         PView<T> Fp{Pp, &p}, Fq{Pq, &p};
@@ -184,12 +202,12 @@ __global__ void __launch_bounds__(256) k_tdgl(DevParams p, const uint8_t* __rest
             fq += T(-1.0) * Gam * landau<T>(p, alpha, pq, pp, r);
         }
         if (p.incl_G) {
-            T gp = -g11 * ddpd<0>(Fp, M, i, j, k) - (g44 + g44p) * ddpd<1>(Fp, M, i, j, k) -
-                   (g44 + g44p) * ddpd<2>(Fp, M, i, j, k) - (g12 + g44 - g44p) * dxdy(Fq, M, i, j, k) -
-                   (g12 + g44 - g44p) * dxdz(Fr, M, i, j, k);
-            T gq = -g11 * ddpd<1>(Fq, M, i, j, k) - (g44 - g44p) * ddpd<0>(Fq, M, i, j, k) -
-                   (g44 - g44p) * ddpd<2>(Fq, M, i, j, k) - (g12 + g44 + g44p) * dxdy(Fp, M, i, j, k) -
-                   (g12 + g44 - g44p) * dydz(Fr, M, i, j, k);
+            T gp = -g11 * ddpd<0, T>(Fp, M, i, j, k) - (g44 + g44p) * ddpd<1, T>(Fp, M, i, j, k) -
+                   (g44 + g44p) * ddpd<2, T>(Fp, M, i, j, k) - (g12 + g44 - g44p) * dxdy<T>(Fq, M, i, j, k) -
+                   (g12 + g44 - g44p) * dxdz<T>(Fr, M, i, j, k);
+            T gq = -g11 * ddpd<1, T>(Fq, M, i, j, k) - (g44 - g44p) * ddpd<0, T>(Fq, M, i, j, k) -
+                   (g44 - g44p) * ddpd<2, T>(Fq, M, i, j, k) - (g12 + g44 + g44p) * dxdy<T>(Fp, M, i, j, k) -
+                   (g12 + g44 - g44p) * dydz<T>(Fr, M, i, j, k);
             fp += T(-1.0) * Gam * gp;
             fq += T(-1.0) * Gam * gq;
         }
@@ -200,8 +218,20 @@ __global__ void __launch_bounds__(256) k_tdgl(DevParams p, const uint8_t* __rest
             fq += T(-1.0) * Gam * (-Eq);
         }
         if (p.scalar) { fp = T(0); fq = T(0); }
-        Pp_out[c] = 1.0 * pp0 + p.dt * (double)fp;
-        Pq_out[c] = 1.0 * pq0 + p.dt * (double)fq;
+        if (MODE == 0) {
+            Pp_out[c] = 1.0 * pp0 + p.dt * (double)fp;
+            Pq_out[c] = 1.0 * pq0 + p.dt * (double)fq;
+        }
+        if (MODE == 1) {
+            fbp[c] = (double)fp; fbq[c] = (double)fq;
+            Pp_out[c] = 1.0 * pp0 + p.dt * (double)fp;
+            Pq_out[c] = 1.0 * pq0 + p.dt * (double)fq;
+        }
+        if (MODE == 2) {
+            const double op = Pp_old[c], oq = Pq_old[c];
+            Pp_out[c] = 1.0 * op + p.dt * (0.5 * fbp[c] + 0.5 * (double)fp);
+            Pq_out[c] = 1.0 * oq + p.dt * (0.5 * fbq[c] + 0.5 * (double)fq);
+        }
     }
 }
 
@@ -231,13 +261,13 @@ __global__ void __launch_bounds__(256) k_rhs_p(DevParams p, const uint8_t* __res
             }
             MView M{code, &p};
             PView<double> Fr{Pr, &p};
-            const double r3 = R[6] * dpd<0>(Fr, M, i, j, k) + R[7] * dpd<1>(Fr, M, i, j, k) + R[8] * dpd<2>(Fr, M, i, j, k);
+            const double r3 = R[6] * dpd<0, double>(Fr, M, i, j, k) + R[7] * dpd<1, double>(Fr, M, i, j, k) + R[8] * dpd<2, double>(Fr, M, i, j, k);
             if (SCALAR) {
                 v = -r3;
             } else {
                 PView<double> Fp{Pp, &p}, Fq{Pq, &p};
-                const double r1 = R[0] * dpd<0>(Fp, M, i, j, k) + R[1] * dpd<1>(Fp, M, i, j, k) + R[2] * dpd<2>(Fp, M, i, j, k);
-                const double r2 = R[3] * dpd<0>(Fq, M, i, j, k) + R[4] * dpd<1>(Fq, M, i, j, k) + R[5] * dpd<2>(Fq, M, i, j, k);
+                const double r1 = R[0] * dpd<0, double>(Fp, M, i, j, k) + R[1] * dpd<1, double>(Fp, M, i, j, k) + R[2] * dpd<2, double>(Fp, M, i, j, k);
+                const double r2 = R[3] * dpd<0, double>(Fq, M, i, j, k) + R[4] * dpd<1, double>(Fq, M, i, j, k) + R[5] * dpd<2, double>(Fq, M, i, j, k);
                 v = -(r1) - (r2) - (r3);
             }
         }
@@ -454,19 +484,24 @@ dim3 cell_grid(const DevParams& p) { return dim3((p.nx + 31) / 32, (p.ny + 7) / 
 }  // namespace
 
 // ------------------------------------------------------------ launchers --
-int launch_tdgl(const DevParams& p, int mixed, const uint8_t* code, const uint8_t* var, const Variant* vt,
-                const double* const Pin[3], double* const Pout[3], const double* phi, cudaStream_t s) {
+int launch_tdgl(const DevParams& p, int mixed, int mode, const uint8_t* code, const uint8_t* var, const Variant* vt,
+                const double* const Pin[3], double* const Pout[3], const double* phi, double* const fbuf[3],
+                const double* const Pold[3], cudaStream_t s) {
     const dim3 g = cell_grid(p), b(32, 8);
     const bool scal = p.scalar && Pin[0] == nullptr;
     const bool rot = var != nullptr;
-#define FX_TDGL(T, S, R) k_tdgl<T, S, R><<<g, b, 0, s>>>(p, code, var, vt, Pin[0], Pin[1], Pin[2], phi, Pout[0], Pout[1], Pout[2])
+    double* fb[3] = {fbuf ? fbuf[0] : nullptr, fbuf ? fbuf[1] : nullptr, fbuf ? fbuf[2] : nullptr};
+    const double* po[3] = {Pold ? Pold[0] : nullptr, Pold ? Pold[1] : nullptr, Pold ? Pold[2] : nullptr};
+#define FX_TDGL(T, S, R, M) k_tdgl<T, S, R, M><<<g, b, 0, s>>>(p, code, var, vt, Pin[0], Pin[1], Pin[2], phi, Pout[0], Pout[1], Pout[2], fb[0], fb[1], fb[2], po[0], po[1], po[2])
+#define FX_TDGL_M(T, S, R) do { if (mode == 0) FX_TDGL(T, S, R, 0); else if (mode == 1) FX_TDGL(T, S, R, 1); else FX_TDGL(T, S, R, 2); } while (0)
     if (!mixed) {
-        if (scal) { if (rot) FX_TDGL(double, true, true); else FX_TDGL(double, true, false); }
-        else { if (rot) FX_TDGL(double, false, true); else FX_TDGL(double, false, false); }
+        if (scal) { if (rot) FX_TDGL_M(double, true, true); else FX_TDGL_M(double, true, false); }
+        else { if (rot) FX_TDGL_M(double, false, true); else FX_TDGL_M(double, false, false); }
     } else {
-        if (scal) { if (rot) FX_TDGL(float, true, true); else FX_TDGL(float, true, false); }
-        else { if (rot) FX_TDGL(float, false, true); else FX_TDGL(float, false, false); }
+        if (scal) { if (rot) FX_TDGL_M(float, true, true); else FX_TDGL_M(float, true, false); }
+        else { if (rot) FX_TDGL_M(float, false, true); else FX_TDGL_M(float, false, false); }
     }
+#undef FX_TDGL_M
 #undef FX_TDGL
     return (int)cudaGetLastError();
 }

@@ -8,9 +8,11 @@
 
 namespace fx {
 
-// Pin/Pout: {Px, Py, Pz}; Px = Py = nullptr selects the scalar-P kernel
-int launch_tdgl(const DevParams& p, int mixed, const uint8_t* code, const uint8_t* var, const Variant* vt,
-                const double* const Pin[3], double* const Pout[3], const double* phi, cudaStream_t s);
+// Pin/Pout: {Px, Py, Pz}; Px = Py = nullptr selects the scalar-P kernel.
+// mode 0: Euler; 1: predictor (writes fbuf); 2: corrector (reads fbuf, Pold)
+int launch_tdgl(const DevParams& p, int mixed, int mode, const uint8_t* code, const uint8_t* var, const Variant* vt,
+                const double* const Pin[3], double* const Pout[3], const double* phi, double* const fbuf[3],
+                const double* const Pold[3], cudaStream_t s);
 int launch_rhs_p(const DevParams& p, const uint8_t* code, const uint8_t* var, const Variant* vt,
                  const double* const P[3], double* rhs, double* norms, cudaStream_t s);
 int launch_newton(const DevParams& p, const uint8_t* code, const double* phi, const double* rho,

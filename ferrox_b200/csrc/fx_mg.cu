@@ -35,20 +35,20 @@ struct Op {
 // the diagonal and the electrode contribution to the right-hand side
 template <typename T, bool FINE>
 __device__ __forceinline__ void coeffs(const Op<T>& o, int i, int j, int k, size_t c, int im, int ip, int jm, int jp,
-                                       T& cw, T& ce, T& cs, T& cn, T& cb, T& ct, T& diag, T& bcv) {
+                                       T& cw, T& ce, T& cs, T& cn, T& cb, T& ct, T& diag, T& bcv, const T* eps) {
     T extra = T(0);
     bcv = T(0);
     if (FINE) {
         const uint8_t* cd = o.code + o.nxy;   // skip the k = -1 ghost layer
         const size_t row = c - i;
-        const T ec = o.eps[__ldg(cd + c) & 7];
-        cw = T(0.5) * (ec + o.eps[__ldg(cd + row + im) & 7]) * o.ih2x;
-        ce = T(0.5) * (o.eps[__ldg(cd + row + ip) & 7] + ec) * o.ih2x;
-        cs = T(0.5) * (ec + o.eps[__ldg(cd + c + (size_t)(jm - j) * o.nx) & 7]) * o.ih2y;
-        cn = T(0.5) * (o.eps[__ldg(cd + c + (size_t)(jp - j) * o.nx) & 7] + ec) * o.ih2y;
-        if (k > 0) cb = T(0.5) * (ec + o.eps[__ldg(cd + c - o.nxy) & 7]) * o.ih2z;
+        const T ec = eps[__ldg(cd + c) & 7];
+        cw = T(0.5) * (ec + eps[__ldg(cd + row + im) & 7]) * o.ih2x;
+        ce = T(0.5) * (eps[__ldg(cd + row + ip) & 7] + ec) * o.ih2x;
+        cs = T(0.5) * (ec + eps[__ldg(cd + c + (size_t)(jm - j) * o.nx) & 7]) * o.ih2y;
+        cn = T(0.5) * (eps[__ldg(cd + c + (size_t)(jp - j) * o.nx) & 7] + ec) * o.ih2y;
+        if (k > 0) cb = T(0.5) * (ec + eps[__ldg(cd + c - o.nxy) & 7]) * o.ih2z;
         else { cb = T(0); extra += T(2) * ec * o.ih2z; bcv += T(2) * ec * o.ih2z * o.vlo; }
-        if (k < o.nz - 1) ct = T(0.5) * (o.eps[__ldg(cd + c + o.nxy) & 7] + ec) * o.ih2z;
+        if (k < o.nz - 1) ct = T(0.5) * (eps[__ldg(cd + c + o.nxy) & 7] + ec) * o.ih2z;
         else { ct = T(0); extra += T(2) * ec * o.ih2z; bcv += T(2) * ec * o.ih2z * o.vhi; }
     } else {
         const size_t row = c - i;
@@ -100,6 +100,13 @@ __device__ double block_max_all(double v) {
 // red-black point Gauss-Seidel half sweep: color = parity of i + j + k
 template <typename T, bool FINE>
 __global__ void __launch_bounds__(256) k_rbgs(Op<T> o, T* __restrict__ x, const T* __restrict__ b, int color) {
+    __shared__ T seps[8];
+    if (FINE) {
+        if (threadIdx.x == 0 && threadIdx.y == 0)
+#pragma unroll
+            for (int q = 0; q < 8; ++q) seps[q] = o.eps[q];
+        __syncthreads();
+    }
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int k = blockIdx.z;
     const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((j + k + color) & 1);
@@ -109,7 +116,7 @@ __global__ void __launch_bounds__(256) k_rbgs(Op<T> o, T* __restrict__ x, const 
     nbr(i, o.nx, im, ip);
     nbr(j, o.ny, jm, jp);
     T cw, ce, cs, cn, cb, ct, diag, bcv;
-    coeffs<T, FINE>(o, i, j, k, c, im, ip, jm, jp, cw, ce, cs, cn, cb, ct, diag, bcv);
+    coeffs<T, FINE>(o, i, j, k, c, im, ip, jm, jp, cw, ce, cs, cn, cb, ct, diag, bcv, seps);
     const size_t row = c - i;
     T s = b[c] + bcv + cw * x[row + im] + ce * x[row + ip] + cs * x[c + (size_t)(jm - j) * o.nx] +
           cn * x[c + (size_t)(jp - j) * o.nx];
@@ -124,6 +131,13 @@ __global__ void __launch_bounds__(256) k_rbgs(Op<T> o, T* __restrict__ x, const 
 template <typename T, bool FINE>
 __global__ void __launch_bounds__(128) k_line(Op<T> o, T* __restrict__ x, const T* __restrict__ b, T* __restrict__ q,
                                               int color) {
+    __shared__ T seps[8];
+    if (FINE) {
+        if (threadIdx.x == 0 && threadIdx.y == 0)
+#pragma unroll
+            for (int q = 0; q < 8; ++q) seps[q] = o.eps[q];
+        __syncthreads();
+    }
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((j + color) & 1);
     if (j >= o.ny || i >= o.nx) return;
@@ -134,7 +148,7 @@ __global__ void __launch_bounds__(128) k_line(Op<T> o, T* __restrict__ x, const 
     size_t c = (size_t)i + (size_t)o.nx * (size_t)j;
     for (int k = 0; k < o.nz; ++k, c += o.nxy) {
         T cw, ce, cs, cn, cb, ct, diag, bcv;
-        coeffs<T, FINE>(o, i, j, k, c, im, ip, jm, jp, cw, ce, cs, cn, cb, ct, diag, bcv);
+        coeffs<T, FINE>(o, i, j, k, c, im, ip, jm, jp, cw, ce, cs, cn, cb, ct, diag, bcv, seps);
         const size_t row = c - i;
         const T r = b[c] + bcv + cw * x[row + im] + ce * x[row + ip] + cs * x[c + (size_t)(jm - j) * o.nx] +
                     cn * x[c + (size_t)(jp - j) * o.nx];
@@ -156,27 +170,38 @@ __global__ void __launch_bounds__(128) k_line(Op<T> o, T* __restrict__ x, const 
 }
 
 // residual b - A x at the children of each coarse cell, averaged into the
-// coarse right-hand side; optionally the |r|_inf of the level
-template <typename T, bool FINE>
+// coarse right-hand side; optionally the |r|_inf of the level.  RX, RY, RZ
+// are the coarsening ratios (1 or 2).
+template <typename T, bool FINE, int RX, int RY, int RZ>
 __global__ void __launch_bounds__(256) k_resid_restrict(Op<T> o, const T* __restrict__ x, const T* __restrict__ b,
-                                                        T* __restrict__ bc, int ncx, int ncy, int ncz, int rx, int ry,
-                                                        int rz, double* __restrict__ norm) {
+                                                        T* __restrict__ bc, int ncx, int ncy, int ncz,
+                                                        double* __restrict__ norm) {
     const int I = blockIdx.x * blockDim.x + threadIdx.x;
     const int J = blockIdx.y * blockDim.y + threadIdx.y;
     const int K = blockIdx.z;
+    __shared__ T seps[8];
+    if (FINE) {
+        if (threadIdx.x == 0 && threadIdx.y == 0)
+#pragma unroll
+            for (int q = 0; q < 8; ++q) seps[q] = o.eps[q];
+        __syncthreads();
+    }
     double mx = 0.0;
     if (I < ncx && J < ncy) {
         T s = T(0);
-        for (int dk = 0; dk < rz; ++dk)
-            for (int dj = 0; dj < ry; ++dj)
-                for (int di = 0; di < rx; ++di) {
-                    const int i = rx * I + di, j = ry * J + dj, k = rz * K + dk;
+#pragma unroll
+        for (int dk = 0; dk < RZ; ++dk)
+#pragma unroll
+            for (int dj = 0; dj < RY; ++dj)
+#pragma unroll
+                for (int di = 0; di < RX; ++di) {
+                    const int i = RX * I + di, j = RY * J + dj, k = RZ * K + dk;
                     const size_t c = (size_t)i + (size_t)o.nx * ((size_t)j + (size_t)o.ny * k);
                     int im, ip, jm, jp;
                     nbr(i, o.nx, im, ip);
                     nbr(j, o.ny, jm, jp);
                     T cw, ce, cs, cn, cb, ct, diag, bcv;
-                    coeffs<T, FINE>(o, i, j, k, c, im, ip, jm, jp, cw, ce, cs, cn, cb, ct, diag, bcv);
+                    coeffs<T, FINE>(o, i, j, k, c, im, ip, jm, jp, cw, ce, cs, cn, cb, ct, diag, bcv, seps);
                     const size_t row = c - i;
                     T off = cw * x[row + im] + ce * x[row + ip] + cs * x[c + (size_t)(jm - j) * o.nx] +
                             cn * x[c + (size_t)(jp - j) * o.nx];
@@ -186,7 +211,7 @@ __global__ void __launch_bounds__(256) k_resid_restrict(Op<T> o, const T* __rest
                     s += r;
                     mx = fmax(mx, fabs((double)r));
                 }
-        bc[(size_t)I + (size_t)ncx * ((size_t)J + (size_t)ncy * K)] = s / T(rx * ry * rz);
+        bc[(size_t)I + (size_t)ncx * ((size_t)J + (size_t)ncy * K)] = s / T(RX * RY * RZ);
     }
     if (norm) {
         const double m = block_max_all(mx);
@@ -199,6 +224,11 @@ __global__ void __launch_bounds__(256) k_resid_restrict(Op<T> o, const T* __rest
 // copy for the mixed-precision correction solve
 __global__ void __launch_bounds__(256) k_resid64(Op<double> o, const double* __restrict__ x, const double* __restrict__ b,
                                                  float* __restrict__ r32, double* __restrict__ norm) {
+    __shared__ double seps[8];
+    if (threadIdx.x == 0 && threadIdx.y == 0)
+#pragma unroll
+        for (int q = 0; q < 8; ++q) seps[q] = o.eps[q];
+    __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int k = blockIdx.z;
@@ -209,7 +239,7 @@ __global__ void __launch_bounds__(256) k_resid64(Op<double> o, const double* __r
         nbr(i, o.nx, im, ip);
         nbr(j, o.ny, jm, jp);
         double cw, ce, cs, cn, cb, ct, diag, bcv;
-        coeffs<double, true>(o, i, j, k, c, im, ip, jm, jp, cw, ce, cs, cn, cb, ct, diag, bcv);
+        coeffs<double, true>(o, i, j, k, c, im, ip, jm, jp, cw, ce, cs, cn, cb, ct, diag, bcv, seps);
         const size_t row = c - i;
         double off = cw * x[row + im] + ce * x[row + ip] + cs * x[c + (size_t)(jm - j) * o.nx] +
                      cn * x[c + (size_t)(jp - j) * o.nx];
@@ -225,33 +255,58 @@ __global__ void __launch_bounds__(256) k_resid64(Op<double> o, const double* __r
 
 // prolongation in the coarsened directions with the per-cell resistor-chain
 // weights (near parent, far neighbour), added to x; beyond an electrode the
-// far neighbour is the homogeneous Dirichlet value 0
-template <typename T>
+// far neighbour is the homogeneous Dirichlet value 0.  RX, RY, RZ are the
+// coarsening ratios (1 or 2), fixed at compile time.
+template <typename T, int RX, int RY, int RZ>
 __global__ void __launch_bounds__(256) k_prolong(T* __restrict__ xf, const T* __restrict__ xc, const float* __restrict__ wx,
                                                  const float* __restrict__ wy, const float* __restrict__ wz, int nx, int ny,
-                                                 int nz, int ncx, int ncy, int ncz, int rx, int ry, int rz) {
+                                                 int nz, int ncx, int ncy, int ncz) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int k = blockIdx.z;
     if (i >= nx || j >= ny) return;
-    const size_t fc = (size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * k);
-    int I[2], J[2], K[2];
-    T wi[2], wj[2], wk[2];
-    int ni = 1, nj = 1, nk = 1;
-    I[0] = i / rx; wi[0] = T(1);
-    if (rx == 2) { ni = 2; wi[1] = T(__ldg(wx + fc)); wi[0] = T(1) - wi[1]; I[1] = (i & 1) ? I[0] + 1 : I[0] - 1; I[1] = (I[1] + ncx) % ncx; }
-    J[0] = j / ry; wj[0] = T(1);
-    if (ry == 2) { nj = 2; wj[1] = T(__ldg(wy + fc)); wj[0] = T(1) - wj[1]; J[1] = (j & 1) ? J[0] + 1 : J[0] - 1; J[1] = (J[1] + ncy) % ncy; }
-    K[0] = k / rz; wk[0] = T(1);
-    if (rz == 2) {
-        nk = 2; wk[1] = T(__ldg(wz + fc)); wk[0] = T(1) - wk[1]; K[1] = (k & 1) ? K[0] + 1 : K[0] - 1;
-        if (K[1] < 0 || K[1] >= ncz) { K[1] = K[0]; wk[1] = T(0); }
+    const int fc = i + nx * (j + ny * k);
+    const int I0 = RX == 2 ? (i >> 1) : i, J0 = RY == 2 ? (j >> 1) : j, K0 = RZ == 2 ? (k >> 1) : k;
+    int I1 = I0, J1 = J0, K1 = K0;
+    T wxf = T(0), wyf = T(0), wzf = T(0);
+    if (RX == 2) { wxf = T(__ldg(wx + fc)); I1 = (i & 1) ? (I0 + 1 == ncx ? 0 : I0 + 1) : (I0 == 0 ? ncx - 1 : I0 - 1); }
+    if (RY == 2) { wyf = T(__ldg(wy + fc)); J1 = (j & 1) ? (J0 + 1 == ncy ? 0 : J0 + 1) : (J0 == 0 ? ncy - 1 : J0 - 1); }
+    bool zin = true;
+    if (RZ == 2) {
+        wzf = T(__ldg(wz + fc));
+        K1 = (k & 1) ? K0 + 1 : K0 - 1;
+        zin = K1 >= 0 && K1 < ncz;
+        if (!zin) K1 = K0;
     }
-    T s = T(0);
-    for (int a = 0; a < nk; ++a)
-        for (int bb = 0; bb < nj; ++bb)
-            for (int d = 0; d < ni; ++d)
-                s += wk[a] * wj[bb] * wi[d] * xc[(size_t)I[d] + (size_t)ncx * ((size_t)J[bb] + (size_t)ncy * K[a])];
+    const int ncxy = ncx * ncy;
+    auto X = [&](int I, int J, int K) { return xc[I + ncx * J + ncxy * K]; };
+    T s;
+    if (RX == 2 && RY == 2 && RZ == 2) {
+        const T wxn = T(1) - wxf, wyn = T(1) - wyf, wzn = T(1) - wzf, wzf2 = zin ? wzf : T(0);
+        s = wzn * (wyn * (wxn * X(I0, J0, K0) + wxf * X(I1, J0, K0)) + wyf * (wxn * X(I0, J1, K0) + wxf * X(I1, J1, K0))) +
+            wzf2 * (wyn * (wxn * X(I0, J0, K1) + wxf * X(I1, J0, K1)) + wyf * (wxn * X(I0, J1, K1) + wxf * X(I1, J1, K1)));
+    } else if (RX == 2 && RY == 2) {
+        const T wxn = T(1) - wxf, wyn = T(1) - wyf;
+        s = wyn * (wxn * X(I0, J0, K0) + wxf * X(I1, J0, K0)) + wyf * (wxn * X(I0, J1, K0) + wxf * X(I1, J1, K0));
+    } else if (RZ == 2 && RX == 1 && RY == 1) {
+        s = (T(1) - wzf) * X(I0, J0, K0) + (zin ? wzf * X(I0, J0, K1) : T(0));
+    } else {
+        // remaining ratio patterns (single x or y direction, x-z, y-z)
+        T acc = T(0);
+        for (int a = 0; a < (RZ == 2 ? 2 : 1); ++a) {
+            const T wk = RZ == 2 ? (a ? (zin ? wzf : T(0)) : T(1) - wzf) : T(1);
+            const int K = a ? K1 : K0;
+            for (int b = 0; b < (RY == 2 ? 2 : 1); ++b) {
+                const T wj = RY == 2 ? (b ? wyf : T(1) - wyf) : T(1);
+                const int J = b ? J1 : J0;
+                for (int d = 0; d < (RX == 2 ? 2 : 1); ++d) {
+                    const T wi = RX == 2 ? (d ? wxf : T(1) - wxf) : T(1);
+                    acc += wk * wj * wi * X(d ? I1 : I0, J, K);
+                }
+            }
+        }
+        s = acc;
+    }
     xf[fc] += s;
 }
 
@@ -952,14 +1007,46 @@ void Multigrid::vcycle(const DevParams& p, const uint8_t* code, int l, T* x, con
     dim3 b2(32, 8), g2((C.n[0] + 31) / 32, (C.n[1] + 7) / 8, C.n[2]);
     double* norm = (l == 0) ? d_norm_ : nullptr;
     if (prof) prof->begin(l == 0 ? PROF_RESTRICT_L0 : l == 1 ? PROF_MG_L1 : l == 2 ? PROF_MG_L2 : PROF_MG_COARSE, s);
-    if (l == 0) { ++g_launches; k_resid_restrict<T, true><<<g2, b2, 0, s>>>(o, x, b, lb<T>(C), C.n[0], C.n[1], C.n[2], C.cr[0], C.cr[1], C.cr[2], norm); }
-    else { ++g_launches; k_resid_restrict<T, false><<<g2, b2, 0, s>>>(o, x, b, lb<T>(C), C.n[0], C.n[1], C.n[2], C.cr[0], C.cr[1], C.cr[2], norm); }
+    ++g_launches;
+    {
+        const int key = (C.cr[0] == 2) * 4 + (C.cr[1] == 2) * 2 + (C.cr[2] == 2);
+        T* bc = lb<T>(C);
+#define FX_RR(F, RX, RY, RZ) k_resid_restrict<T, F, RX, RY, RZ><<<g2, b2, 0, s>>>(o, x, b, bc, C.n[0], C.n[1], C.n[2], norm)
+#define FX_RR_ALL(F)                                  \
+        switch (key) {                                \
+        case 1: FX_RR(F, 1, 1, 2); break;             \
+        case 2: FX_RR(F, 1, 2, 1); break;             \
+        case 3: FX_RR(F, 1, 2, 2); break;             \
+        case 4: FX_RR(F, 2, 1, 1); break;             \
+        case 5: FX_RR(F, 2, 1, 2); break;             \
+        case 6: FX_RR(F, 2, 2, 1); break;             \
+        default: FX_RR(F, 2, 2, 2); break;            \
+        }
+        if (l == 0) { FX_RR_ALL(true) } else { FX_RR_ALL(false) }
+#undef FX_RR_ALL
+#undef FX_RR
+    }
     if (prof) prof->end(s);
     cudaMemsetAsync(lx<T>(C), 0, C.N * sizeof(T), s);
     vcycle<T>(p, code, l + 1, lx<T>(C), lb<T>(C), false, s);
     dim3 g3((L.n[0] + 31) / 32, (L.n[1] + 7) / 8, L.n[2]);
     if (prof) prof->begin(l == 0 ? PROF_PROLONG_L0 : l == 1 ? PROF_MG_L1 : l == 2 ? PROF_MG_L2 : PROF_MG_COARSE, s);
-    { ++g_launches; k_prolong<T><<<g3, b2, 0, s>>>(x, lx<T>(C), C.wf[0], C.wf[1], C.wf[2], L.n[0], L.n[1], L.n[2], C.n[0], C.n[1], C.n[2], C.cr[0], C.cr[1], C.cr[2]); }
+    ++g_launches;
+    {
+        const int key = (C.cr[0] == 2) * 4 + (C.cr[1] == 2) * 2 + (C.cr[2] == 2);
+        T* xc = lx<T>(C);
+#define FX_PR(RX, RY, RZ) k_prolong<T, RX, RY, RZ><<<g3, b2, 0, s>>>(x, xc, C.wf[0], C.wf[1], C.wf[2], L.n[0], L.n[1], L.n[2], C.n[0], C.n[1], C.n[2])
+        switch (key) {
+        case 1: FX_PR(1, 1, 2); break;
+        case 2: FX_PR(1, 2, 1); break;
+        case 3: FX_PR(1, 2, 2); break;
+        case 4: FX_PR(2, 1, 1); break;
+        case 5: FX_PR(2, 1, 2); break;
+        case 6: FX_PR(2, 2, 1); break;
+        default: FX_PR(2, 2, 2); break;
+        }
+#undef FX_PR
+    }
     if (prof) prof->end(s);
     smooth<T>(p, code, l, x, b, inhom, nu2, s);
 }

@@ -186,6 +186,19 @@ def test_coupled_steps_polycrystal():
         assert relerr(f.field(name), o.field(name)) < 1e-10, name
 
 
+@pytest.mark.parametrize("sc", [False, True])
+def test_order2_predictor_corrector(sc):
+    # TimeIntegratorOrder = 2, main.cpp:308-348
+    text = (decks.mfism(16, 16, 48, extra={"Phi_Bc_hi": 0.5, "TimeIntegratorOrder": 2}) if sc
+            else decks.mfim(16, 16, 24, Phi_Bc_hi=0.4, extra={"TimeIntegratorOrder": 2}))
+    f, o = pair(text, rtol=1e-13)
+    for step in range(1, 9):
+        f.step(1)
+        o.step(step)
+    for name in ["Pz", "Phi"]:
+        assert relerr(f.field(name), o.field(name)) < 1e-10, name
+
+
 def test_named_mfim_size_one_step():
     # the 64x64x36 MFIM workload: one coupled step against the oracle
     f, o = pair(decks.mfim(64, 64, 36), rtol=1e-12)
