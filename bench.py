@@ -9,6 +9,12 @@ seeded synthetic initial polarization.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload mfism|mfim|polycrystal] [--precision fp64|mixed]
+                    [--no-adjoint] [--adjoint-steps-per-leg S]
+
+At N = 1 the line also carries "adjoint": the time of fx_backward over
+fx_forward_record for the hysteresis loss on the 128x128x48 MFIM stack
+(800 steps, checkpoints every 50, gradients in alpha, beta, gamma, g11, g44
+and the voltage amplitude).
 
 Multi-GPU runs are independent replicas (one process per GPU, weak scaling):
 the path has no data exchange between devices.  Rank 0 prints one JSON line.
@@ -155,6 +161,47 @@ def cpu_baseline(text: str, grains, steps: int) -> dict:
             "seconds": dt}
 
 
+def adjoint_ratio(stream, precision: str = "fp64", steps_per_leg: int = 400, k: int = 50) -> dict:
+    """Gradient of the hysteresis loss on the 128x128x48 MFIM stack (5 nm HZO
+    on 4 nm Al2O3) over a triangular sweep -3 V -> +3 V -> -3 V with
+    steps_per_leg steps per leg, with respect to alpha, beta, gamma, g11, g44
+    and the voltage amplitude; checkpoints every k steps.  Times
+    fx_forward_record and fx_backward with CUDA events on the library's
+    stream and returns their ratio."""
+    import torch
+    from ferrox_b200 import api, decks
+    v_amp = 3.0
+    shape = decks.triangular_sweep(1.0, steps_per_leg)
+    target = decks.target_loop(v_amp * shape, seed=7, ps=0.15, vc=1.2)
+    text = decks.hysteresis(128, 128, 48, v_amp=v_amp, steps_per_leg=steps_per_leg)
+    # warm-up on a throwaway context: module load, first graph captures
+    w = api.FerroX(text, precision=precision)
+    w.set_stream(stream.cuda_stream)
+    w.forward_record(target[:2 * k], v_amp, shape[:2 * k], k)
+    w.backward()
+    w.close()
+    f = api.FerroX(text, precision=precision)
+    f.set_stream(stream.cuda_stream)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    torch.cuda.synchronize()
+    ev[0].record(stream)
+    loss = f.forward_record(target, v_amp, shape, k)
+    ev[1].record(stream)
+    g = f.backward()
+    ev[2].record(stream)
+    torch.cuda.synchronize()
+    fwd, bwd = ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])
+    T = len(shape)
+    out = {"workload": f"hysteresis-128x128x48-{precision}", "steps": T, "checkpoint_every": k,
+           "forward_ms": fwd, "backward_ms": bwd, "ratio": bwd / fwd, "loss": loss,
+           "grads": dict(zip(api.GRADS, map(float, g))),
+           "adjoint_mg_cycles_per_step": f.param("adjoint_mg_cycles") / T,
+           "record_bytes": f.param("adjoint_bytes"),
+           "note": "backward = segment recompute + adjoint; ratio = backward / forward"}
+    f.close()
+    return out
+
+
 def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -203,6 +250,8 @@ def main() -> None:
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--adjoint-steps-per-leg", type=int, default=400)
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -325,6 +374,9 @@ def main() -> None:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             cpu = cpu_baseline(text, grains, 3)
+        adj = None
+        if world == 1 and not args.no_adjoint:
+            adj = adjoint_ratio(stream, args.precision, args.adjoint_steps_per_leg)
         line = {
             "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -343,6 +395,7 @@ def main() -> None:
             "kernel_ms_share": {k: round(v[0] / total_ms, 4) for k, v in kt.items() if v[1]},
             "mg_cycles_per_step": (st1["mg_cycles_total"] - st0["mg_cycles_total"]) / args.steps,
             "newton_passes_per_step": (st1["newton_iters_total"] - st0["newton_iters_total"]) / args.steps,
+            "adjoint": adj,
         }
         print(json.dumps(line), flush=True)
     f.close()

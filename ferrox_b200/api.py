@@ -29,7 +29,16 @@ EXPORTS = ["fx_version", "fx_create", "fx_create_error", "fx_destroy", "fx_last_
            "fx_set_precision", "fx_get_field", "fx_set_field", "fx_compute_poisson_rhs", "fx_compute_rho",
            "fx_compute_phi_rho", "fx_compute_E", "fx_tdgl_euler", "fx_set_phi_bc", "fx_check_steady_state",
            "fx_step", "fx_run", "fx_write_plotfile", "fx_get_stats", "fx_mean_P", "fx_sync", "fx_set_stream",
-           "fx_get_kernel_times", "fx_reset_kernel_times", "fx_mean_P_noalloc"]
+           "fx_get_kernel_times", "fx_reset_kernel_times", "fx_mean_P_noalloc", "fx_forward_record",
+           "fx_backward", "fx_get_grad_P0"]
+
+# gradient slots of fx_backward (enum fx_grad); per-grain alphas follow
+GRADS = ["alpha", "beta", "gamma", "g11", "g44", "v_amp"]
+
+
+class LossSpec(C.Structure):
+    _fields_ = [("nsteps", C.c_int), ("checkpoint_every", C.c_int), ("v_amp", C.c_double),
+                ("v_shape", C.POINTER(C.c_double)), ("target", C.POINTER(C.c_double))]
 
 KERNEL_CLASSES = ["tdgl", "rhs_p", "newton", "rho", "steady", "smooth_l0", "restrict_l0", "prolong_l0",
                   "mg_coarse", "resid64", "efield", "mg_l1", "mg_l2", "coarse_cta"]
@@ -94,6 +103,9 @@ def lib():
         L.fx_mean_P_noalloc.argtypes = [vp, vp, vp, vp, C.c_size_t, vp, vp]
         L.fx_get_kernel_times.argtypes = [vp, dp, C.POINTER(C.c_longlong), C.c_int]
         L.fx_reset_kernel_times.argtypes = [vp]
+        L.fx_forward_record.argtypes = [vp, C.POINTER(LossSpec), dp]
+        L.fx_backward.argtypes = [vp, dp, C.c_int]
+        L.fx_get_grad_P0.argtypes = [vp, dp, dp, dp, C.c_size_t]
         _lib = L
     return _lib
 
@@ -225,3 +237,29 @@ class FerroX:
 
     def reset_kernel_times(self) -> None:
         self._check(lib().fx_reset_kernel_times(self.h))
+
+    def forward_record(self, target, v_amp: float, v_shape=None, checkpoint_every: int = 50) -> float:
+        """Run len(target) steps under Phi_Bc_hi = v_amp * v_shape[n], keeping
+        checkpoints for backward(); returns L = mean_n (<Pz>^n - target[n])^2."""
+        t = np.ascontiguousarray(target, dtype=np.float64)
+        shp = None if v_shape is None else np.ascontiguousarray(v_shape, dtype=np.float64)
+        if shp is not None and shp.shape != t.shape:
+            raise ValueError("v_shape and target need the same length")
+        self._keep = (t, shp)
+        spec = LossSpec(len(t), int(checkpoint_every), float(v_amp), _dp(shp), _dp(t))
+        loss = C.c_double()
+        self._check(lib().fx_forward_record(self.h, C.byref(spec), C.byref(loss)))
+        return loss.value
+
+    def backward(self, ngrains: int = 0) -> np.ndarray:
+        """Gradients of the recorded loss: alpha, beta, gamma, g11, g44, v_amp,
+        then the per-grain alphas."""
+        g = np.zeros(len(GRADS) + ngrains)
+        self._check(lib().fx_backward(self.h, _dp(g), len(g)))
+        return g
+
+    def grad_P0(self, components=("Pz",)) -> dict:
+        """dL/dP at the state the recorded run started from."""
+        out = {c: np.zeros(self.N) for c in components}
+        self._check(lib().fx_get_grad_P0(self.h, _dp(out.get("Px")), _dp(out.get("Py")), _dp(out.get("Pz")), self.N))
+        return {c: a.reshape(self.shape) for c, a in out.items()}

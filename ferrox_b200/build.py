@@ -17,7 +17,7 @@ LIB = os.path.join(HERE, "libferrox_b200.so")
 EXE = os.path.join(HERE, "ferrox_b200")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-CU = ["fx_kernels.cu", "fx_mg.cu", "fx_api.cu", "fx_noalloc.cu"]
+CU = ["fx_kernels.cu", "fx_mg.cu", "fx_adjoint.cu", "fx_api.cu", "fx_noalloc.cu"]
 CPP = ["inputs.cpp", "plotfile.cpp"]
 HDR = ["fx_device.cuh", "fx_kernels.h", "fx_mg.h", "fx_params.h", "plotfile.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

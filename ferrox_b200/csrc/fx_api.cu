@@ -109,6 +109,7 @@ struct fx_ctx {
     bool scalarP = true;                 // Px = Py = 0 and is_polarization_scalar
     bool contains_sc = false;
     bool grains_set = false;
+    int ngrains = 0;
     bool user_P = false;
 
     // loop state, main.cpp:238-242
@@ -149,6 +150,35 @@ struct fx_ctx {
     size_t dev_bytes = 0;
     Multigrid mg;
     bool mg_ready = false;
+
+    // bumped by every call that changes the state or a parameter of the
+    // math; fx_backward requires the value fx_forward_record saw
+    long long gen = 0;
+    std::vector<uint8_t> variant_global_alpha;   // per variant: alpha is the global alpha
+
+    // gradient record (fx_forward_record / fx_backward)
+    struct AdjRecord {
+        bool valid = false;
+        long long gen = -1;
+        int T = 0, k = 0, nck = 0;
+        long long nfe = 0;
+        std::vector<double> V, shape, target, m;
+        double loss = 0.0;
+        std::vector<void*> allocs;                 // freed together
+        size_t bytes = 0;
+        std::vector<double*> ckP, ckPhi, ckRho;    // 3 per checkpoint (null for unused components), 1, 1
+        double* finP[3] = {nullptr, nullptr, nullptr};
+        double *finPhi = nullptr, *finRho = nullptr;
+        std::vector<double*> segP, segPhi;         // 3 per segment step, 1 (semiconductor only)
+        double* lam[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+        int lcur = 0;
+        double *mu = nullptr, *psi = nullptr, *drho = nullptr, *grad = nullptr, *dV = nullptr, *hist = nullptr;
+        float* drho32 = nullptr;
+        uint8_t* gid = nullptr;
+        bool have_P0 = false;
+        long long mg_cycles = 0;
+        double fwd_ms = 0.0, bwd_ms = 0.0;
+    } adj;
 };
 
 namespace {
@@ -253,6 +283,7 @@ std::string check_wrapped_mask(fx_ctx* c) {
 void build_variants(fx_ctx* c, const std::vector<uint8_t>* gid, const std::vector<double>* galpha) {
     c->var.clear();
     c->variants.clear();
+    c->variant_global_alpha.clear();
     const size_t N = c->N;
     bool any = false;
     if (gid) any = true;
@@ -260,12 +291,15 @@ void build_variants(fx_ctx* c, const std::vector<uint8_t>* gid, const std::vecto
         for (size_t q = 0; q < N; ++q)
             if (c->ang[d][q] != 0.0) { any = true; break; }
     if (!any) return;
-    std::map<std::tuple<double, double, double, double>, uint8_t> ids;
+    std::map<std::tuple<double, double, double, int, double>, uint8_t> ids;
     c->var.assign(N, 0);
     for (size_t q = 0; q < N; ++q) {
         double al = c->par.alpha;
-        if (gid && galpha && (*gid)[q] != 255 && (*gid)[q] < galpha->size()) al = (*galpha)[(*gid)[q]];
-        auto key = std::make_tuple(c->ang[0][q], c->ang[1][q], c->ang[2][q], al);
+        const bool own = gid && galpha && (*gid)[q] != 255 && (*gid)[q] < galpha->size();
+        if (own) al = (*galpha)[(*gid)[q]];
+        // a grain alpha equal to the global one stays a separate variant, so
+        // that changing the global alpha later leaves it alone
+        auto key = std::make_tuple(c->ang[0][q], c->ang[1][q], c->ang[2][q], own ? 1 : 0, own ? al : 0.0);
         auto it = ids.find(key);
         if (it == ids.end()) {
             if (ids.size() >= 255) throw FxError{FX_ERR_UNSUPPORTED, "more than 255 distinct Euler-angle / alpha combinations"};
@@ -274,6 +308,7 @@ void build_variants(fx_ctx* c, const std::vector<uint8_t>* gid, const std::vecto
             v.alpha = al;
             const uint8_t id = (uint8_t)c->variants.size();
             c->variants.push_back(v);
+            c->variant_global_alpha.push_back(own ? 0 : 1);
             it = ids.emplace(key, id).first;
         }
         c->var[q] = it->second;
@@ -481,13 +516,13 @@ int compute_phi_rho_P(fx_ctx* c, int buf) {
     }
     r = compute_rhs_p(c, false, buf);
     if (r) return r;
-    const double tol = 1.e-5;
+    const double tol = c->par.newton_tol;   // 1e-5 in the reference
     double err = 1.0;
     int iter = 0, passes = 0;
     while (err > tol) {
         if (passes >= c->par.newton_max_iter) {
             std::ostringstream o;
-            o << "Phi-rho Newton iteration did not reach 1e-5 in " << passes << " passes (err = " << err << ")";
+            o << "Phi-rho Newton iteration did not reach " << tol << " in " << passes << " passes (err = " << err << ")";
             return set_err(c, std::isfinite(err) ? FX_ERR_NO_CONVERGENCE : FX_ERR_NONFINITE, o.str());
         }
         ++passes;
@@ -706,6 +741,255 @@ int get_field(fx_ctx* c, int f, double* out) {
     return FX_OK;
 }
 
+// ---- gradient record: checkpoints, segment recompute, reverse sweep ----
+
+void adj_free(fx_ctx* c) {
+    auto& A = c->adj;
+    if (!A.allocs.empty() && c->s) cudaStreamSynchronize(c->s);
+    for (void* q : A.allocs) cudaFree(q);
+    A = fx_ctx::AdjRecord();
+}
+
+template <typename T>
+int adj_alloc(fx_ctx* c, T** q, size_t n) {
+    cudaError_t e = cudaMalloc((void**)q, std::max<size_t>(n, 1) * sizeof(T));
+    if (e != cudaSuccess) {
+        *q = nullptr;
+        return set_err(c, FX_ERR_OUT_OF_MEMORY, std::string("gradient record: cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    c->adj.allocs.push_back(*q);
+    c->adj.bytes += n * sizeof(T);
+    return FX_OK;
+}
+
+// the P components the kernels read (z only with scalar polarization)
+int ncomp_first(const fx_ctx* c) { return c->scalarP ? 2 : 0; }
+
+int dcopy(fx_ctx* c, double* dst, const double* src) {
+    FX_CUDA(c, cudaMemcpyAsync(dst, src, c->N * 8, cudaMemcpyDeviceToDevice, c->s));
+    return FX_OK;
+}
+
+// save / restore the step state: P, phi (the solve's warm start) and, with a
+// semiconductor, rho (the Newton loop's first right-hand side)
+int adj_save(fx_ctx* c, double* const P[3], double* phi, double* rho) {
+    int r = 0;
+    for (int d = ncomp_first(c); d < 3 && !r; ++d) r = dcopy(c, P[d], c->d_P[c->cur][d]);
+    if (!r) r = dcopy(c, phi, c->d_phi);
+    if (!r && rho) r = dcopy(c, rho, c->d_rho);
+    return r;
+}
+
+int adj_restore(fx_ctx* c, double* const P[3], const double* phi, const double* rho) {
+    int r = 0;
+    for (int d = ncomp_first(c); d < 3 && !r; ++d) r = dcopy(c, c->d_P[c->cur][d], P[d]);
+    if (!r) r = dcopy(c, c->d_phi, phi);
+    if (!r && rho) r = dcopy(c, c->d_rho, rho);
+    c->E_valid = false;
+    return r;
+}
+
+// one step of the recorded loop: electrode value, ComputePhi_Rho, TDGL update
+int adj_step(fx_ctx* c, double V) {
+    c->Phi_Bc_hi = V;
+    electrode_values(c);
+    int r = compute_phi_rho(c);
+    if (r) return r;
+    r = tdgl_update(c);
+    c->E_valid = false;
+    c->prof.collect();
+    return r;
+}
+
+double ms_since(std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+int forward_record(fx_ctx* c, const fx_loss_spec* sp, double* loss) {
+    const auto t0 = std::chrono::steady_clock::now();
+    const int T = sp->nsteps, k = sp->checkpoint_every;
+    int r = ensure_device(c);
+    if (r) return r;
+    adj_free(c);
+    auto& A = c->adj;
+    A.T = T;
+    A.k = k;
+    A.nck = (T + k - 1) / k;
+    A.V.resize(T);
+    A.shape.assign(T, 1.0);
+    if (sp->v_shape) A.shape.assign(sp->v_shape, sp->v_shape + T);
+    A.target.assign(sp->target, sp->target + T);
+    for (int n = 0; n < T; ++n) A.V[n] = sp->v_amp * A.shape[n];
+    A.nfe = 0;
+    for (size_t q = 0; q < c->N; ++q) A.nfe += (c->code[q + c->nxy] & 3) == 0;
+    if (A.nfe == 0) return set_err(c, FX_ERR_INVALID_ARGUMENT, "the loss needs ferroelectric cells");
+    const bool sc = c->contains_sc;
+    A.ckP.assign(3 * A.nck, nullptr);
+    A.ckPhi.assign(A.nck, nullptr);
+    A.ckRho.assign(A.nck, nullptr);
+    for (int q = 0; q < A.nck; ++q) {
+        for (int d = ncomp_first(c); d < 3; ++d) if ((r = adj_alloc(c, &A.ckP[3 * q + d], c->N))) return r;
+        if ((r = adj_alloc(c, &A.ckPhi[q], c->N))) return r;
+        if (sc && (r = adj_alloc(c, &A.ckRho[q], c->N))) return r;
+    }
+    for (int d = ncomp_first(c); d < 3; ++d) if ((r = adj_alloc(c, &A.finP[d], c->N))) return r;
+    if ((r = adj_alloc(c, &A.finPhi, c->N))) return r;
+    if (sc && (r = adj_alloc(c, &A.finRho, c->N))) return r;
+    if ((r = adj_alloc(c, &A.hist, 3 * (size_t)T))) return r;
+
+    if ((r = adj_save(c, &A.ckP[0], A.ckPhi[0], A.ckRho[0]))) return r;
+    for (int n = 1; n <= T; ++n) {
+        if ((r = adj_step(c, A.V[n - 1]))) return r;
+        const double* Pin[3];
+        P_in(c, Pin);
+        ++g_launches;
+        r = k_status(c, launch_mean_p(c->dp, c->d_code, Pin, c->d_part, c->d_counter, A.hist + 3 * (n - 1), c->s));
+        if (r) return r;
+        if (n % k == 0 && n / k < A.nck) {
+            const int q = n / k;
+            if ((r = adj_save(c, &A.ckP[3 * q], A.ckPhi[q], A.ckRho[q]))) return r;
+        }
+    }
+    if ((r = adj_save(c, A.finP, A.finPhi, A.finRho))) return r;
+    std::vector<double> h(3 * (size_t)T);
+    FX_CUDA(c, cudaMemcpyAsync(h.data(), A.hist, h.size() * 8, cudaMemcpyDeviceToHost, c->s));
+    FX_CUDA(c, cudaStreamSynchronize(c->s));
+    A.m.resize(T);
+    double L = 0.0;
+    for (int n = 0; n < T; ++n) {
+        A.m[n] = h[3 * n + 2];
+        const double e = A.m[n] - A.target[n];
+        L += e * e;
+    }
+    A.loss = L / T;
+    *loss = A.loss;
+    c->step += T;
+    c->time += T * c->par.dt;
+    A.valid = true;
+    A.gen = c->gen;
+    A.fwd_ms = ms_since(t0);
+    return FX_OK;
+}
+
+int backward(fx_ctx* c, double* grads, int ngrads) {
+    const auto t0 = std::chrono::steady_clock::now();
+    auto& A = c->adj;
+    const int T = A.T, k = A.k;
+    const bool sc = c->contains_sc, vec = !c->scalarP;
+    const int mixed = c->par.precision == 1;
+    const int d0 = ncomp_first(c);
+    int r = 0;
+    if (A.segP.empty()) {
+        A.segP.assign(3 * (size_t)k, nullptr);
+        A.segPhi.assign(k, nullptr);
+        for (int q = 0; q < k; ++q) {
+            for (int d = d0; d < 3; ++d) if ((r = adj_alloc(c, &A.segP[3 * q + d], c->N))) return r;
+            if (sc && (r = adj_alloc(c, &A.segPhi[q], c->N))) return r;
+        }
+        for (int b = 0; b < 2; ++b)
+            for (int d = d0; d < 3; ++d) if ((r = adj_alloc(c, &A.lam[b][d], c->N))) return r;
+        if ((r = adj_alloc(c, &A.mu, c->N))) return r;
+        if ((r = adj_alloc(c, &A.psi, c->N))) return r;
+        if (sc && ((r = adj_alloc(c, &A.drho, c->N)) || (r = adj_alloc(c, &A.drho32, c->N)))) return r;
+        if ((r = adj_alloc(c, &A.grad, 8 + 256))) return r;
+        if ((r = adj_alloc(c, &A.dV, (size_t)T))) return r;
+        if (c->grains_set && !c->gid.empty()) {
+            if ((r = adj_alloc(c, &A.gid, c->N))) return r;
+            FX_CUDA(c, cudaMemcpyAsync(A.gid, c->gid.data(), c->N, cudaMemcpyHostToDevice, c->s));
+        }
+    }
+    FX_CUDA(c, cudaMemsetAsync(A.grad, 0, (8 + 256) * 8, c->s));
+    FX_CUDA(c, cudaMemsetAsync(A.dV, 0, (size_t)T * 8, c->s));
+    FX_CUDA(c, cudaMemsetAsync(A.psi, 0, c->N * 8, c->s));
+    // dL/d<Pz>^n spread over the FE cells
+    std::vector<double> g(T + 1, 0.0);
+    for (int n = 1; n <= T; ++n) g[n] = 2.0 / T * (A.m[n - 1] - A.target[n - 1]) / (double)A.nfe;
+    int cur = 0;
+    if ((r = k_status(c, launch_adj_init(c->dp, c->d_code, A.lam[cur], g[T], c->s)))) return r;
+    ++g_launches;
+    DevParams dp0 = c->dp;   // the adjoint solve: homogeneous electrode values
+    dp0.V_lo = 0.0;
+    dp0.V_hi = 0.0;
+    const int ngalpha = (int)c->galpha.size();
+    for (int s = A.nck - 1; s >= 0; --s) {
+        const int start = s * k, end = std::min(T, start + k);
+        if ((r = adj_restore(c, &A.ckP[3 * s], A.ckPhi[s], A.ckRho[s]))) return r;
+        for (int n = start + 1; n <= end; ++n) {
+            const int idx = n - 1 - start;
+            for (int d = d0; d < 3; ++d)
+                if ((r = dcopy(c, A.segP[3 * idx + d], c->d_P[c->cur][d]))) return r;
+            c->Phi_Bc_hi = A.V[n - 1];
+            electrode_values(c);
+            if ((r = compute_phi_rho(c))) return r;
+            if (sc && (r = dcopy(c, A.segPhi[idx], c->d_phi))) return r;
+            if ((r = tdgl_update(c))) return r;
+            c->prof.collect();
+        }
+        for (int n = end; n >= start + 1; --n) {
+            const int idx = n - 1 - start;
+            const double* psi = nullptr;
+            if (c->par.include_Elec) {
+                FX_CUDA(c, cudaMemsetAsync(c->d_out, 0, sizeof(double), c->s));
+                ++g_launches;
+                r = k_status(c, launch_adj_phi(c->dp, mixed, vec, c->d_code, c->d_var, c->d_vt, A.lam[cur], A.mu,
+                                               c->d_out, A.dV + (n - 1), c->s));
+                if (r) return r;
+                if ((r = read_out(c, 1))) return r;
+                const double nmu = c->h_out[0];
+                if (!std::isfinite(nmu)) return set_err(c, FX_ERR_NONFINITE, "adjoint source is not finite");
+                if (nmu > 0.0) {
+                    if (sc) {
+                        ++g_launches;
+                        r = k_status(c, launch_drho(c->dp, c->d_code, A.segPhi[idx], A.drho, A.drho32, c->s));
+                        if (r) return r;
+                        c->mg.set_alpha(A.drho, A.drho32, true, c->s);
+                    } else {
+                        c->mg.set_alpha(nullptr, nullptr, false, c->s);
+                    }
+                    const double target = std::max(c->par.mg_rtol, 1e-16) * nmu;
+                    MGStats st;
+                    int e = mixed ? c->mg.solve_mixed(dp0, c->d_code, A.psi, A.mu, target, c->par.mg_max_iter, c->s, &st)
+                                  : c->mg.solve64(dp0, c->d_code, A.psi, A.mu, target, c->par.mg_max_iter, c->s, &st);
+                    A.mg_cycles += st.cycles;
+                    if (e == -3) {
+                        std::ostringstream o;
+                        o << "adjoint Poisson multigrid did not reach |r| <= " << target << " (|r| = " << st.resid << ")";
+                        return set_err(c, std::isfinite(st.resid) ? FX_ERR_NO_CONVERGENCE : FX_ERR_NONFINITE, o.str());
+                    }
+                    if (e) return set_err(c, FX_ERR_CUDA, std::string("multigrid: ") + cudaGetErrorString((cudaError_t)e));
+                    psi = A.psi;
+                }
+            }
+            const double* Pn[3] = {A.segP[3 * idx], A.segP[3 * idx + 1], A.segP[3 * idx + 2]};
+            ++g_launches;
+            r = k_status(c, launch_adj_P(c->dp, mixed, vec, c->d_code, c->d_var, c->d_vt, A.gid, ngalpha, Pn,
+                                         A.lam[cur], psi, g[n - 1], A.lam[1 - cur], A.grad, A.dV + (n - 1), c->s));
+            if (r) return r;
+            cur = 1 - cur;
+        }
+    }
+    A.lcur = cur;
+    A.have_P0 = true;
+    if ((r = adj_restore(c, A.finP, A.finPhi, A.finRho))) return r;
+    c->Phi_Bc_hi = A.V[T - 1];
+    electrode_values(c);
+    std::vector<double> hg(8 + 256), hv(T);
+    FX_CUDA(c, cudaMemcpyAsync(hg.data(), A.grad, hg.size() * 8, cudaMemcpyDeviceToHost, c->s));
+    FX_CUDA(c, cudaMemcpyAsync(hv.data(), A.dV, hv.size() * 8, cudaMemcpyDeviceToHost, c->s));
+    FX_CUDA(c, cudaStreamSynchronize(c->s));
+    for (int q = 0; q < 5; ++q) grads[q] = hg[q];
+    double gv = 0.0;
+    for (int n = 0; n < T; ++n) gv += A.shape[n] * hv[n];
+    grads[FX_GRAD_V_AMP] = gv;
+    const int ng = c->grains_set ? c->ngrains : 0;
+    for (int q = FX_GRAD_GRAIN_ALPHA; q < ngrads; ++q) {
+        const int gi = q - FX_GRAD_GRAIN_ALPHA;
+        grads[q] = gi < ng ? hg[8 + gi] : 0.0;
+    }
+    A.bwd_ms = ms_since(t0);
+    return FX_OK;
+}
+
 void read_inputs(const char* inputs, int is_text, std::string& text) {
     if (is_text) { text = inputs; return; }
     std::ifstream f(inputs);
@@ -802,6 +1086,7 @@ void fx_destroy(fx_ctx* c) {
     if (!c) return;
     if (c->dev) {
         cudaStreamSynchronize(c->s);
+        adj_free(c);
         cudaFree(c->d_code); cudaFree(c->d_var); cudaFree(c->d_vt);
         for (int b = 0; b < 2; ++b)
             for (int d = 0; d < 3; ++d) cudaFree(c->d_P[b][d]);
@@ -853,7 +1138,10 @@ int fx_get_param(const fx_ctx* c, const char* key, double* v) {
         {"fx.warm_start", p.warm_start}, {"contains_sc", c->contains_sc ? 1.0 : 0.0},
         {"V_lo", c->dp.V_lo}, {"V_hi", c->dp.V_hi}, {"phi_ref", phi_ref()},
         {"intrinsic_carrier_concentration", std::sqrt(kNc * kNv) * exp(-0.5 * kQ * kEg / (kKb * kT))},
-        {"num_variants", (double)c->variants.size()}};
+        {"num_variants", (double)c->variants.size()}, {"fx.newton_tol", p.newton_tol},
+        {"adjoint_mg_cycles", (double)c->adj.mg_cycles}, {"adjoint_forward_ms", c->adj.fwd_ms},
+        {"adjoint_backward_ms", c->adj.bwd_ms}, {"adjoint_bytes", (double)c->adj.bytes},
+        {"adjoint_loss", c->adj.loss}};
     auto it = m.find(k);
     if (it != m.end()) { *v = it->second; return FX_OK; }
     // "FE_lo[2]" style access to the 3-vectors
@@ -888,6 +1176,7 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
     if (!c || !key) return FX_ERR_INVALID_ARGUMENT;
     const std::string k(key);
     Params& p = c->par;
+    if (k != "fx.profile" && k != "fx.verbose" && k != "fx.graphs") ++c->gen;
     if (k == "Phi_Bc_hi") { c->Phi_Bc_hi = v; electrode_values(c); c->E_valid = false; return FX_OK; }
     if (k == "Phi_Bc_lo") { p.Phi_Bc_lo = v; electrode_values(c); c->E_valid = false; return FX_OK; }
     if (k == "fx.mg_rtol") { p.mg_rtol = v; return FX_OK; }
@@ -901,7 +1190,26 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
     if (k == "fx.mg_nu2") { c->mg.nu2 = (int)v; return FX_OK; }
     if (k == "fx.phi_ghost_mode") { p.phi_ghost_mode = (int)v; c->dp.ghost_mode = (int)v; c->E_valid = false; return FX_OK; }
     if (k == "dt") { p.dt = v; c->dp.dt = v; return FX_OK; }
-    if (k == "alpha") { p.alpha = v; c->dp.alpha = v; return FX_OK; }
+    if (k == "alpha") {
+        p.alpha = v;
+        c->dp.alpha = v;
+        // the rotation table carries alpha per variant: update the ones that
+        // use the global value (grain alphas set by fx_set_grain_alpha stay)
+        bool any = false;
+        for (size_t q = 0; q < c->variants.size(); ++q)
+            if (c->variant_global_alpha[q]) { c->variants[q].alpha = v; any = true; }
+        if (any && c->dev && c->d_vt) {
+            FX_CUDA(c, cudaMemcpyAsync(c->d_vt, c->variants.data(), c->variants.size() * sizeof(Variant),
+                                       cudaMemcpyHostToDevice, c->s));
+            FX_CUDA(c, cudaStreamSynchronize(c->s));
+        }
+        return FX_OK;
+    }
+    if (k == "fx.newton_tol") {
+        if (!(v > 0.0)) return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx.newton_tol must be positive");
+        p.newton_tol = v;
+        return FX_OK;
+    }
     if (k == "beta") { p.beta = v; c->dp.beta = v; return FX_OK; }
     if (k == "gamma") { p.gamma = v; c->dp.gamma = v; return FX_OK; }
     if (k == "g11") { p.g11 = v; c->dp.g11 = v; return FX_OK; }
@@ -913,6 +1221,7 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
 
 int fx_set_precision(fx_ctx* c, int mode) {
     if (!c || (mode != 0 && mode != 1)) return FX_ERR_INVALID_ARGUMENT;
+    if (c) ++c->gen;
     if (c->dev && mode != c->par.precision)
         return set_err(c, FX_ERR_INVALID_ARGUMENT, "precision must be chosen before the first device call");
     c->par.precision = mode;
@@ -920,6 +1229,7 @@ int fx_set_precision(fx_ctx* c, int mode) {
 }
 
 int fx_set_initial_P(fx_ctx* c, const double* Px, const double* Py, const double* Pz, size_t n) {
+    if (c) ++c->gen;
     if (!c || !Pz || n != c->N) return c ? set_err(c, FX_ERR_INVALID_ARGUMENT, "P arrays must hold nx*ny*nz values") : FX_ERR_INVALID_ARGUMENT;
     const double* src[3] = {Px, Py, Pz};
     bool zero_xy = true;
@@ -962,6 +1272,8 @@ int fx_set_grains(fx_ctx* c, const uint8_t* gid, size_t n, const double* ang, co
         return set_err(c, e.code, e.msg);
     }
     c->grains_set = true;
+    c->ngrains = ng;
+    ++c->gen;
     if (!c->user_P) build_P0(c);
     else for (size_t q = 0; q < n; ++q) if (c->tphase[q] == 1.0) c->P0[2][q] = 0.0;
     return FX_OK;
@@ -969,6 +1281,7 @@ int fx_set_grains(fx_ctx* c, const uint8_t* gid, size_t n, const double* ang, co
 
 int fx_set_grain_alpha(fx_ctx* c, const double* alpha, int ng) {
     if (!c || !alpha || ng <= 0) return FX_ERR_INVALID_ARGUMENT;
+    if (c) ++c->gen;
     if (!c->grains_set) return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx_set_grains must come first");
     c->galpha.assign(alpha, alpha + ng);
     try {
@@ -996,6 +1309,7 @@ int fx_get_field(fx_ctx* c, int f, double* out, size_t n) {
 
 int fx_set_field(fx_ctx* c, int f, const double* in, size_t n) {
     if (!c || !in) return FX_ERR_INVALID_ARGUMENT;
+    ++c->gen;
     if (n != c->N) return set_err(c, FX_ERR_INVALID_ARGUMENT, "field buffers hold nx*ny*nz values");
     if (f == FX_FIELD_PX || f == FX_FIELD_PY || f == FX_FIELD_PZ) {
         if (f != FX_FIELD_PZ && c->scalarP) {
@@ -1025,6 +1339,7 @@ int fx_set_field(fx_ctx* c, int f, const double* in, size_t n) {
 
 int fx_compute_poisson_rhs(fx_ctx* c) {
     if (!c) return FX_ERR_INVALID_ARGUMENT;
+    ++c->gen;
     int r = ensure_device(c);
     if (r) return r;
     r = compute_rhs_p(c, false, c->cur);
@@ -1049,6 +1364,7 @@ int fx_compute_poisson_rhs(fx_ctx* c) {
 
 int fx_compute_rho(fx_ctx* c) {
     if (!c) return FX_ERR_INVALID_ARGUMENT;
+    ++c->gen;
     int r = ensure_device(c);
     if (r) return r;
     ++g_launches;
@@ -1061,6 +1377,7 @@ int fx_compute_rho(fx_ctx* c) {
 
 int fx_compute_phi_rho(fx_ctx* c) {
     if (!c) return FX_ERR_INVALID_ARGUMENT;
+    ++c->gen;
     return compute_phi_rho(c);
 }
 
@@ -1075,6 +1392,7 @@ int fx_compute_E(fx_ctx* c) {
 
 int fx_tdgl_euler(fx_ctx* c) {
     if (!c) return FX_ERR_INVALID_ARGUMENT;
+    ++c->gen;
     int r = tdgl_update(c);
     if (r) return r;
     FX_CUDA(c, cudaStreamSynchronize(c->s));
@@ -1083,6 +1401,7 @@ int fx_tdgl_euler(fx_ctx* c) {
 
 int fx_set_phi_bc(fx_ctx* c) {
     if (!c) return FX_ERR_INVALID_ARGUMENT;
+    ++c->gen;
     electrode_values(c);
     c->E_valid = false;
     return FX_OK;
@@ -1095,6 +1414,7 @@ int fx_check_steady_state(fx_ctx* c, int step) {
 
 int fx_step(fx_ctx* c, int nsteps, int* done) {
     if (!c || nsteps < 0) return FX_ERR_INVALID_ARGUMENT;
+    ++c->gen;
     int k = 0;
     if (done) *done = 0;
     for (; k < nsteps && !c->finished; ++k) {
@@ -1144,6 +1464,7 @@ int fx_write_plotfile(fx_ctx* c, int step, const char* dir) {
 
 int fx_run(fx_ctx* c, int* done) {
     if (!c) return FX_ERR_INVALID_ARGUMENT;
+    ++c->gen;
     const Params& p = c->par;
     if (done) *done = 0;
     if (p.plot_int > 0 && c->step == 0) {
@@ -1234,6 +1555,53 @@ int fx_reset_kernel_times(fx_ctx* c) {
     if (c->dev) FX_CUDA(c, cudaStreamSynchronize(c->s));
     c->prof.collect();
     c->prof.reset();
+    return FX_OK;
+}
+
+int fx_forward_record(fx_ctx* c, const fx_loss_spec* sp, double* loss) {
+    if (!c) return FX_ERR_INVALID_ARGUMENT;
+    if (!sp || !loss || sp->nsteps < 1 || sp->checkpoint_every < 1 || !sp->target)
+        return set_err(c, FX_ERR_INVALID_ARGUMENT,
+                       "fx_forward_record: spec and loss are required, with nsteps >= 1, checkpoint_every >= 1 and a target");
+    if (c->par.TimeIntegratorOrder != 1)
+        return set_err(c, FX_ERR_UNSUPPORTED, "gradients are implemented for TimeIntegratorOrder = 1");
+    if (c->nx < 6 || c->ny < 6)
+        return set_err(c, FX_ERR_UNSUPPORTED, "gradients need at least 6 cells in x and y");
+    for (int n = 0; n < sp->nsteps; ++n)
+        if (!std::isfinite(sp->target[n]) || (sp->v_shape && !std::isfinite(sp->v_shape[n])))
+            return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx_forward_record: non-finite target or v_shape");
+    if (!std::isfinite(sp->v_amp)) return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx_forward_record: non-finite v_amp");
+    ++c->gen;
+    const int r = forward_record(c, sp, loss);
+    if (r) c->adj.valid = false;
+    return r;
+}
+
+int fx_backward(fx_ctx* c, double* grads, int ngrads) {
+    if (!c) return FX_ERR_INVALID_ARGUMENT;
+    if (!grads || ngrads < FX_GRAD_GRAIN_ALPHA)
+        return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx_backward: grads needs at least 6 slots");
+    if (!c->adj.valid) return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx_backward: no fx_forward_record to differentiate");
+    if (c->adj.gen != c->gen)
+        return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx_backward: the context changed since fx_forward_record");
+    const int r = backward(c, grads, ngrads);
+    if (r) {
+        c->adj.valid = false;
+        c->adj.have_P0 = false;
+    }
+    return r;
+}
+
+int fx_get_grad_P0(fx_ctx* c, double* dPx, double* dPy, double* dPz, size_t n) {
+    if (!c) return FX_ERR_INVALID_ARGUMENT;
+    if (n != c->N) return set_err(c, FX_ERR_INVALID_ARGUMENT, "field buffers hold nx*ny*nz values");
+    if (!c->adj.have_P0) return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx_get_grad_P0: call fx_backward first");
+    if (c->scalarP && (dPx || dPy))
+        return set_err(c, FX_ERR_UNSUPPORTED, "scalar polarization: only dPz is available (pass NULL for dPx, dPy)");
+    double* out[3] = {dPx, dPy, dPz};
+    for (int d = 0; d < 3; ++d)
+        if (out[d]) FX_CUDA(c, cudaMemcpyAsync(out[d], c->adj.lam[c->adj.lcur][d], n * 8, cudaMemcpyDeviceToHost, c->s));
+    FX_CUDA(c, cudaStreamSynchronize(c->s));
     return FX_OK;
 }
 

@@ -233,6 +233,48 @@ __device__ __forceinline__ void grad_phi(const double* __restrict__ phi, const D
     grad_phi_acc<T>(PhiAt{phi, &p}, p, i, j, k, gx, gy, gz);
 }
 
+// Landau derivative dF/dP_a (TotalEnergyDensity.cpp:88-110) for component a
+// with the other two components b, c
+template <typename T>
+__device__ __forceinline__ T landau(const DevParams& p, T alpha, T a, T b, T c) {
+    const T a2 = a * a, b2 = b * b, c2 = c * c;
+    return alpha * a + T(p.beta) * (a2 * a) + T(p.gamma) * (a2 * a2 * a)
+        + T(2.) * T(p.a12) * a * b2
+        + T(2.) * T(p.a12) * a * c2
+        + T(4.) * T(p.a112) * (a2 * a) * (b2 + c2)
+        + T(2.) * T(p.a112) * a * (b2 * b2)
+        + T(2.) * T(p.a112) * a * (c2 * c2)
+        + T(2.) * T(p.a123) * a * b2 * c2;
+}
+
+// the six second derivatives of one component, for the rotated Pr term
+template <typename T>
+struct Hess { T xx, yy, zz, xy, yz, xz; };
+
+template <typename T, bool ROT, typename FV>
+__device__ __forceinline__ Hess<T> hess(const FV& F, const MView& M, int i, int j, int k) {
+    Hess<T> h;
+    h.xx = ddpd<0, T>(F, M, i, j, k);
+    h.yy = ddpd<1, T>(F, M, i, j, k);
+    h.zz = ddpd<2, T>(F, M, i, j, k);
+    if (ROT) {
+        h.xy = dxdy<T>(F, M, i, j, k);
+        h.yz = dydz<T>(F, M, i, j, k);
+        h.xz = dxdz<T>(F, M, i, j, k);
+    } else {
+        h.xy = h.yz = h.xz = T(0);
+    }
+    return h;
+}
+
+// R_a1 R_a1 Dxx + ... + 2 R_a3 R_a1 Dxz, TotalEnergyDensity.cpp:209-228
+template <typename T>
+__device__ __forceinline__ T rot_quad(const T* R, int a, const Hess<T>& H) {
+    const T r1 = R[3 * a], r2 = R[3 * a + 1], r3 = R[3 * a + 2];
+    return r1 * r1 * H.xx + r2 * r2 * H.yy + r3 * r3 * H.zz + T(2.) * r1 * r2 * H.xy + T(2.) * r2 * r3 * H.yz +
+           T(2.) * r3 * r1 * H.xz;
+}
+
 // ChargeDensity.cpp:4-11
 __device__ __forceinline__ double fd_half(double eta) {
     double nu = pow(eta, 4.0) + 50.0 + 33.6 * eta * (1.0 - 0.68 * exp(-0.17 * pow((eta + 1.0), 2.0)));

@@ -27,4 +27,14 @@ int launch_mean_p(const DevParams& p, const uint8_t* code, const double* const P
 int launch_efield(const DevParams& p, const uint8_t* var, const Variant* vt, const double* phi, double* E[3],
                   cudaStream_t s);
 
+// adjoint (fx_adjoint.cu).  lam = {lambda_x, lambda_y, lambda_z}; vec = the
+// three-component kernels (else only lambda_z is read and written)
+int launch_adj_init(const DevParams& p, const uint8_t* code, double* lam[3], double g, cudaStream_t s);
+int launch_adj_phi(const DevParams& p, int mixed, bool vec, const uint8_t* code, const uint8_t* var, const Variant* vt,
+                   double* const lam[3], double* mu, double* norm, double* dV, cudaStream_t s);
+int launch_adj_P(const DevParams& p, int mixed, bool vec, const uint8_t* code, const uint8_t* var, const Variant* vt,
+                 const uint8_t* gid, int ngalpha, const double* const P[3], double* const lam[3], const double* psi,
+                 double gload, double* const lam_out[3], double* grad, double* dV, cudaStream_t s);
+int launch_drho(const DevParams& p, const uint8_t* code, const double* phi, double* a64, float* a32, cudaStream_t s);
+
 }  // namespace fx

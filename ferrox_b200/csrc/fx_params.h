@@ -53,6 +53,7 @@ struct Params {
     int sweep_mode = 0;          // 0 steady (reference), 1 fixed cadence
     int steps_per_voltage = 0;
     int newton_max_iter = 50;
+    double newton_tol = 1.e-5;      // Newton stopping criterion (ElectrostaticSolver.cpp:697)
     int mg_max_iter = 200;
     int precision = 0;           // 0 fp64, 1 mixed
     int warm_start = 1;

@@ -458,6 +458,7 @@ Params make_params(const Inputs& in) {
     }
     r.query("fx.steps_per_voltage", p.steps_per_voltage);
     r.query("fx.newton_max_iter", p.newton_max_iter);
+    r.query("fx.newton_tol", p.newton_tol);
     r.query("fx.mg_max_iter", p.mg_max_iter);
     if (r.has("fx.precision")) {
         std::string m = r.vals("fx.precision")[0];

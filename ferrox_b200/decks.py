@@ -102,9 +102,9 @@ def mfism(nx=128, ny=128, nz=144, dxy=0.5e-9, nsteps=4000, seed=1, steps_per_vol
 
 
 def hysteresis(nx=128, ny=128, nz=48, dxy=0.5e-9, v_amp=3.0, steps_per_leg=400, seed=1, extra=None) -> str:
-    """MFIM stack under a triangular sweep -v_amp -> +v_amp -> -v_amp (the
-    voltage schedule itself is driven through the API)."""
-    return mfim(nx, ny, nz, dxy, nsteps=4 * steps_per_leg, seed=seed, Phi_Bc_hi=-v_amp, extra=extra)
+    """MFIM stack under a triangular sweep -v_amp -> +v_amp -> -v_amp, one
+    leg per ramp (the voltage schedule itself is driven through the API)."""
+    return mfim(nx, ny, nz, dxy, nsteps=2 * steps_per_leg, seed=seed, Phi_Bc_hi=-v_amp, extra=extra)
 
 
 def _rng(seed: int):
@@ -170,9 +170,10 @@ def grain_fields(grains: dict):
 
 
 def triangular_sweep(v_amp: float, steps_per_leg: int) -> np.ndarray:
-    """Phi_Bc_hi per step: -v_amp -> +v_amp -> -v_amp, 2 legs up, 2 down."""
-    up = np.linspace(-v_amp, v_amp, 2 * steps_per_leg, endpoint=False)
-    down = np.linspace(v_amp, -v_amp, 2 * steps_per_leg, endpoint=False)
+    """Phi_Bc_hi per step: a leg of steps_per_leg steps from -v_amp to
+    +v_amp, then one back to -v_amp (2 * steps_per_leg values)."""
+    up = np.linspace(-v_amp, v_amp, steps_per_leg, endpoint=False)
+    down = np.linspace(v_amp, -v_amp, steps_per_leg, endpoint=False)
     return np.concatenate([up, down])
 
 

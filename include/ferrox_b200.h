@@ -149,6 +149,51 @@ enum fx_kernel_class {
 int fx_get_kernel_times(fx_ctx* ctx, double* ms, long long* counts, int n);
 int fx_reset_kernel_times(fx_ctx* ctx);
 
+/* ---- Gradients (no counterpart in the reference, which has no adjoint).
+ *
+ * A hysteresis loss over nsteps forward-Euler steps of the coupled step
+ * (main.cpp:261-306 without the sweep logic): at step n (1-based) the top
+ * electrode is held at Phi_Bc_hi = v_amp * v_shape[n-1], phi^n is solved
+ * from P^{n-1} (ComputePhi_Rho) and P^n = P^{n-1} + dt f (CalculateTDGL_RHS);
+ *     L = (1/nsteps) sum_n (<Pz>^n - target[n-1])^2,
+ * <Pz> the mean over the ferroelectric cells (mask 0).  fx_forward_record
+ * runs those steps from the context's current state, keeps FP64 checkpoints
+ * of P and phi every checkpoint_every steps, and returns L; fx_backward then
+ * recomputes each checkpoint segment and runs the hand-written adjoint (the
+ * transposed TDGL step, the Poisson adjoint solved by the same multigrid with
+ * rho'(phi) on the semiconductor cells) back to step 0.  Between the two calls
+ * nothing may change the context (no fx_step, fx_set_param, fx_set_field ...);
+ * after fx_backward the context holds the state at the end of the recorded
+ * steps again.  TimeIntegratorOrder 2 is not supported (FX_ERR_UNSUPPORTED).
+ */
+typedef struct fx_loss_spec {
+    int           nsteps;            /* >= 1 */
+    int           checkpoint_every;  /* k >= 1: P and phi kept at steps 0, k, 2k, ... */
+    double        v_amp;             /* volts */
+    const double* v_shape;           /* nsteps values, or NULL for all ones */
+    const double* target;            /* nsteps values of the target <Pz> (C/m^2) */
+} fx_loss_spec;
+
+/* gradient slots of fx_backward */
+enum fx_grad {
+    FX_GRAD_ALPHA = 0,   /* Landau alpha, over the cells that use the global alpha */
+    FX_GRAD_BETA,        /* Landau beta */
+    FX_GRAD_GAMMA,       /* Landau gamma */
+    FX_GRAD_G11,         /* gradient coefficient g11 */
+    FX_GRAD_G44,         /* gradient coefficient g44 */
+    FX_GRAD_V_AMP,       /* the voltage amplitude v_amp */
+    FX_GRAD_GRAIN_ALPHA  /* first of the per-grain alphas: slot 6 + g is dL/d alpha of grain g */
+};
+
+int fx_forward_record(fx_ctx* ctx, const fx_loss_spec* spec, double* loss);
+/* grads: ngrads >= 6 slots (enum fx_grad); with grains set, slots 6 .. 6 +
+ * ngrains - 1 receive the per-grain alpha gradients, further slots 0. */
+int fx_backward(fx_ctx* ctx, double* grads, int ngrads);
+/* dL/dP^0, the gradient with respect to the state fx_forward_record started
+ * from, after fx_backward.  With scalar polarization (is_polarization_scalar
+ * = 1 and Px = Py = 0) only dPz is available: pass NULL for dPx and dPy. */
+int fx_get_grad_P0(fx_ctx* ctx, double* dPx, double* dPy, double* dPz, size_t n);
+
 /* No counterpart in the reference.  fx_mean_P without any device allocation,
  * for callers that cannot call cudaMalloc where they need the number (memory
  * owned by another allocator, or code that must not synchronise the device).

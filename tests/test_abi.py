@@ -144,3 +144,30 @@ def test_odd_periodic_count_is_rejected():
     with pytest.raises(api.FxError) as e:
         api.FerroX(decks.mfim(9, 8, 12))
     assert e.value.code == -3
+
+
+def test_gradient_entry_points_check_arguments_before_any_device_work():
+    f = api.FerroX(decks.mfim(8, 8, 12))
+    with pytest.raises(api.FxError) as e:
+        f.backward()
+    assert e.value.code == -1 and "fx_forward_record" in str(e.value)
+    with pytest.raises(api.FxError) as e:
+        f.grad_P0()
+    assert e.value.code == -1
+    with pytest.raises(api.FxError) as e:
+        f.forward_record(np.zeros(0), 1.0)
+    assert e.value.code == -1
+    with pytest.raises(api.FxError) as e:
+        f.forward_record(np.array([0.0, np.nan]), 1.0)
+    assert e.value.code == -1
+    with pytest.raises(api.FxError) as e:
+        f.forward_record(np.zeros(4), 1.0, checkpoint_every=0)
+    assert e.value.code == -1
+    g = api.FerroX(decks.mfim(8, 8, 12, extra={"TimeIntegratorOrder": 2}))
+    with pytest.raises(api.FxError) as e:
+        g.forward_record(np.zeros(4), 1.0)
+    assert e.value.code == -3
+    h = api.FerroX(decks.mfim(4, 4, 12))
+    with pytest.raises(api.FxError) as e:
+        h.forward_record(np.zeros(4), 1.0)
+    assert e.value.code == -3

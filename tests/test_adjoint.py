@@ -1,0 +1,223 @@
+"""Gradients of the hysteresis loss (fx_forward_record / fx_backward) against
+central finite differences of the forward run, h = 1e-6 relative, and the
+mixed-precision adjoint against the FP64 one.
+
+The loss is L = mean_n (<Pz>^n - target_n)^2 over a triangular sweep of the
+top electrode.  The FD checks need a forward map that is smooth to ~1e-15:
+the multigrid runs to 1e-13 relative and, with a semiconductor, the Newton
+loop to 1e-11 (the adjoint is the implicit-function gradient of a converged
+solve).
+
+A central difference with step h carries a roundoff error of about
+eps_L L / (h |theta dL/dtheta|), eps_L ~ 1e-15 the relative noise of the loss
+(an FP64 sum over the FE cells, per step).  At the h = 1e-6 of the
+specification that error stays below 1e-6 only for parameters whose relative
+sensitivity |theta dL/dtheta| / L is at least 1e-3; those are held to the
+1e-5 bar at h = 1e-6 (SPEC_H).  Every parameter is also held to 1e-5 at
+h = 1e-3 (WIDE_H), where the roundoff error is below 1e-7 and the truncation
+error of the difference below 3e-6 on these runs.
+"""
+import numpy as np
+import pytest
+
+from adjoint_fn import loss_and_grad, loss_with
+from ferrox_b200 import api, decks
+from helpers import relerr
+
+pytestmark = pytest.mark.gpu
+
+FD_TOL = 1e-5          # at SPEC_H
+SPEC_H = 1e-6
+WIDE_TOL = 1e-5        # at WIDE_H
+WIDE_H = 1e-3
+MIN_SENS = 1e-3        # |theta dL/dtheta| / L needed for the SPEC_H check
+
+
+def fd_ok(adj, L, x, loss_at):
+    """Check one derivative: loss_at(dx) is the loss with the parameter moved
+    by dx.  Returns the number of SPEC_H checks made (0 or 1)."""
+    n = 0
+    hs = [(WIDE_H, WIDE_TOL)]
+    if abs(x * adj) / L >= MIN_SENS:
+        hs.append((SPEC_H, FD_TOL))
+        n = 1
+    for h, tol in hs:
+        dx = h * abs(x)
+        fd = (loss_at(dx) - loss_at(-dx)) / (2 * dx)
+        assert abs(adj - fd) <= tol * abs(fd), (h, adj, fd, abs(adj - fd) / abs(fd))
+    return n
+
+
+def sweep(T, v_amp=1.0):
+    shape = decks.triangular_sweep(1.0, T // 2)
+    target = decks.target_loop(v_amp * shape, seed=7, ps=0.15, vc=0.4 * v_amp)
+    return shape, target
+
+
+def start_P(shape, seed, vector=False, scale=0.2):
+    g = np.random.default_rng(seed)
+    Pz = g.uniform(-scale, scale, shape)
+    if not vector:
+        return (None, None, Pz)
+    return (g.uniform(-scale, scale, shape), g.uniform(-scale, scale, shape), Pz)
+
+
+def maker(text, P, grains=None, precision=None, extra=None, grain_alpha=None):
+    def make():
+        f = api.FerroX(text, precision=precision)
+        if grains is not None:
+            f.set_grains(grains["id"], grains["angles"], grains["tphase"])
+            if grain_alpha is not None:
+                f.set_grain_alpha(grain_alpha)
+        # P lives in the ferroelectric, outside the t-phase, as in the reference
+        fe = (f.field("mask") == 0) & (f.field("tphase") == 0)
+        f.set_initial_P(*[None if a is None else np.where(fe, a, 0.0) for a in P])
+        f.set_param("fx.mg_rtol", 1e-13)
+        for k, v in (extra or {}).items():
+            f.set_param(k, v)
+        return f
+    return make
+
+
+def theta_of(make, v_amp):
+    f = make()
+    t = [f.param(k) for k in api.GRADS[:5]] + [v_amp]
+    f.close()
+    return t
+
+
+def check_fd(make, v_amp, T, k, which=range(6), min_spec=1):
+    shape, target = sweep(T, v_amp)
+    theta = theta_of(make, v_amp)
+    L, g = loss_and_grad(theta, make, target, shape, k)
+    assert np.isfinite(L) and L > 0
+    nspec = 0
+    for q in which:
+        def loss_at(dx, q=q):
+            return loss_with(theta, q, dx, make, target, shape, k)
+        try:
+            nspec += fd_ok(g[q], L, theta[q], loss_at)
+        except AssertionError as e:
+            raise AssertionError((api.GRADS[q],) + tuple(e.args)) from None
+    assert nspec >= min_spec
+    return g
+
+
+def test_fd_mfim_all_parameters():
+    # 5 nm HZO on 4 nm Al2O3, scalar Pz; 30 steps, checkpoints every 7
+    text = decks.mfim(16, 16, 12)
+    check_fd(maker(text, start_P((12, 16, 16), 1)), 2.0, 30, 7)
+
+
+def test_fd_mfim_ghost_modes_and_flags():
+    # face ghost for E and the lambda / zero P boundary forms
+    text = decks.mfim(16, 16, 12, extra={"fx.phi_ghost_mode": "face", "P_BC_flag_lo": [3, 3, 1],
+                                         "P_BC_flag_hi": [3, 3, 0]})
+    check_fd(maker(text, start_P((12, 16, 16), 2)), 1.5, 16, 5, which=[0, 3, 4, 5])
+
+
+def test_fd_vector_rotated_grains():
+    # three-component P with anisotropic couplings in rotated grains
+    text, g = decks.polycrystal(16, 16, 24, ngrains=6, seed=3, nsteps=10,
+                                extra={"is_polarization_scalar": 0, "alpha_12": 1.0e8, "alpha_112": 2.0e9,
+                                       "alpha_123": 3.0e9, "g12": 2.0e-11, "g44_p": 1.0e-11})
+    check_fd(maker(text, start_P((24, 16, 16), 3, vector=True), grains=g, extra={"BigGamma": 100.0}), 3.0, 20, 6)
+
+
+def test_fd_semiconductor_newton():
+    # MFISM stack: the Poisson adjoint carries rho'(phi) on the Si cells
+    text = decks.mfism(16, 16, 48)
+    make = maker(text, start_P((48, 16, 16), 4), extra={"fx.newton_tol": 1e-11})
+    check_fd(make, 0.8, 10, 4, which=[0, 3, 5])
+
+
+def test_fd_per_grain_alpha():
+    text, g = decks.polycrystal(16, 16, 24, ngrains=6, seed=5, nsteps=10)
+    ga = np.full(6, -2.5e9) * (1.0 + 0.1 * np.arange(6))
+    P = start_P((24, 16, 16), 6)
+    shape, target = sweep(12, 1.0)
+    f = maker(text, P, grains=g, grain_alpha=ga)()
+    L = f.forward_record(target, 1.0, shape, 5)
+    grads = f.backward(ngrains=6)
+    f.close()
+    fe = [q for q in range(6) if not g["tphase"][q]]
+    assert all(grads[6 + q] != 0 for q in fe)
+    assert all(grads[6 + q] == 0 for q in range(6) if g["tphase"][q])
+
+    def loss_at(dx, q):
+        a = ga.copy()
+        a[q] += dx
+        h = maker(text, P, grains=g, grain_alpha=a)()
+        v = h.forward_record(target, 1.0, shape, 5)
+        h.close()
+        return v
+    for q in fe[:3]:
+        fd_ok(grads[6 + q], L, ga[q], lambda dx: loss_at(dx, q))
+
+
+def test_grad_P0_matches_fd():
+    text = decks.mfim(16, 16, 12)
+    P = start_P((12, 16, 16), 7)
+    shape, target = sweep(10, 1.0)
+    f = maker(text, P)()
+    L = f.forward_record(target, 1.0, shape, 4)
+    f.backward()
+    dP = f.grad_P0()["Pz"]
+    f.close()
+
+    def loss_at(dx, cell):
+        Pz = P[2].copy()
+        Pz[cell] += dx
+        h = maker(text, (None, None, Pz))()
+        v = h.forward_record(target, 1.0, shape, 4)
+        h.close()
+        return v
+    # FE cells at the DE interface, inside and at the top electrode
+    for cell in [(5, 3, 4), (8, 9, 10), (11, 0, 15)]:
+        fd_ok(dP[cell], L, P[2][cell], lambda dx: loss_at(dx, cell))
+
+
+def test_mixed_adjoint_vs_fp64():
+    text = decks.mfim(32, 32, 12)
+    P = start_P((12, 32, 32), 8)
+    shape, target = sweep(20, 2.0)
+    g = {}
+    for prec in ("fp64", "mixed"):
+        f = maker(text, P, precision=prec)()
+        f.set_param("fx.mg_rtol", 1e-10)
+        f.forward_record(target, 2.0, shape, 6)
+        g[prec] = f.backward()
+        f.close()
+    for q in range(6):
+        assert abs(g["mixed"][q] - g["fp64"][q]) <= 1e-4 * abs(g["fp64"][q]), (api.GRADS[q], g["mixed"][q], g["fp64"][q])
+
+
+def test_backward_restores_state_and_repeats():
+    text = decks.mfim(16, 16, 12)
+    f = maker(text, start_P((12, 16, 16), 9))()
+    shape, target = sweep(14, 1.0)
+    L = f.forward_record(target, 1.0, shape, 3)
+    end = f.field("Pz"), f.field("Phi")
+    g1 = f.backward()
+    assert np.array_equal(f.field("Pz"), end[0]) and np.array_equal(f.field("Phi"), end[1])
+    g2 = f.backward()
+    assert np.allclose(g1, g2, rtol=1e-12, atol=0)
+    assert f.param("adjoint_loss") == L
+    f.step(1)
+    with pytest.raises(api.FxError):
+        f.backward()
+    f.close()
+
+
+def test_checkpoint_interval_does_not_change_gradient():
+    text = decks.mfim(16, 16, 12)
+    P = start_P((12, 16, 16), 10)
+    shape, target = sweep(12, 1.0)
+    out = []
+    for k in (1, 5, 12, 50):
+        f = maker(text, P)()
+        f.forward_record(target, 1.0, shape, k)
+        out.append(f.backward())
+        f.close()
+    for g in out[1:]:
+        assert relerr(g, out[0]) < 1e-12
