@@ -120,8 +120,8 @@ def algorithmic_bytes(kernel: str, N: int, Nc1: int, sc: bool, scalar: bool, rot
         return N * (fp + fp + 1 + fp + a) / 2.0
     if kernel == "restrict_l0":
         return N * (fp + fp + 1 + a) + Nc1 * fp
-    if kernel == "prolong_l0":
-        return N * 2 * fp + Nc1 * fp
+    if kernel == "prolong_l0":     # x in and out, the coarse correction, one weight per fine cell
+        return N * 2 * fp + Nc1 * fp + N * 4
     if kernel == "tdgl":
         return N * ((3 if scalar else 7) * 8 + 1 + (1 if rot else 0))
     if kernel == "newton":

@@ -9,6 +9,7 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -37,19 +38,23 @@ def _run(cmd: list[str], verbose: bool) -> None:
 def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(OBJ, exist_ok=True)
     hdrs = [os.path.join(CSRC, h) for h in HDR] + [os.path.join(HERE, "..", "include", "ferrox_b200.h")]
-    objs = []
+    objs, jobs = [], []
     for src in CU:
         s = os.path.join(CSRC, src)
         o = os.path.join(OBJ, src + ".o")
         if force or not _newer(o, [s] + hdrs):
-            _run([NVCC] + NVFLAGS + ["-c", s, "-o", o], verbose)
+            jobs.append([NVCC] + NVFLAGS + ["-c", s, "-o", o])
         objs.append(o)
     for src in CPP:
         s = os.path.join(CSRC, src)
         o = os.path.join(OBJ, src + ".o")
         if force or not _newer(o, [s] + hdrs):
-            _run(["g++", "-O2", "-std=c++17", "-fPIC", "-Wall", "-c", s, "-o", o], verbose)
+            jobs.append(["g++", "-O2", "-std=c++17", "-fPIC", "-Wall", "-c", s, "-o", o])
         objs.append(o)
+    # the translation units are independent: compile them side by side
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(_run, cmd, verbose) for cmd in jobs]:
+            f.result()
     if force or not _newer(LIB, objs):
         _run([NVCC] + ARCH + ["-shared", "-o", LIB + ".tmp"] + objs + ["-lpthread", "-ldl", "-lrt"], verbose)
         os.replace(LIB + ".tmp", LIB)

@@ -321,13 +321,14 @@ constexpr int MAXLEV = 24;
 struct CoarseLevelDesc {
     int nx, ny, nz, N, rx, ry, rz, line;   // r*: ratio to the next (coarser) level
     double ihx, ihy, ihz;
-    long long ox, ob, obw, obs, obb, oa, oq, oi;   // offsets (elements of T) in shared memory
+    long long ox, ob, obw, obs, obb, oa, oq, oi, op;   // offsets (elements of T) in shared memory
     long long ow[3];                            // offsets (floats) of the prolongation weights into this level
     const void* gbw;
     const void* gbs;
     const void* gbb;
     const void* ga;
     const float* gw[3];
+    void* gf[3];                                // global copies of q, 1/pivot, cb/pivot
 };
 
 struct CoarseArgs {
@@ -336,6 +337,7 @@ struct CoarseArgs {
     long long wbase;                 // byte offset of the float region
     const void* b_in;                // right-hand side of the top level (global)
     void* x_out;                     // solution of the top level (global)
+    int* fvalid;                     // the factors in gf are current (else computed and stored)
     CoarseLevelDesc L[MAXLEV];
 };
 
@@ -343,7 +345,7 @@ template <typename T>
 struct SV {
     int nx, ny, nz, N, nxy;
     T ihx, ihy, ihz;
-    T *x, *b, *bw, *bs, *bb, *a, *q, *inv;
+    T *x, *b, *bw, *bs, *bb, *a, *q, *inv, *p;
 };
 
 template <typename T>
@@ -355,6 +357,7 @@ __device__ __forceinline__ SV<T> sview(const CoarseLevelDesc& d, T* sm) {
     v.a = d.oa >= 0 ? sm + d.oa : nullptr;
     v.q = d.oq >= 0 ? sm + d.oq : nullptr;
     v.inv = sm + d.oi;
+    v.p = d.op >= 0 ? sm + d.op : nullptr;
     return v;
 }
 
@@ -376,9 +379,9 @@ __device__ __forceinline__ void s_coeffs(const SV<T>& o, int i, int j, int k, in
     diag = -a + cw + ce + cs + cn + cb + ct + extra;
 }
 
-// factor each z-line once per call (q_k = ct_k / den_k, inv_k = 1 / den_k;
-// stored in q and inv), or invert the point diagonal; the sweeps then need no
-// division
+// factor each z-line (den_k = diag_k - cb_k q_{k-1}: q_k = ct_k / den_k,
+// inv_k = 1 / den_k, p_k = cb_k / den_k), or invert the point diagonal; the
+// sweeps then need no division.  Recomputed only when alpha changes.
 template <typename T>
 __device__ void s_factor(const SV<T>& o, bool line) {
     if (line) {
@@ -393,6 +396,7 @@ __device__ void s_factor(const SV<T>& o, bool line) {
                 const T inv = T(1) / (diag - cb * qprev);
                 o.q[c] = ct * inv;
                 o.inv[c] = inv;
+                o.p[c] = cb * inv;
                 qprev = o.q[c];
             }
         }
@@ -413,29 +417,36 @@ __device__ void s_smooth(const SV<T>& o, bool line, int sweeps) {
     for (int sw = 0; sw < sweeps; ++sw)
         for (int color = 0; color < 2; ++color) {
             if (line) {
-                const int ncol = o.nxy;
-                for (int col = threadIdx.x; col < ncol; col += nt) {
-                    const int i = col % o.nx, j = col / o.nx;
+                // the colour's columns in two phases: (1) every cell's
+                // right-hand side with the x/y neighbours (the other colour),
+                // scaled by 1/pivot, in parallel; (2) per column the
+                // recurrences d_k = g_k + p_k d_{k-1}, x_k = d_k + q_k x_{k+1}
+                for (int c = threadIdx.x; c < o.N; c += nt) {
+                    const int i = c % o.nx, j = (c / o.nx) % o.ny;
                     if (((i + j) & 1) != color) continue;
                     const int im = i == 0 ? o.nx - 1 : i - 1, ip = i == o.nx - 1 ? 0 : i + 1;
                     const int jm = j == 0 ? o.ny - 1 : j - 1, jp = j == o.ny - 1 ? 0 : j + 1;
-                    T dprev = T(0);
+                    const int row = c - i;
+                    T cw = o.bw[c] * o.ihx, ce = o.bw[row + ip] * o.ihx;
+                    T cs = o.bs[c] * o.ihy, cn = o.bs[c + (jp - j) * o.nx] * o.ihy;
+                    if (o.nx == 1) { cw = T(0); ce = T(0); }
+                    if (o.ny == 1) { cs = T(0); cn = T(0); }
+                    const T r = o.b[c] + cw * o.x[row + im] + ce * o.x[row + ip] + cs * o.x[c + (jm - j) * o.nx] +
+                                cn * o.x[c + (jp - j) * o.nx];
+                    o.x[c] = r * o.inv[c];
+                }
+                __syncthreads();
+                for (int col = threadIdx.x; col < o.nxy; col += nt) {
+                    const int i = col % o.nx, j = col / o.nx;
+                    if (((i + j) & 1) != color) continue;
                     int c = col;
-                    for (int k = 0; k < o.nz; ++k, c += o.nxy) {
-                        const int row = c - i;
-                        T cw = o.bw[c] * o.ihx, ce = o.bw[row + ip] * o.ihx;
-                        T cs = o.bs[c] * o.ihy, cn = o.bs[c + (jp - j) * o.nx] * o.ihy;
-                        if (o.nx == 1) { cw = T(0); ce = T(0); }
-                        if (o.ny == 1) { cs = T(0); cn = T(0); }
-                        const T cb = k > 0 ? o.bb[c] * o.ihz : T(0);
-                        const T r = o.b[c] + cw * o.x[row + im] + ce * o.x[row + ip] + cs * o.x[c + (jm - j) * o.nx] +
-                                    cn * o.x[c + (jp - j) * o.nx];
-                        const T dk = (r + cb * dprev) * o.inv[c];
-                        o.x[c] = dk;
-                        dprev = dk;
+                    T d = o.x[c];
+                    for (int k = 1; k < o.nz; ++k) {
+                        c += o.nxy;
+                        d = o.x[c] + o.p[c] * d;
+                        o.x[c] = d;
                     }
-                    c -= o.nxy;
-                    T xn = o.x[c];
+                    T xn = d;
                     for (int k = o.nz - 2; k >= 0; --k) {
                         c -= o.nxy;
                         xn = o.x[c] + o.q[c] * xn;
@@ -514,12 +525,27 @@ __device__ void s_prolong(const SV<T>& f, const SV<T>& c, int rx, int ry, int rz
     __syncthreads();
 }
 
+// one element global -> shared without waiting (cp.async, 4 or 8 bytes)
+template <typename E>
+__device__ __forceinline__ void cp_async_el(E* dst, const E* src) {
+    static_assert(sizeof(E) == 4 || sizeof(E) == 8, "cp.async element size");
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    if (sizeof(E) == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+    else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+
 template <typename T>
 __global__ void __launch_bounds__(1024) k_coarse_vcycle(CoarseArgs A) {
     extern __shared__ __align__(16) unsigned char smraw[];
+    __shared__ int s_valid;
     T* sm = reinterpret_cast<T*>(smraw);
     float* sw = reinterpret_cast<float*>(smraw + A.wbase);
-    // load coefficients and the top right-hand side
+    if (threadIdx.x == 0) s_valid = *(volatile int*)A.fvalid;
+    __syncthreads();
+    const bool valid = s_valid != 0;
+    // load coefficients and the top right-hand side: every copy is issued
+    // asynchronously (cp.async) before the block waits once, so the levels'
+    // global reads overlap instead of costing one round trip each
     for (int l = 0; l < A.nlev; ++l) {
         const CoarseLevelDesc& d = A.L[l];
         const int nxy = d.nx * d.ny;
@@ -528,23 +554,42 @@ __global__ void __launch_bounds__(1024) k_coarse_vcycle(CoarseArgs A) {
         const T* gbb = (const T*)d.gbb;
         const T* ga = (const T*)d.ga;
         for (int c = threadIdx.x; c < d.N; c += blockDim.x) {
-            sm[d.obw + c] = gbw[c];
-            sm[d.obs + c] = gbs[c];
-            if (d.oa >= 0) sm[d.oa + c] = ga[c];
+            cp_async_el(sm + d.obw + c, gbw + c);
+            cp_async_el(sm + d.obs + c, gbs + c);
+            if (d.oa >= 0) cp_async_el(sm + d.oa + c, ga + c);
             sm[d.ox + c] = T(0);
         }
-        for (int c = threadIdx.x; c < d.N + nxy; c += blockDim.x) sm[d.obb + c] = gbb[c];
+        for (int c = threadIdx.x; c < d.N + nxy; c += blockDim.x) cp_async_el(sm + d.obb + c, gbb + c);
         for (int q = 0; q < 3; ++q)
             if (d.gw[q])
-                for (int c = threadIdx.x; c < d.N; c += blockDim.x) sw[d.ow[q] + c] = d.gw[q][c];
+                for (int c = threadIdx.x; c < d.N; c += blockDim.x) cp_async_el(sw + d.ow[q] + c, d.gw[q] + c);
+        if (valid) {
+            const long long fo[3] = {d.oq, d.oi, d.op};
+            for (int q = 0; q < 3; ++q)
+                if (fo[q] >= 0)
+                    for (int c = threadIdx.x; c < d.N; c += blockDim.x) cp_async_el(sm + fo[q] + c, (const T*)d.gf[q] + c);
+        }
     }
     {
         const T* b_in = (const T*)A.b_in;
-        for (int c = threadIdx.x; c < A.L[0].N; c += blockDim.x) sm[A.L[0].ob + c] = b_in[c];
+        for (int c = threadIdx.x; c < A.L[0].N; c += blockDim.x) cp_async_el(sm + A.L[0].ob + c, b_in + c);
     }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncthreads();
-    for (int l = 0; l < A.nlev; ++l) s_factor(sview<T>(A.L[l], sm), A.L[l].line != 0);
-    __syncthreads();
+    if (!valid) {
+        // first call since alpha changed: factor, and keep the factors for
+        // the next calls (visible to them at the kernel boundary)
+        for (int l = 0; l < A.nlev; ++l) s_factor(sview<T>(A.L[l], sm), A.L[l].line != 0);
+        __syncthreads();
+        for (int l = 0; l < A.nlev; ++l) {
+            const CoarseLevelDesc& d = A.L[l];
+            const long long fo[3] = {d.oq, d.oi, d.op};
+            for (int q = 0; q < 3; ++q)
+                if (fo[q] >= 0)
+                    for (int c = threadIdx.x; c < d.N; c += blockDim.x) ((T*)d.gf[q])[c] = sm[fo[q] + c];
+        }
+        if (threadIdx.x == 0) *A.fvalid = 1;
+    }
     // V-cycle over the shared-memory levels
     for (int l = 0; l < A.nlev - 1; ++l) {
         const SV<T> f = sview<T>(A.L[l], sm), c = sview<T>(A.L[l + 1], sm);
@@ -645,8 +690,9 @@ Multigrid::~Multigrid() {
         if (l > 0) { cudaFree(L.x64); cudaFree(L.b64); cudaFree(L.x32); cudaFree(L.b32); }
         cudaFree(L.bw64); cudaFree(L.bs64); cudaFree(L.bb64); cudaFree(L.a64); cudaFree(L.cp64);
         cudaFree(L.bw32); cudaFree(L.bs32); cudaFree(L.bb32); cudaFree(L.a32); cudaFree(L.cp32);
-        for (int d = 0; d < 3; ++d) cudaFree(L.wf[d]);
+        for (int d = 0; d < 3; ++d) { cudaFree(L.wf[d]); cudaFree(L.fac64[d]); cudaFree(L.fac32[d]); }
     }
+    cudaFree(d_fvalid_);
     if (g64_.exec) cudaGraphExecDestroy(g64_.exec);
     if (g32_.exec) cudaGraphExecDestroy(g32_.exec);
     cudaFree(d_norm_);
@@ -678,7 +724,11 @@ int Multigrid::setup(const DevParams& p, const std::vector<uint8_t>& code, bool 
         } else {
             for (int d = 0; d < 2; ++d)
                 if (coarsenable_xy(f.n[d])) cr[d] = 2;
-            f.line = true;
+            // z-lines where z is the strongly coupled direction, and on the
+            // bottom level (an exact solve when it is one column); a level
+            // that keeps z only because nz is odd but is isotropic takes
+            // point red-black sweeps
+            f.line = (cr[0] == 1 && cr[1] == 1) || 1.5 * f.h[2] < std::min(f.h[0], f.h[1]);
             if (cr[0] == 1 && cr[1] == 1) break;   // bottom
         }
         MGLevel c{};
@@ -847,6 +897,8 @@ int Multigrid::setup(const DevParams& p, const std::vector<uint8_t>& code, bool 
 }
 
 int Multigrid::set_alpha(const double* a64, const float* a32, bool has_alpha, cudaStream_t s) {
+    // the one-CTA factors depend on alpha: recompute them at the next call
+    if ((has_alpha || has_alpha_) && d_fvalid_) cudaMemsetAsync(d_fvalid_, 0, 2 * sizeof(int), s);
     a0_64 = a64;
     a0_32 = a32;
     has_alpha_ = has_alpha;
@@ -873,7 +925,7 @@ static size_t coarse_bytes(const std::vector<MGLevel>& lev, int top, size_t es, 
     size_t t = 0, w = 0;
     for (size_t l = top; l < lev.size(); ++l) {
         const size_t N = lev[l].N, nxy = (size_t)lev[l].n[0] * lev[l].n[1];
-        t += (7 * N + nxy) * es + (lev[l].line ? N * es : 0);
+        t += (7 * N + nxy) * es + (lev[l].line ? 2 * N * es : 0);
         if (l + 1 < lev.size())
             for (int d = 0; d < 3; ++d) if (lev[l + 1].cr[d] == 2) w += N;
     }
@@ -883,7 +935,7 @@ static size_t coarse_bytes(const std::vector<MGLevel>& lev, int top, size_t es, 
 }
 
 void Multigrid::plan_coarse(bool want64, bool want32) {
-    constexpr size_t budget = 200 * 1024;
+    constexpr size_t budget = 227 * 1024;   // the sm_100 per-block maximum of dynamic shared memory
     coarse_top64_ = coarse_top32_ = -1;
     for (int top = 1; top < (int)lev_.size(); ++top) {
         if (want64 && coarse_top64_ < 0 && coarse_bytes(lev_, top, 8, nullptr) <= budget) {
@@ -899,6 +951,17 @@ void Multigrid::plan_coarse(bool want64, bool want32) {
         cudaFuncSetAttribute(k_coarse_vcycle<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coarse_smem64_);
     if (coarse_top32_ > 0)
         cudaFuncSetAttribute(k_coarse_vcycle<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coarse_smem32_);
+    // global copies of the one-CTA levels' smoother factors (q and p only on
+    // z-line levels), and the flags that say whether they are current
+    for (int l = 0; l < (int)lev_.size(); ++l) {
+        MGLevel& L = lev_[l];
+        const size_t n[3] = {L.line ? L.N : 0, L.N, L.line ? L.N : 0};
+        for (int k = 0; k < 3; ++k) {
+            if (coarse_top64_ > 0 && l >= coarse_top64_ && n[k]) L.fac64[k] = dalloc<double>(n[k], bytes_);
+            if (coarse_top32_ > 0 && l >= coarse_top32_ && n[k]) L.fac32[k] = dalloc<float>(n[k], bytes_);
+        }
+    }
+    if (cudaMalloc(&d_fvalid_, 2 * sizeof(int)) == cudaSuccess) cudaMemset(d_fvalid_, 0, 2 * sizeof(int));
 }
 
 template <> int Multigrid::coarse_top<double>() const { return coarse_top64_; }
@@ -916,6 +979,7 @@ void Multigrid::launch_coarse(int top, cudaStream_t s) {
     A.wbase = (long long)wbase;
     A.b_in = lb<T>(lev_[top]);
     A.x_out = lx<T>(lev_[top]);
+    A.fvalid = d_fvalid_ + (sizeof(T) == 8 ? 0 : 1);
     long long off = 0, woff = 0;
     for (int q = 0; q < A.nlev; ++q) {
         MGLevel& L = lev_[top + q];
@@ -930,7 +994,12 @@ void Multigrid::launch_coarse(int top, cudaStream_t s) {
         d.obb = off; off += N + nxy;
         d.oa = has_alpha_ ? off : -1; off += N;
         d.oq = L.line ? off : -1; off += L.line ? N : 0;
+        d.op = L.line ? off : -1; off += L.line ? N : 0;
         d.oi = off; off += N;
+        for (int k = 0; k < 3; ++k) {
+            if constexpr (sizeof(T) == 8) d.gf[k] = L.fac64[k];
+            else d.gf[k] = L.fac32[k];
+        }
         if constexpr (sizeof(T) == 8) { d.gbw = L.bw64; d.gbs = L.bs64; d.gbb = L.bb64; d.ga = has_alpha_ ? L.a64 : nullptr; }
         else { d.gbw = L.bw32; d.gbs = L.bs32; d.gbb = L.bb32; d.ga = has_alpha_ ? L.a32 : nullptr; }
         if (top + q + 1 < (int)lev_.size()) {

@@ -33,6 +33,10 @@ struct MGLevel {
     // device storage, FP64 and FP32 copies
     double *x64 = nullptr, *b64 = nullptr, *bw64 = nullptr, *bs64 = nullptr, *bb64 = nullptr, *a64 = nullptr, *cp64 = nullptr;
     float *x32 = nullptr, *b32 = nullptr, *bw32 = nullptr, *bs32 = nullptr, *bb32 = nullptr, *a32 = nullptr, *cp32 = nullptr;
+    // smoother factors of the one-CTA levels (q, 1/pivot, cb/pivot), FP64 and
+    // FP32, kept between calls while alpha is unchanged
+    double* fac64[3] = {nullptr, nullptr, nullptr};
+    float* fac32[3] = {nullptr, nullptr, nullptr};
 };
 
 // Optional per-launch timing: CUDA events around each launch of a kernel
@@ -134,6 +138,7 @@ private:
     bool use_graphs_ = true;
     template <typename F> int replay(GraphCache& g, const void* x, const void* rhs, const DevParams& p, cudaStream_t s, F&& enqueue);
     int coarse_top64_ = -1, coarse_top32_ = -1;   // first level run by the one-CTA kernel
+    int* d_fvalid_ = nullptr;    // [0] FP64, [1] FP32: the one-CTA factors in global memory are current
     size_t coarse_smem64_ = 0, coarse_smem32_ = 0;
     void plan_coarse(bool want64, bool want32);
     double slots_max() const;
