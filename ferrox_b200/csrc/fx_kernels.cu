@@ -256,13 +256,16 @@ __global__ void __launch_bounds__(256) k_newton(DevParams p, const uint8_t* __re
                                                 float* __restrict__ alpha32, double* __restrict__ rhs,
                                                 double* __restrict__ norms) {
     __shared__ double sh[32];
+    __shared__ double seps[8];
     const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+    if (tid == 0)
+#pragma unroll
+        for (int q = 0; q < 8; ++q) seps[q] = p.eps[q];
+    __syncthreads();
     double nb = 0.0, nbp = 0.0;
     for (long long c = (long long)blockIdx.x * 256 + tid; c < p.N; c += (long long)gridDim.x * 256) {
-        const int i = (int)(c % p.nx);
-        const int j = (int)((c / p.nx) % p.ny);
-        const int k = (int)(c / p.nxy);
-        const int m = mcode(code, p, i, j, k);
+        // the code array carries one z ghost layer below: cell c is at c + nxy
+        const int m = __ldg(code + c + p.nxy);
         const int mask = m & 3;
         double a = 0.0, v;
         if (mask >= 2) {
@@ -281,9 +284,8 @@ __global__ void __launch_bounds__(256) k_newton(DevParams p, const uint8_t* __re
         rhs[c] = v;
         nb = fmax(nb, fabs(v));
         double bp = v;
-        const double eps = p.eps[m & 7];
-        if (k == 0) bp += 2.0 * eps * p.ih2[2] * p.V_lo;
-        if (k == p.nz - 1) bp += 2.0 * eps * p.ih2[2] * p.V_hi;
+        if (c < p.nxy) bp += 2.0 * seps[m & 7] * p.ih2[2] * p.V_lo;             // k == 0
+        if (c >= p.N - p.nxy) bp += 2.0 * seps[m & 7] * p.ih2[2] * p.V_hi;      // k == nz - 1
         nbp = fmax(nbp, fabs(bp));
     }
     const double x = block_max(nb, sh);
@@ -306,10 +308,7 @@ __global__ void __launch_bounds__(256) k_rho(DevParams p, const uint8_t* __restr
     __shared__ bool last;
     double s1 = 0.0, s2 = 0.0;
     for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < p.N; c += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(c % p.nx);
-        const int j = (int)((c / p.nx) % p.ny);
-        const int k = (int)(c / p.nxy);
-        const int m = mcode(code, p, i, j, k) & 3;
+        const int m = __ldg(code + c + p.nxy) & 3;   // code has one z ghost layer below
         const double ph = phi[c];
         if (m >= 2) {
             double e, h;
