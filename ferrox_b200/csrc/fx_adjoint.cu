@@ -27,6 +27,7 @@
 #include "fx_kernels.h"
 
 #include <cmath>
+#include <utility>
 
 namespace fx {
 
@@ -117,22 +118,50 @@ __device__ __forceinline__ void load_lam(const DevParams& p, const double* __res
 // offsets (di, dj, dk) of the cells whose TDGL stencil reads a given cell:
 // the 13 axis offsets up to 2 (second derivatives, incl. the one-sided
 // forms), then the 12 plane diagonals (mixed derivatives)
-__constant__ int8_t c_off[25][3] = {
+constexpr int kOff[25][3] = {
     {0, 0, 0},  {1, 0, 0},  {-1, 0, 0}, {2, 0, 0},  {-2, 0, 0}, {0, 1, 0},  {0, -1, 0}, {0, 2, 0},  {0, -2, 0},
     {0, 0, 1},  {0, 0, -1}, {0, 0, 2},  {0, 0, -2}, {1, 1, 0},  {1, -1, 0}, {-1, 1, 0}, {-1, -1, 0}, {1, 0, 1},
     {1, 0, -1}, {-1, 0, 1}, {-1, 0, -1}, {0, 1, 1}, {0, 1, -1}, {0, -1, 1}, {0, -1, -1}};
 
+// which stencils evaluated at a cell c can read the cell c + (DI, DJ, DK):
+// a second derivative along an axis reads up to two cells along it, a mixed
+// one the first-derivative stencil (one cell along its axis) one cell to
+// either side, a first derivative one cell along its axis
+template <int DI, int DJ, int DK>
+struct Reach {
+    static constexpr bool xx = DJ == 0 && DK == 0;
+    static constexpr bool yy = DI == 0 && DK == 0;
+    static constexpr bool zz = DI == 0 && DJ == 0;
+    static constexpr bool xy = (DI == 1 || DI == -1) && DK == 0;
+    static constexpr bool xz = (DI == 1 || DI == -1) && DJ == 0;
+    static constexpr bool yz = (DJ == 1 || DJ == -1) && DI == 0;
+    static constexpr bool dx = DJ == 0 && DK == 0 && DI >= -1 && DI <= 1;
+    static constexpr bool dy = DI == 0 && DK == 0 && DJ >= -1 && DJ <= 1;
+    static constexpr bool dz = DI == 0 && DJ == 0 && DK >= -1 && DK <= 1;
+    static constexpr bool gx = (DI == 1 || DI == -1) && DJ == 0 && DK == 0;   // central phi differences
+    static constexpr bool gy = (DJ == 1 || DJ == -1) && DI == 0 && DK == 0;
+    static constexpr bool gz = DI == 0 && DJ == 0;
+};
+
 // sum_a lambda_a d g_a(c) / d P_B(c') for the gradient-energy parts g_a of
-// TotalEnergyDensity.cpp:133-251 (as in k_tdgl), D the impulse at c'
-template <typename T, bool VEC, bool ROT, int B>
+// TotalEnergyDensity.cpp:133-251 (as in k_tdgl), D the impulse at c' =
+// c + (DI, DJ, DK); stencils that cannot reach c' are skipped (they are zero)
+template <typename T, bool VEC, bool ROT, int B, int DI, int DJ, int DK>
 __device__ __forceinline__ T grad_rows_T(const DevParams& p, const MView& M, const T* R, const T lam[3],
                                          const DeltaView<T>& D, int i, int j, int k) {
+    using Rc = Reach<DI, DJ, DK>;
     const T g11 = T(p.g11), g44 = T(p.g44), g44p = T(p.g44p), g12 = T(p.g12);
     T s = T(0);
-    if (B == 2) {
-        const Hess<T> H = hess<T, ROT>(D, M, i, j, k);
+    if constexpr (B == 2) {
+        Hess<T> H;
+        H.xx = Rc::xx ? ddpd<0, T>(D, M, i, j, k) : T(0);
+        H.yy = Rc::yy ? ddpd<1, T>(D, M, i, j, k) : T(0);
+        H.zz = Rc::zz ? ddpd<2, T>(D, M, i, j, k) : T(0);
         T A11, A44;
-        if (ROT) {
+        if constexpr (ROT) {
+            H.xy = Rc::xy ? dxdy<T>(D, M, i, j, k) : T(0);
+            H.yz = Rc::yz ? dydz<T>(D, M, i, j, k) : T(0);
+            H.xz = Rc::xz ? dxdz<T>(D, M, i, j, k) : T(0);
             A11 = rot_quad(R, 2, H);
             A44 = rot_quad(R, 0, H) + rot_quad(R, 1, H);
         } else {
@@ -140,18 +169,24 @@ __device__ __forceinline__ T grad_rows_T(const DevParams& p, const MView& M, con
             A44 = H.xx + H.yy;
         }
         s = lam[2] * (-g11 * A11 - (g44 - g44p) * A44);
-        if (VEC) {
-            s += lam[0] * (-(g12 + g44 - g44p) * dxdz<T>(D, M, i, j, k));
-            s += lam[1] * (-(g12 + g44 - g44p) * dydz<T>(D, M, i, j, k));
+        if constexpr (VEC) {
+            if constexpr (Rc::xz) s += lam[0] * (-(g12 + g44 - g44p) * dxdz<T>(D, M, i, j, k));
+            if constexpr (Rc::yz) s += lam[1] * (-(g12 + g44 - g44p) * dydz<T>(D, M, i, j, k));
         }
-    } else if (B == 0) {
-        s = lam[2] * (-(g44 + g44p + g12) * dxdz<T>(D, M, i, j, k));
-        s += lam[0] * (-g11 * ddpd<0, T>(D, M, i, j, k) - (g44 + g44p) * (ddpd<1, T>(D, M, i, j, k) + ddpd<2, T>(D, M, i, j, k)));
-        s += lam[1] * (-(g12 + g44 + g44p) * dxdy<T>(D, M, i, j, k));
+    } else if constexpr (B == 0) {
+        if constexpr (Rc::xz) s += lam[2] * (-(g44 + g44p + g12) * dxdz<T>(D, M, i, j, k));
+        const T pxx = Rc::xx ? ddpd<0, T>(D, M, i, j, k) : T(0);
+        const T pyy = Rc::yy ? ddpd<1, T>(D, M, i, j, k) : T(0);
+        const T pzz = Rc::zz ? ddpd<2, T>(D, M, i, j, k) : T(0);
+        s += lam[0] * (-g11 * pxx - (g44 + g44p) * (pyy + pzz));
+        if constexpr (Rc::xy) s += lam[1] * (-(g12 + g44 + g44p) * dxdy<T>(D, M, i, j, k));
     } else {
-        s = lam[2] * (-(g44 + g44p + g12) * dydz<T>(D, M, i, j, k));
-        s += lam[0] * (-(g12 + g44 - g44p) * dxdy<T>(D, M, i, j, k));
-        s += lam[1] * (-g11 * ddpd<1, T>(D, M, i, j, k) - (g44 - g44p) * (ddpd<0, T>(D, M, i, j, k) + ddpd<2, T>(D, M, i, j, k)));
+        if constexpr (Rc::yz) s += lam[2] * (-(g44 + g44p + g12) * dydz<T>(D, M, i, j, k));
+        if constexpr (Rc::xy) s += lam[0] * (-(g12 + g44 - g44p) * dxdy<T>(D, M, i, j, k));
+        const T qxx = Rc::xx ? ddpd<0, T>(D, M, i, j, k) : T(0);
+        const T qyy = Rc::yy ? ddpd<1, T>(D, M, i, j, k) : T(0);
+        const T qzz = Rc::zz ? ddpd<2, T>(D, M, i, j, k) : T(0);
+        s += lam[1] * (-g11 * qyy - (g44 - g44p) * (qxx + qzz));
     }
     return s;
 }
@@ -165,6 +200,136 @@ __device__ __forceinline__ void landau_jac(const DevParams& p, T alpha, T a, T b
          T(12) * a112 * a2 * (b2 + c2) + T(2) * a112 * (b2 * b2 + c2 * c2) + T(2) * a123 * b2 * c2;
     Jb = T(4) * a12 * a * b + T(8) * a112 * a2 * a * b + T(8) * a112 * a * b2 * b + T(4) * a123 * a * b * c2;
     Jc = T(4) * a12 * a * c + T(8) * a112 * a2 * a * c + T(8) * a112 * a * c2 * c + T(4) * a123 * a * b2 * c;
+}
+
+// the TDGL-updated cell c = c' + kOff[Q]: its rows' transposed gradient
+// stencils at the impulse c' (the offset is a compile-time constant, so only
+// the stencils that can reach c' are evaluated)
+template <typename T, bool VEC, bool ROT, int Q>
+__device__ __forceinline__ void grad_from(const DevParams& p, const MView& M, const uint8_t* __restrict__ code,
+                                          const uint8_t* __restrict__ var, const Variant* __restrict__ vt,
+                                          const double* __restrict__ lp, const double* __restrict__ lq,
+                                          const double* __restrict__ lr, const DeltaView<T>& D, int i, int j, int k,
+                                          T adj[3]) {
+    constexpr int OX = kOff[Q][0], OY = kOff[Q][1], OZ = kOff[Q][2];
+    const int ck = k + OZ;
+    if (ck < 0 || ck >= p.nz) return;
+    const int ci = wrap(i + OX, p.nx), cj = wrap(j + OY, p.ny);
+    if (!updated(mcode(code, p, ci, cj, ck))) return;
+    const size_t cc = cidx(p, ci, cj, ck);
+    T R[9], al;
+    load_R<T, ROT>(var, vt, cc, R, al, p);
+    T lam[3];
+    load_lam<T, VEC>(p, lp, lq, lr, cc, lam);
+    adj[2] += grad_rows_T<T, VEC, ROT, 2, -OX, -OY, -OZ>(p, M, R, lam, D, ci, cj, ck);
+    if constexpr (VEC) {
+        adj[0] += grad_rows_T<T, VEC, ROT, 0, -OX, -OY, -OZ>(p, M, R, lam, D, ci, cj, ck);
+        adj[1] += grad_rows_T<T, VEC, ROT, 1, -OX, -OY, -OZ>(p, M, R, lam, D, ci, cj, ck);
+    }
+}
+
+template <typename T, bool VEC, bool ROT, int... Q>
+__device__ __forceinline__ void grad_visit(std::integer_sequence<int, Q...>, const DevParams& p, const MView& M,
+                                           const uint8_t* code, const uint8_t* var, const Variant* vt,
+                                           const double* lp, const double* lq, const double* lr,
+                                           const DeltaView<T>& D, int i, int j, int k, T adj[3]) {
+    (grad_from<T, VEC, ROT, Q>(p, M, code, var, vt, lp, lq, lr, D, i, j, k, adj), ...);
+}
+
+// the seven cells whose first-derivative (dpd, grad phi) stencils can read a
+// cell: itself and its face neighbours (entries of kOff)
+constexpr int kFace[7] = {0, 1, 2, 5, 6, 9, 10};
+
+// (ds/dP)^T psi from the FE cell c = c' + kOff[kFace[Q]] (k_rhs_p's
+// -sum_a R_a . grad P_a, FP64)
+template <bool VEC, bool ROT, int Q>
+__device__ __forceinline__ void rhs_from(const DevParams& p, const MView& M, const uint8_t* __restrict__ code,
+                                         const uint8_t* __restrict__ var, const Variant* __restrict__ vt,
+                                         const double* __restrict__ psi, const DeltaView<double>& D, int i, int j,
+                                         int k, double rs[3]) {
+    constexpr int OX = kOff[kFace[Q]][0], OY = kOff[kFace[Q]][1], OZ = kOff[kFace[Q]][2];
+    using Rc = Reach<-OX, -OY, -OZ>;
+    const int ck = k + OZ;
+    if (ck < 0 || ck >= p.nz) return;
+    const int ci = wrap(i + OX, p.nx), cj = wrap(j + OY, p.ny);
+    if ((mcode(code, p, ci, cj, ck) & 3) != 0) return;
+    const size_t cc = cidx(p, ci, cj, ck);
+    const double ps = psi[cc];
+    if (ps == 0.0) return;
+    double R[9], al;
+    load_R<double, ROT>(var, vt, cc, R, al, p);
+    const double d0 = Rc::dx ? dpd<0, double>(D, M, ci, cj, ck) : 0.0;
+    const double d1 = Rc::dy ? dpd<1, double>(D, M, ci, cj, ck) : 0.0;
+    const double d2 = Rc::dz ? dpd<2, double>(D, M, ci, cj, ck) : 0.0;
+    rs[2] -= ps * (R[6] * d0 + R[7] * d1 + R[8] * d2);
+    if constexpr (VEC) {
+        rs[0] -= ps * (R[0] * d0 + R[1] * d1 + R[2] * d2);
+        rs[1] -= ps * (R[3] * d0 + R[4] * d1 + R[5] * d2);
+    }
+}
+
+template <bool VEC, bool ROT, int... Q>
+__device__ __forceinline__ void rhs_visit(std::integer_sequence<int, Q...>, const DevParams& p, const MView& M,
+                                          const uint8_t* code, const uint8_t* var, const Variant* vt,
+                                          const double* psi, const DeltaView<double>& D, int i, int j, int k,
+                                          double rs[3]) {
+    (rhs_from<VEC, ROT, Q>(p, M, code, var, vt, psi, D, i, j, k, rs), ...);
+}
+
+// the components of grad_phi_acc that can depend on the accessor's cell
+// c + (DI, DJ, DK); the others are left at zero (same formulas otherwise)
+template <typename T, int DI, int DJ, int DK, typename A>
+__device__ __forceinline__ void grad_phi_reach(const A& f, const DevParams& p, int i, int j, int k, T& gx, T& gy, T& gz) {
+    using Rc = Reach<DI, DJ, DK>;
+    gx = gy = gz = T(0);
+    if constexpr (Rc::gx) gx = T((f(i + 1, j, k) - f(i - 1, j, k)) / (2. * p.dx[0]));
+    if constexpr (Rc::gy) gy = T((f(i, j + 1, k) - f(i, j - 1, k)) / (2. * p.dx[1]));
+    if constexpr (Rc::gz) {
+        const double dz = p.dx[2];
+        if (k == 0) gz = T((-4. * f(i, j, k - 1) + 3. * f(i, j, k) + f(i, j, k + 1)) / (3. * dz));
+        else if (k == p.nz - 1) gz = T((4. * f(i, j, k + 1) - 3. * f(i, j, k) - f(i, j, k - 1)) / (3. * dz));
+        else gz = T((f(i, j, k + 1) - f(i, j, k - 1)) / (2. * dz));
+    }
+}
+
+// mu contribution of the TDGL-updated cell c = c' + kOff[kFace[Q]] (its E term
+// reads phi at c'); the top-layer cell itself also carries the direct
+// dependence on the electrode value
+template <typename T, bool VEC, bool ROT, int Q>
+__device__ __forceinline__ void phi_from(const DevParams& p, const uint8_t* __restrict__ code,
+                                         const uint8_t* __restrict__ var, const Variant* __restrict__ vt,
+                                         const double* __restrict__ lp, const double* __restrict__ lq,
+                                         const double* __restrict__ lr, const PhiDelta& D, int i, int j, int k,
+                                         T& acc, T& dvacc) {
+    constexpr int OX = kOff[kFace[Q]][0], OY = kOff[kFace[Q]][1], OZ = kOff[kFace[Q]][2];
+    const int ck = k + OZ;
+    if (ck < 0 || ck >= p.nz) return;
+    const int ci = wrap(i + OX, p.nx), cj = wrap(j + OY, p.ny);
+    if (!updated(mcode(code, p, ci, cj, ck))) return;
+    const size_t cc = cidx(p, ci, cj, ck);
+    T R[9], al;
+    load_R<T, ROT>(var, vt, cc, R, al, p);
+    T lam[3];
+    load_lam<T, VEC>(p, lp, lq, lr, cc, lam);
+    T w[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) w[d] = lam[2] * R[6 + d] + (VEC ? lam[0] * R[d] + lam[1] * R[3 + d] : T(0));
+    T gx, gy, gz;
+    grad_phi_reach<T, -OX, -OY, -OZ>(D, p, ci, cj, ck, gx, gy, gz);
+    acc += w[0] * gx + w[1] * gy + w[2] * gz;
+    if constexpr (Q == 0) {
+        if (k == p.nz - 1) {
+            grad_phi_acc<T>(VDelta{&p}, p, ci, cj, ck, gx, gy, gz);
+            dvacc = w[0] * gx + w[1] * gy + w[2] * gz;
+        }
+    }
+}
+
+template <typename T, bool VEC, bool ROT, int... Q>
+__device__ __forceinline__ void phi_visit(std::integer_sequence<int, Q...>, const DevParams& p, const uint8_t* code,
+                                          const uint8_t* var, const Variant* vt, const double* lp, const double* lq,
+                                          const double* lr, const PhiDelta& D, int i, int j, int k, T& acc, T& dvacc) {
+    (phi_from<T, VEC, ROT, Q>(p, code, var, vt, lp, lq, lr, D, i, j, k, acc, dvacc), ...);
 }
 
 // ---------------------------------------------------------------------------
@@ -197,29 +362,9 @@ __global__ void __launch_bounds__(256) k_adj_phi(DevParams p, const uint8_t* __r
         const T mGam = T(-1.0) * T(p.BigGamma);
         T acc = T(0);
         const PhiDelta D{i, j, k, &p};
-        for (int q = 0; q < 7; ++q) {
-            // the seven cells: 0, +-x, +-y, +-z (entries 0, 1, 2, 5, 6, 9, 10 of c_off)
-            const int e = q == 0 ? 0 : q == 1 ? 1 : q == 2 ? 2 : q == 3 ? 5 : q == 4 ? 6 : q == 5 ? 9 : 10;
-            const int ci = wrap(i + c_off[e][0], p.nx), cj = wrap(j + c_off[e][1], p.ny), ck = k + c_off[e][2];
-            if (ck < 0 || ck >= p.nz) continue;
-            const int m = mcode(code, p, ci, cj, ck);
-            if (!updated(m)) continue;
-            const size_t cc = cidx(p, ci, cj, ck);
-            T R[9], al;
-            load_R<T, ROT>(var, vt, cc, R, al, p);
-            T lam[3];
-            load_lam<T, VEC>(p, lp, lq, lr, cc, lam);
-            T w[3];
-#pragma unroll
-            for (int d = 0; d < 3; ++d) w[d] = lam[2] * R[6 + d] + (VEC ? lam[0] * R[d] + lam[1] * R[3 + d] : T(0));
-            T gx, gy, gz;
-            grad_phi_acc<T>(D, p, ci, cj, ck, gx, gy, gz);
-            acc += w[0] * gx + w[1] * gy + w[2] * gz;
-            if (e == 0 && k == p.nz - 1) {
-                grad_phi_acc<T>(VDelta{&p}, p, ci, cj, ck, gx, gy, gz);
-                dv = p.dt * (double)(mGam * (w[0] * gx + w[1] * gy + w[2] * gz));
-            }
-        }
+        T dvacc = T(0);
+        phi_visit<T, VEC, ROT>(std::make_integer_sequence<int, 7>{}, p, code, var, vt, lp, lq, lr, D, i, j, k, acc, dvacc);
+        dv = p.dt * (double)(mGam * dvacc);
         const double v = p.dt * (double)(mGam * acc);
         mu[cidx(p, i, j, k)] = v;
         amax = fabs(v);
@@ -339,22 +484,10 @@ __global__ void __launch_bounds__(256) k_adj_P(DevParams p, const uint8_t* __res
         // ---- transposed gradient-energy stencils of the cells that read this one
         if (p.incl_G) {
             const DeltaView<T> D{i, j, k, &p};
-            const int nn = (VEC || ROT) ? 25 : 13;
-            for (int q = 0; q < nn; ++q) {
-                const int ci = wrap(i + c_off[q][0], p.nx), cj = wrap(j + c_off[q][1], p.ny), ck = k + c_off[q][2];
-                if (ck < 0 || ck >= p.nz) continue;
-                if (!updated(mcode(code, p, ci, cj, ck))) continue;
-                const size_t cc = cidx(p, ci, cj, ck);
-                T R[9], al;
-                load_R<T, ROT>(var, vt, cc, R, al, p);
-                T lam[3];
-                load_lam<T, VEC>(p, lp, lq, lr, cc, lam);
-                adj[2] += grad_rows_T<T, VEC, ROT, 2>(p, M, R, lam, D, ci, cj, ck);
-                if (VEC) {
-                    adj[0] += grad_rows_T<T, VEC, ROT, 0>(p, M, R, lam, D, ci, cj, ck);
-                    adj[1] += grad_rows_T<T, VEC, ROT, 1>(p, M, R, lam, D, ci, cj, ck);
-                }
-            }
+            if constexpr (VEC || ROT)
+                grad_visit<T, VEC, ROT>(std::make_integer_sequence<int, 25>{}, p, M, code, var, vt, lp, lq, lr, D, i, j, k, adj);
+            else   // without rotation or Px, Py only the axis second derivatives reach
+                grad_visit<T, VEC, ROT>(std::make_integer_sequence<int, 13>{}, p, M, code, var, vt, lp, lq, lr, D, i, j, k, adj);
         }
         const double f = p.dt * (double)mGam;
         out[2] += f * (double)adj[2];
@@ -368,25 +501,7 @@ __global__ void __launch_bounds__(256) k_adj_P(DevParams p, const uint8_t* __res
         if (psi) {
             const DeltaView<double> D{i, j, k, &p};
             double rs[3] = {0.0, 0.0, 0.0};
-            for (int q = 0; q < 7; ++q) {
-                const int e = q == 0 ? 0 : q == 1 ? 1 : q == 2 ? 2 : q == 3 ? 5 : q == 4 ? 6 : q == 5 ? 9 : 10;
-                const int ci = wrap(i + c_off[e][0], p.nx), cj = wrap(j + c_off[e][1], p.ny), ck = k + c_off[e][2];
-                if (ck < 0 || ck >= p.nz) continue;
-                if ((mcode(code, p, ci, cj, ck) & 3) != 0) continue;
-                const size_t cc = cidx(p, ci, cj, ck);
-                const double ps = psi[cc];
-                if (ps == 0.0) continue;
-                double R[9], al;
-                load_R<double, ROT>(var, vt, cc, R, al, p);
-                const double d0 = dpd<0, double>(D, M, ci, cj, ck);
-                const double d1 = dpd<1, double>(D, M, ci, cj, ck);
-                const double d2 = dpd<2, double>(D, M, ci, cj, ck);
-                rs[2] -= ps * (R[6] * d0 + R[7] * d1 + R[8] * d2);
-                if (VEC) {
-                    rs[0] -= ps * (R[0] * d0 + R[1] * d1 + R[2] * d2);
-                    rs[1] -= ps * (R[3] * d0 + R[4] * d1 + R[5] * d2);
-                }
-            }
+            rhs_visit<VEC, ROT>(std::make_integer_sequence<int, 7>{}, p, M, code, var, vt, psi, D, i, j, k, rs);
             out[2] += rs[2];
             if (VEC) {
                 out[0] += rs[0];
