@@ -39,6 +39,10 @@ WORKLOADS = {
     "polycrystal": dict(shape=(256, 256, 128), label="64-grain polycrystalline HZO on Al2O3"),
 }
 METRIC = "coupled-step cell-updates/s"
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum, one ncu
+# capture, cold cache) of the dominant bandwidth-bound kernel class, by
+# (workload, precision, class); see profiles/k_rbgs_l0_mfism_128x128x144.md
+TRAFFIC = {("mfism", "fp64", "smooth_l0"): 59.35e6}
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -366,7 +370,10 @@ def main() -> None:
         achieved = per_launch / (dms / dcnt / 1e3) / 1e9 if dcnt else None
         total_ms = sum(v[0] for v in kt.values())
         roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak if achieved else None, "traffic": None,
+                "frac": achieved / peak if achieved else None,
+                "traffic": TRAFFIC.get((args.workload, args.precision, dom)),
+                "traffic_source": "ncu dram bytes per launch, profiles/k_rbgs_l0_mfism_128x128x144.md"
+                if (args.workload, args.precision, dom) in TRAFFIC else None,
                 "peak_source": f"{peak_src} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured"
                 else "fallback 6.65 TB/s",
                 "algorithmic_bytes_per_launch": per_launch, "launches": dcnt, "avg_launch_us": 1e3 * dms / dcnt,
