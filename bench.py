@@ -11,7 +11,9 @@ seeded synthetic initial polarization.
                     [--workload mfism|mfim|polycrystal] [--precision fp64|mixed]
                     [--no-adjoint] [--adjoint-steps-per-leg S]
 
-At N = 1 the line also carries "adjoint": the time of fx_backward over
+With --precision mixed the line carries "mixed_vs_fp64": the FP64 and mixed
+steps timed side by side on the same deck and the per-field max relative
+difference after the run.  At N = 1 the line also carries "adjoint": the time of fx_backward over
 fx_forward_record for the hysteresis loss on the 128x128x48 MFIM stack
 (800 steps, checkpoints every 50, gradients in alpha, beta, gamma, g11, g44
 and the voltage amplitude).
@@ -163,6 +165,44 @@ def cpu_baseline(text: str, grains, steps: int) -> dict:
             "sample": f"{steps} full coupled steps of the same deck after 1 warm-up step (restated CPU oracle, "
                       f"OpenMP, {threads} threads; the reference build needs AMReX, absent)",
             "seconds": dt}
+
+
+def precision_compare(stream, workload: str, steps: int, warmup: int) -> dict:
+    """The mixed-precision step next to the plain FP64 step on the same seeded
+    deck: ms per step of each (CUDA events on the library's stream) and the
+    max-norm relative difference of the output fields after warmup + steps
+    steps (FP64 taken as the reference)."""
+    import numpy as np
+    import torch
+    from ferrox_b200 import api
+    text, grains = deck(workload)
+    out, fields = {}, {}
+    for prec in ("fp64", "mixed"):
+        f = api.FerroX(text, precision=prec)
+        if grains is not None:
+            f.set_grains(grains["id"], grains["angles"], grains["tphase"])
+        f.set_stream(stream.cuda_stream)
+        f.step(warmup)
+        f.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        f.step(steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        out[f"{prec}_ms_per_step"] = e0.elapsed_time(e1) / steps
+        f.compute_E()
+        names = ["Px", "Py", "Pz", "Phi", "Ex", "Ey", "Ez"] + (["charge", "electrons", "holes"]
+                                                              if f.param("contains_sc") == 1.0 else [])
+        fields[prec] = {n: f.field(n) for n in names}
+        f.close()
+    rel = {}
+    for n, ref in fields["fp64"].items():
+        scale = float(np.abs(ref).max())
+        if scale > 0:
+            rel[n] = float(np.abs(fields["mixed"][n] - ref).max() / scale)
+    out.update({"speedup": out["fp64_ms_per_step"] / out["mixed_ms_per_step"], "steps": warmup + steps,
+                "relerr_vs_fp64": rel, "max_relerr": max(rel.values())})
+    return out
 
 
 def adjoint_ratio(stream, precision: str = "fp64", steps_per_leg: int = 400, k: int = 50) -> dict:
@@ -381,6 +421,9 @@ def main() -> None:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             cpu = cpu_baseline(text, grains, 3)
+        prec_cmp = None
+        if world == 1 and args.precision == "mixed":
+            prec_cmp = precision_compare(stream, args.workload, args.steps, args.warmup)
         adj = None
         if world == 1 and not args.no_adjoint:
             adj = adjoint_ratio(stream, args.precision, args.adjoint_steps_per_leg)
@@ -403,6 +446,7 @@ def main() -> None:
             "mg_cycles_per_step": (st1["mg_cycles_total"] - st0["mg_cycles_total"]) / args.steps,
             "newton_passes_per_step": (st1["newton_iters_total"] - st0["newton_iters_total"]) / args.steps,
             "adjoint": adj,
+            "mixed_vs_fp64": prec_cmp,
         }
         print(json.dumps(line), flush=True)
     f.close()

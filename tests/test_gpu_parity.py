@@ -235,3 +235,16 @@ def test_kernel_launches_counted():
     a = f.stats()["kernel_launches"]
     f.step(1)
     assert f.stats()["kernel_launches"] > a
+
+
+@pytest.mark.parametrize("deck", ["mfim", "mfism"])
+def test_thousand_steps_drift(deck):
+    # FP64 fields within 1e-8 of the oracle after 1000 coupled steps
+    text = (decks.mfism(16, 16, 48, extra={"Phi_Bc_hi": 0.4}) if deck == "mfism"
+            else decks.mfim(16, 16, 12, Phi_Bc_hi=0.6))
+    f, o = pair(text, rtol=1e-13)
+    done = f.step(1000)
+    last = o.run(1000)
+    assert done == last      # the same break step, if the steady-state test ends the loop
+    for name in ["Pz", "Phi"] + (["charge"] if deck == "mfism" else []):
+        assert relerr(f.field(name), o.field(name)) < 1e-8, (name, relerr(f.field(name), o.field(name)))
