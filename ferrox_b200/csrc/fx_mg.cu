@@ -20,7 +20,7 @@ namespace {
 template <typename T>
 struct Op {
     int nx, ny, nz;
-    long long nxy;
+    int nxy;               // cells per z plane (every level holds fewer than 2^31 cells)
     T ih2x, ih2y, ih2z;
     const uint8_t* code;   // level 0: material codes (with z ghost layers)
     T eps[8];
@@ -34,28 +34,28 @@ struct Op {
 // couplings of cell (i,j,k) to its six neighbours (already divided by h^2),
 // the diagonal and the electrode contribution to the right-hand side
 template <typename T, bool FINE>
-__device__ __forceinline__ void coeffs(const Op<T>& o, int i, int j, int k, size_t c, int im, int ip, int jm, int jp,
+__device__ __forceinline__ void coeffs(const Op<T>& o, int i, int j, int k, int c, int im, int ip, int jm, int jp,
                                        T& cw, T& ce, T& cs, T& cn, T& cb, T& ct, T& diag, T& bcv, const T* eps) {
     T extra = T(0);
     bcv = T(0);
     if (FINE) {
         const uint8_t* cd = o.code + o.nxy;   // skip the k = -1 ghost layer
-        const size_t row = c - i;
+        const int row = c - i;
         const T ec = eps[__ldg(cd + c) & 7];
         cw = T(0.5) * (ec + eps[__ldg(cd + row + im) & 7]) * o.ih2x;
         ce = T(0.5) * (eps[__ldg(cd + row + ip) & 7] + ec) * o.ih2x;
-        cs = T(0.5) * (ec + eps[__ldg(cd + c + (size_t)(jm - j) * o.nx) & 7]) * o.ih2y;
-        cn = T(0.5) * (eps[__ldg(cd + c + (size_t)(jp - j) * o.nx) & 7] + ec) * o.ih2y;
+        cs = T(0.5) * (ec + eps[__ldg(cd + c + (jm - j) * o.nx) & 7]) * o.ih2y;
+        cn = T(0.5) * (eps[__ldg(cd + c + (jp - j) * o.nx) & 7] + ec) * o.ih2y;
         if (k > 0) cb = T(0.5) * (ec + eps[__ldg(cd + c - o.nxy) & 7]) * o.ih2z;
         else { cb = T(0); extra += T(2) * ec * o.ih2z; bcv += T(2) * ec * o.ih2z * o.vlo; }
         if (k < o.nz - 1) ct = T(0.5) * (eps[__ldg(cd + c + o.nxy) & 7] + ec) * o.ih2z;
         else { ct = T(0); extra += T(2) * ec * o.ih2z; bcv += T(2) * ec * o.ih2z * o.vhi; }
     } else {
-        const size_t row = c - i;
+        const int row = c - i;
         cw = __ldg(o.bw + c) * o.ih2x;
         ce = __ldg(o.bw + row + ip) * o.ih2x;
         cs = __ldg(o.bs + c) * o.ih2y;
-        cn = __ldg(o.bs + c + (size_t)(jp - j) * o.nx) * o.ih2y;
+        cn = __ldg(o.bs + c + (jp - j) * o.nx) * o.ih2y;
         const T fb = __ldg(o.bb + c), ft = __ldg(o.bb + c + o.nxy);
         if (k > 0) cb = fb * o.ih2z;
         else { cb = T(0); extra += T(2) * fb * o.ih2z; }
@@ -98,6 +98,12 @@ __device__ double block_max_all(double v) {
 }
 
 // red-black point Gauss-Seidel half sweep: color = parity of i + j + k
+// the smoother's division: exact in FP64; in the FP32 correction cycle of
+// the mixed path the fast single-precision divide (the update is a smoothing
+// step; the FP64 outer residual decides convergence)
+__device__ __forceinline__ double sdiv(double a, double b) { return a / b; }
+__device__ __forceinline__ float sdiv(float a, float b) { return __fdividef(a, b); }
+
 template <typename T, bool FINE>
 __global__ void __launch_bounds__(256) k_rbgs(Op<T> o, T* __restrict__ x, const T* __restrict__ b, int color) {
     __shared__ T seps[8];
@@ -111,18 +117,18 @@ __global__ void __launch_bounds__(256) k_rbgs(Op<T> o, T* __restrict__ x, const 
     const int k = blockIdx.z;
     const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((j + k + color) & 1);
     if (j >= o.ny || i >= o.nx) return;
-    const size_t c = (size_t)i + (size_t)o.nx * ((size_t)j + (size_t)o.ny * k);
+    const int c = i + o.nx * (j + o.ny * k);
     int im, ip, jm, jp;
     nbr(i, o.nx, im, ip);
     nbr(j, o.ny, jm, jp);
     T cw, ce, cs, cn, cb, ct, diag, bcv;
     coeffs<T, FINE>(o, i, j, k, c, im, ip, jm, jp, cw, ce, cs, cn, cb, ct, diag, bcv, seps);
-    const size_t row = c - i;
-    T s = b[c] + bcv + cw * x[row + im] + ce * x[row + ip] + cs * x[c + (size_t)(jm - j) * o.nx] +
-          cn * x[c + (size_t)(jp - j) * o.nx];
+    const int row = c - i;
+    T s = b[c] + bcv + cw * x[row + im] + ce * x[row + ip] + cs * x[c + (jm - j) * o.nx] +
+          cn * x[c + (jp - j) * o.nx];
     if (k > 0) s += cb * x[c - o.nxy];
     if (k < o.nz - 1) s += ct * x[c + o.nxy];
-    x[c] = s / diag;
+    x[c] = sdiv(s, diag);
 }
 
 // red-black z-line Gauss-Seidel half sweep: color = parity of i + j; each
@@ -145,13 +151,13 @@ __global__ void __launch_bounds__(128) k_line(Op<T> o, T* __restrict__ x, const 
     nbr(i, o.nx, im, ip);
     nbr(j, o.ny, jm, jp);
     T qprev = T(0), dprev = T(0);
-    size_t c = (size_t)i + (size_t)o.nx * (size_t)j;
+    int c = i + o.nx * j;
     for (int k = 0; k < o.nz; ++k, c += o.nxy) {
         T cw, ce, cs, cn, cb, ct, diag, bcv;
         coeffs<T, FINE>(o, i, j, k, c, im, ip, jm, jp, cw, ce, cs, cn, cb, ct, diag, bcv, seps);
-        const size_t row = c - i;
-        const T r = b[c] + bcv + cw * x[row + im] + ce * x[row + ip] + cs * x[c + (size_t)(jm - j) * o.nx] +
-                    cn * x[c + (size_t)(jp - j) * o.nx];
+        const int row = c - i;
+        const T r = b[c] + bcv + cw * x[row + im] + ce * x[row + ip] + cs * x[c + (jm - j) * o.nx] +
+                    cn * x[c + (jp - j) * o.nx];
         const T den = diag - cb * qprev;
         const T qk = ct / den;
         const T dk = (r + cb * dprev) / den;
@@ -196,22 +202,22 @@ __global__ void __launch_bounds__(256) k_resid_restrict(Op<T> o, const T* __rest
 #pragma unroll
                 for (int di = 0; di < RX; ++di) {
                     const int i = RX * I + di, j = RY * J + dj, k = RZ * K + dk;
-                    const size_t c = (size_t)i + (size_t)o.nx * ((size_t)j + (size_t)o.ny * k);
+                    const int c = i + o.nx * (j + o.ny * k);
                     int im, ip, jm, jp;
                     nbr(i, o.nx, im, ip);
                     nbr(j, o.ny, jm, jp);
                     T cw, ce, cs, cn, cb, ct, diag, bcv;
                     coeffs<T, FINE>(o, i, j, k, c, im, ip, jm, jp, cw, ce, cs, cn, cb, ct, diag, bcv, seps);
-                    const size_t row = c - i;
-                    T off = cw * x[row + im] + ce * x[row + ip] + cs * x[c + (size_t)(jm - j) * o.nx] +
-                            cn * x[c + (size_t)(jp - j) * o.nx];
+                    const int row = c - i;
+                    T off = cw * x[row + im] + ce * x[row + ip] + cs * x[c + (jm - j) * o.nx] +
+                            cn * x[c + (jp - j) * o.nx];
                     if (k > 0) off += cb * x[c - o.nxy];
                     if (k < o.nz - 1) off += ct * x[c + o.nxy];
                     const T r = (b[c] + bcv) - (diag * x[c] - off);
                     s += r;
                     mx = fmax(mx, fabs((double)r));
                 }
-        bc[(size_t)I + (size_t)ncx * ((size_t)J + (size_t)ncy * K)] = s / T(RX * RY * RZ);
+        bc[I + ncx * (J + ncy * K)] = s / T(RX * RY * RZ);
     }
     if (norm) {
         const double m = block_max_all(mx);
@@ -221,7 +227,12 @@ __global__ void __launch_bounds__(256) k_resid_restrict(Op<T> o, const T* __rest
 }
 
 // FP64 residual of the level-0 operator with electrode terms; optional FP32
-// copy for the mixed-precision correction solve
+// copy for the mixed-precision correction solve.  Each thread walks R64_ZP
+// consecutive cells of its z column, carrying the column's x and code values
+// from one cell to the next (the coefficients are those of coeffs<double,
+// true>, same operations); block maxima go to NORM_SLOTS spread slots.
+constexpr int R64_ZP = 4;
+
 __global__ void __launch_bounds__(256) k_resid64(Op<double> o, const double* __restrict__ x, const double* __restrict__ b,
                                                  float* __restrict__ r32, double* __restrict__ norm) {
     __shared__ double seps[8];
@@ -231,26 +242,52 @@ __global__ void __launch_bounds__(256) k_resid64(Op<double> o, const double* __r
     __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int k = blockIdx.z;
+    const int k0 = blockIdx.z * R64_ZP;
     double mx = 0.0;
     if (i < o.nx && j < o.ny) {
-        const size_t c = (size_t)i + (size_t)o.nx * ((size_t)j + (size_t)o.ny * k);
         int im, ip, jm, jp;
         nbr(i, o.nx, im, ip);
         nbr(j, o.ny, jm, jp);
-        double cw, ce, cs, cn, cb, ct, diag, bcv;
-        coeffs<double, true>(o, i, j, k, c, im, ip, jm, jp, cw, ce, cs, cn, cb, ct, diag, bcv, seps);
-        const size_t row = c - i;
-        double off = cw * x[row + im] + ce * x[row + ip] + cs * x[c + (size_t)(jm - j) * o.nx] +
-                     cn * x[c + (size_t)(jp - j) * o.nx];
-        if (k > 0) off += cb * x[c - o.nxy];
-        if (k < o.nz - 1) off += ct * x[c + o.nxy];
-        const double r = (b[c] + bcv) - (diag * x[c] - off);
-        if (r32) r32[c] = (float)r;
-        mx = fabs(r);
+        const int col = i + o.nx * j;
+        const int row = col - i;
+        const int dso = (jm - j) * o.nx, dno = (jp - j) * o.nx;
+        const uint8_t* cd = o.code + o.nxy;   // the k = -1 ghost layer is cd - nxy
+        double xm = k0 > 0 ? x[col + o.nxy * (k0 - 1)] : 0.0;
+        double xc = x[col + o.nxy * k0];
+        double em = seps[__ldg(cd + col + o.nxy * (k0 - 1)) & 7];
+        double ec = seps[__ldg(cd + col + o.nxy * k0) & 7];
+        const int k1 = min(o.nz, k0 + R64_ZP);
+        for (int k = k0; k < k1; ++k) {
+            const int c = col + o.nxy * k;
+            const double xp = k < o.nz - 1 ? x[c + o.nxy] : 0.0;
+            const double ep = seps[__ldg(cd + c + o.nxy) & 7];
+            double extra = 0.0, bcv = 0.0, cb, ct;
+            double cw = 0.5 * (ec + seps[__ldg(cd + row + o.nxy * k + im) & 7]) * o.ih2x;
+            double ce = 0.5 * (seps[__ldg(cd + row + o.nxy * k + ip) & 7] + ec) * o.ih2x;
+            double cs = 0.5 * (ec + seps[__ldg(cd + c + dso) & 7]) * o.ih2y;
+            double cn = 0.5 * (seps[__ldg(cd + c + dno) & 7] + ec) * o.ih2y;
+            if (k > 0) cb = 0.5 * (ec + em) * o.ih2z;
+            else { cb = 0.0; extra += 2.0 * ec * o.ih2z; bcv += 2.0 * ec * o.ih2z * o.vlo; }
+            if (k < o.nz - 1) ct = 0.5 * (ep + ec) * o.ih2z;
+            else { ct = 0.0; extra += 2.0 * ec * o.ih2z; bcv += 2.0 * ec * o.ih2z * o.vhi; }
+            if (o.nx == 1) { cw = 0.0; ce = 0.0; }
+            if (o.ny == 1) { cs = 0.0; cn = 0.0; }
+            const double a = o.a ? o.a[c] : 0.0;
+            const double diag = -a + cw + ce + cs + cn + cb + ct + extra;
+            const int rk = row + o.nxy * k;
+            double off = cw * x[rk + im] + ce * x[rk + ip] + cs * x[c + dso] + cn * x[c + dno];
+            if (k > 0) off += cb * xm;
+            if (k < o.nz - 1) off += ct * xp;
+            const double r = (b[c] + bcv) - (diag * xc - off);
+            if (r32) r32[c] = (float)r;
+            mx = fmax(mx, fabs(r));
+            xm = xc; xc = xp;
+            em = ec; ec = ep;
+        }
     }
     const double m = block_max_all(mx);
-    if (threadIdx.x == 0 && threadIdx.y == 0) atomic_max_nonneg(norm, m);
+    const int slot = (blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)) & (NORM_SLOTS - 1);
+    if (threadIdx.x == 0 && threadIdx.y == 0) atomic_max_nonneg(norm + slot, m);
 }
 
 // prolongation in the coarsened directions with the per-cell resistor-chain
@@ -647,7 +684,7 @@ Op<T> make_op(const MGLevel& L, int l, const uint8_t* code, const double* eps, c
               const DevParams& p) {
     Op<T> o;
     o.nx = L.n[0]; o.ny = L.n[1]; o.nz = L.n[2];
-    o.nxy = (long long)L.n[0] * L.n[1];
+    o.nxy = L.n[0] * L.n[1];
     o.ih2x = T(1.0 / (L.h[0] * L.h[0]));
     o.ih2y = T(1.0 / (L.h[1] * L.h[1]));
     o.ih2z = T(1.0 / (L.h[2] * L.h[2]));
@@ -702,6 +739,7 @@ Multigrid::~Multigrid() {
 }
 
 int Multigrid::setup(const DevParams& p, const std::vector<uint8_t>& code, bool want64, bool want32) {
+    if ((long long)p.nx * p.ny * (p.nz + 2) >= (1LL << 31)) return -1;   // 32-bit cell indices in the kernels
     for (int q = 0; q < 8; ++q) eps_[q] = p.eps[q];
     lev_.clear();
     MGLevel L0{};
@@ -1128,7 +1166,7 @@ int Multigrid::residual64(const DevParams& p, const uint8_t* code, const double*
     dim3 b2(32, 8), g2((L.n[0] + 31) / 32, (L.n[1] + 7) / 8, L.n[2]);
     (void)r;
     if (prof) prof->begin(PROF_RESID64, s);
-    { ++g_launches; k_resid64<<<g2, b2, 0, s>>>(o, phi, rhs, nullptr, d_norm_); }
+    { ++g_launches; k_resid64<<<dim3(g2.x, g2.y, (L.n[2] + R64_ZP - 1) / R64_ZP), b2, 0, s>>>(o, phi, rhs, nullptr, d_norm_); }
     if (prof) prof->end(s);
     cudaMemcpyAsync(h_norm_, d_norm_, NORM_SLOTS * 8, cudaMemcpyDeviceToHost, s);
     cudaError_t e = cudaStreamSynchronize(s);
@@ -1206,7 +1244,7 @@ int Multigrid::solve_mixed(const DevParams& p, const uint8_t* code, double* phi,
         cudaMemsetAsync(d_norm_, 0, NORM_SLOTS * 8, s);
         if (prof) prof->begin(PROF_RESID64, s);
         ++g_launches;
-        k_resid64<<<g2, b2, 0, s>>>(o64, phi, rhs, r32_, d_norm_);
+        k_resid64<<<dim3(g2.x, g2.y, (L.n[2] + R64_ZP - 1) / R64_ZP), b2, 0, s>>>(o64, phi, rhs, r32_, d_norm_);
         if (prof) prof->end(s);
         cudaMemcpyAsync(h_norm_, d_norm_, NORM_SLOTS * 8, cudaMemcpyDeviceToHost, s);
     };
