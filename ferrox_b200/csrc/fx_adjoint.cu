@@ -31,6 +31,26 @@
 
 namespace fx {
 
+// which stencils evaluated at a cell c can read the cell c + (DI, DJ, DK):
+// a second derivative along an axis reads up to two cells along it, a mixed
+// one the first-derivative stencil (one cell along its axis) one cell to
+// either side, a first derivative one cell along its axis
+template <int DI, int DJ, int DK>
+struct Reach {
+    static constexpr bool xx = DJ == 0 && DK == 0;
+    static constexpr bool yy = DI == 0 && DK == 0;
+    static constexpr bool zz = DI == 0 && DJ == 0;
+    static constexpr bool xy = (DI == 1 || DI == -1) && DK == 0;
+    static constexpr bool xz = (DI == 1 || DI == -1) && DJ == 0;
+    static constexpr bool yz = (DJ == 1 || DJ == -1) && DI == 0;
+    static constexpr bool dx = DJ == 0 && DK == 0 && DI >= -1 && DI <= 1;
+    static constexpr bool dy = DI == 0 && DK == 0 && DJ >= -1 && DJ <= 1;
+    static constexpr bool dz = DI == 0 && DJ == 0 && DK >= -1 && DK <= 1;
+    static constexpr bool gx = (DI == 1 || DI == -1) && DJ == 0 && DK == 0;   // central phi differences
+    static constexpr bool gy = (DJ == 1 || DJ == -1) && DI == 0 && DK == 0;
+    static constexpr bool gz = DI == 0 && DJ == 0;
+};
+
 namespace {
 
 __device__ __forceinline__ double warp_sum_d(double v) {
@@ -122,26 +142,6 @@ constexpr int kOff[25][3] = {
     {0, 0, 0},  {1, 0, 0},  {-1, 0, 0}, {2, 0, 0},  {-2, 0, 0}, {0, 1, 0},  {0, -1, 0}, {0, 2, 0},  {0, -2, 0},
     {0, 0, 1},  {0, 0, -1}, {0, 0, 2},  {0, 0, -2}, {1, 1, 0},  {1, -1, 0}, {-1, 1, 0}, {-1, -1, 0}, {1, 0, 1},
     {1, 0, -1}, {-1, 0, 1}, {-1, 0, -1}, {0, 1, 1}, {0, 1, -1}, {0, -1, 1}, {0, -1, -1}};
-
-// which stencils evaluated at a cell c can read the cell c + (DI, DJ, DK):
-// a second derivative along an axis reads up to two cells along it, a mixed
-// one the first-derivative stencil (one cell along its axis) one cell to
-// either side, a first derivative one cell along its axis
-template <int DI, int DJ, int DK>
-struct Reach {
-    static constexpr bool xx = DJ == 0 && DK == 0;
-    static constexpr bool yy = DI == 0 && DK == 0;
-    static constexpr bool zz = DI == 0 && DJ == 0;
-    static constexpr bool xy = (DI == 1 || DI == -1) && DK == 0;
-    static constexpr bool xz = (DI == 1 || DI == -1) && DJ == 0;
-    static constexpr bool yz = (DJ == 1 || DJ == -1) && DI == 0;
-    static constexpr bool dx = DJ == 0 && DK == 0 && DI >= -1 && DI <= 1;
-    static constexpr bool dy = DI == 0 && DK == 0 && DJ >= -1 && DJ <= 1;
-    static constexpr bool dz = DI == 0 && DJ == 0 && DK >= -1 && DK <= 1;
-    static constexpr bool gx = (DI == 1 || DI == -1) && DJ == 0 && DK == 0;   // central phi differences
-    static constexpr bool gy = (DJ == 1 || DJ == -1) && DI == 0 && DK == 0;
-    static constexpr bool gz = DI == 0 && DJ == 0;
-};
 
 // sum_a lambda_a d g_a(c) / d P_B(c') for the gradient-energy parts g_a of
 // TotalEnergyDensity.cpp:133-251 (as in k_tdgl), D the impulse at c' =

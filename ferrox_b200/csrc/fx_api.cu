@@ -1188,6 +1188,11 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
     if (k == "fx.mg_nu1") { c->mg.nu1 = (int)v; return FX_OK; }
     if (k == "fx.graphs") { c->mg.set_graphs(v != 0.0); return FX_OK; }
     if (k == "fx.mg_nu2") { c->mg.nu2 = (int)v; return FX_OK; }
+    if (k == "fx.mg_mixed_cycles") {
+        if (v < 1) return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx.mg_mixed_cycles must be at least 1");
+        c->mg.mixed_cycles = (int)v;
+        return FX_OK;
+    }
     if (k == "fx.phi_ghost_mode") { p.phi_ghost_mode = (int)v; c->dp.ghost_mode = (int)v; c->E_valid = false; return FX_OK; }
     if (k == "dt") { p.dt = v; c->dp.dt = v; return FX_OK; }
     if (k == "alpha") {

@@ -227,14 +227,20 @@ __global__ void __launch_bounds__(256) k_resid_restrict(Op<T> o, const T* __rest
 }
 
 // FP64 residual of the level-0 operator with electrode terms; optional FP32
-// copy for the mixed-precision correction solve.  Each thread walks R64_ZP
+// copy for the mixed-precision correction solve.  With CORR the iterate is
+// x + e (the FP32 correction added in FP64, at every stencil point) and is
+// written to xout (out of place), so the update and the next residual take one
+// pass.  Each thread walks R64_ZP
 // consecutive cells of its z column, carrying the column's x and code values
 // from one cell to the next (the coefficients are those of coeffs<double,
 // true>, same operations); block maxima go to NORM_SLOTS spread slots.
 constexpr int R64_ZP = 4;
 
-__global__ void __launch_bounds__(256) k_resid64(Op<double> o, const double* __restrict__ x, const double* __restrict__ b,
+template <bool CORR>
+__global__ void __launch_bounds__(256) k_resid64(Op<double> o, const double* __restrict__ x, const float* __restrict__ e,
+                                                 const double* __restrict__ b, double* __restrict__ xout,
                                                  float* __restrict__ r32, double* __restrict__ norm) {
+    auto X = [&](int n) -> double { return CORR ? x[n] + (double)e[n] : x[n]; };
     __shared__ double seps[8];
     if (threadIdx.x == 0 && threadIdx.y == 0)
 #pragma unroll
@@ -252,14 +258,14 @@ __global__ void __launch_bounds__(256) k_resid64(Op<double> o, const double* __r
         const int row = col - i;
         const int dso = (jm - j) * o.nx, dno = (jp - j) * o.nx;
         const uint8_t* cd = o.code + o.nxy;   // the k = -1 ghost layer is cd - nxy
-        double xm = k0 > 0 ? x[col + o.nxy * (k0 - 1)] : 0.0;
-        double xc = x[col + o.nxy * k0];
+        double xm = k0 > 0 ? X(col + o.nxy * (k0 - 1)) : 0.0;
+        double xc = X(col + o.nxy * k0);
         double em = seps[__ldg(cd + col + o.nxy * (k0 - 1)) & 7];
         double ec = seps[__ldg(cd + col + o.nxy * k0) & 7];
         const int k1 = min(o.nz, k0 + R64_ZP);
         for (int k = k0; k < k1; ++k) {
             const int c = col + o.nxy * k;
-            const double xp = k < o.nz - 1 ? x[c + o.nxy] : 0.0;
+            const double xp = k < o.nz - 1 ? X(c + o.nxy) : 0.0;
             const double ep = seps[__ldg(cd + c + o.nxy) & 7];
             double extra = 0.0, bcv = 0.0, cb, ct;
             double cw = 0.5 * (ec + seps[__ldg(cd + row + o.nxy * k + im) & 7]) * o.ih2x;
@@ -275,11 +281,12 @@ __global__ void __launch_bounds__(256) k_resid64(Op<double> o, const double* __r
             const double a = o.a ? o.a[c] : 0.0;
             const double diag = -a + cw + ce + cs + cn + cb + ct + extra;
             const int rk = row + o.nxy * k;
-            double off = cw * x[rk + im] + ce * x[rk + ip] + cs * x[c + dso] + cn * x[c + dno];
+            double off = cw * X(rk + im) + ce * X(rk + ip) + cs * X(c + dso) + cn * X(c + dno);
             if (k > 0) off += cb * xm;
             if (k < o.nz - 1) off += ct * xp;
             const double r = (b[c] + bcv) - (diag * xc - off);
             if (r32) r32[c] = (float)r;
+            if (CORR) xout[c] = xc;
             mx = fmax(mx, fabs(r));
             xm = xc; xc = xp;
             em = ec; ec = ep;
@@ -665,10 +672,6 @@ __global__ void __launch_bounds__(256) k_avg_alpha(const Tin* __restrict__ af, T
     ac[(size_t)I + (size_t)ncx * ((size_t)J + (size_t)ncy * K)] = (T)(s / (rx * ry * rz));
 }
 
-__global__ void __launch_bounds__(256) k_add_corr(double* __restrict__ phi, const float* __restrict__ e, long long n) {
-    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x)
-        phi[c] += (double)e[c];
-}
 
 template <typename T>
 T* dalloc(size_t n, size_t& bytes) {
@@ -732,9 +735,11 @@ Multigrid::~Multigrid() {
     cudaFree(d_fvalid_);
     if (g64_.exec) cudaGraphExecDestroy(g64_.exec);
     if (g32_.exec) cudaGraphExecDestroy(g32_.exec);
+    if (g32b_.exec) cudaGraphExecDestroy(g32b_.exec);
     cudaFree(d_norm_);
     if (h_norm_) cudaFreeHost(h_norm_);
     cudaFree(e32_);
+    cudaFree(alt64m_);
     cudaFree(r32_);
 }
 
@@ -919,6 +924,7 @@ int Multigrid::setup(const DevParams& p, const std::vector<uint8_t>& code, bool 
     if (want32) {
         e32_ = dalloc<float>(L0.N, bytes_);
         r32_ = dalloc<float>(L0.N, bytes_);
+        alt64m_ = dalloc<double>(L0.N, bytes_);
         if (!e32_ || !r32_) return -2;
         lev_[0].x32 = e32_;
         lev_[0].b32 = r32_;
@@ -1166,7 +1172,7 @@ int Multigrid::residual64(const DevParams& p, const uint8_t* code, const double*
     dim3 b2(32, 8), g2((L.n[0] + 31) / 32, (L.n[1] + 7) / 8, L.n[2]);
     (void)r;
     if (prof) prof->begin(PROF_RESID64, s);
-    { ++g_launches; k_resid64<<<dim3(g2.x, g2.y, (L.n[2] + R64_ZP - 1) / R64_ZP), b2, 0, s>>>(o, phi, rhs, nullptr, d_norm_); }
+    { ++g_launches; k_resid64<false><<<dim3(g2.x, g2.y, (L.n[2] + R64_ZP - 1) / R64_ZP), b2, 0, s>>>(o, phi, nullptr, rhs, nullptr, nullptr, d_norm_); }
     if (prof) prof->end(s);
     cudaMemcpyAsync(h_norm_, d_norm_, NORM_SLOTS * 8, cudaMemcpyDeviceToHost, s);
     cudaError_t e = cudaStreamSynchronize(s);
@@ -1239,41 +1245,52 @@ int Multigrid::solve_mixed(const DevParams& p, const uint8_t* code, double* phi,
                            int maxit, cudaStream_t s, MGStats* st) {
     MGLevel& L = lev_[0];
     Op<double> o64 = make_op<double>(L, 0, code, eps_, has_alpha_ ? a0_64 : nullptr, true, p);
-    dim3 b2(32, 8), g2((L.n[0] + 31) / 32, (L.n[1] + 7) / 8, L.n[2]);
-    auto resid = [&]() {
-        cudaMemsetAsync(d_norm_, 0, NORM_SLOTS * 8, s);
-        if (prof) prof->begin(PROF_RESID64, s);
-        ++g_launches;
-        k_resid64<<<dim3(g2.x, g2.y, (L.n[2] + R64_ZP - 1) / R64_ZP), b2, 0, s>>>(o64, phi, rhs, r32_, d_norm_);
-        if (prof) prof->end(s);
-        cudaMemcpyAsync(h_norm_, d_norm_, NORM_SLOTS * 8, cudaMemcpyDeviceToHost, s);
-    };
-    resid();
+    dim3 b2(32, 8), g2((L.n[0] + 31) / 32, (L.n[1] + 7) / 8, (L.n[2] + R64_ZP - 1) / R64_ZP);
+    // the FP64 iterate alternates between phi and alt64m_: each refinement
+    // step adds the FP32 correction while it forms the next residual
+    double* buf[2] = {phi, alt64m_};
+    int cur = 0;
+    cudaMemsetAsync(d_norm_, 0, NORM_SLOTS * 8, s);
+    if (prof) prof->begin(PROF_RESID64, s);
+    ++g_launches;
+    k_resid64<false><<<g2, b2, 0, s>>>(o64, phi, nullptr, rhs, nullptr, r32_, d_norm_);
+    if (prof) prof->end(s);
+    cudaMemcpyAsync(h_norm_, d_norm_, NORM_SLOTS * 8, cudaMemcpyDeviceToHost, s);
     int e = (int)cudaStreamSynchronize(s);
     if (e) return e;
     double rn = slots_max();
-    int it = 0;
+    int it = 0, cycles = 0;
+    const int inner = std::max(1, mixed_cycles);
     if (verbose > 1) printf("  refinement %d: |r|/target = %.3e\n", it, rn / target);
-    while (!(rn <= target) && it < maxit) {
-        // FP32 correction cycle on the FP32 residual, FP64 update and FP64
-        // residual of the updated phi
-        e = replay(g32_, phi, rhs, p, s, [&]() {
+    while (!(rn <= target) && cycles < maxit) {
+        // FP32 correction cycles on the FP32 residual, then the FP64 update
+        // fused with the FP64 residual of the updated iterate
+        double* xin = buf[cur];
+        double* xout = buf[1 - cur];
+        e = replay(cur == 0 ? g32_ : g32b_, xin, rhs, p, s, [&]() {
             cudaMemsetAsync(e32_, 0, L.N * sizeof(float), s);
-            vcycle<float>(p, code, 0, e32_, r32_, false, s);
+            for (int q = 0; q < inner; ++q) vcycle<float>(p, code, 0, e32_, r32_, false, s);
+            cudaMemsetAsync(d_norm_, 0, NORM_SLOTS * 8, s);
             if (prof) prof->begin(PROF_RESID64, s);
             ++g_launches;
-            k_add_corr<<<592, 256, 0, s>>>(phi, e32_, (long long)L.N);
+            k_resid64<true><<<g2, b2, 0, s>>>(o64, xin, e32_, rhs, xout, r32_, d_norm_);
             if (prof) prof->end(s);
-            resid();
+            cudaMemcpyAsync(h_norm_, d_norm_, NORM_SLOTS * 8, cudaMemcpyDeviceToHost, s);
         });
         if (e) return e;
         e = (int)cudaStreamSynchronize(s);
         if (e) return e;
+        cur = 1 - cur;
         ++it;
+        cycles += inner;
         rn = slots_max();
         if (verbose > 1) printf("  refinement %d: |r|/target = %.3e\n", it, rn / target);
     }
-    if (st) { st->cycles = it; st->resid = rn; }
+    if (cur == 1) {
+        e = (int)cudaMemcpyAsync(phi, buf[1], L.N * sizeof(double), cudaMemcpyDeviceToDevice, s);
+        if (e) return e;
+    }
+    if (st) { st->cycles = cycles; st->resid = rn; }
     return rn <= target ? 0 : -3;
 }
 

@@ -106,6 +106,7 @@ public:
     size_t bytes() const { return bytes_; }
     const std::vector<MGLevel>& levels() const { return lev_; }
     int nu1 = 2, nu2 = 1, nu_bottom = 40;
+    int mixed_cycles = 2;    // FP32 V-cycles per FP64 refinement step
     Prof* prof = nullptr;
     int verbose = 0;
     void set_graphs(bool on) { use_graphs_ = on; }
@@ -120,6 +121,7 @@ private:
     double* h_norm_ = nullptr;       // pinned host
     float* e32_ = nullptr;           // level-0 FP32 correction
     float* r32_ = nullptr;           // level-0 FP32 residual
+    double* alt64m_ = nullptr;       // second FP64 level-0 iterate of the mixed solve
     double* cp0_64_ = nullptr;       // level-0 line scratch
     float* cp0_32_ = nullptr;
     size_t bytes_ = 0;
@@ -134,7 +136,7 @@ private:
         int nu1 = 0, nu2 = 0;
         long long launches = 0;
     };
-    GraphCache g64_, g32_;
+    GraphCache g64_, g32_, g32b_;   // g32b_: the refinement step from the second FP64 buffer
     bool use_graphs_ = true;
     template <typename F> int replay(GraphCache& g, const void* x, const void* rhs, const DevParams& p, cudaStream_t s, F&& enqueue);
     int coarse_top64_ = -1, coarse_top32_ = -1;   // first level run by the one-CTA kernel
