@@ -104,7 +104,10 @@ __device__ double block_max_all(double v) {
 __device__ __forceinline__ double sdiv(double a, double b) { return a / b; }
 __device__ __forceinline__ float sdiv(float a, float b) { return __fdividef(a, b); }
 
-template <typename T, bool FINE>
+// ZERO: the first half sweep (colour 0) from x = 0: the colour-0 value is
+// (b + electrode terms) / diag and the colour-1 cell of the same x pair is
+// set to 0, so the caller need not clear x first (even nx only)
+template <typename T, bool FINE, bool ZERO = false>
 __global__ void __launch_bounds__(256) k_rbgs(Op<T> o, T* __restrict__ x, const T* __restrict__ b, int color) {
     __shared__ T seps[8];
     if (FINE) {
@@ -124,6 +127,11 @@ __global__ void __launch_bounds__(256) k_rbgs(Op<T> o, T* __restrict__ x, const 
     T cw, ce, cs, cn, cb, ct, diag, bcv;
     coeffs<T, FINE>(o, i, j, k, c, im, ip, jm, jp, cw, ce, cs, cn, cb, ct, diag, bcv, seps);
     const int row = c - i;
+    if (ZERO) {
+        x[c] = sdiv(b[c] + bcv, diag);
+        x[c + ((i & 1) ? -1 : 1)] = T(0);
+        return;
+    }
     T s = b[c] + bcv + cw * x[row + im] + ce * x[row + ip] + cs * x[c + (jm - j) * o.nx] +
           cn * x[c + (jp - j) * o.nx];
     if (k > 0) s += cb * x[c - o.nxy];
@@ -1064,9 +1072,13 @@ void Multigrid::launch_coarse(int top, cudaStream_t s) {
     if (prof) prof->end(s);
 }
 
+// a level whose first half sweep can start from an uncleared x (point
+// red-black with x / colour pairs)
+static bool zero_first_ok(const MGLevel& L) { return !L.line && L.n[0] % 2 == 0; }
+
 template <typename T>
 void Multigrid::smooth(const DevParams& p, const uint8_t* code, int l, T* x, const T* b, bool inhom, int sweeps,
-                       cudaStream_t s) {
+                       cudaStream_t s, bool zero) {
     MGLevel& L = lev_[l];
     const T* a = nullptr;
     if (has_alpha_) {
@@ -1089,15 +1101,23 @@ void Multigrid::smooth(const DevParams& p, const uint8_t* code, int l, T* x, con
         for (int it = 0; it < sweeps; ++it)
             for (int color = 0; color < 2; ++color) {
                 if (prof) prof->begin(l == 0 ? PROF_SMOOTH_L0 : l == 1 ? PROF_MG_L1 : l == 2 ? PROF_MG_L2 : PROF_MG_COARSE, s);
-                if (l == 0) { ++g_launches; k_rbgs<T, true><<<g2, b2, 0, s>>>(o, x, b, color); }
-                else { ++g_launches; k_rbgs<T, false><<<g2, b2, 0, s>>>(o, x, b, color); }
+                const bool z = zero && it == 0 && color == 0;
+                ++g_launches;
+                if (l == 0) {
+                    if (z) k_rbgs<T, true, true><<<g2, b2, 0, s>>>(o, x, b, color);
+                    else k_rbgs<T, true><<<g2, b2, 0, s>>>(o, x, b, color);
+                } else {
+                    if (z) k_rbgs<T, false, true><<<g2, b2, 0, s>>>(o, x, b, color);
+                    else k_rbgs<T, false><<<g2, b2, 0, s>>>(o, x, b, color);
+                }
                 if (prof) prof->end(s);
             }
     }
 }
 
 template <typename T>
-void Multigrid::vcycle(const DevParams& p, const uint8_t* code, int l, T* x, const T* b, bool inhom, cudaStream_t s) {
+void Multigrid::vcycle(const DevParams& p, const uint8_t* code, int l, T* x, const T* b, bool inhom, cudaStream_t s,
+                       bool zero) {
     MGLevel& L = lev_[l];
     const int last = (int)lev_.size() - 1;
     if (l > 0 && l == coarse_top<T>()) {
@@ -1106,10 +1126,12 @@ void Multigrid::vcycle(const DevParams& p, const uint8_t* code, int l, T* x, con
     }
     if (l == last) {
         const bool exact = L.line && L.n[0] * L.n[1] == 1;
-        smooth<T>(p, code, l, x, b, inhom, exact ? 1 : nu_bottom, s);
+        if (zero && !zero_first_ok(L)) cudaMemsetAsync(x, 0, L.N * sizeof(T), s);
+        smooth<T>(p, code, l, x, b, inhom, exact ? 1 : nu_bottom, s, zero && zero_first_ok(L));
         return;
     }
-    smooth<T>(p, code, l, x, b, inhom, nu1, s);
+    if (zero && !zero_first_ok(L)) cudaMemsetAsync(x, 0, L.N * sizeof(T), s);
+    smooth<T>(p, code, l, x, b, inhom, nu1, s, zero && zero_first_ok(L));
     MGLevel& C = lev_[l + 1];
     const T* a = nullptr;
     if (has_alpha_) {
@@ -1140,8 +1162,7 @@ void Multigrid::vcycle(const DevParams& p, const uint8_t* code, int l, T* x, con
 #undef FX_RR
     }
     if (prof) prof->end(s);
-    cudaMemsetAsync(lx<T>(C), 0, C.N * sizeof(T), s);
-    vcycle<T>(p, code, l + 1, lx<T>(C), lb<T>(C), false, s);
+    vcycle<T>(p, code, l + 1, lx<T>(C), lb<T>(C), false, s, true);   // coarse correction from zero
     dim3 g3((L.n[0] + 31) / 32, (L.n[1] + 7) / 8, L.n[2]);
     if (prof) prof->begin(l == 0 ? PROF_PROLONG_L0 : l == 1 ? PROF_MG_L1 : l == 2 ? PROF_MG_L2 : PROF_MG_COARSE, s);
     ++g_launches;
@@ -1161,7 +1182,7 @@ void Multigrid::vcycle(const DevParams& p, const uint8_t* code, int l, T* x, con
 #undef FX_PR
     }
     if (prof) prof->end(s);
-    smooth<T>(p, code, l, x, b, inhom, nu2, s);
+    smooth<T>(p, code, l, x, b, inhom, nu2, s, false);
 }
 
 int Multigrid::residual64(const DevParams& p, const uint8_t* code, const double* phi, const double* rhs, double* r,
@@ -1220,7 +1241,7 @@ int Multigrid::solve64(const DevParams& p, const uint8_t* code, double* phi, con
         // final residual is checked before returning
         e = replay(g64_, phi, rhs, p, s, [&]() {
             cudaMemsetAsync(d_norm_, 0, NORM_SLOTS * 8, s);
-            vcycle<double>(p, code, 0, phi, rhs, true, s);
+            vcycle<double>(p, code, 0, phi, rhs, true, s, false);
             cudaMemcpyAsync(h_norm_, d_norm_, NORM_SLOTS * 8, cudaMemcpyDeviceToHost, s);
         });
         if (e) return e;
@@ -1268,8 +1289,7 @@ int Multigrid::solve_mixed(const DevParams& p, const uint8_t* code, double* phi,
         double* xin = buf[cur];
         double* xout = buf[1 - cur];
         e = replay(cur == 0 ? g32_ : g32b_, xin, rhs, p, s, [&]() {
-            cudaMemsetAsync(e32_, 0, L.N * sizeof(float), s);
-            for (int q = 0; q < inner; ++q) vcycle<float>(p, code, 0, e32_, r32_, false, s);
+            for (int q = 0; q < inner; ++q) vcycle<float>(p, code, 0, e32_, r32_, false, s, q == 0);
             cudaMemsetAsync(d_norm_, 0, NORM_SLOTS * 8, s);
             if (prof) prof->begin(PROF_RESID64, s);
             ++g_launches;
@@ -1294,7 +1314,7 @@ int Multigrid::solve_mixed(const DevParams& p, const uint8_t* code, double* phi,
     return rn <= target ? 0 : -3;
 }
 
-template void Multigrid::vcycle<double>(const DevParams&, const uint8_t*, int, double*, const double*, bool, cudaStream_t);
-template void Multigrid::vcycle<float>(const DevParams&, const uint8_t*, int, float*, const float*, bool, cudaStream_t);
+template void Multigrid::vcycle<double>(const DevParams&, const uint8_t*, int, double*, const double*, bool, cudaStream_t, bool);
+template void Multigrid::vcycle<float>(const DevParams&, const uint8_t*, int, float*, const float*, bool, cudaStream_t, bool);
 
 }  // namespace fx

@@ -146,8 +146,11 @@ private:
     double slots_max() const;
     template <typename T> int coarse_top() const;
     template <typename T> void launch_coarse(int top, cudaStream_t s);
-    template <typename T> void vcycle(const DevParams& p, const uint8_t* code, int l, T* x0, const T* b0, bool inhom, cudaStream_t s);
-    template <typename T> void smooth(const DevParams& p, const uint8_t* code, int l, T* x, const T* b, bool inhom, int sweeps, cudaStream_t s);
+    // zero: x starts at 0 (not read, not cleared by the caller)
+    template <typename T> void vcycle(const DevParams& p, const uint8_t* code, int l, T* x0, const T* b0, bool inhom, cudaStream_t s,
+                                      bool zero);
+    template <typename T> void smooth(const DevParams& p, const uint8_t* code, int l, T* x, const T* b, bool inhom, int sweeps, cudaStream_t s,
+                                      bool zero);
 };
 
 }  // namespace fx
