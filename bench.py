@@ -48,6 +48,23 @@ TRAFFIC = {("mfism", "fp64", "smooth_l0"): 59.35e6}
 FALLBACK_HBM_GBS = 6650.0
 
 
+def max_over_ranks(ms: float, world: int, device: str = "cuda") -> float:
+    """The slowest rank's time: every rank takes part in the same MAX
+    all-reduce (a no-op on one rank)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(cells: int, steps: int, world: int, ms_max: float) -> float:
+    """Cell updates per second of the whole job: every replica advances its
+    own copy of the deck (weak scaling), timed by the slowest rank."""
+    return cells * steps * world / (ms_max / 1e3)
+
+
 def deck(name: str):
     from ferrox_b200 import decks
     nx, ny, nz = WORKLOADS[name]["shape"]
@@ -397,11 +414,8 @@ def main() -> None:
     f.set_param("fx.profile", 0)
     if done != args.steps:
         raise RuntimeError(f"the reference loop ended after {done} of {args.steps} steps")
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = N * args.steps * world / (ms_max / 1e3)
+    ms_max = max_over_ranks(ms, world)
+    value = whole_job_rate(N, args.steps, world, ms_max)
 
     # end to end through the public API with host buffers: the initial P
     # uploaded from pinned host memory, per step the applied voltage in and the
@@ -427,11 +441,8 @@ def main() -> None:
     e1.record(stream)
     torch.cuda.synchronize()
     barrier()
-    ems = e0.elapsed_time(e1)
-    t = torch.tensor([ems], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = N * ke * world / (float(t.item()) / 1e3)
+    ems = max_over_ranks(e0.elapsed_time(e1), world)
+    e2e_value = whole_job_rate(N, ke, world, ems)
     h2d = (3 * N * 8 + ke * 8) / ke
     d2h = (ke * 24 + 2 * N * 8) / ke
 
