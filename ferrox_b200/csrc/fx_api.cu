@@ -147,6 +147,11 @@ struct fx_ctx {
     double* h_out = nullptr;
     bool E_valid = false;
     bool rhs_is_newton = false;
+    // phi of the previous step's first solve, for the extrapolated initial
+    // iterate; valid only while nothing but time steps changed the state
+    double* d_phi_hist = nullptr;
+    bool hist_valid = false;
+    double hist_vlo = 0.0, hist_vhi = 0.0;
     size_t dev_bytes = 0;
     Multigrid mg;
     bool mg_ready = false;
@@ -494,7 +499,30 @@ int mg_solve(fx_ctx* c, const double* rhs, double nb, double nbp) {
 }
 
 // ComputePhi_Rho, ElectrostaticSolver.cpp:678-747, for P in buffer `buf`
-int compute_phi_rho_P(fx_ctx* c, int buf) {
+// the first solve of a time step starts from 2 phi^n - phi^(n-1) (the
+// multigrid's initial iterate only: the Newton linearisation point stays
+// phi^n); skipped after a voltage change or any other change of the state
+int start_guess(fx_ctx* c) {
+    if (!c->par.phi_extrapolate || !c->par.warm_start) return FX_OK;
+    if (!c->d_phi_hist) {
+        int r = dmalloc(c, &c->d_phi_hist, c->N);
+        if (r) return r;
+        c->hist_valid = false;
+    }
+    if (c->hist_valid && c->hist_vlo == c->dp.V_lo && c->hist_vhi == c->dp.V_hi) {
+        ++g_launches;
+        int r = k_status(c, launch_phi_extrap(c->dp, c->d_phi, c->d_phi_hist, c->s));
+        if (r) return r;
+    } else {
+        FX_CUDA(c, cudaMemcpyAsync(c->d_phi_hist, c->d_phi, c->N * 8, cudaMemcpyDeviceToDevice, c->s));
+    }
+    c->hist_valid = true;
+    c->hist_vlo = c->dp.V_lo;
+    c->hist_vhi = c->dp.V_hi;
+    return FX_OK;
+}
+
+int compute_phi_rho_P(fx_ctx* c, int buf, bool step_start) {
     int r = ensure_device(c);
     if (r) return r;
     c->E_valid = false;
@@ -506,6 +534,7 @@ int compute_phi_rho_P(fx_ctx* c, int buf) {
         if (r) return r;
         const double nb = c->h_out[0], nbp = c->h_out[1];
         c->mg.set_alpha(nullptr, nullptr, false, c->s);
+        if (step_start && (r = start_guess(c))) return r;
         r = mg_solve(c, c->d_rhsP, nb, nbp);
         if (r) return r;
         c->rhs_is_newton = false;
@@ -537,6 +566,7 @@ int compute_phi_rho_P(fx_ctx* c, int buf) {
         if (r) return r;
         const double nb = c->h_out[0], nbp = c->h_out[1];
         c->mg.set_alpha(c->d_alpha, c->d_alpha32, true, c->s);
+        if (step_start && passes == 1 && (r = start_guess(c))) return r;
         r = mg_solve(c, c->d_rhs, nb, nbp);
         if (r) return r;
         ++g_launches;
@@ -558,9 +588,7 @@ int compute_phi_rho_P(fx_ctx* c, int buf) {
     return FX_OK;
 }
 
-int compute_phi_rho(fx_ctx* c) { return compute_phi_rho_P(c, c->cur); }
-
-int compute_phi_rho_P(fx_ctx* c, int buf);
+int compute_phi_rho(fx_ctx* c) { return compute_phi_rho_P(c, c->cur, false); }
 
 // main.cpp:280-348: Order 1 is one fused Euler pass; Order 2 is a predictor
 // pass (f^n kept, P* into the other buffer), ComputePhi_Rho at P*, and a
@@ -590,7 +618,7 @@ int tdgl_update(fx_ctx* c) {
     r = k_status(c, launch_tdgl(c->dp, mixed, 1, c->d_code, c->d_var, c->d_vt, Pin, Pout, c->d_phi, fb, nullptr, c->s));
     c->prof.end(c->s);
     if (r) return r;
-    r = compute_phi_rho_P(c, nb);
+    r = compute_phi_rho_P(c, nb, false);
     if (r) return r;
     const double* Ppre[3] = {Pout[0], Pout[1], Pout[2]};
     double* Pnew[3] = {c->scalarP ? nullptr : c->d_P[c->cur][0], c->scalarP ? nullptr : c->d_P[c->cur][1], c->d_P[c->cur][2]};
@@ -630,7 +658,7 @@ int check_steady(fx_ctx* c, int step) {
 // one pass of main.cpp:261-621; returns 1 when the loop breaks
 int step_once(fx_ctx* c) {
     const int step = c->step + 1;
-    int r = compute_phi_rho(c);
+    int r = compute_phi_rho_P(c, c->cur, true);
     if (r) return r;
     r = tdgl_update(c);
     if (r) return r;
@@ -1092,7 +1120,7 @@ void fx_destroy(fx_ctx* c) {
             for (int d = 0; d < 3; ++d) cudaFree(c->d_P[b][d]);
         for (double* a : {c->d_phi, c->d_phi_old, c->d_phi_prev, c->d_rho, c->d_e, c->d_h, c->d_alpha, c->d_rhs,
                           c->d_rhsP, c->d_dphi, c->d_E[0], c->d_E[1], c->d_E[2], c->d_f[0], c->d_f[1], c->d_f[2],
-                          c->d_part, c->d_out})
+                          c->d_part, c->d_out, c->d_phi_hist})
             cudaFree(a);
         cudaFree(c->d_alpha32);
         cudaFree(c->d_counter);
@@ -1135,7 +1163,8 @@ int fx_get_param(const fx_ctx* c, const char* key, double* v) {
         {"plot_int", p.plot_int}, {"fx.mg_rtol", p.mg_rtol}, {"fx.phi_ghost_mode", p.phi_ghost_mode},
         {"fx.sweep_mode", p.sweep_mode}, {"fx.steps_per_voltage", p.steps_per_voltage},
         {"fx.newton_max_iter", p.newton_max_iter}, {"fx.mg_max_iter", p.mg_max_iter}, {"fx.precision", p.precision},
-        {"fx.warm_start", p.warm_start}, {"contains_sc", c->contains_sc ? 1.0 : 0.0},
+        {"fx.warm_start", p.warm_start}, {"fx.phi_extrapolate", p.phi_extrapolate},
+        {"contains_sc", c->contains_sc ? 1.0 : 0.0},
         {"V_lo", c->dp.V_lo}, {"V_hi", c->dp.V_hi}, {"phi_ref", phi_ref()},
         {"intrinsic_carrier_concentration", std::sqrt(kNc * kNv) * exp(-0.5 * kQ * kEg / (kKb * kT))},
         {"num_variants", (double)c->variants.size()}, {"fx.newton_tol", p.newton_tol},
@@ -1176,13 +1205,14 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
     if (!c || !key) return FX_ERR_INVALID_ARGUMENT;
     const std::string k(key);
     Params& p = c->par;
-    if (k != "fx.profile" && k != "fx.verbose" && k != "fx.graphs") ++c->gen;
+    if (k != "fx.profile" && k != "fx.verbose" && k != "fx.graphs") { ++c->gen; c->hist_valid = false; }
     if (k == "Phi_Bc_hi") { c->Phi_Bc_hi = v; electrode_values(c); c->E_valid = false; return FX_OK; }
     if (k == "Phi_Bc_lo") { p.Phi_Bc_lo = v; electrode_values(c); c->E_valid = false; return FX_OK; }
     if (k == "fx.mg_rtol") { p.mg_rtol = v; return FX_OK; }
     if (k == "fx.mg_max_iter") { p.mg_max_iter = (int)v; return FX_OK; }
     if (k == "fx.newton_max_iter") { p.newton_max_iter = (int)v; return FX_OK; }
     if (k == "fx.warm_start") { p.warm_start = (int)v; return FX_OK; }
+    if (k == "fx.phi_extrapolate") { p.phi_extrapolate = (int)v; return FX_OK; }
     if (k == "fx.verbose") { p.verbose = (int)v; c->mg.verbose = (int)v; return FX_OK; }
     if (k == "fx.profile") { c->prof.collect(); c->prof.on = v != 0.0; return FX_OK; }
     if (k == "fx.mg_nu1") { c->mg.nu1 = (int)v; return FX_OK; }
@@ -1226,7 +1256,7 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
 
 int fx_set_precision(fx_ctx* c, int mode) {
     if (!c || (mode != 0 && mode != 1)) return FX_ERR_INVALID_ARGUMENT;
-    if (c) ++c->gen;
+    if (c) { ++c->gen; c->hist_valid = false; }
     if (c->dev && mode != c->par.precision)
         return set_err(c, FX_ERR_INVALID_ARGUMENT, "precision must be chosen before the first device call");
     c->par.precision = mode;
@@ -1234,7 +1264,7 @@ int fx_set_precision(fx_ctx* c, int mode) {
 }
 
 int fx_set_initial_P(fx_ctx* c, const double* Px, const double* Py, const double* Pz, size_t n) {
-    if (c) ++c->gen;
+    if (c) { ++c->gen; c->hist_valid = false; }
     if (!c || !Pz || n != c->N) return c ? set_err(c, FX_ERR_INVALID_ARGUMENT, "P arrays must hold nx*ny*nz values") : FX_ERR_INVALID_ARGUMENT;
     const double* src[3] = {Px, Py, Pz};
     bool zero_xy = true;
@@ -1286,7 +1316,7 @@ int fx_set_grains(fx_ctx* c, const uint8_t* gid, size_t n, const double* ang, co
 
 int fx_set_grain_alpha(fx_ctx* c, const double* alpha, int ng) {
     if (!c || !alpha || ng <= 0) return FX_ERR_INVALID_ARGUMENT;
-    if (c) ++c->gen;
+    if (c) { ++c->gen; c->hist_valid = false; }
     if (!c->grains_set) return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx_set_grains must come first");
     c->galpha.assign(alpha, alpha + ng);
     try {
@@ -1314,7 +1344,7 @@ int fx_get_field(fx_ctx* c, int f, double* out, size_t n) {
 
 int fx_set_field(fx_ctx* c, int f, const double* in, size_t n) {
     if (!c || !in) return FX_ERR_INVALID_ARGUMENT;
-    ++c->gen;
+    ++c->gen; c->hist_valid = false;
     if (n != c->N) return set_err(c, FX_ERR_INVALID_ARGUMENT, "field buffers hold nx*ny*nz values");
     if (f == FX_FIELD_PX || f == FX_FIELD_PY || f == FX_FIELD_PZ) {
         if (f != FX_FIELD_PZ && c->scalarP) {
@@ -1344,7 +1374,7 @@ int fx_set_field(fx_ctx* c, int f, const double* in, size_t n) {
 
 int fx_compute_poisson_rhs(fx_ctx* c) {
     if (!c) return FX_ERR_INVALID_ARGUMENT;
-    ++c->gen;
+    ++c->gen; c->hist_valid = false;
     int r = ensure_device(c);
     if (r) return r;
     r = compute_rhs_p(c, false, c->cur);
@@ -1369,7 +1399,7 @@ int fx_compute_poisson_rhs(fx_ctx* c) {
 
 int fx_compute_rho(fx_ctx* c) {
     if (!c) return FX_ERR_INVALID_ARGUMENT;
-    ++c->gen;
+    ++c->gen; c->hist_valid = false;
     int r = ensure_device(c);
     if (r) return r;
     ++g_launches;
@@ -1382,7 +1412,7 @@ int fx_compute_rho(fx_ctx* c) {
 
 int fx_compute_phi_rho(fx_ctx* c) {
     if (!c) return FX_ERR_INVALID_ARGUMENT;
-    ++c->gen;
+    ++c->gen; c->hist_valid = false;
     return compute_phi_rho(c);
 }
 
@@ -1397,7 +1427,7 @@ int fx_compute_E(fx_ctx* c) {
 
 int fx_tdgl_euler(fx_ctx* c) {
     if (!c) return FX_ERR_INVALID_ARGUMENT;
-    ++c->gen;
+    ++c->gen; c->hist_valid = false;
     int r = tdgl_update(c);
     if (r) return r;
     FX_CUDA(c, cudaStreamSynchronize(c->s));
@@ -1406,7 +1436,7 @@ int fx_tdgl_euler(fx_ctx* c) {
 
 int fx_set_phi_bc(fx_ctx* c) {
     if (!c) return FX_ERR_INVALID_ARGUMENT;
-    ++c->gen;
+    ++c->gen; c->hist_valid = false;
     electrode_values(c);
     c->E_valid = false;
     return FX_OK;
@@ -1577,6 +1607,7 @@ int fx_forward_record(fx_ctx* c, const fx_loss_spec* sp, double* loss) {
             return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx_forward_record: non-finite target or v_shape");
     if (!std::isfinite(sp->v_amp)) return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx_forward_record: non-finite v_amp");
     ++c->gen;
+    c->hist_valid = false;
     const int r = forward_record(c, sp, loss);
     if (r) c->adj.valid = false;
     return r;
@@ -1589,6 +1620,7 @@ int fx_backward(fx_ctx* c, double* grads, int ngrads) {
     if (!c->adj.valid) return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx_backward: no fx_forward_record to differentiate");
     if (c->adj.gen != c->gen)
         return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx_backward: the context changed since fx_forward_record");
+    c->hist_valid = false;
     const int r = backward(c, grads, ngrads);
     if (r) {
         c->adj.valid = false;

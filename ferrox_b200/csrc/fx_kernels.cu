@@ -503,6 +503,21 @@ int launch_mean_p(const DevParams& p, const uint8_t* code, const double* const P
     return (int)cudaGetLastError();
 }
 
+// initial iterate of a step's first Poisson solve: phi := 2 phi - hist and
+// hist := the old phi (linear extrapolation in time from the last two steps)
+__global__ void __launch_bounds__(256) k_phi_extrap(double* __restrict__ phi, double* __restrict__ hist, long long n) {
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        const double t = phi[c];
+        phi[c] = 2.0 * t - hist[c];
+        hist[c] = t;
+    }
+}
+
+int launch_phi_extrap(const DevParams& p, double* phi, double* hist, cudaStream_t s) {
+    k_phi_extrap<<<p.ngrid_red, RED_THREADS, 0, s>>>(phi, hist, p.N);
+    return (int)cudaGetLastError();
+}
+
 int launch_efield(const DevParams& p, const uint8_t* var, const Variant* vt, const double* phi, double* E[3],
                   cudaStream_t s) {
     const dim3 g = cell_grid(p), b(32, 8);

@@ -467,6 +467,7 @@ Params make_params(const Inputs& in) {
         else throw std::runtime_error("inputs: fx.precision must be fp64 or mixed");
     }
     r.query("fx.warm_start", p.warm_start);
+    r.query("fx.phi_extrapolate", p.phi_extrapolate);
     r.query("fx.verbose", p.verbose);
     if (r.has("fx.plot_dir")) p.plot_dir = r.vals("fx.plot_dir")[0];
 
