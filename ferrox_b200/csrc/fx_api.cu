@@ -149,7 +149,8 @@ struct fx_ctx {
     bool rhs_is_newton = false;
     // phi of the previous step's first solve, for the extrapolated initial
     // iterate; valid only while nothing but time steps changed the state
-    double* d_phi_hist = nullptr;
+    double* d_phi_hist[3] = {nullptr, nullptr, nullptr};   // phi of the last steps' first solves
+    int hist_n = 0;                                // how many of them are current
     bool hist_valid = false;
     double hist_vlo = 0.0, hist_vhi = 0.0;
     size_t dev_bytes = 0;
@@ -503,19 +504,26 @@ int mg_solve(fx_ctx* c, const double* rhs, double nb, double nbp) {
 // multigrid's initial iterate only: the Newton linearisation point stays
 // phi^n); skipped after a voltage change or any other change of the state
 int start_guess(fx_ctx* c) {
-    if (!c->par.phi_extrapolate || !c->par.warm_start) return FX_OK;
-    if (!c->d_phi_hist) {
-        int r = dmalloc(c, &c->d_phi_hist, c->N);
-        if (r) return r;
-        c->hist_valid = false;
-    }
-    if (c->hist_valid && c->hist_vlo == c->dp.V_lo && c->hist_vhi == c->dp.V_hi) {
+    const int order = std::min(3, c->par.phi_extrapolate);
+    if (order <= 0 || !c->par.warm_start) return FX_OK;
+    for (int q = 0; q < order; ++q)
+        if (!c->d_phi_hist[q]) {
+            int r = dmalloc(c, &c->d_phi_hist[q], c->N);
+            if (r) return r;
+            c->hist_n = 0;
+        }
+    if (!c->hist_valid || c->hist_vlo != c->dp.V_lo || c->hist_vhi != c->dp.V_hi) c->hist_n = 0;
+    const int use = std::min(order, c->hist_n);   // steps of history available
+    if (use > 0) {
+        // the histories kept are those of `order`; shift all of them
+        double* h[3] = {c->d_phi_hist[0], order >= 2 ? c->d_phi_hist[1] : nullptr, order >= 3 ? c->d_phi_hist[2] : nullptr};
         ++g_launches;
-        int r = k_status(c, launch_phi_extrap(c->dp, c->d_phi, c->d_phi_hist, c->s));
+        int r = k_status(c, launch_phi_extrap(c->dp, use, c->d_phi, h, c->s));
         if (r) return r;
     } else {
-        FX_CUDA(c, cudaMemcpyAsync(c->d_phi_hist, c->d_phi, c->N * 8, cudaMemcpyDeviceToDevice, c->s));
+        FX_CUDA(c, cudaMemcpyAsync(c->d_phi_hist[0], c->d_phi, c->N * 8, cudaMemcpyDeviceToDevice, c->s));
     }
+    c->hist_n = std::min(order, c->hist_n + 1);
     c->hist_valid = true;
     c->hist_vlo = c->dp.V_lo;
     c->hist_vhi = c->dp.V_hi;
@@ -1120,7 +1128,7 @@ void fx_destroy(fx_ctx* c) {
             for (int d = 0; d < 3; ++d) cudaFree(c->d_P[b][d]);
         for (double* a : {c->d_phi, c->d_phi_old, c->d_phi_prev, c->d_rho, c->d_e, c->d_h, c->d_alpha, c->d_rhs,
                           c->d_rhsP, c->d_dphi, c->d_E[0], c->d_E[1], c->d_E[2], c->d_f[0], c->d_f[1], c->d_f[2],
-                          c->d_part, c->d_out, c->d_phi_hist})
+                          c->d_part, c->d_out, c->d_phi_hist[0], c->d_phi_hist[1], c->d_phi_hist[2]})
             cudaFree(a);
         cudaFree(c->d_alpha32);
         cudaFree(c->d_counter);
@@ -1205,7 +1213,11 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
     if (!c || !key) return FX_ERR_INVALID_ARGUMENT;
     const std::string k(key);
     Params& p = c->par;
-    if (k != "fx.profile" && k != "fx.verbose" && k != "fx.graphs") { ++c->gen; c->hist_valid = false; }
+    if (k != "fx.profile" && k != "fx.verbose" && k != "fx.graphs") ++c->gen;
+    // the time history of phi only seeds the next solve's initial iterate;
+    // electrode values are compared on their own, solver settings leave the
+    // trajectory alone, anything else starts the history afresh
+    if (k != "Phi_Bc_hi" && k != "Phi_Bc_lo" && k.compare(0, 3, "fx.") != 0) c->hist_valid = false;
     if (k == "Phi_Bc_hi") { c->Phi_Bc_hi = v; electrode_values(c); c->E_valid = false; return FX_OK; }
     if (k == "Phi_Bc_lo") { p.Phi_Bc_lo = v; electrode_values(c); c->E_valid = false; return FX_OK; }
     if (k == "fx.mg_rtol") { p.mg_rtol = v; return FX_OK; }

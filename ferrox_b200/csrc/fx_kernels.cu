@@ -503,18 +503,30 @@ int launch_mean_p(const DevParams& p, const uint8_t* code, const double* const P
     return (int)cudaGetLastError();
 }
 
-// initial iterate of a step's first Poisson solve: phi := 2 phi - hist and
-// hist := the old phi (linear extrapolation in time from the last two steps)
-__global__ void __launch_bounds__(256) k_phi_extrap(double* __restrict__ phi, double* __restrict__ hist, long long n) {
+// initial iterate of a step's first Poisson solve, extrapolated in time from
+// the last steps' phi (h[0] the previous step's, h[1] the one before, ...):
+// order 1: 2 phi - h0; order 2: 3 phi - 3 h0 + h1; order 3: 4 phi - 6 h0 +
+// 4 h1 - h2.  The histories shift by one step.
+template <int ORDER>
+__global__ void __launch_bounds__(256) k_phi_extrap(double* __restrict__ phi, double* __restrict__ h0,
+                                                    double* __restrict__ h1, double* __restrict__ h2,
+                                                    long long n) {
     for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
-        const double t = phi[c];
-        phi[c] = 2.0 * t - hist[c];
-        hist[c] = t;
+        const double t = phi[c], a = h0[c];
+        const double b = ORDER >= 2 ? h1[c] : 0.0;
+        if (ORDER == 1) phi[c] = 2.0 * t - a;
+        if (ORDER == 2) phi[c] = 3.0 * t - 3.0 * a + b;
+        if (ORDER == 3) phi[c] = 4.0 * t - 6.0 * a + 4.0 * b - h2[c];
+        if (h2) h2[c] = b;
+        if (h1) h1[c] = a;
+        h0[c] = t;
     }
 }
 
-int launch_phi_extrap(const DevParams& p, double* phi, double* hist, cudaStream_t s) {
-    k_phi_extrap<<<p.ngrid_red, RED_THREADS, 0, s>>>(phi, hist, p.N);
+int launch_phi_extrap(const DevParams& p, int order, double* phi, double* const h[3], cudaStream_t s) {
+    if (order >= 3) k_phi_extrap<3><<<p.ngrid_red, RED_THREADS, 0, s>>>(phi, h[0], h[1], h[2], p.N);
+    else if (order == 2) k_phi_extrap<2><<<p.ngrid_red, RED_THREADS, 0, s>>>(phi, h[0], h[1], h[2], p.N);
+    else k_phi_extrap<1><<<p.ngrid_red, RED_THREADS, 0, s>>>(phi, h[0], h[1], h[2], p.N);
     return (int)cudaGetLastError();
 }
 
