@@ -147,6 +147,9 @@ struct fx_ctx {
     double* h_out = nullptr;
     bool E_valid = false;
     bool rhs_is_newton = false;
+    // the Newton loop leaves the carrier densities unwritten: they are formed
+    // from phi (which the last charge evaluation used) when read
+    bool carriers_stale = false;
     // phi of the previous step's first solve, for the extrapolated initial
     // iterate; valid only while nothing but time steps changed the state
     double* d_phi_hist[3] = {nullptr, nullptr, nullptr};   // phi of the last steps' first solves
@@ -580,7 +583,8 @@ int compute_phi_rho_P(fx_ctx* c, int buf, bool step_start) {
         ++g_launches;
         c->prof.begin(PROF_RHO, c->s);
         r = k_status(c, launch_rho(c->dp, c->d_code, c->d_phi, c->d_phi_prev, c->d_rho, c->d_e, c->d_h, c->d_part,
-                                   c->d_counter, c->d_out, 1, c->s));
+                                   c->d_counter, c->d_out, 1, 0, c->s));
+        c->carriers_stale = true;
         c->prof.end(c->s);
         if (r) return r;
         r = read_out(c, 2);
@@ -738,6 +742,19 @@ int host_field(fx_ctx* c, int f, std::vector<double>& out) {
     return 0;
 }
 
+// the carrier densities at the phi of the last charge evaluation (phi has not
+// changed since: the Newton loop ends with it, and fx_set_field forms them
+// before replacing phi)
+int carriers_now(fx_ctx* c) {
+    if (!c->carriers_stale) return FX_OK;
+    ++g_launches;
+    int r = k_status(c, launch_rho(c->dp, c->d_code, c->d_phi, c->d_phi_prev, c->d_rho, c->d_e, c->d_h, c->d_part,
+                                   c->d_counter, c->d_out, 0, 1, c->s));
+    if (r) return r;
+    c->carriers_stale = false;
+    return FX_OK;
+}
+
 int get_field(fx_ctx* c, int f, double* out) {
     std::vector<double> h;
     if (host_field(c, f, h)) {
@@ -760,8 +777,8 @@ int get_field(fx_ctx* c, int f, double* out) {
         if (r) return r;
         src = c->d_E[f - FX_FIELD_EX];
         break;
-    case FX_FIELD_HOLES: src = c->d_h; break;
-    case FX_FIELD_ELECTRONS: src = c->d_e; break;
+    case FX_FIELD_HOLES: { int r = carriers_now(c); if (r) return r; src = c->d_h; break; }
+    case FX_FIELD_ELECTRONS: { int r = carriers_now(c); if (r) return r; src = c->d_e; break; }
     case FX_FIELD_CHARGE: src = c->d_rho; break;
     case FX_FIELD_PHIDIFF: src = c->d_dphi; break;
     case FX_FIELD_ALPHA_CC: src = c->d_alpha; break;
@@ -1374,6 +1391,7 @@ int fx_set_field(fx_ctx* c, int f, const double* in, size_t n) {
         return FX_OK;
     }
     if (f == FX_FIELD_PHI) {
+        if (c->dev) { int r = carriers_now(c); if (r) return r; }
         int r = ensure_device(c);
         if (r) return r;
         FX_CUDA(c, cudaMemcpyAsync(c->d_phi, in, n * 8, cudaMemcpyHostToDevice, c->s));
@@ -1415,8 +1433,9 @@ int fx_compute_rho(fx_ctx* c) {
     int r = ensure_device(c);
     if (r) return r;
     ++g_launches;
+    c->carriers_stale = false;
     r = k_status(c, launch_rho(c->dp, c->d_code, c->d_phi, c->d_phi_prev, c->d_rho, c->d_e, c->d_h, c->d_part,
-                               c->d_counter, c->d_out, 0, c->s));
+                               c->d_counter, c->d_out, 0, 1, c->s));
     if (r) return r;
     FX_CUDA(c, cudaStreamSynchronize(c->s));
     return FX_OK;

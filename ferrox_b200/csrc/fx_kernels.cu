@@ -303,23 +303,29 @@ __global__ void __launch_bounds__(256) k_rho(DevParams p, const uint8_t* __restr
                                              double* __restrict__ rho, double* __restrict__ e_den,
                                              double* __restrict__ h_den, double* __restrict__ part,
                                              unsigned int* __restrict__ counter, double* __restrict__ out,
-                                             int track) {
+                                             int track, int carriers) {
     __shared__ double sh[32];
     __shared__ bool last;
     double s1 = 0.0, s2 = 0.0;
+    // all loads of a cell are issued before its exponentials, and four cells
+    // are in flight per thread, so the memory rounds overlap
+#pragma unroll 4
     for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < p.N; c += (long long)gridDim.x * blockDim.x) {
         const int m = __ldg(code + c + p.nxy) & 3;   // code has one z ghost layer below
         const double ph = phi[c];
+        const double pp = track ? phi_prev[c] : 0.0;
         if (m >= 2) {
             double e, h;
             rho[c] = sc_charge(p, ph, e, h);
-            e_den[c] = e;
-            h_den[c] = h;
+            if (carriers) {
+                e_den[c] = e;
+                h_den[c] = h;
+            }
         } else {
             rho[c] = 0.0;
         }
         if (track) {
-            s1 += fabs(ph - phi_prev[c]);
+            s1 += fabs(ph - pp);
             s2 += fabs(ph);
             phi_prev[c] = ph;
         }
@@ -486,8 +492,9 @@ int launch_newton(const DevParams& p, const uint8_t* code, const double* phi, co
 
 int launch_rho(const DevParams& p, const uint8_t* code, const double* phi, double* phi_prev, double* rho,
                double* e_den, double* h_den, double* part, unsigned int* counter, double* out, int track,
-               cudaStream_t s) {
-    k_rho<<<p.ngrid_red, RED_THREADS, 0, s>>>(p, code, phi, phi_prev, rho, e_den, h_den, part, counter, out, track);
+               int carriers, cudaStream_t s) {
+    k_rho<<<p.ngrid_red, RED_THREADS, 0, s>>>(p, code, phi, phi_prev, rho, e_den, h_den, part, counter, out, track,
+                                             carriers);
     return (int)cudaGetLastError();
 }
 

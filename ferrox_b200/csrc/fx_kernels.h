@@ -19,7 +19,7 @@ int launch_newton(const DevParams& p, const uint8_t* code, const double* phi, co
                   const double* rhs_p, double* alpha, float* alpha32, double* rhs, double* norms, cudaStream_t s);
 int launch_rho(const DevParams& p, const uint8_t* code, const double* phi, double* phi_prev, double* rho,
                double* e_den, double* h_den, double* part, unsigned int* counter, double* out, int track,
-               cudaStream_t s);
+               int carriers, cudaStream_t s);
 int launch_steady(const DevParams& p, const double* phi, double* phi_old, double* dphi, double* out,
                   cudaStream_t s);
 int launch_mean_p(const DevParams& p, const uint8_t* code, const double* const P[3], double* part,
