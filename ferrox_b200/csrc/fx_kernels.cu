@@ -263,6 +263,7 @@ __global__ void __launch_bounds__(256) k_newton(DevParams p, const uint8_t* __re
         for (int q = 0; q < 8; ++q) seps[q] = p.eps[q];
     __syncthreads();
     double nb = 0.0, nbp = 0.0;
+#pragma unroll 4
     for (long long c = (long long)blockIdx.x * 256 + tid; c < p.N; c += (long long)gridDim.x * 256) {
         // the code array carries one z ghost layer below: cell c is at c + nxy
         const int m = __ldg(code + c + p.nxy);

@@ -28,17 +28,22 @@ struct Op {
     const T* bs;
     const T* bb;           // nz + 1 layers
     const T* a;            // alpha (may be null)
+    const T* zc;           // coarse: face beta by plane (bw[nz], bs[nz], bb[nz+1]) when laterally uniform
     T vlo, vhi;            // electrode values (inhomogeneous level-0 operator only)
 };
 
 // couplings of cell (i,j,k) to its six neighbours (already divided by h^2),
 // the diagonal and the electrode contribution to the right-hand side
-template <typename T, bool FINE>
+// KIND: CK_FINE level 0 (material codes), CK_ARRAYS coarse face-beta arrays,
+// CK_PLANES coarse face beta by plane (laterally uniform)
+constexpr int CK_ARRAYS = 0, CK_FINE = 1, CK_PLANES = 2;
+
+template <typename T, int KIND>
 __device__ __forceinline__ void coeffs(const Op<T>& o, int i, int j, int k, int c, int im, int ip, int jm, int jp,
                                        T& cw, T& ce, T& cs, T& cn, T& cb, T& ct, T& diag, T& bcv, const T* eps) {
     T extra = T(0);
     bcv = T(0);
-    if (FINE) {
+    if constexpr (KIND == CK_FINE) {
         const uint8_t* cd = o.code + o.nxy;   // skip the k = -1 ghost layer
         const int row = c - i;
         const T ec = eps[__ldg(cd + c) & 7];
@@ -50,6 +55,15 @@ __device__ __forceinline__ void coeffs(const Op<T>& o, int i, int j, int k, int 
         else { cb = T(0); extra += T(2) * ec * o.ih2z; bcv += T(2) * ec * o.ih2z * o.vlo; }
         if (k < o.nz - 1) ct = T(0.5) * (eps[__ldg(cd + c + o.nxy) & 7] + ec) * o.ih2z;
         else { ct = T(0); extra += T(2) * ec * o.ih2z; bcv += T(2) * ec * o.ih2z * o.vhi; }
+    } else if constexpr (KIND == CK_PLANES) {
+        // a layered stack: every face of a plane has the same beta
+        cw = ce = __ldg(o.zc + k) * o.ih2x;
+        cs = cn = __ldg(o.zc + o.nz + k) * o.ih2y;
+        const T fb = __ldg(o.zc + 2 * o.nz + k), ft = __ldg(o.zc + 2 * o.nz + k + 1);
+        if (k > 0) cb = fb * o.ih2z;
+        else { cb = T(0); extra += T(2) * fb * o.ih2z; }
+        if (k < o.nz - 1) ct = ft * o.ih2z;
+        else { ct = T(0); extra += T(2) * ft * o.ih2z; }
     } else {
         const int row = c - i;
         cw = __ldg(o.bw + c) * o.ih2x;
@@ -107,10 +121,10 @@ __device__ __forceinline__ float sdiv(float a, float b) { return __fdividef(a, b
 // ZERO: the first half sweep (colour 0) from x = 0: the colour-0 value is
 // (b + electrode terms) / diag and the colour-1 cell of the same x pair is
 // set to 0, so the caller need not clear x first (even nx only)
-template <typename T, bool FINE, bool ZERO = false>
+template <typename T, int KIND, bool ZERO = false>
 __global__ void __launch_bounds__(256) k_rbgs(Op<T> o, T* __restrict__ x, const T* __restrict__ b, int color) {
     __shared__ T seps[8];
-    if (FINE) {
+    if (KIND == CK_FINE) {
         if (threadIdx.x == 0 && threadIdx.y == 0)
 #pragma unroll
             for (int q = 0; q < 8; ++q) seps[q] = o.eps[q];
@@ -125,7 +139,7 @@ __global__ void __launch_bounds__(256) k_rbgs(Op<T> o, T* __restrict__ x, const 
     nbr(i, o.nx, im, ip);
     nbr(j, o.ny, jm, jp);
     T cw, ce, cs, cn, cb, ct, diag, bcv;
-    coeffs<T, FINE>(o, i, j, k, c, im, ip, jm, jp, cw, ce, cs, cn, cb, ct, diag, bcv, seps);
+    coeffs<T, KIND>(o, i, j, k, c, im, ip, jm, jp, cw, ce, cs, cn, cb, ct, diag, bcv, seps);
     const int row = c - i;
     if (ZERO) {
         x[c] = sdiv(b[c] + bcv, diag);
@@ -142,11 +156,11 @@ __global__ void __launch_bounds__(256) k_rbgs(Op<T> o, T* __restrict__ x, const 
 // red-black z-line Gauss-Seidel half sweep: color = parity of i + j; each
 // thread solves the tridiagonal system of one column (Thomas), q holds the
 // forward-elimination ratios
-template <typename T, bool FINE>
+template <typename T, int KIND>
 __global__ void __launch_bounds__(128) k_line(Op<T> o, T* __restrict__ x, const T* __restrict__ b, T* __restrict__ q,
                                               int color) {
     __shared__ T seps[8];
-    if (FINE) {
+    if (KIND == CK_FINE) {
         if (threadIdx.x == 0 && threadIdx.y == 0)
 #pragma unroll
             for (int q = 0; q < 8; ++q) seps[q] = o.eps[q];
@@ -162,7 +176,7 @@ __global__ void __launch_bounds__(128) k_line(Op<T> o, T* __restrict__ x, const 
     int c = i + o.nx * j;
     for (int k = 0; k < o.nz; ++k, c += o.nxy) {
         T cw, ce, cs, cn, cb, ct, diag, bcv;
-        coeffs<T, FINE>(o, i, j, k, c, im, ip, jm, jp, cw, ce, cs, cn, cb, ct, diag, bcv, seps);
+        coeffs<T, KIND>(o, i, j, k, c, im, ip, jm, jp, cw, ce, cs, cn, cb, ct, diag, bcv, seps);
         const int row = c - i;
         const T r = b[c] + bcv + cw * x[row + im] + ce * x[row + ip] + cs * x[c + (jm - j) * o.nx] +
                     cn * x[c + (jp - j) * o.nx];
@@ -186,7 +200,7 @@ __global__ void __launch_bounds__(128) k_line(Op<T> o, T* __restrict__ x, const 
 // residual b - A x at the children of each coarse cell, averaged into the
 // coarse right-hand side; optionally the |r|_inf of the level.  RX, RY, RZ
 // are the coarsening ratios (1 or 2).
-template <typename T, bool FINE, int RX, int RY, int RZ>
+template <typename T, int KIND, int RX, int RY, int RZ>
 __global__ void __launch_bounds__(256) k_resid_restrict(Op<T> o, const T* __restrict__ x, const T* __restrict__ b,
                                                         T* __restrict__ bc, int ncx, int ncy, int ncz,
                                                         double* __restrict__ norm) {
@@ -194,7 +208,7 @@ __global__ void __launch_bounds__(256) k_resid_restrict(Op<T> o, const T* __rest
     const int J = blockIdx.y * blockDim.y + threadIdx.y;
     const int K = blockIdx.z;
     __shared__ T seps[8];
-    if (FINE) {
+    if (KIND == CK_FINE) {
         if (threadIdx.x == 0 && threadIdx.y == 0)
 #pragma unroll
             for (int q = 0; q < 8; ++q) seps[q] = o.eps[q];
@@ -215,7 +229,7 @@ __global__ void __launch_bounds__(256) k_resid_restrict(Op<T> o, const T* __rest
                     nbr(i, o.nx, im, ip);
                     nbr(j, o.ny, jm, jp);
                     T cw, ce, cs, cn, cb, ct, diag, bcv;
-                    coeffs<T, FINE>(o, i, j, k, c, im, ip, jm, jp, cw, ce, cs, cn, cb, ct, diag, bcv, seps);
+                    coeffs<T, KIND>(o, i, j, k, c, im, ip, jm, jp, cw, ce, cs, cn, cb, ct, diag, bcv, seps);
                     const int row = c - i;
                     T off = cw * x[row + im] + ce * x[row + ip] + cs * x[c + (jm - j) * o.nx] +
                             cn * x[c + (jp - j) * o.nx];
@@ -270,8 +284,10 @@ __global__ void __launch_bounds__(256) k_resid64(Op<double> o, const double* __r
         double xc = X(col + o.nxy * k0);
         double em = seps[__ldg(cd + col + o.nxy * (k0 - 1)) & 7];
         double ec = seps[__ldg(cd + col + o.nxy * k0) & 7];
-        const int k1 = min(o.nz, k0 + R64_ZP);
-        for (int k = k0; k < k1; ++k) {
+#pragma unroll
+        for (int q = 0; q < R64_ZP; ++q) {
+            const int k = k0 + q;
+            if (k >= o.nz) break;
             const int c = col + o.nxy * k;
             const double xp = k < o.nz - 1 ? X(c + o.nxy) : 0.0;
             const double ep = seps[__ldg(cd + c + o.nxy) & 7];
@@ -704,6 +720,8 @@ Op<T> make_op(const MGLevel& L, int l, const uint8_t* code, const double* eps, c
     if constexpr (sizeof(T) == 8) { o.bw = (const T*)L.bw64; o.bs = (const T*)L.bs64; o.bb = (const T*)L.bb64; }
     else { o.bw = (const T*)L.bw32; o.bs = (const T*)L.bs32; o.bb = (const T*)L.bb32; }
     o.a = a;
+    if constexpr (sizeof(T) == 8) o.zc = l > 0 ? (const T*)L.zc64 : nullptr;
+    else o.zc = l > 0 ? (const T*)L.zc32 : nullptr;
     o.vlo = inhom ? T(p.V_lo) : T(0);
     o.vhi = inhom ? T(p.V_hi) : T(0);
     (void)l;
@@ -739,6 +757,8 @@ Multigrid::~Multigrid() {
         cudaFree(L.bw64); cudaFree(L.bs64); cudaFree(L.bb64); cudaFree(L.a64); cudaFree(L.cp64);
         cudaFree(L.bw32); cudaFree(L.bs32); cudaFree(L.bb32); cudaFree(L.a32); cudaFree(L.cp32);
         for (int d = 0; d < 3; ++d) { cudaFree(L.wf[d]); cudaFree(L.fac64[d]); cudaFree(L.fac32[d]); }
+        cudaFree(L.zc64);
+        cudaFree(L.zc32);
     }
     cudaFree(d_fvalid_);
     if (g64_.exec) cudaGraphExecDestroy(g64_.exec);
@@ -898,6 +918,32 @@ int Multigrid::setup(const DevParams& p, const std::vector<uint8_t>& code, bool 
                         cb[(size_t)i + L.n[0] * ((size_t)j + (size_t)L.n[1] * k)] = s / (rx * ry);
                     }
             fw.swap(cw); fs.swap(cs); fb.swap(cb);
+            // laterally uniform face beta (a layered stack): keep it by plane
+            std::vector<double> zc(3 * L.n[2] + 1);
+            bool uni = true;
+            for (int k = 0; k < L.n[2] && uni; ++k) {
+                const size_t c0 = (size_t)lnxy * k;
+                zc[k] = fw[c0];
+                zc[L.n[2] + k] = fs[c0];
+                for (size_t q = 0; q < lnxy && uni; ++q) uni = fw[c0 + q] == fw[c0] && fs[c0 + q] == fs[c0];
+            }
+            for (int k = 0; k <= L.n[2] && uni; ++k) {
+                const size_t c0 = (size_t)lnxy * k;
+                zc[2 * L.n[2] + k] = fb[c0];
+                for (size_t q = 0; q < lnxy && uni; ++q) uni = fb[c0 + q] == fb[c0];
+            }
+            if (uni) {
+                const size_t nzc = zc.size();
+                if (want64) {
+                    L.zc64 = dalloc<double>(nzc, bytes_);
+                    if (!L.zc64 || cudaMemcpy(L.zc64, zc.data(), nzc * 8, cudaMemcpyHostToDevice) != cudaSuccess) return -2;
+                }
+                if (want32) {
+                    std::vector<float> z32(zc.begin(), zc.end());
+                    L.zc32 = dalloc<float>(nzc, bytes_);
+                    if (!L.zc32 || cudaMemcpy(L.zc32, z32.data(), nzc * 4, cudaMemcpyHostToDevice) != cudaSuccess) return -2;
+                }
+            }
             if (want64) {
                 L.x64 = dalloc<double>(N, bytes_); L.b64 = dalloc<double>(N, bytes_); L.a64 = dalloc<double>(N, bytes_);
                 L.bw64 = dalloc<double>(N, bytes_); L.bs64 = dalloc<double>(N, bytes_); L.bb64 = dalloc<double>(N + lnxy, bytes_);
@@ -1092,8 +1138,10 @@ void Multigrid::smooth(const DevParams& p, const uint8_t* code, int l, T* x, con
         for (int it = 0; it < sweeps; ++it)
             for (int color = 0; color < 2; ++color) {
                 if (prof) prof->begin(l == 0 ? PROF_SMOOTH_L0 : l == 1 ? PROF_MG_L1 : l == 2 ? PROF_MG_L2 : PROF_MG_COARSE, s);
-                if (l == 0) { ++g_launches; k_line<T, true><<<g2, b2, 0, s>>>(o, x, b, q, color); }
-                else { ++g_launches; k_line<T, false><<<g2, b2, 0, s>>>(o, x, b, q, color); }
+                ++g_launches;
+                if (l == 0) k_line<T, CK_FINE><<<g2, b2, 0, s>>>(o, x, b, q, color);
+                else if (o.zc) k_line<T, CK_PLANES><<<g2, b2, 0, s>>>(o, x, b, q, color);
+                else k_line<T, CK_ARRAYS><<<g2, b2, 0, s>>>(o, x, b, q, color);
                 if (prof) prof->end(s);
             }
     } else {
@@ -1104,11 +1152,16 @@ void Multigrid::smooth(const DevParams& p, const uint8_t* code, int l, T* x, con
                 const bool z = zero && it == 0 && color == 0;
                 ++g_launches;
                 if (l == 0) {
-                    if (z) k_rbgs<T, true, true><<<g2, b2, 0, s>>>(o, x, b, color);
-                    else k_rbgs<T, true><<<g2, b2, 0, s>>>(o, x, b, color);
+                    if (z) k_rbgs<T, CK_FINE, true><<<g2, b2, 0, s>>>(o, x, b, color);
+                    else k_rbgs<T, CK_FINE><<<g2, b2, 0, s>>>(o, x, b, color);
                 } else {
-                    if (z) k_rbgs<T, false, true><<<g2, b2, 0, s>>>(o, x, b, color);
-                    else k_rbgs<T, false><<<g2, b2, 0, s>>>(o, x, b, color);
+                    if (o.zc) {
+                        if (z) k_rbgs<T, CK_PLANES, true><<<g2, b2, 0, s>>>(o, x, b, color);
+                        else k_rbgs<T, CK_PLANES><<<g2, b2, 0, s>>>(o, x, b, color);
+                    } else {
+                        if (z) k_rbgs<T, CK_ARRAYS, true><<<g2, b2, 0, s>>>(o, x, b, color);
+                        else k_rbgs<T, CK_ARRAYS><<<g2, b2, 0, s>>>(o, x, b, color);
+                    }
                 }
                 if (prof) prof->end(s);
             }
@@ -1157,7 +1210,7 @@ void Multigrid::vcycle(const DevParams& p, const uint8_t* code, int l, T* x, con
         case 6: FX_RR(F, 2, 2, 1); break;             \
         default: FX_RR(F, 2, 2, 2); break;            \
         }
-        if (l == 0) { FX_RR_ALL(true) } else { FX_RR_ALL(false) }
+        if (l == 0) { FX_RR_ALL(CK_FINE) } else if (o.zc) { FX_RR_ALL(CK_PLANES) } else { FX_RR_ALL(CK_ARRAYS) }
 #undef FX_RR_ALL
 #undef FX_RR
     }

@@ -37,6 +37,10 @@ struct MGLevel {
     // FP32, kept between calls while alpha is unchanged
     double* fac64[3] = {nullptr, nullptr, nullptr};
     float* fac32[3] = {nullptr, nullptr, nullptr};
+    // coarse face beta that depends on z only (layered stacks): per plane
+    // bw[nz], bs[nz], bb[nz + 1] in one array, else null
+    double* zc64 = nullptr;
+    float* zc32 = nullptr;
 };
 
 // Optional per-launch timing: CUDA events around each launch of a kernel
