@@ -59,11 +59,12 @@ __device__ __forceinline__ void coeffs(const Op<T>& o, int i, int j, int k, int 
         // a layered stack: every face of a plane has the same beta
         cw = ce = __ldg(o.zc + k) * o.ih2x;
         cs = cn = __ldg(o.zc + o.nz + k) * o.ih2y;
+        // (level 0: bb[0], bb[nz] are the eps of the electrode-layer cells)
         const T fb = __ldg(o.zc + 2 * o.nz + k), ft = __ldg(o.zc + 2 * o.nz + k + 1);
         if (k > 0) cb = fb * o.ih2z;
-        else { cb = T(0); extra += T(2) * fb * o.ih2z; }
+        else { cb = T(0); extra += T(2) * fb * o.ih2z; bcv += T(2) * fb * o.ih2z * o.vlo; }
         if (k < o.nz - 1) ct = ft * o.ih2z;
-        else { ct = T(0); extra += T(2) * ft * o.ih2z; }
+        else { ct = T(0); extra += T(2) * ft * o.ih2z; bcv += T(2) * ft * o.ih2z * o.vhi; }
     } else {
         const int row = c - i;
         cw = __ldg(o.bw + c) * o.ih2x;
@@ -720,8 +721,8 @@ Op<T> make_op(const MGLevel& L, int l, const uint8_t* code, const double* eps, c
     if constexpr (sizeof(T) == 8) { o.bw = (const T*)L.bw64; o.bs = (const T*)L.bs64; o.bb = (const T*)L.bb64; }
     else { o.bw = (const T*)L.bw32; o.bs = (const T*)L.bs32; o.bb = (const T*)L.bb32; }
     o.a = a;
-    if constexpr (sizeof(T) == 8) o.zc = l > 0 ? (const T*)L.zc64 : nullptr;
-    else o.zc = l > 0 ? (const T*)L.zc32 : nullptr;
+    if constexpr (sizeof(T) == 8) o.zc = (const T*)L.zc64;
+    else o.zc = (const T*)L.zc32;
     o.vlo = inhom ? T(p.V_lo) : T(0);
     o.vhi = inhom ? T(p.V_hi) : T(0);
     (void)l;
@@ -828,9 +829,44 @@ int Multigrid::setup(const DevParams& p, const std::vector<uint8_t>& code, bool 
         for (int i = 0; i < nx; ++i) fb[nz * nxy + (size_t)i + nx * (size_t)j] = ecode(i, j, nz - 1);
 
     bytes_ = 0;
+    // face beta that depends on z only (a layered stack): keep it by plane
+    auto try_planes = [&](MGLevel& L, const std::vector<double>& bw, const std::vector<double>& bs,
+                          const std::vector<double>& bb) -> int {
+        const size_t lnxy = (size_t)L.n[0] * L.n[1];
+        std::vector<double> zc(3 * L.n[2] + 1);
+        for (int k = 0; k < L.n[2]; ++k) {
+            const size_t c0 = lnxy * k;
+            zc[k] = bw[c0];
+            zc[L.n[2] + k] = bs[c0];
+            for (size_t q = 0; q < lnxy; ++q)
+                if (bw[c0 + q] != bw[c0] || bs[c0 + q] != bs[c0]) return 0;
+        }
+        for (int k = 0; k <= L.n[2]; ++k) {
+            const size_t c0 = lnxy * k;
+            zc[2 * L.n[2] + k] = bb[c0];
+            for (size_t q = 0; q < lnxy; ++q)
+                if (bb[c0 + q] != bb[c0]) return 0;
+        }
+        const size_t nzc = zc.size();
+        if (want64) {
+            L.zc64 = dalloc<double>(nzc, bytes_);
+            if (!L.zc64 || cudaMemcpy(L.zc64, zc.data(), nzc * 8, cudaMemcpyHostToDevice) != cudaSuccess) return -2;
+        }
+        if (want32) {
+            std::vector<float> z32(zc.begin(), zc.end());
+            L.zc32 = dalloc<float>(nzc, bytes_);
+            if (!L.zc32 || cudaMemcpy(L.zc32, z32.data(), nzc * 4, cudaMemcpyHostToDevice) != cudaSuccess) return -2;
+        }
+        return 0;
+    };
     for (size_t l = 0; l < lev_.size(); ++l) {
         MGLevel& L = lev_[l];
         const size_t N = L.N, lnxy = (size_t)L.n[0] * L.n[1];
+        if (l == 0) {
+            // level 0's face beta from the codes, as coeffs<T, CK_FINE> forms
+            // it; bb[0] and bb[nz] are the electrode-layer cells' eps
+            if (try_planes(L, fw, fs, fb)) return -2;
+        }
         if (l > 0) {
             const MGLevel& F = lev_[l - 1];
             const int rx = L.cr[0], ry = L.cr[1], rz = L.cr[2];
@@ -918,32 +954,7 @@ int Multigrid::setup(const DevParams& p, const std::vector<uint8_t>& code, bool 
                         cb[(size_t)i + L.n[0] * ((size_t)j + (size_t)L.n[1] * k)] = s / (rx * ry);
                     }
             fw.swap(cw); fs.swap(cs); fb.swap(cb);
-            // laterally uniform face beta (a layered stack): keep it by plane
-            std::vector<double> zc(3 * L.n[2] + 1);
-            bool uni = true;
-            for (int k = 0; k < L.n[2] && uni; ++k) {
-                const size_t c0 = (size_t)lnxy * k;
-                zc[k] = fw[c0];
-                zc[L.n[2] + k] = fs[c0];
-                for (size_t q = 0; q < lnxy && uni; ++q) uni = fw[c0 + q] == fw[c0] && fs[c0 + q] == fs[c0];
-            }
-            for (int k = 0; k <= L.n[2] && uni; ++k) {
-                const size_t c0 = (size_t)lnxy * k;
-                zc[2 * L.n[2] + k] = fb[c0];
-                for (size_t q = 0; q < lnxy && uni; ++q) uni = fb[c0 + q] == fb[c0];
-            }
-            if (uni) {
-                const size_t nzc = zc.size();
-                if (want64) {
-                    L.zc64 = dalloc<double>(nzc, bytes_);
-                    if (!L.zc64 || cudaMemcpy(L.zc64, zc.data(), nzc * 8, cudaMemcpyHostToDevice) != cudaSuccess) return -2;
-                }
-                if (want32) {
-                    std::vector<float> z32(zc.begin(), zc.end());
-                    L.zc32 = dalloc<float>(nzc, bytes_);
-                    if (!L.zc32 || cudaMemcpy(L.zc32, z32.data(), nzc * 4, cudaMemcpyHostToDevice) != cudaSuccess) return -2;
-                }
-            }
+            if (try_planes(L, fw, fs, fb)) return -2;
             if (want64) {
                 L.x64 = dalloc<double>(N, bytes_); L.b64 = dalloc<double>(N, bytes_); L.a64 = dalloc<double>(N, bytes_);
                 L.bw64 = dalloc<double>(N, bytes_); L.bs64 = dalloc<double>(N, bytes_); L.bb64 = dalloc<double>(N + lnxy, bytes_);
@@ -1139,8 +1150,8 @@ void Multigrid::smooth(const DevParams& p, const uint8_t* code, int l, T* x, con
             for (int color = 0; color < 2; ++color) {
                 if (prof) prof->begin(l == 0 ? PROF_SMOOTH_L0 : l == 1 ? PROF_MG_L1 : l == 2 ? PROF_MG_L2 : PROF_MG_COARSE, s);
                 ++g_launches;
-                if (l == 0) k_line<T, CK_FINE><<<g2, b2, 0, s>>>(o, x, b, q, color);
-                else if (o.zc) k_line<T, CK_PLANES><<<g2, b2, 0, s>>>(o, x, b, q, color);
+                if (o.zc) k_line<T, CK_PLANES><<<g2, b2, 0, s>>>(o, x, b, q, color);
+                else if (l == 0) k_line<T, CK_FINE><<<g2, b2, 0, s>>>(o, x, b, q, color);
                 else k_line<T, CK_ARRAYS><<<g2, b2, 0, s>>>(o, x, b, q, color);
                 if (prof) prof->end(s);
             }
@@ -1151,7 +1162,7 @@ void Multigrid::smooth(const DevParams& p, const uint8_t* code, int l, T* x, con
                 if (prof) prof->begin(l == 0 ? PROF_SMOOTH_L0 : l == 1 ? PROF_MG_L1 : l == 2 ? PROF_MG_L2 : PROF_MG_COARSE, s);
                 const bool z = zero && it == 0 && color == 0;
                 ++g_launches;
-                if (l == 0) {
+                if (l == 0 && !o.zc) {
                     if (z) k_rbgs<T, CK_FINE, true><<<g2, b2, 0, s>>>(o, x, b, color);
                     else k_rbgs<T, CK_FINE><<<g2, b2, 0, s>>>(o, x, b, color);
                 } else {
@@ -1210,7 +1221,7 @@ void Multigrid::vcycle(const DevParams& p, const uint8_t* code, int l, T* x, con
         case 6: FX_RR(F, 2, 2, 1); break;             \
         default: FX_RR(F, 2, 2, 2); break;            \
         }
-        if (l == 0) { FX_RR_ALL(CK_FINE) } else if (o.zc) { FX_RR_ALL(CK_PLANES) } else { FX_RR_ALL(CK_ARRAYS) }
+        if (o.zc) { FX_RR_ALL(CK_PLANES) } else if (l == 0) { FX_RR_ALL(CK_FINE) } else { FX_RR_ALL(CK_ARRAYS) }
 #undef FX_RR_ALL
 #undef FX_RR
     }
