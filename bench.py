@@ -43,8 +43,9 @@ WORKLOADS = {
 METRIC = "coupled-step cell-updates/s"
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum, one ncu
 # capture, cold cache) of the dominant bandwidth-bound kernel class, by
-# (workload, precision, class); see profiles/k_rbgs_l0_mfism_128x128x144.md
-TRAFFIC = {("mfism", "fp64", "smooth_l0"): 59.35e6}
+# (workload, precision, class): the level-0 half sweep of the layered MFISM
+# stack, coefficients by z plane (profiles/k_rbgs_l0_mfism_128x128x144.txt)
+TRAFFIC = {("mfism", "fp64", "smooth_l0"): 56.76e6}
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -97,10 +98,14 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                                          "-lms", "200", "-i", str(self.idx)], stdout=subprocess.PIPE,
+                                          "-lms", "50", "-i", str(self.idx)], stdout=subprocess.PIPE,
                                          stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # the timed region starts once the sampler is live
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 3.0:
+                time.sleep(0.01)
         except (OSError, ValueError):
             self.proc = None
 
@@ -135,12 +140,16 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def algorithmic_bytes(kernel: str, N: int, Nc1: int, sc: bool, scalar: bool, rot: bool, fp: int = 8) -> float:
+def algorithmic_bytes(kernel: str, N: int, Nc1: int, sc: bool, scalar: bool, rot: bool, fp: int = 8,
+                      planes: bool = False) -> float:
     """Compulsory bytes of one launch: each distinct array read once, each
-    output written once; stencil neighbours and ghosts count once."""
+    output written once; stencil neighbours and ghosts count once.  planes:
+    level 0's coefficients depend on z only (a layered stack), so its
+    smoother needs no material codes."""
     a = fp if sc else 0
+    code = 0 if planes else 1
     if kernel == "smooth_l0":      # one red or black half-sweep: half of a full sweep
-        return N * (fp + fp + 1 + fp + a) / 2.0
+        return N * (fp + fp + code + fp + a) / 2.0
     if kernel == "restrict_l0":
         return N * (fp + fp + 1 + a) + Nc1 * fp
     if kernel == "prolong_l0":     # x in and out, the coarse correction, one weight per fine cell
@@ -344,7 +353,7 @@ def run_reference(args) -> None:
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="mfism", choices=list(WORKLOADS))
@@ -428,6 +437,7 @@ def main() -> None:
     V0 = f.param("Phi_Bc_hi")
     barrier()
     torch.cuda.synchronize()
+    se0 = f.stats()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     f.set_initial_P(None, None, Pz_host)
@@ -441,6 +451,7 @@ def main() -> None:
     e1.record(stream)
     torch.cuda.synchronize()
     barrier()
+    se1 = f.stats()
     ems = max_over_ranks(e0.elapsed_time(e1), world)
     e2e_value = whole_job_rate(N, ke, world, ems)
     h2d = (3 * N * 8 + ke * 8) / ke
@@ -459,13 +470,14 @@ def main() -> None:
         nz1 = WORKLOADS[args.workload]["shape"]
         Nc1 = N // 2  # level 1 halves z on these stacks (dz < dx)
         fp = 4 if args.precision == "mixed" and dom in ("smooth_l0", "restrict_l0", "prolong_l0") else 8
-        per_launch = algorithmic_bytes(dom, N, Nc1, sc, True, rot, fp)
+        planes = f.param("mg_level0_planes") == 1.0
+        per_launch = algorithmic_bytes(dom, N, Nc1, sc, True, rot, fp, planes)
         achieved = per_launch / (dms / dcnt / 1e3) / 1e9 if dcnt else None
         total_ms = sum(v[0] for v in kt.values())
         roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak if achieved else None,
                 "traffic": TRAFFIC.get((args.workload, args.precision, dom)),
-                "traffic_source": "ncu dram bytes per launch, profiles/k_rbgs_l0_mfism_128x128x144.md"
+                "traffic_source": "ncu dram bytes per launch, profiles/k_rbgs_l0_mfism_128x128x144.txt"
                 if (args.workload, args.precision, dom) in TRAFFIC else None,
                 "peak_source": f"{peak_src} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured"
                 else "fallback 6.65 TB/s",
@@ -495,7 +507,10 @@ def main() -> None:
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "steps": ke},
+                    "d2h_bytes_per_step": d2h, "steps": ke,
+                    # the leg continues the sweep after the timed and the per-launch passes
+                    "after_steps": args.warmup + 2 * args.steps,
+                    "mg_cycles_per_step": (se1["mg_cycles_total"] - se0["mg_cycles_total"]) / ke},
             "gpu_launches": int(st1["kernel_launches"] - st0["kernel_launches"]),
             "clocks": clocks,
             "kernel_ms_share": {k: round(v[0] / total_ms, 4) for k, v in kt.items() if v[1]},

@@ -1195,7 +1195,10 @@ int fx_get_param(const fx_ctx* c, const char* key, double* v) {
         {"num_variants", (double)c->variants.size()}, {"fx.newton_tol", p.newton_tol},
         {"adjoint_mg_cycles", (double)c->adj.mg_cycles}, {"adjoint_forward_ms", c->adj.fwd_ms},
         {"adjoint_backward_ms", c->adj.bwd_ms}, {"adjoint_bytes", (double)c->adj.bytes},
-        {"adjoint_loss", c->adj.loss}};
+        {"adjoint_loss", c->adj.loss},
+        // 1 when level 0's face coefficients depend on z only and its smoother
+        // reads them by plane instead of from the material codes
+        {"mg_level0_planes", !c->mg.levels().empty() && (c->mg.levels()[0].zc64 || c->mg.levels()[0].zc32) ? 1.0 : 0.0}};
     auto it = m.find(k);
     if (it != m.end()) { *v = it->second; return FX_OK; }
     // "FE_lo[2]" style access to the 3-vectors

@@ -85,7 +85,11 @@ const char* fx_last_error(const fx_ctx* ctx);
 
 int fx_get_dims(const fx_ctx* ctx, int n_cell[3], double dx[3]);
 /* Scalar parameters by inputs-file key (FerroX namespace globals,
- * Source/FerroX_namespace.H:1-115), plus fx.* keys. */
+ * Source/FerroX_namespace.H:1-115), plus fx.* keys.  fx_get_param also
+ * answers read-only diagnostics: contains_sc, num_variants, V_lo, V_hi,
+ * phi_ref, intrinsic_carrier_concentration, adjoint_* (the last recorded
+ * run) and mg_level0_planes (1 when level 0's face coefficients depend on z
+ * only and are read by plane). */
 int fx_get_param(const fx_ctx* ctx, const char* key, double* value);
 int fx_set_param(fx_ctx* ctx, const char* key, double value);
 
