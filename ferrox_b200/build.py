@@ -20,7 +20,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 CU = ["fx_kernels.cu", "fx_mg.cu", "fx_adjoint.cu", "fx_api.cu", "fx_noalloc.cu"]
 CPP = ["inputs.cpp", "plotfile.cpp"]
-HDR = ["fx_device.cuh", "fx_kernels.h", "fx_mg.h", "fx_params.h", "plotfile.h"]
+HDR = ["fx_ctl.h", "fx_device.cuh", "fx_kernels.h", "fx_mg.h", "fx_params.h", "plotfile.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xptxas", "-O3"]
 

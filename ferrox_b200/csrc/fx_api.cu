@@ -160,6 +160,21 @@ struct fx_ctx {
     Multigrid mg;
     bool mg_ready = false;
 
+    // the step as one CUDA graph with its loops controlled on the device
+    // (fx_ctl.h); graphs are cached by everything their capture bakes in
+    struct StepGraph {
+        cudaGraphExec_t exec = nullptr;
+        std::vector<unsigned char> key;
+        long long top = 0;                 // kernel launches outside conditional bodies
+        long long own[KIND_N] = {};        // per execution of each body kind
+    };
+    std::vector<StepGraph> sgraphs;
+    StepCtl* d_ctl = nullptr;
+    StepCtl* h_ctl = nullptr;              // pinned
+    CondCapture cap;
+    bool sg_off = false;                   // capture failed once: the host-driven loop from then on
+    bool sg_ran = false;                   // the last step ran as a graph
+
     // bumped by every call that changes the state or a parameter of the
     // math; fx_backward requires the value fx_forward_record saw
     long long gen = 0;
@@ -381,6 +396,14 @@ void fill_devparams(fx_ctx* c) {
     for (int q = 0; q < 8; ++q) d.eps[q] = eps_of_code(p, q);
     d.q = kQ; d.kb = kKb; d.T = kT; d.Nc = kNc; d.Nv = kNv; d.Eg = kEg; d.Chi = kChi; d.Ea = kEa; d.Ed = kEd;
     d.NA = p.acceptor_doping; d.ND = p.donor_doping; d.phi_ref = phi_ref(); d.use_FD = p.use_Fermi_Dirac;
+    // the constants of the product form of the Boltzmann charge (Ef = 0,
+    // g_A = 4, g_D = 2, ChargeDensity.cpp:46-93)
+    const double kbT = kKb * kT;
+    d.sc_qkT = kQ / kbT;
+    d.sc_Ce = kNc * std::exp(kQ * kChi / kbT);
+    d.sc_Ch = kNv * std::exp(-(kQ * kChi + kQ * kEg) / kbT);
+    d.sc_Ca = 4.0 * std::exp((kQ * kEa - kQ * kChi - kQ * kEg) / kbT);
+    d.sc_Cd = 2.0 * std::exp((kQ * kEd + kQ * kChi) / kbT);
     d.delta = p.delta; d.inv_delta = 1. / p.delta; d.neg_inv_delta = -1. / p.delta;
     d.ghost_mode = p.phi_ghost_mode;
     electrode_values(c);
@@ -642,6 +665,8 @@ int tdgl_update(fx_ctx* c) {
     return r;
 }
 
+void steady_update(fx_ctx* c, int step, double phi_max, double dmax);
+
 int check_steady(fx_ctx* c, int step) {
     int r = ensure_device(c);
     if (r) return r;
@@ -653,7 +678,12 @@ int check_steady(fx_ctx* c, int step) {
     if (r) return r;
     r = read_out(c, 2);
     if (r) return r;
-    const double phi_max = c->h_out[0], dmax = c->h_out[1];
+    steady_update(c, step, c->h_out[0], c->h_out[1]);
+    return FX_OK;
+}
+
+// the host side of CheckSteadyState from max|phi| and max|phi - phi_old|
+void steady_update(fx_ctx* c, int step, double phi_max, double dmax) {
     double max_phi_err;
     if (phi_max > 0) max_phi_err = dmax / phi_max;
     else max_phi_err = dmax > 0 ? INFINITY : 0.0;   // all-NaN Phidiff passes norm0 as 0
@@ -664,18 +694,298 @@ int check_steady(fx_ctx* c, int step) {
     }
     c->steady_err_last = max_phi_err;
     if (c->par.verbose) printf("Steady state check : (phi(t) - phi(t-1)).norm0() = %g\n", max_phi_err);
+}
+
+// ---- one step as one CUDA graph (fx_ctl.h)
+//
+// The graph holds what step_once's host path runs before its voltage
+// bookkeeping -- ComputePhi_Rho with the extrapolated start, the TDGL update,
+// CheckSteadyState -- with the same kernels in the same order, so the results
+// are bit-identical; the Newton and multigrid loop tests run on the device.
+// A failure in ComputePhi_Rho closes the gates (IF nodes) in front of the
+// TDGL update and the steady-state check, as the host path returns there.
+
+int sg_hist_before(fx_ctx* c, int* use) {
+    *use = 0;
+    const int order = std::min(3, c->par.phi_extrapolate);
+    if (order <= 0 || !c->par.warm_start) return FX_OK;
+    for (int q = 0; q < order; ++q)
+        if (!c->d_phi_hist[q]) {
+            int r = dmalloc(c, &c->d_phi_hist[q], c->N);
+            if (r) return r;
+            c->hist_n = 0;
+        }
+    if (!c->hist_valid || c->hist_vlo != c->dp.V_lo || c->hist_vhi != c->dp.V_hi) c->hist_n = 0;
+    *use = std::min(order, c->hist_n);
+    return FX_OK;
+}
+
+void sg_hist_after(fx_ctx* c) {
+    const int order = std::min(3, c->par.phi_extrapolate);
+    if (order <= 0 || !c->par.warm_start) return;
+    c->hist_n = std::min(order, c->hist_n + 1);
+    c->hist_valid = true;
+    c->hist_vlo = c->dp.V_lo;
+    c->hist_vhi = c->dp.V_hi;
+}
+
+// start_guess's launches for `use` steps of history (bookkeeping on the host)
+void sg_start_guess(fx_ctx* c, cudaStream_t q, int use) {
+    const int order = std::min(3, c->par.phi_extrapolate);
+    if (order <= 0 || !c->par.warm_start) return;
+    if (use > 0) {
+        double* h[3] = {c->d_phi_hist[0], order >= 2 ? c->d_phi_hist[1] : nullptr, order >= 3 ? c->d_phi_hist[2] : nullptr};
+        ++g_launches;
+        launch_phi_extrap(c->dp, use, c->d_phi, h, q);
+    } else {
+        cudaMemcpyAsync(c->d_phi_hist[0], c->d_phi, c->N * 8, cudaMemcpyDeviceToDevice, q);
+    }
+}
+
+// mg_solve with the target formed on the device from the norms in d_out
+void sg_mg_solve(fx_ctx* c, cudaStream_t q, const double* rhs) {
+    if (!c->par.warm_start) cudaMemsetAsync(c->d_phi, 0, c->N * 8, q);
+    if (c->par.precision == 1)
+        c->mg.enqueue_solve_mixed_ctl(c->dp, c->d_code, c->d_phi, rhs, c->d_out, c->par.mg_rtol, c->par.mg_max_iter,
+                                      c->d_ctl, c->cap, q);
+    else
+        c->mg.enqueue_solve64_ctl(c->dp, c->d_code, c->d_phi, rhs, c->d_out, c->par.mg_rtol, c->par.mg_max_iter,
+                                  c->d_ctl, c->cap, q);
+}
+
+// one pass of the ComputePhi_Rho loop (compute_phi_rho_P's loop body)
+void sg_newton_pass(fx_ctx* c, cudaStream_t q, bool start, int use, cudaGraphConditionalHandle hn, int in_body) {
+    cudaMemsetAsync(c->d_out, 0, 2 * sizeof(double), q);
+    ++g_launches;
+    launch_newton(c->dp, c->d_code, c->d_phi, c->d_rho, c->d_rhsP, c->d_alpha, c->d_alpha32, c->d_rhs, c->d_out, q);
+    c->mg.set_alpha(c->d_alpha, c->d_alpha32, true, q);
+    if (start) sg_start_guess(c, q, use);
+    sg_mg_solve(c, q, c->d_rhs);
+    ++g_launches;
+    launch_rho(c->dp, c->d_code, c->d_phi, c->d_phi_prev, c->d_rho, c->d_e, c->d_h, c->d_part, c->d_counter, c->d_out,
+               1, 0, q);
+    ++g_launches;
+    launch_newton_ctl(c->d_ctl, c->d_out, c->par.newton_tol, c->par.newton_max_iter, hn, in_body, q);
+}
+
+// ComputePhi_Rho for P in buffer `buf` on stream q
+void sg_phirho(fx_ctx* c, cudaStream_t q, int buf, bool step_start, int use) {
+    ++g_launches;
+    launch_ctl_phirho_begin(c->d_ctl, q);
+    const double* P[3] = {c->scalarP ? nullptr : c->d_P[buf][0], c->scalarP ? nullptr : c->d_P[buf][1], c->d_P[buf][2]};
+    if (!c->contains_sc) {
+        cudaMemsetAsync(c->d_out, 0, 2 * sizeof(double), q);
+        ++g_launches;
+        launch_rhs_p(c->dp, c->d_code, c->d_var, c->d_vt, P, c->d_rhsP, c->d_out, q);
+        c->mg.set_alpha(nullptr, nullptr, false, q);
+        if (step_start) sg_start_guess(c, q, use);
+        sg_mg_solve(c, q, c->d_rhsP);
+    } else {
+        ++g_launches;
+        launch_rhs_p(c->dp, c->d_code, c->d_var, c->d_vt, P, c->d_rhsP, nullptr, q);
+        const cudaGraphConditionalHandle hn = c->cap.handle(q);
+        sg_newton_pass(c, q, step_start, use, hn, 0);
+        c->cap.node(q, cudaGraphCondTypeWhile, hn, KIND_NEWTON_PASS,
+                    [&](cudaStream_t b) { sg_newton_pass(c, b, false, 0, hn, 1); });
+    }
+    ++g_launches;
+    launch_ctl_phirho_end(c->d_ctl, c->contains_sc ? 1 : 0, q);
+}
+
+// an IF node whose body runs only while no failure is recorded
+template <typename F>
+void sg_gate(fx_ctx* c, cudaStream_t q, int kind, F&& body) {
+    const cudaGraphConditionalHandle h = c->cap.handle(q);
+    ++g_launches;
+    launch_ctl_gate(c->d_ctl, kind, h, q);
+    c->cap.node(q, cudaGraphCondTypeIf, h, kind, body);
+}
+
+void sg_steady(fx_ctx* c, cudaStream_t q) {
+    cudaMemsetAsync(c->d_out, 0, 2 * sizeof(double), q);
+    ++g_launches;
+    launch_steady(c->dp, c->d_phi, c->d_phi_old, c->d_dphi, c->d_out, q);
+}
+
+void sg_enqueue_step(fx_ctx* c, int use) {
+    cudaStream_t s = c->s;
+    const int cur = c->cur, nb = 1 - cur;
+    const int mixed = c->par.precision == 1;
+    ++g_launches;
+    launch_ctl_step_begin(c->d_ctl, s);
+    sg_phirho(c, s, cur, true, use);
+    const double* Pin[3] = {c->scalarP ? nullptr : c->d_P[cur][0], c->scalarP ? nullptr : c->d_P[cur][1], c->d_P[cur][2]};
+    double* Pout[3] = {c->scalarP ? nullptr : c->d_P[nb][0], c->scalarP ? nullptr : c->d_P[nb][1], c->d_P[nb][2]};
+    if (c->par.TimeIntegratorOrder == 1) {
+        sg_gate(c, s, KIND_GATE_TDGL, [&](cudaStream_t q) {
+            ++g_launches;
+            launch_tdgl(c->dp, mixed, 0, c->d_code, c->d_var, c->d_vt, Pin, Pout, c->d_phi, nullptr, nullptr, q);
+            sg_steady(c, q);
+        });
+    } else {
+        double* fb[3] = {c->d_f[0], c->d_f[1], c->d_f[2]};
+        sg_gate(c, s, KIND_GATE_TDGL, [&](cudaStream_t q) {
+            ++g_launches;
+            launch_tdgl(c->dp, mixed, 1, c->d_code, c->d_var, c->d_vt, Pin, Pout, c->d_phi, fb, nullptr, q);
+            sg_phirho(c, q, nb, false, 0);
+            sg_gate(c, q, KIND_GATE_CORRECTOR, [&](cudaStream_t b) {
+                const double* Ppre[3] = {Pout[0], Pout[1], Pout[2]};
+                double* Pnew[3] = {c->scalarP ? nullptr : c->d_P[cur][0], c->scalarP ? nullptr : c->d_P[cur][1], c->d_P[cur][2]};
+                const double* Pold[3] = {Pnew[0], Pnew[1], Pnew[2]};
+                ++g_launches;
+                launch_tdgl(c->dp, mixed, 2, c->d_code, c->d_var, c->d_vt, Ppre, Pnew, c->d_phi, fb, Pold, b);
+                sg_steady(c, b);
+            });
+        });
+    }
+    cudaMemcpyAsync(c->h_ctl, c->d_ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(c->h_out, c->d_out, 2 * sizeof(double), cudaMemcpyDeviceToHost, s);
+}
+
+// the captured launch parameters and graph shape of a step
+std::vector<unsigned char> sg_key(const fx_ctx* c, int use) {
+    std::vector<unsigned char> k;
+    auto put = [&](const void* v, size_t n) {
+        const unsigned char* b = static_cast<const unsigned char*>(v);
+        k.insert(k.end(), b, b + n);
+    };
+    put(&c->dp, sizeof(DevParams));
+    const int iv[] = {c->cur, use, c->par.TimeIntegratorOrder, c->par.precision, c->par.warm_start,
+                      c->par.phi_extrapolate, c->par.newton_max_iter, c->par.mg_max_iter, c->mg.nu1, c->mg.nu2,
+                      c->mg.mixed_cycles, c->scalarP ? 1 : 0, c->contains_sc ? 1 : 0};
+    put(iv, sizeof(iv));
+    const double dv[] = {c->par.mg_rtol, c->par.newton_tol};
+    put(dv, sizeof(dv));
+    const void* pv[] = {c->s, c->d_var, c->d_vt, c->d_f[0], c->d_f[1], c->d_f[2], c->d_phi_hist[0], c->d_phi_hist[1],
+                        c->d_phi_hist[2]};
+    put(pv, sizeof(pv));
+    return k;
+}
+
+int sg_build(fx_ctx* c, int use, fx_ctx::StepGraph& g) {
+    c->cap.reset();
+    const long long l0 = g_launches.load();
+    cudaError_t e = cudaStreamBeginCapture(c->s, cudaStreamCaptureModeThreadLocal);
+    if (e) return (int)e;
+    sg_enqueue_step(c, use);
+    cudaGraph_t graph = nullptr;
+    e = cudaStreamEndCapture(c->s, &graph);
+    const long long total = g_launches.load() - l0;
+    g_launches -= total;   // counted per execution
+    if (!e) e = c->cap.err;
+    if (!e) e = cudaGetLastError();
+    if (!e) e = cudaGraphInstantiate(&g.exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (e) {
+        if (g.exec) { cudaGraphExecDestroy(g.exec); g.exec = nullptr; }
+        return (int)e;
+    }
+    g.top = total - c->cap.in_bodies;
+    for (int q = 0; q < KIND_N; ++q) g.own[q] = c->cap.own[q];
+    return 0;
+}
+
+// Runs ComputePhi_Rho, the TDGL update and CheckSteadyState of one step as a
+// graph.  *ran = false leaves the step to the host-driven path (profiling on,
+// the graph path switched off, or no capture possible on this setup).
+int step_graph(fx_ctx* c, int step, bool* ran) {
+    *ran = false;
+    c->sg_ran = false;
+    if (!c->par.step_graph || c->sg_off || c->prof.on || c->par.newton_max_iter < 1) return FX_OK;
+    int r = ensure_device(c);
+    if (r) return r;
+    if (!c->d_ctl) {
+        r = dmalloc(c, &c->d_ctl, 1);
+        if (r) return r;
+        FX_CUDA(c, cudaMallocHost(&c->h_ctl, sizeof(StepCtl)));
+        FX_CUDA(c, c->cap.init());
+    }
+    if (c->par.TimeIntegratorOrder != 1)
+        for (int d = 0; d < 3; ++d)
+            if (!c->d_f[d]) { r = dmalloc(c, &c->d_f[d], c->N); if (r) return r; }
+    int use = 0;
+    r = sg_hist_before(c, &use);
+    if (r) return r;
+    std::vector<unsigned char> key = sg_key(c, use);
+    fx_ctx::StepGraph* g = nullptr;
+    for (auto& x : c->sgraphs)
+        if (x.key == key) { g = &x; break; }
+    if (!g) {
+        // a changed parameter makes every cached step stale
+        bool same_params = true;
+        if (!c->sgraphs.empty()) {
+            const size_t n = sizeof(DevParams);
+            same_params = std::memcmp(c->sgraphs[0].key.data(), key.data(), n) == 0 &&
+                          std::memcmp(c->sgraphs[0].key.data() + n + 2 * sizeof(int), key.data() + n + 2 * sizeof(int),
+                                      key.size() - n - 2 * sizeof(int)) == 0;
+        }
+        if (!same_params || c->sgraphs.size() >= 8) {
+            for (auto& x : c->sgraphs) if (x.exec) cudaGraphExecDestroy(x.exec);
+            c->sgraphs.clear();
+        }
+        fx_ctx::StepGraph ng;
+        ng.key = key;
+        const int e = sg_build(c, use, ng);
+        if (e) {
+            // stream capture of conditional nodes is not available here:
+            // the host-driven loop runs this and every later step
+            cudaGetLastError();
+            c->sg_off = true;
+            return FX_OK;
+        }
+        c->sgraphs.push_back(ng);
+        g = &c->sgraphs.back();
+    }
+    FX_CUDA(c, cudaGraphLaunch(g->exec, c->s));
+    FX_CUDA(c, cudaStreamSynchronize(c->s));
+    *ran = true;
+    c->sg_ran = true;
+    const StepCtl& t = *c->h_ctl;
+    long long launches = g->top;
+    for (int q = 0; q < KIND_N; ++q) launches += g->own[q] * t.nexec[q];
+    g_launches += launches;
+    c->E_valid = false;
+    c->mg_last = t.mg_cycles_phirho;
+    c->mg_total += t.mg_cycles_step;
+    c->mg_resid_last = t.mg_resid_last;
+    c->mg_target_last = t.mg_target_last;
+    c->newton_last = t.passes;
+    c->newton_total += t.newton_passes_step;
+    c->phi_err_last = t.err;
+    c->rhs_is_newton = c->contains_sc;
+    if (c->contains_sc) c->carriers_stale = true;
+    if (t.status != CTL_OK) {
+        c->hist_valid = false;
+        std::ostringstream o;
+        if (t.status == CTL_MG_NO_CONV || t.status == CTL_MG_NONFINITE) {
+            o << "Poisson multigrid did not reach |r| <= " << t.status_target << " in " << c->par.mg_max_iter
+              << " cycles (|r| = " << t.status_val << ")";
+            return set_err(c, t.status == CTL_MG_NO_CONV ? FX_ERR_NO_CONVERGENCE : FX_ERR_NONFINITE, o.str());
+        }
+        o << "Phi-rho Newton iteration did not reach " << c->par.newton_tol << " in " << t.status_n
+          << " passes (err = " << t.status_val << ")";
+        return set_err(c, t.status == CTL_NEWTON_NO_CONV ? FX_ERR_NO_CONVERGENCE : FX_ERR_NONFINITE, o.str());
+    }
+    sg_hist_after(c);
+    if (c->par.TimeIntegratorOrder == 1) c->cur = 1 - c->cur;
+    steady_update(c, step, c->h_out[0], c->h_out[1]);
     return FX_OK;
 }
 
 // one pass of main.cpp:261-621; returns 1 when the loop breaks
 int step_once(fx_ctx* c) {
     const int step = c->step + 1;
-    int r = compute_phi_rho_P(c, c->cur, true);
+    bool ran = false;
+    int r = step_graph(c, step, &ran);
     if (r) return r;
-    r = tdgl_update(c);
-    if (r) return r;
-    r = check_steady(c, step);
-    if (r) return r;
+    if (!ran) {
+        r = compute_phi_rho_P(c, c->cur, true);
+        if (r) return r;
+        r = tdgl_update(c);
+        if (r) return r;
+        r = check_steady(c, step);
+        if (r) return r;
+    }
     c->E_valid = false;
     c->time = c->time + c->par.dt;
     c->step = step;
@@ -1150,6 +1460,11 @@ void fx_destroy(fx_ctx* c) {
         cudaFree(c->d_alpha32);
         cudaFree(c->d_counter);
         if (c->h_out) cudaFreeHost(c->h_out);
+        for (auto& g : c->sgraphs) if (g.exec) cudaGraphExecDestroy(g.exec);
+        c->sgraphs.clear();
+        cudaFree(c->d_ctl);
+        if (c->h_ctl) cudaFreeHost(c->h_ctl);
+        c->cap.release();
         c->prof.collect();
         if (c->own_stream) cudaStreamDestroy(c->s);
     }
@@ -1188,7 +1503,7 @@ int fx_get_param(const fx_ctx* c, const char* key, double* v) {
         {"plot_int", p.plot_int}, {"fx.mg_rtol", p.mg_rtol}, {"fx.phi_ghost_mode", p.phi_ghost_mode},
         {"fx.sweep_mode", p.sweep_mode}, {"fx.steps_per_voltage", p.steps_per_voltage},
         {"fx.newton_max_iter", p.newton_max_iter}, {"fx.mg_max_iter", p.mg_max_iter}, {"fx.precision", p.precision},
-        {"fx.warm_start", p.warm_start}, {"fx.phi_extrapolate", p.phi_extrapolate},
+        {"fx.warm_start", p.warm_start}, {"fx.phi_extrapolate", p.phi_extrapolate}, {"fx.step_graph", p.step_graph},
         {"contains_sc", c->contains_sc ? 1.0 : 0.0},
         {"V_lo", c->dp.V_lo}, {"V_hi", c->dp.V_hi}, {"phi_ref", phi_ref()},
         {"intrinsic_carrier_concentration", std::sqrt(kNc * kNv) * exp(-0.5 * kQ * kEg / (kKb * kT))},
@@ -1198,6 +1513,7 @@ int fx_get_param(const fx_ctx* c, const char* key, double* v) {
         {"adjoint_loss", c->adj.loss},
         // 1 when level 0's face coefficients depend on z only and its smoother
         // reads them by plane instead of from the material codes
+        {"step_graph_ran", c->sg_ran ? 1.0 : 0.0},
         {"mg_level0_planes", !c->mg.levels().empty() && (c->mg.levels()[0].zc64 || c->mg.levels()[0].zc32) ? 1.0 : 0.0}};
     auto it = m.find(k);
     if (it != m.end()) { *v = it->second; return FX_OK; }
@@ -1233,7 +1549,7 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
     if (!c || !key) return FX_ERR_INVALID_ARGUMENT;
     const std::string k(key);
     Params& p = c->par;
-    if (k != "fx.profile" && k != "fx.verbose" && k != "fx.graphs") ++c->gen;
+    if (k != "fx.profile" && k != "fx.verbose" && k != "fx.graphs" && k != "fx.step_graph") ++c->gen;
     // the time history of phi only seeds the next solve's initial iterate;
     // electrode values are compared on their own, solver settings leave the
     // trajectory alone, anything else starts the history afresh
@@ -1245,6 +1561,7 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
     if (k == "fx.newton_max_iter") { p.newton_max_iter = (int)v; return FX_OK; }
     if (k == "fx.warm_start") { p.warm_start = (int)v; return FX_OK; }
     if (k == "fx.phi_extrapolate") { p.phi_extrapolate = (int)v; return FX_OK; }
+    if (k == "fx.step_graph") { p.step_graph = (int)v; return FX_OK; }
     if (k == "fx.verbose") { p.verbose = (int)v; c->mg.verbose = (int)v; return FX_OK; }
     if (k == "fx.profile") { c->prof.collect(); c->prof.on = v != 0.0; return FX_OK; }
     if (k == "fx.mg_nu1") { c->mg.nu1 = (int)v; return FX_OK; }

@@ -42,6 +42,10 @@ struct DevParams {
     double eps[8];             // eps_r * eps_0 by material code
     // semiconductor (ChargeDensity.cpp, FerroX.cpp:534-554)
     double q, kb, T, Nc, Nv, Eg, Chi, Ea, Ed, NA, ND, phi_ref;
+    // Boltzmann statistics in product form: with E = exp(sc_qkT (phi - phi_ref)),
+    // e = sc_Ce E, h = sc_Ch / E, acceptors NA / (1 + sc_Ca / E), donors
+    // ND / (1 + sc_Cd E) (Ef = 0)
+    double sc_qkT, sc_Ce, sc_Ch, sc_Ca, sc_Cd;
     int use_FD;
     double delta, inv_delta, neg_inv_delta;
     // z Dirichlet values of phi held by the solver and the ghost mode
@@ -282,8 +286,22 @@ __device__ __forceinline__ double fd_half(double eta) {
     return pow(exp(-eta) + xi, -1.0);
 }
 
-// ChargeDensity.cpp:46-93: carrier densities and charge at potential phi
+// ChargeDensity.cpp:46-93: carrier densities and charge at potential phi.
+// With Boltzmann statistics the four exponentials of the reference,
+// exp(+-q (phi - phi_ref) / kT + const), are one exponential E and its
+// reciprocal times constants formed on the host; the product form agrees with
+// the reference's expressions to rounding (the exponent's own rounding,
+// ~1e-14 relative at |exponent| ~ 150, dominates both).
 __device__ __forceinline__ double sc_charge(const DevParams& p, double phi, double& e_den, double& h_den) {
+    if (p.use_FD != 1) {
+        const double E = exp(p.sc_qkT * (phi - p.phi_ref));
+        const double r = 1.0 / E;
+        e_den = p.sc_Ce * E;
+        h_den = p.sc_Ch * r;
+        const double acc = p.NA != 0.0 ? p.NA / (1.0 + p.sc_Ca * r) : 0.0;
+        const double don = p.ND != 0.0 ? p.ND / (1.0 + p.sc_Cd * E) : 0.0;
+        return p.q * (h_den - e_den - acc + don);
+    }
     const double Ef = 0.0;
     const double q = p.q, kb = p.kb, T = p.T, Chi = p.Chi, Eg = p.Eg, phi_ref = p.phi_ref;
     double Ec_corr = -q * (phi - phi_ref) - Chi * q;

@@ -499,6 +499,92 @@ int launch_rho(const DevParams& p, const uint8_t* code, const double* phi, doubl
     return (int)cudaGetLastError();
 }
 
+namespace {
+
+__global__ void k_ctl_step_begin(StepCtl* ctl) {
+    ctl->mg_cycles_step = 0;
+    ctl->newton_passes_step = 0;
+    ctl->status = CTL_OK;
+    ctl->status_n = 0;
+    ctl->status_val = 0.0;
+    ctl->status_target = 0.0;
+    for (int k = 0; k < KIND_N; ++k) ctl->nexec[k] = 0;
+}
+
+__global__ void k_ctl_phirho_begin(StepCtl* ctl) {
+    ctl->passes = 0;
+    ctl->iter = 0;
+    ctl->err = 1.0;
+    ctl->mg_cycles_phirho = 0;
+}
+
+// the test of the ComputePhi_Rho loop (ElectrostaticSolver.cpp:690-742) after
+// a pass: err = sum|phi - phi_prev| / sum|phi| from the second pass on, as the
+// host loop forms it; the pass cap turns a loop that would go on into a failure
+__global__ void k_newton_ctl(StepCtl* ctl, const double* __restrict__ out, double tol, int max_iter,
+                             cudaGraphConditionalHandle h, int in_body) {
+    if (in_body) ctl->nexec[KIND_NEWTON_PASS] += 1;
+    const int passes = ctl->passes + 1;
+    ctl->passes = passes;
+    double err = ctl->err;
+    if (ctl->iter > 0) err = out[0] / out[1];
+    ctl->err = err;
+    ctl->iter += 1;
+    bool go = err > tol;
+    if (ctl->status != CTL_OK) {
+        go = false;
+    } else if (go && passes >= max_iter) {
+        ctl->status = isfinite(err) ? CTL_NEWTON_NO_CONV : CTL_NEWTON_NONFINITE;
+        ctl->status_n = passes;
+        ctl->status_val = err;
+        go = false;
+    }
+    cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
+// without a semiconductor ComputePhi_Rho is one solve, counted as one pass
+__global__ void k_ctl_phirho_end(StepCtl* ctl, int sc) {
+    if (!sc) {
+        ctl->passes = 1;
+        ctl->err = 0.0;
+    }
+    ctl->newton_passes_step += ctl->passes;
+}
+
+__global__ void k_ctl_gate(StepCtl* ctl, int kind, cudaGraphConditionalHandle h) {
+    const bool ok = ctl->status == CTL_OK;
+    if (ok) ctl->nexec[kind] += 1;
+    cudaGraphSetConditional(h, ok ? 1u : 0u);
+}
+
+}  // namespace
+
+int launch_ctl_gate(StepCtl* ctl, int kind, cudaGraphConditionalHandle h, cudaStream_t s) {
+    k_ctl_gate<<<1, 1, 0, s>>>(ctl, kind, h);
+    return (int)cudaGetLastError();
+}
+
+int launch_ctl_step_begin(StepCtl* ctl, cudaStream_t s) {
+    k_ctl_step_begin<<<1, 1, 0, s>>>(ctl);
+    return (int)cudaGetLastError();
+}
+
+int launch_ctl_phirho_begin(StepCtl* ctl, cudaStream_t s) {
+    k_ctl_phirho_begin<<<1, 1, 0, s>>>(ctl);
+    return (int)cudaGetLastError();
+}
+
+int launch_newton_ctl(StepCtl* ctl, const double* out, double tol, int max_iter, cudaGraphConditionalHandle h,
+                      int in_body, cudaStream_t s) {
+    k_newton_ctl<<<1, 1, 0, s>>>(ctl, out, tol, max_iter, h, in_body);
+    return (int)cudaGetLastError();
+}
+
+int launch_ctl_phirho_end(StepCtl* ctl, int sc, cudaStream_t s) {
+    k_ctl_phirho_end<<<1, 1, 0, s>>>(ctl, sc);
+    return (int)cudaGetLastError();
+}
+
 int launch_steady(const DevParams& p, const double* phi, double* phi_old, double* dphi, double* out,
                   cudaStream_t s) {
     k_steady<<<p.ngrid_red, RED_THREADS, 0, s>>>(p, phi, phi_old, dphi, out);

@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include "fx_ctl.h"
 #include "fx_device.cuh"
 
 namespace fx {
@@ -27,6 +28,17 @@ int launch_mean_p(const DevParams& p, const uint8_t* code, const double* const P
 int launch_phi_extrap(const DevParams& p, int order, double* phi, double* const h[3], cudaStream_t s);
 int launch_efield(const DevParams& p, const uint8_t* var, const Variant* vt, const double* phi, double* E[3],
                   cudaStream_t s);
+
+// control of a step graph (fx_ctl.h): step and ComputePhi_Rho bookkeeping,
+// and the Newton loop test after each pass (h: the loop's condition; in_body:
+// the pass runs inside the WHILE node, not the unrolled first pass)
+int launch_ctl_step_begin(StepCtl* ctl, cudaStream_t s);
+int launch_ctl_phirho_begin(StepCtl* ctl, cudaStream_t s);
+int launch_newton_ctl(StepCtl* ctl, const double* out, double tol, int max_iter, cudaGraphConditionalHandle h,
+                      int in_body, cudaStream_t s);
+int launch_ctl_phirho_end(StepCtl* ctl, int sc, cudaStream_t s);
+// opens the IF node h (and counts an execution of `kind`) while no failure is recorded
+int launch_ctl_gate(StepCtl* ctl, int kind, cudaGraphConditionalHandle h, cudaStream_t s);
 
 // adjoint (fx_adjoint.cu).  lam = {lambda_x, lambda_y, lambda_z}; vec = the
 // three-component kernels (else only lambda_z is read and written)

@@ -742,6 +742,94 @@ template <typename T> T* lq(MGLevel& L);
 template <> double* lq<double>(MGLevel& L) { return L.cp64; }
 template <> float* lq<float>(MGLevel& L) { return L.cp32; }
 
+// ---- loop control of the device-controlled solves (fx_ctl.h); one thread each
+
+// the max of the NORM_SLOTS slots, as the host takes it (std::max from 0)
+__device__ __forceinline__ double ctl_slots_max(const double* __restrict__ slots) {
+    double m = 0.0;
+#pragma unroll 16
+    for (int q = 0; q < NORM_SLOTS; ++q) {
+        const double v = slots[q];
+        m = m < v ? v : m;
+    }
+    return m;
+}
+
+// the solve's target from the right-hand side norms, and the first loop test
+__global__ void k_mg_begin(const double* __restrict__ slots, const double* __restrict__ nb, double rtol, int maxit,
+                           StepCtl* ctl, cudaGraphConditionalHandle hw) {
+    const double rn = ctl_slots_max(slots);
+    const double r = rtol < 1e-16 ? 1e-16 : rtol;
+    const double m = nb[0] < nb[1] ? nb[1] : nb[0];
+    const double target = r * m;
+    ctl->target = target;
+    ctl->rn = rn;
+    ctl->it = 0;
+    ctl->parity = 0;
+    cudaGraphSetConditional(hw, (!(rn <= target) && 0 < maxit) ? 1u : 0u);
+}
+
+// after a V-cycle: the level-0 norm after pre-smoothing bounds the residual
+// after the cycle; the exact residual is formed (IF body) once it is within
+// the target, or always with a single level
+__global__ void k_mg_mid(const double* __restrict__ slots, int single_level, int maxit, StepCtl* ctl,
+                         cudaGraphConditionalHandle hif, cudaGraphConditionalHandle hw) {
+    ctl->nexec[KIND_MG_CYCLE] += 1;
+    const double mid = ctl_slots_max(slots);
+    const int it = ctl->it + 1;
+    ctl->it = it;
+    const bool need = single_level || mid <= ctl->target;
+    if (!need) ctl->rn = mid;
+    cudaGraphSetConditional(hif, need ? 1u : 0u);
+    cudaGraphSetConditional(hw, (!need && it < maxit) ? 1u : 0u);
+}
+
+__global__ void k_mg_rn(const double* __restrict__ slots, int maxit, StepCtl* ctl, cudaGraphConditionalHandle hw) {
+    ctl->nexec[KIND_MG_RESID] += 1;
+    const double rn = ctl_slots_max(slots);
+    ctl->rn = rn;
+    cudaGraphSetConditional(hw, (!(rn <= ctl->target) && ctl->it < maxit) ? 1u : 0u);
+}
+
+// after a mixed refinement step: `inner` FP32 cycles were spent; parity says
+// which buffer holds the iterate.  hc is the condition of the next step in
+// the same body (the IF node), or the loop's own
+__global__ void k_mx_step(const double* __restrict__ slots, int inner, int maxit, int parity, int kind, StepCtl* ctl,
+                          cudaGraphConditionalHandle hc, cudaGraphConditionalHandle hw) {
+    ctl->nexec[kind] += 1;
+    const double rn = ctl_slots_max(slots);
+    const int it = ctl->it + inner;
+    ctl->rn = rn;
+    ctl->it = it;
+    ctl->parity = parity;
+    const unsigned go = (!(rn <= ctl->target) && it < maxit) ? 1u : 0u;
+    cudaGraphSetConditional(hc, go);
+    if (hw != hc) cudaGraphSetConditional(hw, 0u);
+}
+
+// the iterate back into phi when the last refinement step wrote the second buffer
+__global__ void __launch_bounds__(256) k_mx_copy(const double* __restrict__ src, double* __restrict__ dst, int n,
+                                                 const StepCtl* __restrict__ ctl) {
+    if (!ctl->parity) return;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) dst[c] = src[c];
+}
+
+// the solve's statistics and, when it stopped short of the target, the failure
+__global__ void k_mg_end(StepCtl* ctl) {
+    const int it = ctl->it;
+    const double rn = ctl->rn, t = ctl->target;
+    ctl->mg_cycles_phirho += it;
+    ctl->mg_cycles_step += it;
+    ctl->mg_resid_last = rn;
+    ctl->mg_target_last = t;
+    if (!(rn <= t) && ctl->status == CTL_OK) {
+        ctl->status = isfinite(rn) ? CTL_MG_NO_CONV : CTL_MG_NONFINITE;
+        ctl->status_n = it;
+        ctl->status_val = rn;
+        ctl->status_target = t;
+    }
+}
+
 }  // namespace
 
 double Multigrid::slots_max() const {
@@ -1376,6 +1464,81 @@ int Multigrid::solve_mixed(const DevParams& p, const uint8_t* code, double* phi,
     }
     if (st) { st->cycles = cycles; st->resid = rn; }
     return rn <= target ? 0 : -3;
+}
+
+// The loop of solve64 with its tests on the device: a WHILE node runs one
+// V-cycle per pass; k_mg_mid decides from the pre-smoothing norm whether the
+// exact residual is needed (an IF node) and whether another cycle follows.
+void Multigrid::enqueue_solve64_ctl(const DevParams& p, const uint8_t* code, double* phi, const double* rhs,
+                                    const double* nb, double rtol, int maxit, StepCtl* ctl, CondCapture& cap,
+                                    cudaStream_t s) {
+    MGLevel& L = lev_[0];
+    Op<double> o = make_op<double>(L, 0, code, eps_, has_alpha_ ? a0_64 : nullptr, true, p);
+    const dim3 b2(32, 8), g2((L.n[0] + 31) / 32, (L.n[1] + 7) / 8, (L.n[2] + R64_ZP - 1) / R64_ZP);
+    const int single = lev_.size() == 1 ? 1 : 0;
+    auto resid = [&](cudaStream_t q) {
+        cudaMemsetAsync(d_norm_, 0, NORM_SLOTS * 8, q);
+        ++g_launches;
+        k_resid64<false><<<g2, b2, 0, q>>>(o, phi, nullptr, rhs, nullptr, nullptr, d_norm_);
+    };
+    const cudaGraphConditionalHandle hw = cap.handle(s);
+    resid(s);
+    ++g_launches;
+    k_mg_begin<<<1, 1, 0, s>>>(d_norm_, nb, rtol, maxit, ctl, hw);
+    cap.node(s, cudaGraphCondTypeWhile, hw, KIND_MG_CYCLE, [&](cudaStream_t b) {
+        const cudaGraphConditionalHandle hif = cap.handle(b);
+        cudaMemsetAsync(d_norm_, 0, NORM_SLOTS * 8, b);
+        vcycle<double>(p, code, 0, phi, rhs, true, b, false);
+        ++g_launches;
+        k_mg_mid<<<1, 1, 0, b>>>(d_norm_, single, maxit, ctl, hif, hw);
+        cap.node(b, cudaGraphCondTypeIf, hif, KIND_MG_RESID, [&](cudaStream_t q) {
+            resid(q);
+            ++g_launches;
+            k_mg_rn<<<1, 1, 0, q>>>(d_norm_, maxit, ctl, hw);
+        });
+    });
+    ++g_launches;
+    k_mg_end<<<1, 1, 0, s>>>(ctl);
+}
+
+// The loop of solve_mixed with its tests on the device.  The iterate
+// alternates between phi and the second buffer, so one WHILE pass holds two
+// refinement steps, the second inside an IF node; k_mx_copy brings the
+// iterate back into phi when it ends in the second buffer.
+void Multigrid::enqueue_solve_mixed_ctl(const DevParams& p, const uint8_t* code, double* phi, const double* rhs,
+                                        const double* nb, double rtol, int maxit, StepCtl* ctl, CondCapture& cap,
+                                        cudaStream_t s) {
+    MGLevel& L = lev_[0];
+    Op<double> o64 = make_op<double>(L, 0, code, eps_, has_alpha_ ? a0_64 : nullptr, true, p);
+    const dim3 b2(32, 8), g2((L.n[0] + 31) / 32, (L.n[1] + 7) / 8, (L.n[2] + R64_ZP - 1) / R64_ZP);
+    const int inner = std::max(1, mixed_cycles);
+    const cudaGraphConditionalHandle hw = cap.handle(s);
+    cudaMemsetAsync(d_norm_, 0, NORM_SLOTS * 8, s);
+    ++g_launches;
+    k_resid64<false><<<g2, b2, 0, s>>>(o64, phi, nullptr, rhs, nullptr, r32_, d_norm_);
+    ++g_launches;
+    k_mg_begin<<<1, 1, 0, s>>>(d_norm_, nb, rtol, maxit, ctl, hw);
+    auto refine = [&](cudaStream_t q, const double* xin, double* xout) {
+        for (int k = 0; k < inner; ++k) vcycle<float>(p, code, 0, e32_, r32_, false, q, k == 0);
+        cudaMemsetAsync(d_norm_, 0, NORM_SLOTS * 8, q);
+        ++g_launches;
+        k_resid64<true><<<g2, b2, 0, q>>>(o64, xin, e32_, rhs, xout, r32_, d_norm_);
+    };
+    cap.node(s, cudaGraphCondTypeWhile, hw, KIND_MX_FIRST, [&](cudaStream_t b) {
+        const cudaGraphConditionalHandle hif = cap.handle(b);
+        refine(b, phi, alt64m_);
+        ++g_launches;
+        k_mx_step<<<1, 1, 0, b>>>(d_norm_, inner, maxit, 1, KIND_MX_FIRST, ctl, hif, hw);
+        cap.node(b, cudaGraphCondTypeIf, hif, KIND_MX_SECOND, [&](cudaStream_t q) {
+            refine(q, alt64m_, phi);
+            ++g_launches;
+            k_mx_step<<<1, 1, 0, q>>>(d_norm_, inner, maxit, 0, KIND_MX_SECOND, ctl, hw, hw);
+        });
+    });
+    ++g_launches;
+    k_mx_copy<<<(int)std::min<size_t>((L.N + 255) / 256, 4 * 148), 256, 0, s>>>(alt64m_, phi, (int)L.N, ctl);
+    ++g_launches;
+    k_mg_end<<<1, 1, 0, s>>>(ctl);
 }
 
 template void Multigrid::vcycle<double>(const DevParams&, const uint8_t*, int, double*, const double*, bool, cudaStream_t, bool);

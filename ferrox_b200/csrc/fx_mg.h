@@ -19,6 +19,7 @@
 
 #include <cuda_runtime.h>
 
+#include "fx_ctl.h"
 #include "fx_device.cuh"
 
 namespace fx {
@@ -104,6 +105,15 @@ public:
     // FP64 iterative refinement around FP32 V-cycles
     int solve_mixed(const DevParams& p, const uint8_t* code, double* phi, const double* rhs, double target,
                     int maxit, cudaStream_t s, MGStats* st);
+    // The same two solves for a step graph being captured on s: the cycle
+    // loop is a conditional WHILE node whose test runs on the device (fx_ctl.h).
+    // nb points at max|b|, max|b'| on the device; the target, the cycles and a
+    // failure are recorded in ctl.
+    void enqueue_solve64_ctl(const DevParams& p, const uint8_t* code, double* phi, const double* rhs,
+                             const double* nb, double rtol, int maxit, StepCtl* ctl, CondCapture& cap, cudaStream_t s);
+    void enqueue_solve_mixed_ctl(const DevParams& p, const uint8_t* code, double* phi, const double* rhs,
+                                 const double* nb, double rtol, int maxit, StepCtl* ctl, CondCapture& cap,
+                                 cudaStream_t s);
     // |b' - A phi|_inf with the electrode terms (FP64); r may be null
     int residual64(const DevParams& p, const uint8_t* code, const double* phi, const double* rhs, double* r,
                    cudaStream_t s, double* norm_out);

@@ -468,6 +468,7 @@ Params make_params(const Inputs& in) {
     }
     r.query("fx.warm_start", p.warm_start);
     r.query("fx.phi_extrapolate", p.phi_extrapolate);
+    r.query("fx.step_graph", p.step_graph);
     r.query("fx.verbose", p.verbose);
     if (r.has("fx.plot_dir")) p.plot_dir = r.vals("fx.plot_dir")[0];
 

@@ -88,8 +88,10 @@ int fx_get_dims(const fx_ctx* ctx, int n_cell[3], double dx[3]);
  * Source/FerroX_namespace.H:1-115), plus fx.* keys.  fx_get_param also
  * answers read-only diagnostics: contains_sc, num_variants, V_lo, V_hi,
  * phi_ref, intrinsic_carrier_concentration, adjoint_* (the last recorded
- * run) and mg_level0_planes (1 when level 0's face coefficients depend on z
- * only and are read by plane). */
+ * run), mg_level0_planes (1 when level 0's face coefficients depend on z
+ * only and are read by plane) and step_graph_ran (1 when the last step ran
+ * as one CUDA graph with its Newton and multigrid loop tests on the device,
+ * fx.step_graph = 1; 0 when the host-driven loop ran it). */
 int fx_get_param(const fx_ctx* ctx, const char* key, double* value);
 int fx_set_param(fx_ctx* ctx, const char* key, double value);
 

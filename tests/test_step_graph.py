@@ -1,0 +1,123 @@
+"""A coupled step as one CUDA graph with its Newton and multigrid loop tests
+on the device (fx.step_graph = 1, the default) against the host-driven loop
+(fx.step_graph = 0).  Both launch the same kernels in the same order on the
+same data, so every field must be bit-identical after several steps, and so
+must the V-cycle and Newton counts; a failure in ComputePhi_Rho must stop the
+step before the TDGL update with the same error in both.
+"""
+import numpy as np
+import pytest
+
+from ferrox_b200 import api, decks
+from helpers import small_grains
+
+pytestmark = pytest.mark.gpu
+
+
+def start_P(shape, seed, vector=False):
+    g = np.random.default_rng(seed)
+    Pz = g.uniform(-0.05, 0.05, shape)
+    if not vector:
+        return (None, None, Pz)
+    return (g.uniform(-0.05, 0.05, shape), g.uniform(-0.05, 0.05, shape), Pz)
+
+
+def make(text, P, graph, precision=None, grains=None, params=None):
+    f = api.FerroX(text, precision=precision)
+    if grains is not None:
+        f.set_grains(grains["id"], grains["angles"], grains["tphase"])
+    f.set_initial_P(*P)
+    f.set_param("fx.step_graph", graph)
+    for k, v in (params or {}).items():
+        f.set_param(k, v)
+    return f
+
+
+FIELDS = ["Px", "Py", "Pz", "Phi", "charge", "Ez"]
+
+CASES = {
+    # Newton-coupled semiconductor stack, the voltage stepping every 3 steps
+    "mfism_fp64": dict(text=decks.mfism(16, 16, 48, steps_per_voltage=3, v_step=0.1), shape=(48, 16, 16)),
+    "mfism_mixed": dict(text=decks.mfism(16, 16, 48, steps_per_voltage=3, v_step=0.1), shape=(48, 16, 16),
+                        precision="mixed"),
+    "mfism_order2": dict(text=decks.mfism(16, 16, 48, steps_per_voltage=4, extra={"TimeIntegratorOrder": 2}),
+                         shape=(48, 16, 16)),
+    "mfim_fp64": dict(text=decks.mfim(32, 32, 12, Phi_Bc_hi=0.8), shape=(12, 32, 32)),
+    "mfim_mixed": dict(text=decks.mfim(32, 32, 12, Phi_Bc_hi=0.8), shape=(12, 32, 32), precision="mixed"),
+    "mfim_order2_cold": dict(text=decks.mfim(32, 32, 12, Phi_Bc_hi=0.8, extra={"TimeIntegratorOrder": 2}),
+                             shape=(12, 32, 32), params={"fx.warm_start": 0}),
+    "mfim_no_extrapolation": dict(text=decks.mfim(32, 32, 12, Phi_Bc_hi=0.8), shape=(12, 32, 32),
+                                  params={"fx.phi_extrapolate": 0}),
+}
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_graph_step_bit_identical(case):
+    cfg = CASES[case]
+    P = start_P(cfg["shape"], 11)
+    runs = []
+    for graph in (0, 1):
+        f = make(cfg["text"], P, graph, precision=cfg.get("precision"), params=cfg.get("params"))
+        f.set_param("fx.mg_rtol", 1e-12)
+        f.step(11)
+        assert f.param("step_graph_ran") == graph
+        runs.append(({n: f.field(n) for n in FIELDS}, f.stats()))
+        f.close()
+    (a, sa), (b, sb) = runs
+    for n in FIELDS:
+        assert np.array_equal(a[n], b[n]), (case, n)
+    for k in ("mg_cycles_total", "newton_iters_total", "mg_cycles_last", "newton_iters_last", "step", "num_Vapp"):
+        assert sa[k] == sb[k], (case, k, sa[k], sb[k])
+    assert sa["mg_resid_last"] == sb["mg_resid_last"]
+    assert sa["phi_err_last"] == sb["phi_err_last"]
+    assert sa["steady_err_last"] == sb["steady_err_last"]
+
+
+def test_graph_step_rotated_grains_vector_P():
+    text, g = small_grains(16, 16, 24)
+    text = text.replace("is_polarization_scalar = 1", "is_polarization_scalar = 0")
+    P = start_P((24, 16, 16), 12, vector=True)
+    out = []
+    for graph in (0, 1):
+        f = make(text, P, graph, precision="mixed", grains=g)
+        f.step(6)
+        assert f.param("step_graph_ran") == graph
+        out.append({n: f.field(n) for n in FIELDS})
+        f.close()
+    for n in FIELDS:
+        assert np.array_equal(out[0][n], out[1][n]), n
+
+
+@pytest.mark.parametrize("key,val,fragment", [("fx.mg_max_iter", 1, "Poisson multigrid did not reach"),
+                                               ("fx.newton_max_iter", 1, "Phi-rho Newton iteration did not reach")])
+def test_graph_step_failure_stops_before_tdgl(key, val, fragment):
+    text = decks.mfism(16, 16, 48)
+    P = start_P((48, 16, 16), 13)
+    res = []
+    for graph in (0, 1):
+        f = make(text, P, graph)
+        f.set_param("fx.mg_rtol", 1e-13)
+        f.step(2)
+        before = f.field("Pz")
+        f.set_param(key, val)
+        with pytest.raises(api.FxError) as e:
+            f.step(1)
+        assert e.value.code == -5
+        assert fragment in str(e.value)
+        assert np.array_equal(f.field("Pz"), before)
+        assert f.stats()["step"] == 2
+        res.append(str(e.value))
+        f.close()
+    assert res[0] == res[1]
+
+
+def test_graph_step_launches_counted():
+    f = make(decks.mfism(16, 16, 48), start_P((48, 16, 16), 14), 1)
+    f.step(1)
+    l0 = f.stats()["kernel_launches"]
+    f.step(3)
+    s = f.stats()
+    # per step at least the TDGL update, two Newton passes of charge and
+    # linearisation kernels, and a V-cycle of a handful of levels
+    assert s["kernel_launches"] - l0 >= 3 * 20
+    f.close()
