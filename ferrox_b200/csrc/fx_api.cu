@@ -31,6 +31,7 @@ thread_local std::string t_create_error;
 
 namespace fx {
 std::atomic<long long> g_launches{0};
+bool g_pdl = true;
 // message of the last failed call that has no context (fx_create and the
 // context-free entry points)
 void set_free_error(const std::string& m) { t_create_error = m; }
@@ -743,43 +744,47 @@ void sg_start_guess(fx_ctx* c, cudaStream_t q, int use) {
 }
 
 // mg_solve with the target formed on the device from the norms in d_out
-void sg_mg_solve(fx_ctx* c, cudaStream_t q, const double* rhs) {
+void sg_mg_solve(fx_ctx* c, cudaStream_t q, const double* rhs, bool end_in_next) {
     if (!c->par.warm_start) cudaMemsetAsync(c->d_phi, 0, c->N * 8, q);
     if (c->par.precision == 1)
         c->mg.enqueue_solve_mixed_ctl(c->dp, c->d_code, c->d_phi, rhs, c->d_out, c->par.mg_rtol, c->par.mg_max_iter,
-                                      c->d_ctl, c->cap, q);
+                                      c->d_ctl, c->cap, q, end_in_next);
     else
         c->mg.enqueue_solve64_ctl(c->dp, c->d_code, c->d_phi, rhs, c->d_out, c->par.mg_rtol, c->par.mg_max_iter,
-                                  c->d_ctl, c->cap, q);
+                                  c->d_ctl, c->cap, q, end_in_next);
 }
 
-// one pass of the ComputePhi_Rho loop (compute_phi_rho_P's loop body)
+// one pass of the ComputePhi_Rho loop (compute_phi_rho_P's loop body); the
+// charge kernel's last block closes the solve and runs the loop test, and
+// leaves the norm accumulators of the next pass's linearisation zeroed
 void sg_newton_pass(fx_ctx* c, cudaStream_t q, bool start, int use, cudaGraphConditionalHandle hn, int in_body) {
-    cudaMemsetAsync(c->d_out, 0, 2 * sizeof(double), q);
     ++g_launches;
     launch_newton(c->dp, c->d_code, c->d_phi, c->d_rho, c->d_rhsP, c->d_alpha, c->d_alpha32, c->d_rhs, c->d_out, q);
     c->mg.set_alpha(c->d_alpha, c->d_alpha32, true, q);
     if (start) sg_start_guess(c, q, use);
-    sg_mg_solve(c, q, c->d_rhs);
+    sg_mg_solve(c, q, c->d_rhs, true);
+    const RhoCtl rc = {c->d_ctl, c->par.newton_tol, c->par.newton_max_iter, in_body, 1, hn};
     ++g_launches;
     launch_rho(c->dp, c->d_code, c->d_phi, c->d_phi_prev, c->d_rho, c->d_e, c->d_h, c->d_part, c->d_counter, c->d_out,
-               1, 0, q);
-    ++g_launches;
-    launch_newton_ctl(c->d_ctl, c->d_out, c->par.newton_tol, c->par.newton_max_iter, hn, in_body, q);
+               1, 0, q, &rc);
 }
 
-// ComputePhi_Rho for P in buffer `buf` on stream q
-void sg_phirho(fx_ctx* c, cudaStream_t q, int buf, bool step_start, int use) {
-    ++g_launches;
-    launch_ctl_phirho_begin(c->d_ctl, q);
+// ComputePhi_Rho for P in buffer `buf` on stream q; its last kernel opens the
+// IF node `gate` (of body kind `kind`) while no failure is recorded.  The
+// step's first ComputePhi_Rho is begun by the step's first kernel.
+void sg_phirho(fx_ctx* c, cudaStream_t q, int buf, bool step_start, int use, cudaGraphConditionalHandle gate, int kind) {
+    if (!step_start) {
+        ++g_launches;
+        launch_ctl_phirho_begin(c->d_ctl, c->d_out, q);
+    }
     const double* P[3] = {c->scalarP ? nullptr : c->d_P[buf][0], c->scalarP ? nullptr : c->d_P[buf][1], c->d_P[buf][2]};
     if (!c->contains_sc) {
-        cudaMemsetAsync(c->d_out, 0, 2 * sizeof(double), q);
+        // (out[] zeroed by the step's or this ComputePhi_Rho's first kernel)
         ++g_launches;
         launch_rhs_p(c->dp, c->d_code, c->d_var, c->d_vt, P, c->d_rhsP, c->d_out, q);
         c->mg.set_alpha(nullptr, nullptr, false, q);
         if (step_start) sg_start_guess(c, q, use);
-        sg_mg_solve(c, q, c->d_rhsP);
+        sg_mg_solve(c, q, c->d_rhsP, false);
     } else {
         ++g_launches;
         launch_rhs_p(c->dp, c->d_code, c->d_var, c->d_vt, P, c->d_rhsP, nullptr, q);
@@ -789,22 +794,23 @@ void sg_phirho(fx_ctx* c, cudaStream_t q, int buf, bool step_start, int use) {
                     [&](cudaStream_t b) { sg_newton_pass(c, b, false, 0, hn, 1); });
     }
     ++g_launches;
-    launch_ctl_phirho_end(c->d_ctl, c->contains_sc ? 1 : 0, q);
+    launch_ctl_phirho_end(c->d_ctl, c->contains_sc ? 1 : 0, gate, kind, q);
 }
 
-// an IF node whose body runs only while no failure is recorded
+// ComputePhi_Rho, then `body` inside an IF node that runs only while no
+// failure is recorded
 template <typename F>
-void sg_gate(fx_ctx* c, cudaStream_t q, int kind, F&& body) {
+void sg_phirho_gated(fx_ctx* c, cudaStream_t q, int buf, bool step_start, int use, int kind, F&& body) {
     const cudaGraphConditionalHandle h = c->cap.handle(q);
-    ++g_launches;
-    launch_ctl_gate(c->d_ctl, kind, h, q);
+    sg_phirho(c, q, buf, step_start, use, h, kind);
     c->cap.node(q, cudaGraphCondTypeIf, h, kind, body);
 }
 
+// CheckSteadyState's norms into the control block (zeroed by the step's first
+// kernel); skipped after a failure
 void sg_steady(fx_ctx* c, cudaStream_t q) {
-    cudaMemsetAsync(c->d_out, 0, 2 * sizeof(double), q);
     ++g_launches;
-    launch_steady(c->dp, c->d_phi, c->d_phi_old, c->d_dphi, c->d_out, q);
+    launch_steady(c->dp, c->d_phi, c->d_phi_old, c->d_dphi, c->d_ctl->steady, q, &c->d_ctl->status);
 }
 
 void sg_enqueue_step(fx_ctx* c, int use) {
@@ -812,23 +818,23 @@ void sg_enqueue_step(fx_ctx* c, int use) {
     const int cur = c->cur, nb = 1 - cur;
     const int mixed = c->par.precision == 1;
     ++g_launches;
-    launch_ctl_step_begin(c->d_ctl, s);
-    sg_phirho(c, s, cur, true, use);
+    launch_ctl_step_begin(c->d_ctl, c->d_out, s);
     const double* Pin[3] = {c->scalarP ? nullptr : c->d_P[cur][0], c->scalarP ? nullptr : c->d_P[cur][1], c->d_P[cur][2]};
     double* Pout[3] = {c->scalarP ? nullptr : c->d_P[nb][0], c->scalarP ? nullptr : c->d_P[nb][1], c->d_P[nb][2]};
     if (c->par.TimeIntegratorOrder == 1) {
-        sg_gate(c, s, KIND_GATE_TDGL, [&](cudaStream_t q) {
-            ++g_launches;
-            launch_tdgl(c->dp, mixed, 0, c->d_code, c->d_var, c->d_vt, Pin, Pout, c->d_phi, nullptr, nullptr, q);
-            sg_steady(c, q);
-        });
+        // the update and the check return at once after a failure (a flag
+        // test costs less than an IF node)
+        sg_phirho(c, s, cur, true, use, 0, 0);
+        ++g_launches;
+        launch_tdgl(c->dp, mixed, 0, c->d_code, c->d_var, c->d_vt, Pin, Pout, c->d_phi, nullptr, nullptr, s,
+                    &c->d_ctl->status);
+        sg_steady(c, s);
     } else {
         double* fb[3] = {c->d_f[0], c->d_f[1], c->d_f[2]};
-        sg_gate(c, s, KIND_GATE_TDGL, [&](cudaStream_t q) {
+        sg_phirho_gated(c, s, cur, true, use, KIND_GATE_TDGL, [&](cudaStream_t q) {
             ++g_launches;
             launch_tdgl(c->dp, mixed, 1, c->d_code, c->d_var, c->d_vt, Pin, Pout, c->d_phi, fb, nullptr, q);
-            sg_phirho(c, q, nb, false, 0);
-            sg_gate(c, q, KIND_GATE_CORRECTOR, [&](cudaStream_t b) {
+            sg_phirho_gated(c, q, nb, false, 0, KIND_GATE_CORRECTOR, [&](cudaStream_t b) {
                 const double* Ppre[3] = {Pout[0], Pout[1], Pout[2]};
                 double* Pnew[3] = {c->scalarP ? nullptr : c->d_P[cur][0], c->scalarP ? nullptr : c->d_P[cur][1], c->d_P[cur][2]};
                 const double* Pold[3] = {Pnew[0], Pnew[1], Pnew[2]};
@@ -839,7 +845,6 @@ void sg_enqueue_step(fx_ctx* c, int use) {
         });
     }
     cudaMemcpyAsync(c->h_ctl, c->d_ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(c->h_out, c->d_out, 2 * sizeof(double), cudaMemcpyDeviceToHost, s);
 }
 
 // the captured launch parameters and graph shape of a step
@@ -852,7 +857,8 @@ std::vector<unsigned char> sg_key(const fx_ctx* c, int use) {
     put(&c->dp, sizeof(DevParams));
     const int iv[] = {c->cur, use, c->par.TimeIntegratorOrder, c->par.precision, c->par.warm_start,
                       c->par.phi_extrapolate, c->par.newton_max_iter, c->par.mg_max_iter, c->mg.nu1, c->mg.nu2,
-                      c->mg.mixed_cycles, c->scalarP ? 1 : 0, c->contains_sc ? 1 : 0};
+                      c->mg.mixed_cycles, c->scalarP ? 1 : 0, c->contains_sc ? 1 : 0, g_pdl ? 1 : 0,
+                      c->mg.alpha_tiles ? 1 : 0};
     put(iv, sizeof(iv));
     const double dv[] = {c->par.mg_rtol, c->par.newton_tol};
     put(dv, sizeof(dv));
@@ -968,7 +974,7 @@ int step_graph(fx_ctx* c, int step, bool* ran) {
     }
     sg_hist_after(c);
     if (c->par.TimeIntegratorOrder == 1) c->cur = 1 - c->cur;
-    steady_update(c, step, c->h_out[0], c->h_out[1]);
+    steady_update(c, step, t.steady[0], t.steady[1]);
     return FX_OK;
 }
 
@@ -1513,7 +1519,7 @@ int fx_get_param(const fx_ctx* c, const char* key, double* v) {
         {"adjoint_loss", c->adj.loss},
         // 1 when level 0's face coefficients depend on z only and its smoother
         // reads them by plane instead of from the material codes
-        {"step_graph_ran", c->sg_ran ? 1.0 : 0.0},
+        {"step_graph_ran", c->sg_ran ? 1.0 : 0.0}, {"fx.pdl", g_pdl ? 1.0 : 0.0},
         {"mg_level0_planes", !c->mg.levels().empty() && (c->mg.levels()[0].zc64 || c->mg.levels()[0].zc32) ? 1.0 : 0.0}};
     auto it = m.find(k);
     if (it != m.end()) { *v = it->second; return FX_OK; }
@@ -1549,7 +1555,9 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
     if (!c || !key) return FX_ERR_INVALID_ARGUMENT;
     const std::string k(key);
     Params& p = c->par;
-    if (k != "fx.profile" && k != "fx.verbose" && k != "fx.graphs" && k != "fx.step_graph") ++c->gen;
+    if (k != "fx.profile" && k != "fx.verbose" && k != "fx.graphs" && k != "fx.step_graph" && k != "fx.pdl" &&
+        k != "fx.alpha_tiles")
+        ++c->gen;
     // the time history of phi only seeds the next solve's initial iterate;
     // electrode values are compared on their own, solver settings leave the
     // trajectory alone, anything else starts the history afresh
@@ -1562,11 +1570,14 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
     if (k == "fx.warm_start") { p.warm_start = (int)v; return FX_OK; }
     if (k == "fx.phi_extrapolate") { p.phi_extrapolate = (int)v; return FX_OK; }
     if (k == "fx.step_graph") { p.step_graph = (int)v; return FX_OK; }
+    // process-wide: launches of every context
+    if (k == "fx.pdl") { g_pdl = v != 0.0; return FX_OK; }
     if (k == "fx.verbose") { p.verbose = (int)v; c->mg.verbose = (int)v; return FX_OK; }
     if (k == "fx.profile") { c->prof.collect(); c->prof.on = v != 0.0; return FX_OK; }
     if (k == "fx.mg_nu1") { c->mg.nu1 = (int)v; return FX_OK; }
     if (k == "fx.graphs") { c->mg.set_graphs(v != 0.0); return FX_OK; }
     if (k == "fx.mg_nu2") { c->mg.nu2 = (int)v; return FX_OK; }
+    if (k == "fx.alpha_tiles") { c->mg.alpha_tiles = v != 0.0; return FX_OK; }
     if (k == "fx.mg_mixed_cycles") {
         if (v < 1) return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx.mg_mixed_cycles must be at least 1");
         c->mg.mixed_cycles = (int)v;

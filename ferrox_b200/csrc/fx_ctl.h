@@ -23,10 +23,39 @@ namespace fx {
 
 extern std::atomic<long long> g_launches;
 
+// Programmatic dependent launch for the step kernels (fx.pdl, on by default):
+// a kernel launched with programmatic stream serialisation may be scheduled
+// while its predecessor drains; every kernel so launched calls pdl_entry()
+// before it touches memory, which waits for the predecessor's completion and
+// the visibility of its writes, then lets its own successor be scheduled.
+// Without the attribute the wait returns at once, so the same kernels serve
+// both forms.
+extern bool g_pdl;
+
+__device__ __forceinline__ void pdl_entry() {
+    asm volatile("griddepcontrol.wait;\n" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+}
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_k(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                            Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = g_pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 // bodies of conditional nodes whose executions the control kernels count
 enum CtlKind {
-    KIND_MG_CYCLE = 0, KIND_MG_RESID, KIND_NEWTON_PASS, KIND_MX_FIRST, KIND_MX_SECOND, KIND_GATE_TDGL,
-    KIND_GATE_CORRECTOR, KIND_N
+    KIND_MG_CYCLE = 0, KIND_NEWTON_PASS, KIND_MX_FIRST, KIND_MX_SECOND, KIND_GATE_TDGL, KIND_GATE_CORRECTOR, KIND_N
 };
 
 // failure recorded on the device (first one wins)
@@ -38,6 +67,7 @@ struct StepCtl {
     double rn;              // |r|_inf that the loop tests
     int it;                 // V-cycles (FP64) or FP32 cycles (mixed) of this solve
     int parity;             // mixed: 1 while the iterate sits in the second buffer
+    int need;               // FP64: the exact residual is formed after this cycle
     // the ComputePhi_Rho in progress (the step's last one when the step ends)
     int passes, iter;
     double err;
@@ -51,6 +81,75 @@ struct StepCtl {
     double status_val;      // |r| or Newton error at the failure
     double status_target;
     long long nexec[KIND_N];
+    double steady[2];       // CheckSteadyState: max|phi|, max|phi - phi_old|
+};
+
+// ---- loop control, run by one thread of the kernel that produces the tested
+// quantity (the last block of a residual or charge kernel), or by a
+// one-thread kernel
+
+// the multigrid solve ended: its statistics and, short of the target, the failure
+__device__ __forceinline__ void ctl_mg_end(StepCtl* ctl) {
+    const int it = ctl->it;
+    const double rn = ctl->rn, t = ctl->target;
+    ctl->mg_cycles_phirho += it;
+    ctl->mg_cycles_step += it;
+    ctl->mg_resid_last = rn;
+    ctl->mg_target_last = t;
+    if (!(rn <= t) && ctl->status == CTL_OK) {
+        ctl->status = isfinite(rn) ? CTL_MG_NO_CONV : CTL_MG_NONFINITE;
+        ctl->status_n = it;
+        ctl->status_val = rn;
+        ctl->status_target = t;
+    }
+}
+
+// the test of the ComputePhi_Rho loop (ElectrostaticSolver.cpp:690-742) after
+// a pass from the L1 sums s1 = sum|phi - phi_prev|, s2 = sum|phi|: err = s1 / s2
+// from the second pass on, as the host loop forms it; the pass cap turns a
+// loop that would go on into a failure
+__device__ __forceinline__ void ctl_newton(StepCtl* ctl, double s1, double s2, double tol, int max_iter,
+                                           cudaGraphConditionalHandle h, int in_body) {
+    if (in_body) ctl->nexec[KIND_NEWTON_PASS] += 1;
+    const int passes = ctl->passes + 1;
+    ctl->passes = passes;
+    double err = ctl->err;
+    if (ctl->iter > 0) err = s1 / s2;
+    ctl->err = err;
+    ctl->iter += 1;
+    bool go = err > tol;
+    if (ctl->status != CTL_OK) {
+        go = false;
+    } else if (go && passes >= max_iter) {
+        ctl->status = isfinite(err) ? CTL_NEWTON_NO_CONV : CTL_NEWTON_NONFINITE;
+        ctl->status_n = passes;
+        ctl->status_val = err;
+        go = false;
+    }
+    cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
+// control carried by the charge kernel's last block (null ctl: none)
+struct RhoCtl {
+    StepCtl* ctl;
+    double tol;
+    int max_iter;
+    int in_body;
+    int mg_end;            // first close the multigrid solve before it
+    cudaGraphConditionalHandle h;
+};
+
+// control carried by the FP64 residual kernel's last block (null ctl: none)
+enum ResidMode { RC_BEGIN = 1, RC_RN = 2, RC_MX = 3 };
+struct ResidCtl {
+    StepCtl* ctl;
+    int mode;
+    const double* nb;      // RC_BEGIN: max|b|, max|b'|
+    double rtol;
+    int maxit;
+    int inner, parity, kind;   // RC_MX: FP32 cycles spent, buffer holding the iterate, body kind
+    cudaGraphConditionalHandle h, h2;
+    unsigned int* counter;
 };
 
 // Builds conditional nodes while a stream is being captured.  node() adds a

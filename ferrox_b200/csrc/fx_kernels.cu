@@ -84,7 +84,10 @@ __global__ void __launch_bounds__(256) k_tdgl(DevParams p, const uint8_t* __rest
                                               const double* __restrict__ Pr, const double* __restrict__ phi,
                                               double* Pp_out, double* Pq_out, double* Pr_out,
                                               double* fbp, double* fbq, double* fbr,
-                                              const double* Pp_old, const double* Pq_old, const double* Pr_old) {
+                                              const double* Pp_old, const double* Pq_old, const double* Pr_old,
+                                              const int* __restrict__ skip) {
+    pdl_entry();
+    if (skip && *skip) return;   // a step graph whose ComputePhi_Rho failed
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int k = blockIdx.z;
@@ -202,6 +205,7 @@ __global__ void __launch_bounds__(256) k_rhs_p(DevParams p, const uint8_t* __res
                                                const double* __restrict__ Pp, const double* __restrict__ Pq,
                                                const double* __restrict__ Pr, double* __restrict__ rhs,
                                                double* __restrict__ norms) {
+    pdl_entry();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int k = blockIdx.z;
@@ -255,6 +259,7 @@ __global__ void __launch_bounds__(256) k_newton(DevParams p, const uint8_t* __re
                                                 const double* __restrict__ rhs_p, double* __restrict__ alpha,
                                                 float* __restrict__ alpha32, double* __restrict__ rhs,
                                                 double* __restrict__ norms) {
+    pdl_entry();
     __shared__ double sh[32];
     __shared__ double seps[8];
     const int tid = threadIdx.x + blockDim.x * threadIdx.y;
@@ -304,7 +309,8 @@ __global__ void __launch_bounds__(256) k_rho(DevParams p, const uint8_t* __restr
                                              double* __restrict__ rho, double* __restrict__ e_den,
                                              double* __restrict__ h_den, double* __restrict__ part,
                                              unsigned int* __restrict__ counter, double* __restrict__ out,
-                                             int track, int carriers) {
+                                             int track, int carriers, RhoCtl rc) {
+    pdl_entry();
     __shared__ double sh[32];
     __shared__ bool last;
     double s1 = 0.0, s2 = 0.0;
@@ -352,8 +358,17 @@ __global__ void __launch_bounds__(256) k_rho(DevParams p, const uint8_t* __restr
         t1 = block_sum(t1, sh);
         t2 = block_sum(t2, sh);
         if (threadIdx.x == 0) {
-            out[0] = t1;
-            out[1] = t2;
+            if (rc.ctl) {
+                // a step graph: close the solve, test the Newton loop, and
+                // leave out[] zeroed for the next linearisation's norms
+                if (rc.mg_end) ctl_mg_end(rc.ctl);
+                ctl_newton(rc.ctl, t1, t2, rc.tol, rc.max_iter, rc.h, rc.in_body);
+                out[0] = 0.0;
+                out[1] = 0.0;
+            } else {
+                out[0] = t1;
+                out[1] = t2;
+            }
             *counter = 0;
         }
     }
@@ -363,7 +378,9 @@ __global__ void __launch_bounds__(256) k_rho(DevParams p, const uint8_t* __restr
 // phi_old := phi; optionally keeps |phi - phi_old| for the PhiDiff output
 __global__ void __launch_bounds__(256) k_steady(DevParams p, const double* __restrict__ phi,
                                                 double* __restrict__ phi_old, double* __restrict__ dphi,
-                                                double* __restrict__ out) {
+                                                double* __restrict__ out, const int* __restrict__ skip) {
+    pdl_entry();
+    if (skip && *skip) return;
     __shared__ double sh[32];
     double m1 = 0.0, m2 = 0.0;
     for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < p.N; c += (long long)gridDim.x * blockDim.x) {
@@ -389,6 +406,7 @@ __global__ void __launch_bounds__(256) k_mean_p(DevParams p, const uint8_t* __re
                                                 const double* __restrict__ Px, const double* __restrict__ Py,
                                                 const double* __restrict__ Pz, double* __restrict__ part,
                                                 unsigned int* __restrict__ counter, double* __restrict__ out) {
+    pdl_entry();
     __shared__ double sh[32];
     __shared__ bool last;
     double s[4] = {0.0, 0.0, 0.0, 0.0};
@@ -426,6 +444,7 @@ __global__ void __launch_bounds__(256) k_efield(DevParams p, const uint8_t* __re
                                                 const Variant* __restrict__ vt, const double* __restrict__ phi,
                                                 double* __restrict__ Ex, double* __restrict__ Ey,
                                                 double* __restrict__ Ez) {
+    pdl_entry();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int k = blockIdx.z;
@@ -450,13 +469,13 @@ dim3 cell_grid(const DevParams& p) { return dim3((p.nx + 31) / 32, (p.ny + 7) / 
 // ------------------------------------------------------------ launchers --
 int launch_tdgl(const DevParams& p, int mixed, int mode, const uint8_t* code, const uint8_t* var, const Variant* vt,
                 const double* const Pin[3], double* const Pout[3], const double* phi, double* const fbuf[3],
-                const double* const Pold[3], cudaStream_t s) {
+                const double* const Pold[3], cudaStream_t s, const int* skip) {
     const dim3 g = cell_grid(p), b(32, 8);
     const bool scal = p.scalar && Pin[0] == nullptr;
     const bool rot = var != nullptr;
     double* fb[3] = {fbuf ? fbuf[0] : nullptr, fbuf ? fbuf[1] : nullptr, fbuf ? fbuf[2] : nullptr};
     const double* po[3] = {Pold ? Pold[0] : nullptr, Pold ? Pold[1] : nullptr, Pold ? Pold[2] : nullptr};
-#define FX_TDGL(T, S, R, M) k_tdgl<T, S, R, M><<<g, b, 0, s>>>(p, code, var, vt, Pin[0], Pin[1], Pin[2], phi, Pout[0], Pout[1], Pout[2], fb[0], fb[1], fb[2], po[0], po[1], po[2])
+#define FX_TDGL(T, S, R, M) launch_k(k_tdgl<T, S, R, M>, g, b, 0, s, p, code, var, vt, Pin[0], Pin[1], Pin[2], phi, Pout[0], Pout[1], Pout[2], fb[0], fb[1], fb[2], po[0], po[1], po[2], skip)
 #define FX_TDGL_M(T, S, R) do { if (mode == 0) FX_TDGL(T, S, R, 0); else if (mode == 1) FX_TDGL(T, S, R, 1); else FX_TDGL(T, S, R, 2); } while (0)
     if (!mixed) {
         if (scal) { if (rot) FX_TDGL_M(double, true, true); else FX_TDGL_M(double, true, false); }
@@ -476,32 +495,39 @@ int launch_rhs_p(const DevParams& p, const uint8_t* code, const uint8_t* var, co
     const bool scal = p.scalar && P[0] == nullptr;
     const bool rot = var != nullptr;
     if (scal) {
-        if (rot) k_rhs_p<true, true><<<g, b, 0, s>>>(p, code, var, vt, P[0], P[1], P[2], rhs, norms);
-        else k_rhs_p<true, false><<<g, b, 0, s>>>(p, code, var, vt, P[0], P[1], P[2], rhs, norms);
+        if (rot) launch_k(k_rhs_p<true, true>, g, b, 0, s, p, code, var, vt, P[0], P[1], P[2], rhs, norms);
+        else launch_k(k_rhs_p<true, false>, g, b, 0, s, p, code, var, vt, P[0], P[1], P[2], rhs, norms);
     } else {
-        if (rot) k_rhs_p<false, true><<<g, b, 0, s>>>(p, code, var, vt, P[0], P[1], P[2], rhs, norms);
-        else k_rhs_p<false, false><<<g, b, 0, s>>>(p, code, var, vt, P[0], P[1], P[2], rhs, norms);
+        if (rot) launch_k(k_rhs_p<false, true>, g, b, 0, s, p, code, var, vt, P[0], P[1], P[2], rhs, norms);
+        else launch_k(k_rhs_p<false, false>, g, b, 0, s, p, code, var, vt, P[0], P[1], P[2], rhs, norms);
     }
     return (int)cudaGetLastError();
 }
 
 int launch_newton(const DevParams& p, const uint8_t* code, const double* phi, const double* rho,
                   const double* rhs_p, double* alpha, float* alpha32, double* rhs, double* norms, cudaStream_t s) {
-    k_newton<<<p.ngrid_red, dim3(256), 0, s>>>(p, code, phi, rho, rhs_p, alpha, alpha32, rhs, norms);
+    launch_k(k_newton, p.ngrid_red, dim3(256), 0, s, p, code, phi, rho, rhs_p, alpha, alpha32, rhs, norms);
     return (int)cudaGetLastError();
 }
 
 int launch_rho(const DevParams& p, const uint8_t* code, const double* phi, double* phi_prev, double* rho,
                double* e_den, double* h_den, double* part, unsigned int* counter, double* out, int track,
-               int carriers, cudaStream_t s) {
-    k_rho<<<p.ngrid_red, RED_THREADS, 0, s>>>(p, code, phi, phi_prev, rho, e_den, h_den, part, counter, out, track,
-                                             carriers);
+               int carriers, cudaStream_t s, const RhoCtl* rc) {
+    RhoCtl none = {};
+    launch_k(k_rho, p.ngrid_red, RED_THREADS, 0, s, p, code, phi, phi_prev, rho, e_den, h_den, part, counter, out, track,
+             carriers, rc ? *rc : none);
     return (int)cudaGetLastError();
 }
 
 namespace {
 
-__global__ void k_ctl_step_begin(StepCtl* ctl) {
+__global__ void k_ctl_step_begin(StepCtl* ctl, double* out) {
+    pdl_entry();
+    // the norm accumulators of the first linearisation (or of ComputePoissonRHS)
+    out[0] = 0.0;
+    out[1] = 0.0;
+    ctl->steady[0] = 0.0;
+    ctl->steady[1] = 0.0;
     ctl->mg_cycles_step = 0;
     ctl->newton_passes_step = 0;
     ctl->status = CTL_OK;
@@ -509,91 +535,66 @@ __global__ void k_ctl_step_begin(StepCtl* ctl) {
     ctl->status_val = 0.0;
     ctl->status_target = 0.0;
     for (int k = 0; k < KIND_N; ++k) ctl->nexec[k] = 0;
-}
-
-__global__ void k_ctl_phirho_begin(StepCtl* ctl) {
+    // and the step's first ComputePhi_Rho begins
     ctl->passes = 0;
     ctl->iter = 0;
     ctl->err = 1.0;
     ctl->mg_cycles_phirho = 0;
 }
 
-// the test of the ComputePhi_Rho loop (ElectrostaticSolver.cpp:690-742) after
-// a pass: err = sum|phi - phi_prev| / sum|phi| from the second pass on, as the
-// host loop forms it; the pass cap turns a loop that would go on into a failure
-__global__ void k_newton_ctl(StepCtl* ctl, const double* __restrict__ out, double tol, int max_iter,
-                             cudaGraphConditionalHandle h, int in_body) {
-    if (in_body) ctl->nexec[KIND_NEWTON_PASS] += 1;
-    const int passes = ctl->passes + 1;
-    ctl->passes = passes;
-    double err = ctl->err;
-    if (ctl->iter > 0) err = out[0] / out[1];
-    ctl->err = err;
-    ctl->iter += 1;
-    bool go = err > tol;
-    if (ctl->status != CTL_OK) {
-        go = false;
-    } else if (go && passes >= max_iter) {
-        ctl->status = isfinite(err) ? CTL_NEWTON_NO_CONV : CTL_NEWTON_NONFINITE;
-        ctl->status_n = passes;
-        ctl->status_val = err;
-        go = false;
-    }
-    cudaGraphSetConditional(h, go ? 1u : 0u);
+__global__ void k_ctl_phirho_begin(StepCtl* ctl, double* out) {
+    pdl_entry();
+    out[0] = 0.0;
+    out[1] = 0.0;
+    ctl->passes = 0;
+    ctl->iter = 0;
+    ctl->err = 1.0;
+    ctl->mg_cycles_phirho = 0;
 }
 
 // without a semiconductor ComputePhi_Rho is one solve, counted as one pass
-__global__ void k_ctl_phirho_end(StepCtl* ctl, int sc) {
+// (gate != 0: also opens the IF node `gate` of body `kind` while no failure
+// is recorded, as k_ctl_gate)
+__global__ void k_ctl_phirho_end(StepCtl* ctl, int sc, cudaGraphConditionalHandle gate, int kind) {
+    pdl_entry();
     if (!sc) {
         ctl->passes = 1;
         ctl->err = 0.0;
     }
     ctl->newton_passes_step += ctl->passes;
-}
-
-__global__ void k_ctl_gate(StepCtl* ctl, int kind, cudaGraphConditionalHandle h) {
-    const bool ok = ctl->status == CTL_OK;
-    if (ok) ctl->nexec[kind] += 1;
-    cudaGraphSetConditional(h, ok ? 1u : 0u);
+    if (gate) {
+        const bool ok = ctl->status == CTL_OK;
+        if (ok) ctl->nexec[kind] += 1;
+        cudaGraphSetConditional(gate, ok ? 1u : 0u);
+    }
 }
 
 }  // namespace
 
-int launch_ctl_gate(StepCtl* ctl, int kind, cudaGraphConditionalHandle h, cudaStream_t s) {
-    k_ctl_gate<<<1, 1, 0, s>>>(ctl, kind, h);
+int launch_ctl_step_begin(StepCtl* ctl, double* out, cudaStream_t s) {
+    launch_k(k_ctl_step_begin, 1, 1, 0, s, ctl, out);
     return (int)cudaGetLastError();
 }
 
-int launch_ctl_step_begin(StepCtl* ctl, cudaStream_t s) {
-    k_ctl_step_begin<<<1, 1, 0, s>>>(ctl);
+int launch_ctl_phirho_begin(StepCtl* ctl, double* out, cudaStream_t s) {
+    launch_k(k_ctl_phirho_begin, 1, 1, 0, s, ctl, out);
     return (int)cudaGetLastError();
 }
 
-int launch_ctl_phirho_begin(StepCtl* ctl, cudaStream_t s) {
-    k_ctl_phirho_begin<<<1, 1, 0, s>>>(ctl);
-    return (int)cudaGetLastError();
-}
-
-int launch_newton_ctl(StepCtl* ctl, const double* out, double tol, int max_iter, cudaGraphConditionalHandle h,
-                      int in_body, cudaStream_t s) {
-    k_newton_ctl<<<1, 1, 0, s>>>(ctl, out, tol, max_iter, h, in_body);
-    return (int)cudaGetLastError();
-}
-
-int launch_ctl_phirho_end(StepCtl* ctl, int sc, cudaStream_t s) {
-    k_ctl_phirho_end<<<1, 1, 0, s>>>(ctl, sc);
+int launch_ctl_phirho_end(StepCtl* ctl, int sc, cudaGraphConditionalHandle gate, int kind, cudaStream_t s) {
+    launch_k(k_ctl_phirho_end, 1, 1, 0, s, ctl, sc, gate, kind);
     return (int)cudaGetLastError();
 }
 
 int launch_steady(const DevParams& p, const double* phi, double* phi_old, double* dphi, double* out,
-                  cudaStream_t s) {
-    k_steady<<<p.ngrid_red, RED_THREADS, 0, s>>>(p, phi, phi_old, dphi, out);
+                  cudaStream_t s, const int* skip) {
+    launch_k(k_steady, p.ngrid_red, RED_THREADS, 0, s, p, phi, phi_old, dphi, out, skip);
     return (int)cudaGetLastError();
 }
 
 int launch_mean_p(const DevParams& p, const uint8_t* code, const double* const P[3], double* part,
                   unsigned int* counter, double* out, cudaStream_t s) {
-    k_mean_p<<<p.ngrid_red, RED_THREADS, 0, s>>>(p, code, P[0], P[1], P[2], part, counter, out);
+    launch_k(k_mean_p, p.ngrid_red, RED_THREADS, 0, s, p, code, P[0], P[1], P[2], part, counter, out);
     return (int)cudaGetLastError();
 }
 
@@ -605,6 +606,7 @@ template <int ORDER>
 __global__ void __launch_bounds__(256) k_phi_extrap(double* __restrict__ phi, double* __restrict__ h0,
                                                     double* __restrict__ h1, double* __restrict__ h2,
                                                     long long n) {
+    pdl_entry();
     for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
         const double t = phi[c], a = h0[c];
         const double b = ORDER >= 2 ? h1[c] : 0.0;
@@ -618,17 +620,17 @@ __global__ void __launch_bounds__(256) k_phi_extrap(double* __restrict__ phi, do
 }
 
 int launch_phi_extrap(const DevParams& p, int order, double* phi, double* const h[3], cudaStream_t s) {
-    if (order >= 3) k_phi_extrap<3><<<p.ngrid_red, RED_THREADS, 0, s>>>(phi, h[0], h[1], h[2], p.N);
-    else if (order == 2) k_phi_extrap<2><<<p.ngrid_red, RED_THREADS, 0, s>>>(phi, h[0], h[1], h[2], p.N);
-    else k_phi_extrap<1><<<p.ngrid_red, RED_THREADS, 0, s>>>(phi, h[0], h[1], h[2], p.N);
+    if (order >= 3) launch_k(k_phi_extrap<3>, p.ngrid_red, RED_THREADS, 0, s, phi, h[0], h[1], h[2], p.N);
+    else if (order == 2) launch_k(k_phi_extrap<2>, p.ngrid_red, RED_THREADS, 0, s, phi, h[0], h[1], h[2], p.N);
+    else launch_k(k_phi_extrap<1>, p.ngrid_red, RED_THREADS, 0, s, phi, h[0], h[1], h[2], p.N);
     return (int)cudaGetLastError();
 }
 
 int launch_efield(const DevParams& p, const uint8_t* var, const Variant* vt, const double* phi, double* E[3],
                   cudaStream_t s) {
     const dim3 g = cell_grid(p), b(32, 8);
-    if (var) k_efield<true><<<g, b, 0, s>>>(p, var, vt, phi, E[0], E[1], E[2]);
-    else k_efield<false><<<g, b, 0, s>>>(p, var, vt, phi, E[0], E[1], E[2]);
+    if (var) launch_k(k_efield<true>, g, b, 0, s, p, var, vt, phi, E[0], E[1], E[2]);
+    else launch_k(k_efield<false>, g, b, 0, s, p, var, vt, phi, E[0], E[1], E[2]);
     return (int)cudaGetLastError();
 }
 

@@ -10,35 +10,35 @@
 namespace fx {
 
 // Pin/Pout: {Px, Py, Pz}; Px = Py = nullptr selects the scalar-P kernel.
-// mode 0: Euler; 1: predictor (writes fbuf); 2: corrector (reads fbuf, Pold)
+// mode 0: Euler; 1: predictor (writes fbuf); 2: corrector (reads fbuf, Pold);
+// skip (step graphs): a device flag; nonzero leaves the launch without effect
 int launch_tdgl(const DevParams& p, int mixed, int mode, const uint8_t* code, const uint8_t* var, const Variant* vt,
                 const double* const Pin[3], double* const Pout[3], const double* phi, double* const fbuf[3],
-                const double* const Pold[3], cudaStream_t s);
+                const double* const Pold[3], cudaStream_t s, const int* skip = nullptr);
 int launch_rhs_p(const DevParams& p, const uint8_t* code, const uint8_t* var, const Variant* vt,
                  const double* const P[3], double* rhs, double* norms, cudaStream_t s);
 int launch_newton(const DevParams& p, const uint8_t* code, const double* phi, const double* rho,
                   const double* rhs_p, double* alpha, float* alpha32, double* rhs, double* norms, cudaStream_t s);
+// rc (step graphs): the last block also runs the loop control of fx_ctl.h
 int launch_rho(const DevParams& p, const uint8_t* code, const double* phi, double* phi_prev, double* rho,
                double* e_den, double* h_den, double* part, unsigned int* counter, double* out, int track,
-               int carriers, cudaStream_t s);
+               int carriers, cudaStream_t s, const RhoCtl* rc = nullptr);
+// skip (step graphs): a device flag; nonzero leaves the launch without effect
 int launch_steady(const DevParams& p, const double* phi, double* phi_old, double* dphi, double* out,
-                  cudaStream_t s);
+                  cudaStream_t s, const int* skip = nullptr);
 int launch_mean_p(const DevParams& p, const uint8_t* code, const double* const P[3], double* part,
                   unsigned int* counter, double* out, cudaStream_t s);
 int launch_phi_extrap(const DevParams& p, int order, double* phi, double* const h[3], cudaStream_t s);
 int launch_efield(const DevParams& p, const uint8_t* var, const Variant* vt, const double* phi, double* E[3],
                   cudaStream_t s);
 
-// control of a step graph (fx_ctl.h): step and ComputePhi_Rho bookkeeping,
-// and the Newton loop test after each pass (h: the loop's condition; in_body:
-// the pass runs inside the WHILE node, not the unrolled first pass)
-int launch_ctl_step_begin(StepCtl* ctl, cudaStream_t s);
-int launch_ctl_phirho_begin(StepCtl* ctl, cudaStream_t s);
-int launch_newton_ctl(StepCtl* ctl, const double* out, double tol, int max_iter, cudaGraphConditionalHandle h,
-                      int in_body, cudaStream_t s);
-int launch_ctl_phirho_end(StepCtl* ctl, int sc, cudaStream_t s);
-// opens the IF node h (and counts an execution of `kind`) while no failure is recorded
-int launch_ctl_gate(StepCtl* ctl, int kind, cudaGraphConditionalHandle h, cudaStream_t s);
+// control of a step graph (fx_ctl.h): step and ComputePhi_Rho bookkeeping;
+// phirho_end also opens the IF node `gate` (0: none) of body `kind` while no
+// failure is recorded
+// (both zero out[0..1], the norm accumulators of what follows)
+int launch_ctl_step_begin(StepCtl* ctl, double* out, cudaStream_t s);
+int launch_ctl_phirho_begin(StepCtl* ctl, double* out, cudaStream_t s);
+int launch_ctl_phirho_end(StepCtl* ctl, int sc, cudaGraphConditionalHandle gate, int kind, cudaStream_t s);
 
 // adjoint (fx_adjoint.cu).  lam = {lambda_x, lambda_y, lambda_z}; vec = the
 // three-component kernels (else only lambda_z is read and written)

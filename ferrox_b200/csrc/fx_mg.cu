@@ -124,6 +124,7 @@ __device__ __forceinline__ float sdiv(float a, float b) { return __fdividef(a, b
 // set to 0, so the caller need not clear x first (even nx only)
 template <typename T, int KIND, bool ZERO = false>
 __global__ void __launch_bounds__(256) k_rbgs(Op<T> o, T* __restrict__ x, const T* __restrict__ b, int color) {
+    pdl_entry();
     __shared__ T seps[8];
     if (KIND == CK_FINE) {
         if (threadIdx.x == 0 && threadIdx.y == 0)
@@ -160,6 +161,7 @@ __global__ void __launch_bounds__(256) k_rbgs(Op<T> o, T* __restrict__ x, const 
 template <typename T, int KIND>
 __global__ void __launch_bounds__(128) k_line(Op<T> o, T* __restrict__ x, const T* __restrict__ b, T* __restrict__ q,
                                               int color) {
+    pdl_entry();
     __shared__ T seps[8];
     if (KIND == CK_FINE) {
         if (threadIdx.x == 0 && threadIdx.y == 0)
@@ -205,6 +207,7 @@ template <typename T, int KIND, int RX, int RY, int RZ>
 __global__ void __launch_bounds__(256) k_resid_restrict(Op<T> o, const T* __restrict__ x, const T* __restrict__ b,
                                                         T* __restrict__ bc, int ncx, int ncy, int ncz,
                                                         double* __restrict__ norm) {
+    pdl_entry();
     const int I = blockIdx.x * blockDim.x + threadIdx.x;
     const int J = blockIdx.y * blockDim.y + threadIdx.y;
     const int K = blockIdx.z;
@@ -259,10 +262,51 @@ __global__ void __launch_bounds__(256) k_resid_restrict(Op<T> o, const T* __rest
 // true>, same operations); block maxima go to NORM_SLOTS spread slots.
 constexpr int R64_ZP = 4;
 
+// the loop test of a device-controlled solve on a residual norm (one thread):
+// the max of the norm slots, which are left zeroed for their next user
+__device__ void resid_ctl(const ResidCtl& rc, double* slots) {
+    double rn = 0.0;
+    for (int q = 0; q < NORM_SLOTS; ++q) {
+        const double v = __ldcg(slots + q);
+        rn = rn < v ? v : rn;
+        slots[q] = 0.0;
+    }
+    StepCtl* ctl = rc.ctl;
+    if (rc.mode == RC_BEGIN) {
+        // the solve's target from the right-hand side norms, and the first test
+        const double r = rc.rtol < 1e-16 ? 1e-16 : rc.rtol;
+        const double m = rc.nb[0] < rc.nb[1] ? rc.nb[1] : rc.nb[0];
+        const double target = r * m;
+        ctl->target = target;
+        ctl->rn = rn;
+        ctl->it = 0;
+        ctl->parity = 0;
+        cudaGraphSetConditional(rc.h, (!(rn <= target) && 0 < rc.maxit) ? 1u : 0u);
+    } else if (rc.mode == RC_RN) {
+        // the exact residual after a V-cycle
+        ctl->rn = rn;
+        cudaGraphSetConditional(rc.h, (!(rn <= ctl->target) && ctl->it < rc.maxit) ? 1u : 0u);
+    } else {
+        // a mixed refinement step: `inner` FP32 cycles spent; h is the
+        // condition of the next step in the same body (the IF node) or the
+        // loop's own, h2 the loop's
+        ctl->nexec[rc.kind] += 1;
+        const int it = ctl->it + rc.inner;
+        ctl->rn = rn;
+        ctl->it = it;
+        ctl->parity = rc.parity;
+        cudaGraphSetConditional(rc.h, (!(rn <= ctl->target) && it < rc.maxit) ? 1u : 0u);
+        if (rc.h2 != rc.h) cudaGraphSetConditional(rc.h2, 0u);
+    }
+}
+
 template <bool CORR>
 __global__ void __launch_bounds__(256) k_resid64(Op<double> o, const double* __restrict__ x, const float* __restrict__ e,
                                                  const double* __restrict__ b, double* __restrict__ xout,
-                                                 float* __restrict__ r32, double* __restrict__ norm) {
+                                                 float* __restrict__ r32, double* __restrict__ norm, ResidCtl rc) {
+    pdl_entry();
+    // a step graph's exact residual after a V-cycle, not needed this time
+    if (rc.mode == RC_RN && !rc.ctl->need) return;
     auto X = [&](int n) -> double { return CORR ? x[n] + (double)e[n] : x[n]; };
     __shared__ double seps[8];
     if (threadIdx.x == 0 && threadIdx.y == 0)
@@ -320,6 +364,20 @@ __global__ void __launch_bounds__(256) k_resid64(Op<double> o, const double* __r
     const double m = block_max_all(mx);
     const int slot = (blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)) & (NORM_SLOTS - 1);
     if (threadIdx.x == 0 && threadIdx.y == 0) atomic_max_nonneg(norm + slot, m);
+    if (rc.ctl) {
+        // a step graph: the last block tests the solve's loop on the norm
+        __shared__ bool last;
+        if (threadIdx.x == 0 && threadIdx.y == 0) {
+            __threadfence();
+            last = atomicAdd(rc.counter, 1u) == gridDim.x * gridDim.y * gridDim.z - 1;
+        }
+        __syncthreads();
+        if (last && threadIdx.x == 0 && threadIdx.y == 0) {
+            __threadfence();
+            resid_ctl(rc, norm);
+            *rc.counter = 0;
+        }
+    }
 }
 
 // prolongation in the coarsened directions with the per-cell resistor-chain
@@ -330,6 +388,7 @@ template <typename T, int RX, int RY, int RZ>
 __global__ void __launch_bounds__(256) k_prolong(T* __restrict__ xf, const T* __restrict__ xc, const float* __restrict__ wx,
                                                  const float* __restrict__ wy, const float* __restrict__ wz, int nx, int ny,
                                                  int nz, int ncx, int ncy, int ncz) {
+    pdl_entry();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int k = blockIdx.z;
@@ -386,6 +445,7 @@ __global__ void __launch_bounds__(256) k_prolong(T* __restrict__ xf, const T* __
 // line solve) with __syncthreads() between phases instead of one kernel
 // launch per phase.
 constexpr int MAXLEV = 24;
+static_assert(MAXLEV == Multigrid::kMaxLev, "level tables");
 
 struct CoarseLevelDesc {
     int nx, ny, nz, N, rx, ry, rz, line;   // r*: ratio to the next (coarser) level
@@ -605,6 +665,7 @@ __device__ __forceinline__ void cp_async_el(E* dst, const E* src) {
 
 template <typename T>
 __global__ void __launch_bounds__(1024) k_coarse_vcycle(CoarseArgs A) {
+    pdl_entry();
     extern __shared__ __align__(16) unsigned char smraw[];
     __shared__ int s_valid;
     T* sm = reinterpret_cast<T*>(smraw);
@@ -685,6 +746,7 @@ __global__ void __launch_bounds__(1024) k_coarse_vcycle(CoarseArgs A) {
 template <typename Tin, typename T>
 __global__ void __launch_bounds__(256) k_avg_alpha(const Tin* __restrict__ af, T* __restrict__ ac, int nx, int ny,
                                                    int ncx, int ncy, int ncz, int rx, int ry, int rz) {
+    pdl_entry();
     const int I = blockIdx.x * blockDim.x + threadIdx.x;
     const int J = blockIdx.y * blockDim.y + threadIdx.y;
     const int K = blockIdx.z;
@@ -695,6 +757,100 @@ __global__ void __launch_bounds__(256) k_avg_alpha(const Tin* __restrict__ af, T
             for (int di = 0; di < rx; ++di)
                 s += (double)af[(size_t)(rx * I + di) + (size_t)nx * ((size_t)(ry * J + dj) + (size_t)ny * (rz * K + dk))];
     ac[(size_t)I + (size_t)ncx * ((size_t)J + (size_t)ncy * K)] = (T)(s / (rx * ry * rz));
+}
+
+// Every coarse alpha below level 1 in one launch.  Block b owns one cell of
+// the tile level T and the cells of levels 2..T inside it (tile dims tl[l]),
+// staged level by level in shared memory; the last block to finish forms the
+// levels below T from the level-T arrays.  Each coarse cell is the same
+// double sum in the same order as k_avg_alpha forms it (FP64 chain from the
+// FP64 level above, FP32 chain from the FP32 level above), so the values are
+// those of the per-level launches.
+struct AlphaTiles {
+    int* fvalid;                 // cleared: the one-CTA factors depend on alpha
+    int nlev, T, cap;
+    int n[MAXLEV][3], cr[MAXLEV][3], tl[MAXLEV][3];
+    double* a64[MAXLEV];
+    float* a32[MAXLEV];
+    unsigned int* counter;
+};
+
+__global__ void __launch_bounds__(256) k_alpha_tiles(AlphaTiles A) {
+    pdl_entry();
+    extern __shared__ __align__(16) double atile[];
+    __shared__ bool last;
+    if (blockIdx.x == 0 && threadIdx.x < 2 && A.fvalid) A.fvalid[threadIdx.x] = 0;
+    float* const f32 = reinterpret_cast<float*>(atile + 2 * A.cap);
+    const bool has32 = A.a32[1] != nullptr;
+    const int nT0 = A.n[A.T][0], nT1 = A.n[A.T][1];
+    const int IT = blockIdx.x % nT0, JT = (blockIdx.x / nT0) % nT1, KT = blockIdx.x / (nT0 * nT1);
+    int cur = 0;
+    for (int l = 2; l <= A.T; ++l) {
+        const double* src64 = atile + cur * A.cap;
+        const float* src32 = f32 + cur * A.cap;
+        double* dst64 = atile + (1 - cur) * A.cap;
+        float* dst32 = f32 + (1 - cur) * A.cap;
+        const int tx = A.tl[l][0], ty = A.tl[l][1], tz = A.tl[l][2];
+        const int rx = A.cr[l][0], ry = A.cr[l][1], rz = A.cr[l][2];
+        const int ox = IT * tx, oy = JT * ty, oz = KT * tz;
+        const int ptx = A.tl[l - 1][0], pty = A.tl[l - 1][1];
+        const int fnx = A.n[l - 1][0], fny = A.n[l - 1][1];
+        for (int q = threadIdx.x; q < tx * ty * tz; q += blockDim.x) {
+            const int i = q % tx, j = (q / tx) % ty, k = q / (tx * ty);
+            double s = 0.0, s2 = 0.0;
+            for (int dk = 0; dk < rz; ++dk)
+                for (int dj = 0; dj < ry; ++dj)
+                    for (int di = 0; di < rx; ++di) {
+                        if (l == 2) {
+                            const size_t g = (size_t)(rx * (ox + i) + di) +
+                                             (size_t)fnx * ((size_t)(ry * (oy + j) + dj) + (size_t)fny * (size_t)(rz * (oz + k) + dk));
+                            s += A.a64[1][g];
+                            if (has32) s2 += (double)A.a32[1][g];
+                        } else {
+                            const int lq = (rx * i + di) + ptx * ((ry * j + dj) + pty * (rz * k + dk));
+                            s += src64[lq];
+                            if (has32) s2 += (double)src32[lq];
+                        }
+                    }
+            const double v = s / (rx * ry * rz);
+            const size_t gc = (size_t)(ox + i) + (size_t)A.n[l][0] * ((size_t)(oy + j) + (size_t)A.n[l][1] * (size_t)(oz + k));
+            A.a64[l][gc] = v;
+            dst64[q] = v;
+            if (has32) {
+                const float v2 = (float)(s2 / (rx * ry * rz));
+                A.a32[l][gc] = v2;
+                dst32[q] = v2;
+            }
+        }
+        __syncthreads();
+        cur = 1 - cur;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(A.counter, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    for (int l = A.T + 1; l < A.nlev; ++l) {
+        const int rx = A.cr[l][0], ry = A.cr[l][1], rz = A.cr[l][2];
+        const int nx = A.n[l][0], ny = A.n[l][1], nz = A.n[l][2];
+        const int fnx = A.n[l - 1][0], fny = A.n[l - 1][1];
+        for (int q = threadIdx.x; q < nx * ny * nz; q += blockDim.x) {
+            const int I = q % nx, J = (q / nx) % ny, K = q / (nx * ny);
+            double s = 0.0, s2 = 0.0;
+            for (int dk = 0; dk < rz; ++dk)
+                for (int dj = 0; dj < ry; ++dj)
+                    for (int di = 0; di < rx; ++di) {
+                        const size_t g = (size_t)(rx * I + di) + (size_t)fnx * ((size_t)(ry * J + dj) + (size_t)fny * (rz * K + dk));
+                        s += __ldcg(A.a64[l - 1] + g);
+                        if (has32) s2 += (double)__ldcg(A.a32[l - 1] + g);
+                    }
+            A.a64[l][q] = s / (rx * ry * rz);
+            if (has32) A.a32[l][q] = (float)(s2 / (rx * ry * rz));
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *A.counter = 0;
 }
 
 
@@ -755,79 +911,36 @@ __device__ __forceinline__ double ctl_slots_max(const double* __restrict__ slots
     return m;
 }
 
-// the solve's target from the right-hand side norms, and the first loop test
-__global__ void k_mg_begin(const double* __restrict__ slots, const double* __restrict__ nb, double rtol, int maxit,
-                           StepCtl* ctl, cudaGraphConditionalHandle hw) {
-    const double rn = ctl_slots_max(slots);
-    const double r = rtol < 1e-16 ? 1e-16 : rtol;
-    const double m = nb[0] < nb[1] ? nb[1] : nb[0];
-    const double target = r * m;
-    ctl->target = target;
-    ctl->rn = rn;
-    ctl->it = 0;
-    ctl->parity = 0;
-    cudaGraphSetConditional(hw, (!(rn <= target) && 0 < maxit) ? 1u : 0u);
-}
-
 // after a V-cycle: the level-0 norm after pre-smoothing bounds the residual
-// after the cycle; the exact residual is formed (IF body) once it is within
-// the target, or always with a single level
-__global__ void k_mg_mid(const double* __restrict__ slots, int single_level, int maxit, StepCtl* ctl,
-                         cudaGraphConditionalHandle hif, cudaGraphConditionalHandle hw) {
+// after the cycle; the exact residual is formed (the next residual kernel,
+// which otherwise returns at once) once it is within the target, or always
+// with a single level
+__global__ void k_mg_mid(double* __restrict__ slots, int single_level, int maxit, StepCtl* ctl,
+                         cudaGraphConditionalHandle hw) {
+    pdl_entry();
     ctl->nexec[KIND_MG_CYCLE] += 1;
     const double mid = ctl_slots_max(slots);
+    for (int q = 0; q < NORM_SLOTS; ++q) slots[q] = 0.0;
     const int it = ctl->it + 1;
     ctl->it = it;
     const bool need = single_level || mid <= ctl->target;
     if (!need) ctl->rn = mid;
-    cudaGraphSetConditional(hif, need ? 1u : 0u);
+    ctl->need = need ? 1 : 0;
     cudaGraphSetConditional(hw, (!need && it < maxit) ? 1u : 0u);
-}
-
-__global__ void k_mg_rn(const double* __restrict__ slots, int maxit, StepCtl* ctl, cudaGraphConditionalHandle hw) {
-    ctl->nexec[KIND_MG_RESID] += 1;
-    const double rn = ctl_slots_max(slots);
-    ctl->rn = rn;
-    cudaGraphSetConditional(hw, (!(rn <= ctl->target) && ctl->it < maxit) ? 1u : 0u);
-}
-
-// after a mixed refinement step: `inner` FP32 cycles were spent; parity says
-// which buffer holds the iterate.  hc is the condition of the next step in
-// the same body (the IF node), or the loop's own
-__global__ void k_mx_step(const double* __restrict__ slots, int inner, int maxit, int parity, int kind, StepCtl* ctl,
-                          cudaGraphConditionalHandle hc, cudaGraphConditionalHandle hw) {
-    ctl->nexec[kind] += 1;
-    const double rn = ctl_slots_max(slots);
-    const int it = ctl->it + inner;
-    ctl->rn = rn;
-    ctl->it = it;
-    ctl->parity = parity;
-    const unsigned go = (!(rn <= ctl->target) && it < maxit) ? 1u : 0u;
-    cudaGraphSetConditional(hc, go);
-    if (hw != hc) cudaGraphSetConditional(hw, 0u);
 }
 
 // the iterate back into phi when the last refinement step wrote the second buffer
 __global__ void __launch_bounds__(256) k_mx_copy(const double* __restrict__ src, double* __restrict__ dst, int n,
                                                  const StepCtl* __restrict__ ctl) {
+    pdl_entry();
     if (!ctl->parity) return;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) dst[c] = src[c];
 }
 
 // the solve's statistics and, when it stopped short of the target, the failure
 __global__ void k_mg_end(StepCtl* ctl) {
-    const int it = ctl->it;
-    const double rn = ctl->rn, t = ctl->target;
-    ctl->mg_cycles_phirho += it;
-    ctl->mg_cycles_step += it;
-    ctl->mg_resid_last = rn;
-    ctl->mg_target_last = t;
-    if (!(rn <= t) && ctl->status == CTL_OK) {
-        ctl->status = isfinite(rn) ? CTL_MG_NO_CONV : CTL_MG_NONFINITE;
-        ctl->status_n = it;
-        ctl->status_val = rn;
-        ctl->status_target = t;
-    }
+    pdl_entry();
+    ctl_mg_end(ctl);
 }
 
 }  // namespace
@@ -850,6 +963,8 @@ Multigrid::~Multigrid() {
         cudaFree(L.zc32);
     }
     cudaFree(d_fvalid_);
+    cudaFree(at_counter_);
+    cudaFree(rc_counter_);
     if (g64_.exec) cudaGraphExecDestroy(g64_.exec);
     if (g32_.exec) cudaGraphExecDestroy(g32_.exec);
     if (g32b_.exec) cudaGraphExecDestroy(g32b_.exec);
@@ -1073,6 +1188,9 @@ int Multigrid::setup(const DevParams& p, const std::vector<uint8_t>& code, bool 
         }
     }
     if (cudaMalloc(&d_norm_, NORM_SLOTS * 8) != cudaSuccess) return -2;
+    if (cudaMemset(d_norm_, 0, NORM_SLOTS * 8) != cudaSuccess) return -1;
+    if (cudaMalloc(&rc_counter_, sizeof(unsigned int)) != cudaSuccess) return -2;
+    if (cudaMemset(rc_counter_, 0, sizeof(unsigned int)) != cudaSuccess) return -1;
     if (cudaMallocHost(&h_norm_, NORM_SLOTS * 8) != cudaSuccess) return -2;
     if (want32) {
         e32_ = dalloc<float>(L0.N, bytes_);
@@ -1083,6 +1201,28 @@ int Multigrid::setup(const DevParams& p, const std::vector<uint8_t>& code, bool 
         lev_[0].b32 = r32_;
     }
     plan_coarse(want64, want32);
+    // the tile level of k_alpha_tiles: the deepest level whose cells cover at
+    // most 4096 level-1 cells, with few cells left below it for the last block
+    at_T_ = 0;
+    if (lev_.size() >= 3 && lev_.size() <= (size_t)kMaxLev) {
+        int best = 0;
+        for (int T = 2; T < (int)lev_.size(); ++T) {
+            long long f = 1;
+            for (int m = 2; m <= T; ++m) f *= (long long)lev_[m].cr[0] * lev_[m].cr[1] * lev_[m].cr[2];
+            if (f > 4096) break;
+            long long below = 0;
+            for (size_t m = T + 1; m < lev_.size(); ++m) below += (long long)lev_[m].N;
+            if (below <= 16384) best = T;
+        }
+        if (best >= 2 && cudaMalloc(&at_counter_, sizeof(unsigned int)) == cudaSuccess &&
+            cudaMemset(at_counter_, 0, sizeof(unsigned int)) == cudaSuccess) {
+            at_T_ = best;
+            for (int d = 0; d < 3; ++d) at_tl_[best][d] = 1;
+            for (int l = best; l >= 2; --l)
+                for (int d = 0; d < 3; ++d) at_tl_[l - 1][d] = at_tl_[l][d] * lev_[l].cr[d];
+            at_cap_ = at_tl_[2][0] * at_tl_[2][1] * at_tl_[2][2];
+        }
+    }
     if (verbose) {
         printf("  one-CTA coarse cycle from level %d (FP64, %zu B smem), %d (FP32, %zu B smem)\n", coarse_top64_,
                coarse_smem64_, coarse_top32_, coarse_smem32_);
@@ -1095,23 +1235,43 @@ int Multigrid::setup(const DevParams& p, const std::vector<uint8_t>& code, bool 
 
 int Multigrid::set_alpha(const double* a64, const float* a32, bool has_alpha, cudaStream_t s) {
     // the one-CTA factors depend on alpha: recompute them at the next call
-    if ((has_alpha || has_alpha_) && d_fvalid_) cudaMemsetAsync(d_fvalid_, 0, 2 * sizeof(int), s);
+    // (the tile kernel below clears the flags itself)
+    const bool tiles = has_alpha && at_T_ >= 2 && alpha_tiles;
+    if ((has_alpha || has_alpha_) && d_fvalid_ && !tiles) cudaMemsetAsync(d_fvalid_, 0, 2 * sizeof(int), s);
     a0_64 = a64;
     a0_32 = a32;
     has_alpha_ = has_alpha;
     if (!has_alpha) return 0;
-    for (size_t l = 1; l < lev_.size(); ++l) {
+    const size_t lmax = tiles ? 2 : lev_.size();   // per-level launches below this level
+    for (size_t l = 1; l < lmax; ++l) {
         MGLevel& L = lev_[l];
         const MGLevel& F = lev_[l - 1];
         dim3 b(32, 8), g((L.n[0] + 31) / 32, (L.n[1] + 7) / 8, L.n[2]);
         if (L.a64) {
-            if (l == 1) { ++g_launches; k_avg_alpha<double, double><<<g, b, 0, s>>>(a64, L.a64, F.n[0], F.n[1], L.n[0], L.n[1], L.n[2], L.cr[0], L.cr[1], L.cr[2]); }
-            else { ++g_launches; k_avg_alpha<double, double><<<g, b, 0, s>>>(F.a64, L.a64, F.n[0], F.n[1], L.n[0], L.n[1], L.n[2], L.cr[0], L.cr[1], L.cr[2]); }
+            if (l == 1) { ++g_launches; launch_k(k_avg_alpha<double, double>, g, b, 0, s, a64, L.a64, F.n[0], F.n[1], L.n[0], L.n[1], L.n[2], L.cr[0], L.cr[1], L.cr[2]); }
+            else { ++g_launches; launch_k(k_avg_alpha<double, double>, g, b, 0, s, F.a64, L.a64, F.n[0], F.n[1], L.n[0], L.n[1], L.n[2], L.cr[0], L.cr[1], L.cr[2]); }
         }
         if (L.a32) {
-            if (l == 1) { ++g_launches; k_avg_alpha<double, float><<<g, b, 0, s>>>(a64, L.a32, F.n[0], F.n[1], L.n[0], L.n[1], L.n[2], L.cr[0], L.cr[1], L.cr[2]); }
-            else { ++g_launches; k_avg_alpha<float, float><<<g, b, 0, s>>>(F.a32, L.a32, F.n[0], F.n[1], L.n[0], L.n[1], L.n[2], L.cr[0], L.cr[1], L.cr[2]); }
+            if (l == 1) { ++g_launches; launch_k(k_avg_alpha<double, float>, g, b, 0, s, a64, L.a32, F.n[0], F.n[1], L.n[0], L.n[1], L.n[2], L.cr[0], L.cr[1], L.cr[2]); }
+            else { ++g_launches; launch_k(k_avg_alpha<float, float>, g, b, 0, s, F.a32, L.a32, F.n[0], F.n[1], L.n[0], L.n[1], L.n[2], L.cr[0], L.cr[1], L.cr[2]); }
         }
+    }
+    if (tiles) {
+        AlphaTiles A;
+        std::memset(&A, 0, sizeof(A));
+        A.nlev = (int)lev_.size();
+        A.T = at_T_;
+        A.cap = at_cap_;
+        for (int l = 0; l < A.nlev; ++l) {
+            for (int d = 0; d < 3; ++d) { A.n[l][d] = lev_[l].n[d]; A.cr[l][d] = lev_[l].cr[d]; A.tl[l][d] = at_tl_[l][d]; }
+            A.a64[l] = l == 0 ? nullptr : lev_[l].a64;
+            A.a32[l] = l == 0 ? nullptr : lev_[l].a32;
+        }
+        A.counter = at_counter_;
+        A.fvalid = d_fvalid_;
+        const MGLevel& LT = lev_[at_T_];
+        ++g_launches;
+        launch_k(k_alpha_tiles, (unsigned)LT.N, 256, (size_t)at_cap_ * 24, s, A);
     }
     return (int)cudaGetLastError();
 }
@@ -1213,7 +1373,7 @@ void Multigrid::launch_coarse(int top, cudaStream_t s) {
     }
     if (prof) prof->begin(PROF_COARSE_CTA, s);
     ++g_launches;
-    k_coarse_vcycle<T><<<1, 1024, bytes, s>>>(A);
+    launch_k(k_coarse_vcycle<T>, 1, 1024, bytes, s, A);
     if (prof) prof->end(s);
 }
 
@@ -1238,9 +1398,9 @@ void Multigrid::smooth(const DevParams& p, const uint8_t* code, int l, T* x, con
             for (int color = 0; color < 2; ++color) {
                 if (prof) prof->begin(l == 0 ? PROF_SMOOTH_L0 : l == 1 ? PROF_MG_L1 : l == 2 ? PROF_MG_L2 : PROF_MG_COARSE, s);
                 ++g_launches;
-                if (o.zc) k_line<T, CK_PLANES><<<g2, b2, 0, s>>>(o, x, b, q, color);
-                else if (l == 0) k_line<T, CK_FINE><<<g2, b2, 0, s>>>(o, x, b, q, color);
-                else k_line<T, CK_ARRAYS><<<g2, b2, 0, s>>>(o, x, b, q, color);
+                if (o.zc) launch_k(k_line<T, CK_PLANES>, g2, b2, 0, s, o, x, b, q, color);
+                else if (l == 0) launch_k(k_line<T, CK_FINE>, g2, b2, 0, s, o, x, b, q, color);
+                else launch_k(k_line<T, CK_ARRAYS>, g2, b2, 0, s, o, x, b, q, color);
                 if (prof) prof->end(s);
             }
     } else {
@@ -1251,15 +1411,15 @@ void Multigrid::smooth(const DevParams& p, const uint8_t* code, int l, T* x, con
                 const bool z = zero && it == 0 && color == 0;
                 ++g_launches;
                 if (l == 0 && !o.zc) {
-                    if (z) k_rbgs<T, CK_FINE, true><<<g2, b2, 0, s>>>(o, x, b, color);
-                    else k_rbgs<T, CK_FINE><<<g2, b2, 0, s>>>(o, x, b, color);
+                    if (z) launch_k(k_rbgs<T, CK_FINE, true>, g2, b2, 0, s, o, x, b, color);
+                    else launch_k(k_rbgs<T, CK_FINE>, g2, b2, 0, s, o, x, b, color);
                 } else {
                     if (o.zc) {
-                        if (z) k_rbgs<T, CK_PLANES, true><<<g2, b2, 0, s>>>(o, x, b, color);
-                        else k_rbgs<T, CK_PLANES><<<g2, b2, 0, s>>>(o, x, b, color);
+                        if (z) launch_k(k_rbgs<T, CK_PLANES, true>, g2, b2, 0, s, o, x, b, color);
+                        else launch_k(k_rbgs<T, CK_PLANES>, g2, b2, 0, s, o, x, b, color);
                     } else {
-                        if (z) k_rbgs<T, CK_ARRAYS, true><<<g2, b2, 0, s>>>(o, x, b, color);
-                        else k_rbgs<T, CK_ARRAYS><<<g2, b2, 0, s>>>(o, x, b, color);
+                        if (z) launch_k(k_rbgs<T, CK_ARRAYS, true>, g2, b2, 0, s, o, x, b, color);
+                        else launch_k(k_rbgs<T, CK_ARRAYS>, g2, b2, 0, s, o, x, b, color);
                     }
                 }
                 if (prof) prof->end(s);
@@ -1292,13 +1452,13 @@ void Multigrid::vcycle(const DevParams& p, const uint8_t* code, int l, T* x, con
     }
     Op<T> o = make_op<T>(L, l, code, eps_, a, inhom, p);
     dim3 b2(32, 8), g2((C.n[0] + 31) / 32, (C.n[1] + 7) / 8, C.n[2]);
-    double* norm = (l == 0) ? d_norm_ : nullptr;
+    double* norm = (l == 0 && sizeof(T) == 8) ? d_norm_ : nullptr;
     if (prof) prof->begin(l == 0 ? PROF_RESTRICT_L0 : l == 1 ? PROF_MG_L1 : l == 2 ? PROF_MG_L2 : PROF_MG_COARSE, s);
     ++g_launches;
     {
         const int key = (C.cr[0] == 2) * 4 + (C.cr[1] == 2) * 2 + (C.cr[2] == 2);
         T* bc = lb<T>(C);
-#define FX_RR(F, RX, RY, RZ) k_resid_restrict<T, F, RX, RY, RZ><<<g2, b2, 0, s>>>(o, x, b, bc, C.n[0], C.n[1], C.n[2], norm)
+#define FX_RR(F, RX, RY, RZ) launch_k(k_resid_restrict<T, F, RX, RY, RZ>, g2, b2, 0, s, o, x, b, bc, C.n[0], C.n[1], C.n[2], norm)
 #define FX_RR_ALL(F)                                  \
         switch (key) {                                \
         case 1: FX_RR(F, 1, 1, 2); break;             \
@@ -1321,7 +1481,7 @@ void Multigrid::vcycle(const DevParams& p, const uint8_t* code, int l, T* x, con
     {
         const int key = (C.cr[0] == 2) * 4 + (C.cr[1] == 2) * 2 + (C.cr[2] == 2);
         T* xc = lx<T>(C);
-#define FX_PR(RX, RY, RZ) k_prolong<T, RX, RY, RZ><<<g3, b2, 0, s>>>(x, xc, C.wf[0], C.wf[1], C.wf[2], L.n[0], L.n[1], L.n[2], C.n[0], C.n[1], C.n[2])
+#define FX_PR(RX, RY, RZ) launch_k(k_prolong<T, RX, RY, RZ>, g3, b2, 0, s, x, xc, C.wf[0], C.wf[1], C.wf[2], L.n[0], L.n[1], L.n[2], C.n[0], C.n[1], C.n[2])
         switch (key) {
         case 1: FX_PR(1, 1, 2); break;
         case 2: FX_PR(1, 2, 1); break;
@@ -1345,11 +1505,12 @@ int Multigrid::residual64(const DevParams& p, const uint8_t* code, const double*
     dim3 b2(32, 8), g2((L.n[0] + 31) / 32, (L.n[1] + 7) / 8, L.n[2]);
     (void)r;
     if (prof) prof->begin(PROF_RESID64, s);
-    { ++g_launches; k_resid64<false><<<dim3(g2.x, g2.y, (L.n[2] + R64_ZP - 1) / R64_ZP), b2, 0, s>>>(o, phi, nullptr, rhs, nullptr, nullptr, d_norm_); }
+    { ++g_launches; launch_k(k_resid64<false>, dim3(g2.x, g2.y, (L.n[2] + R64_ZP - 1) / R64_ZP), b2, 0, s, o, phi, nullptr, rhs, nullptr, nullptr, d_norm_, ResidCtl{}); }
     if (prof) prof->end(s);
     cudaMemcpyAsync(h_norm_, d_norm_, NORM_SLOTS * 8, cudaMemcpyDeviceToHost, s);
     cudaError_t e = cudaStreamSynchronize(s);
     if (norm_out) *norm_out = slots_max();
+    cudaMemsetAsync(d_norm_, 0, NORM_SLOTS * 8, s);   // the slots are zero between uses
     return (int)e;
 }
 
@@ -1361,7 +1522,7 @@ int Multigrid::replay(GraphCache& g, const void* x, const void* rhs, const DevPa
         return (int)cudaGetLastError();
     }
     if (!g.exec || g.x != x || g.rhs != rhs || g.has_alpha != has_alpha_ || g.vlo != p.V_lo || g.vhi != p.V_hi ||
-        g.nu1 != nu1 || g.nu2 != nu2) {
+        g.nu1 != nu1 || g.nu2 != nu2 || g.pdl != g_pdl) {
         if (g.exec) { cudaGraphExecDestroy(g.exec); g.exec = nullptr; }
         cudaGraph_t graph;
         const long long l0 = g_launches.load();
@@ -1376,6 +1537,7 @@ int Multigrid::replay(GraphCache& g, const void* x, const void* rhs, const DevPa
         cudaGraphDestroy(graph);
         if (e) return (int)e;
         g.x = x; g.rhs = rhs; g.has_alpha = has_alpha_; g.vlo = p.V_lo; g.vhi = p.V_hi; g.nu1 = nu1; g.nu2 = nu2;
+        g.pdl = g_pdl;
     }
     g_launches += g.launches;
     return (int)cudaGraphLaunch(g.exec, s);
@@ -1411,6 +1573,7 @@ int Multigrid::solve64(const DevParams& p, const uint8_t* code, double* phi, con
         }
     }
     if (st) { st->cycles = it; st->resid = rn; }
+    cudaMemsetAsync(d_norm_, 0, NORM_SLOTS * 8, s);
     return rn <= target ? 0 : -3;
 }
 
@@ -1426,7 +1589,7 @@ int Multigrid::solve_mixed(const DevParams& p, const uint8_t* code, double* phi,
     cudaMemsetAsync(d_norm_, 0, NORM_SLOTS * 8, s);
     if (prof) prof->begin(PROF_RESID64, s);
     ++g_launches;
-    k_resid64<false><<<g2, b2, 0, s>>>(o64, phi, nullptr, rhs, nullptr, r32_, d_norm_);
+    launch_k(k_resid64<false>, g2, b2, 0, s, o64, phi, nullptr, rhs, nullptr, r32_, d_norm_, ResidCtl{});
     if (prof) prof->end(s);
     cudaMemcpyAsync(h_norm_, d_norm_, NORM_SLOTS * 8, cudaMemcpyDeviceToHost, s);
     int e = (int)cudaStreamSynchronize(s);
@@ -1445,7 +1608,7 @@ int Multigrid::solve_mixed(const DevParams& p, const uint8_t* code, double* phi,
             cudaMemsetAsync(d_norm_, 0, NORM_SLOTS * 8, s);
             if (prof) prof->begin(PROF_RESID64, s);
             ++g_launches;
-            k_resid64<true><<<g2, b2, 0, s>>>(o64, xin, e32_, rhs, xout, r32_, d_norm_);
+            launch_k(k_resid64<true>, g2, b2, 0, s, o64, xin, e32_, rhs, xout, r32_, d_norm_, ResidCtl{});
             if (prof) prof->end(s);
             cudaMemcpyAsync(h_norm_, d_norm_, NORM_SLOTS * 8, cudaMemcpyDeviceToHost, s);
         });
@@ -1463,82 +1626,77 @@ int Multigrid::solve_mixed(const DevParams& p, const uint8_t* code, double* phi,
         if (e) return e;
     }
     if (st) { st->cycles = cycles; st->resid = rn; }
+    cudaMemsetAsync(d_norm_, 0, NORM_SLOTS * 8, s);
     return rn <= target ? 0 : -3;
 }
 
 // The loop of solve64 with its tests on the device: a WHILE node runs one
 // V-cycle per pass; k_mg_mid decides from the pre-smoothing norm whether the
-// exact residual is needed (an IF node) and whether another cycle follows.
+// exact residual is needed (the residual kernel after it returns at once
+// otherwise) and whether another cycle follows.  The residual kernel's last
+// block runs the test on the exact residual (and the first test, on the
+// initial residual).  The norm slots are left zeroed by whoever reads them.  end_in_next: the next kernel (the charge kernel of
+// a Newton pass) closes the solve, else k_mg_end does.
 void Multigrid::enqueue_solve64_ctl(const DevParams& p, const uint8_t* code, double* phi, const double* rhs,
                                     const double* nb, double rtol, int maxit, StepCtl* ctl, CondCapture& cap,
-                                    cudaStream_t s) {
+                                    cudaStream_t s, bool end_in_next) {
     MGLevel& L = lev_[0];
     Op<double> o = make_op<double>(L, 0, code, eps_, has_alpha_ ? a0_64 : nullptr, true, p);
     const dim3 b2(32, 8), g2((L.n[0] + 31) / 32, (L.n[1] + 7) / 8, (L.n[2] + R64_ZP - 1) / R64_ZP);
     const int single = lev_.size() == 1 ? 1 : 0;
-    auto resid = [&](cudaStream_t q) {
-        cudaMemsetAsync(d_norm_, 0, NORM_SLOTS * 8, q);
-        ++g_launches;
-        k_resid64<false><<<g2, b2, 0, q>>>(o, phi, nullptr, rhs, nullptr, nullptr, d_norm_);
-    };
     const cudaGraphConditionalHandle hw = cap.handle(s);
-    resid(s);
+    // the norm slots are zero between uses
+    ResidCtl rb = {ctl, RC_BEGIN, nb, rtol, maxit, 0, 0, 0, hw, hw, rc_counter_};
     ++g_launches;
-    k_mg_begin<<<1, 1, 0, s>>>(d_norm_, nb, rtol, maxit, ctl, hw);
+    launch_k(k_resid64<false>, g2, b2, 0, s, o, phi, nullptr, rhs, nullptr, nullptr, d_norm_, rb);
     cap.node(s, cudaGraphCondTypeWhile, hw, KIND_MG_CYCLE, [&](cudaStream_t b) {
-        const cudaGraphConditionalHandle hif = cap.handle(b);
-        cudaMemsetAsync(d_norm_, 0, NORM_SLOTS * 8, b);
         vcycle<double>(p, code, 0, phi, rhs, true, b, false);
         ++g_launches;
-        k_mg_mid<<<1, 1, 0, b>>>(d_norm_, single, maxit, ctl, hif, hw);
-        cap.node(b, cudaGraphCondTypeIf, hif, KIND_MG_RESID, [&](cudaStream_t q) {
-            resid(q);
-            ++g_launches;
-            k_mg_rn<<<1, 1, 0, q>>>(d_norm_, maxit, ctl, hw);
-        });
+        launch_k(k_mg_mid, 1, 1, 0, b, d_norm_, single, maxit, ctl, hw);
+        ResidCtl rr = {ctl, RC_RN, nullptr, 0.0, maxit, 0, 0, 0, hw, hw, rc_counter_};
+        ++g_launches;
+        launch_k(k_resid64<false>, g2, b2, 0, b, o, phi, nullptr, rhs, nullptr, nullptr, d_norm_, rr);
     });
-    ++g_launches;
-    k_mg_end<<<1, 1, 0, s>>>(ctl);
+    if (!end_in_next) {
+        ++g_launches;
+        launch_k(k_mg_end, 1, 1, 0, s, ctl);
+    }
 }
 
 // The loop of solve_mixed with its tests on the device.  The iterate
 // alternates between phi and the second buffer, so one WHILE pass holds two
-// refinement steps, the second inside an IF node; k_mx_copy brings the
-// iterate back into phi when it ends in the second buffer.
+// refinement steps, the second inside an IF node; each step's FP64 residual
+// kernel runs the test in its last block; k_mx_copy brings the iterate back
+// into phi when it ends in the second buffer.
 void Multigrid::enqueue_solve_mixed_ctl(const DevParams& p, const uint8_t* code, double* phi, const double* rhs,
                                         const double* nb, double rtol, int maxit, StepCtl* ctl, CondCapture& cap,
-                                        cudaStream_t s) {
+                                        cudaStream_t s, bool end_in_next) {
     MGLevel& L = lev_[0];
     Op<double> o64 = make_op<double>(L, 0, code, eps_, has_alpha_ ? a0_64 : nullptr, true, p);
     const dim3 b2(32, 8), g2((L.n[0] + 31) / 32, (L.n[1] + 7) / 8, (L.n[2] + R64_ZP - 1) / R64_ZP);
     const int inner = std::max(1, mixed_cycles);
     const cudaGraphConditionalHandle hw = cap.handle(s);
-    cudaMemsetAsync(d_norm_, 0, NORM_SLOTS * 8, s);
+    ResidCtl rb = {ctl, RC_BEGIN, nb, rtol, maxit, 0, 0, 0, hw, hw, rc_counter_};
     ++g_launches;
-    k_resid64<false><<<g2, b2, 0, s>>>(o64, phi, nullptr, rhs, nullptr, r32_, d_norm_);
-    ++g_launches;
-    k_mg_begin<<<1, 1, 0, s>>>(d_norm_, nb, rtol, maxit, ctl, hw);
-    auto refine = [&](cudaStream_t q, const double* xin, double* xout) {
+    launch_k(k_resid64<false>, g2, b2, 0, s, o64, phi, nullptr, rhs, nullptr, r32_, d_norm_, rb);
+    auto refine = [&](cudaStream_t q, const double* xin, double* xout, const ResidCtl& rc) {
         for (int k = 0; k < inner; ++k) vcycle<float>(p, code, 0, e32_, r32_, false, q, k == 0);
-        cudaMemsetAsync(d_norm_, 0, NORM_SLOTS * 8, q);
         ++g_launches;
-        k_resid64<true><<<g2, b2, 0, q>>>(o64, xin, e32_, rhs, xout, r32_, d_norm_);
+        launch_k(k_resid64<true>, g2, b2, 0, q, o64, xin, e32_, rhs, xout, r32_, d_norm_, rc);
     };
     cap.node(s, cudaGraphCondTypeWhile, hw, KIND_MX_FIRST, [&](cudaStream_t b) {
         const cudaGraphConditionalHandle hif = cap.handle(b);
-        refine(b, phi, alt64m_);
-        ++g_launches;
-        k_mx_step<<<1, 1, 0, b>>>(d_norm_, inner, maxit, 1, KIND_MX_FIRST, ctl, hif, hw);
+        refine(b, phi, alt64m_, ResidCtl{ctl, RC_MX, nullptr, 0.0, maxit, inner, 1, KIND_MX_FIRST, hif, hw, rc_counter_});
         cap.node(b, cudaGraphCondTypeIf, hif, KIND_MX_SECOND, [&](cudaStream_t q) {
-            refine(q, alt64m_, phi);
-            ++g_launches;
-            k_mx_step<<<1, 1, 0, q>>>(d_norm_, inner, maxit, 0, KIND_MX_SECOND, ctl, hw, hw);
+            refine(q, alt64m_, phi, ResidCtl{ctl, RC_MX, nullptr, 0.0, maxit, inner, 0, KIND_MX_SECOND, hw, hw, rc_counter_});
         });
     });
     ++g_launches;
-    k_mx_copy<<<(int)std::min<size_t>((L.N + 255) / 256, 4 * 148), 256, 0, s>>>(alt64m_, phi, (int)L.N, ctl);
-    ++g_launches;
-    k_mg_end<<<1, 1, 0, s>>>(ctl);
+    launch_k(k_mx_copy, (int)std::min<size_t>((L.N + 255) / 256, 4 * 148), 256, 0, s, alt64m_, phi, (int)L.N, ctl);
+    if (!end_in_next) {
+        ++g_launches;
+        launch_k(k_mg_end, 1, 1, 0, s, ctl);
+    }
 }
 
 template void Multigrid::vcycle<double>(const DevParams&, const uint8_t*, int, double*, const double*, bool, cudaStream_t, bool);

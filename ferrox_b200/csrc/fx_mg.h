@@ -109,11 +109,13 @@ public:
     // loop is a conditional WHILE node whose test runs on the device (fx_ctl.h).
     // nb points at max|b|, max|b'| on the device; the target, the cycles and a
     // failure are recorded in ctl.
+    // end_in_next: the kernel that follows closes the solve's bookkeeping
     void enqueue_solve64_ctl(const DevParams& p, const uint8_t* code, double* phi, const double* rhs,
-                             const double* nb, double rtol, int maxit, StepCtl* ctl, CondCapture& cap, cudaStream_t s);
+                             const double* nb, double rtol, int maxit, StepCtl* ctl, CondCapture& cap, cudaStream_t s,
+                             bool end_in_next);
     void enqueue_solve_mixed_ctl(const DevParams& p, const uint8_t* code, double* phi, const double* rhs,
                                  const double* nb, double rtol, int maxit, StepCtl* ctl, CondCapture& cap,
-                                 cudaStream_t s);
+                                 cudaStream_t s, bool end_in_next);
     // |b' - A phi|_inf with the electrode terms (FP64); r may be null
     int residual64(const DevParams& p, const uint8_t* code, const double* phi, const double* rhs, double* r,
                    cudaStream_t s, double* norm_out);
@@ -121,6 +123,8 @@ public:
     const std::vector<MGLevel>& levels() const { return lev_; }
     int nu1 = 2, nu2 = 1, nu_bottom = 40;
     int mixed_cycles = 2;    // FP32 V-cycles per FP64 refinement step
+    bool alpha_tiles = true; // coarse alphas below level 1 in one launch (k_alpha_tiles)
+    static constexpr int kMaxLev = 24;
     Prof* prof = nullptr;
     int verbose = 0;
     void set_graphs(bool on) { use_graphs_ = on; }
@@ -148,6 +152,7 @@ private:
         bool has_alpha = false;
         double vlo = 0, vhi = 0;
         int nu1 = 0, nu2 = 0;
+        bool pdl = false;
         long long launches = 0;
     };
     GraphCache g64_, g32_, g32b_;   // g32b_: the refinement step from the second FP64 buffer
@@ -155,6 +160,13 @@ private:
     template <typename F> int replay(GraphCache& g, const void* x, const void* rhs, const DevParams& p, cudaStream_t s, F&& enqueue);
     int coarse_top64_ = -1, coarse_top32_ = -1;   // first level run by the one-CTA kernel
     int* d_fvalid_ = nullptr;    // [0] FP64, [1] FP32: the one-CTA factors in global memory are current
+    // k_alpha_tiles: tile level (0: per-level launches), level-l cells per
+    // tile, the largest staged tile, and the last-block counter
+    int at_T_ = 0;
+    int at_tl_[kMaxLev][3] = {};
+    int at_cap_ = 0;
+    unsigned int* at_counter_ = nullptr;
+    unsigned int* rc_counter_ = nullptr;   // last-block counter of the controlled residual kernel
     size_t coarse_smem64_ = 0, coarse_smem32_ = 0;
     void plan_coarse(bool want64, bool want32);
     double slots_max() const;

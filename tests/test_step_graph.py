@@ -121,3 +121,44 @@ def test_graph_step_launches_counted():
     # linearisation kernels, and a V-cycle of a handful of levels
     assert s["kernel_launches"] - l0 >= 3 * 20
     f.close()
+
+
+@pytest.mark.parametrize("precision", [None, "mixed"])
+def test_programmatic_launch_bit_identical(precision):
+    # fx.pdl lets a kernel be scheduled while its predecessor drains; every
+    # kernel waits for its predecessor before touching memory, so the fields
+    # are those of plain stream order
+    text = decks.mfism(32, 32, 48, steps_per_voltage=3, v_step=0.1)
+    P = start_P((48, 32, 32), 15)
+    out = []
+    try:
+        for pdl in (0, 1):
+            f = make(text, P, 1, precision=precision)
+            f.set_param("fx.pdl", pdl)
+            f.step(8)
+            assert f.param("fx.pdl") == pdl
+            out.append({n: f.field(n) for n in FIELDS})
+            f.close()
+    finally:
+        f = api.FerroX(decks.mfim(8, 8, 12))
+        f.set_param("fx.pdl", 1)
+        f.close()
+    for n in FIELDS:
+        assert np.array_equal(out[0][n], out[1][n]), n
+
+
+@pytest.mark.parametrize("precision", [None, "mixed"])
+def test_coarse_alpha_tiles_bit_identical(precision):
+    # every coarse Newton coefficient below level 1 from one tiled launch
+    # equals the per-level averaging launches
+    text = decks.mfism(32, 32, 48, steps_per_voltage=3, v_step=0.1)
+    P = start_P((48, 32, 32), 16)
+    out = []
+    for tiles in (0, 1):
+        f = make(text, P, 1, precision=precision, params={"fx.alpha_tiles": tiles})
+        f.step(7)
+        out.append(({n: f.field(n) for n in FIELDS}, f.stats()["mg_cycles_total"]))
+        f.close()
+    for n in FIELDS:
+        assert np.array_equal(out[0][0][n], out[1][0][n]), n
+    assert out[0][1] == out[1][1]
