@@ -300,7 +300,7 @@ __device__ void resid_ctl(const ResidCtl& rc, double* slots) {
     }
 }
 
-template <bool CORR>
+template <bool CORR, int KIND = CK_FINE>
 __global__ void __launch_bounds__(256) k_resid64(Op<double> o, const double* __restrict__ x, const float* __restrict__ e,
                                                  const double* __restrict__ b, double* __restrict__ xout,
                                                  float* __restrict__ r32, double* __restrict__ norm, ResidCtl rc) {
@@ -327,24 +327,37 @@ __global__ void __launch_bounds__(256) k_resid64(Op<double> o, const double* __r
         const uint8_t* cd = o.code + o.nxy;   // the k = -1 ghost layer is cd - nxy
         double xm = k0 > 0 ? X(col + o.nxy * (k0 - 1)) : 0.0;
         double xc = X(col + o.nxy * k0);
-        double em = seps[__ldg(cd + col + o.nxy * (k0 - 1)) & 7];
-        double ec = seps[__ldg(cd + col + o.nxy * k0) & 7];
+        double em = KIND == CK_PLANES ? 0.0 : seps[__ldg(cd + col + o.nxy * (k0 - 1)) & 7];
+        double ec = KIND == CK_PLANES ? 0.0 : seps[__ldg(cd + col + o.nxy * k0) & 7];
 #pragma unroll
         for (int q = 0; q < R64_ZP; ++q) {
             const int k = k0 + q;
             if (k >= o.nz) break;
             const int c = col + o.nxy * k;
             const double xp = k < o.nz - 1 ? X(c + o.nxy) : 0.0;
-            const double ep = seps[__ldg(cd + c + o.nxy) & 7];
-            double extra = 0.0, bcv = 0.0, cb, ct;
-            double cw = 0.5 * (ec + seps[__ldg(cd + row + o.nxy * k + im) & 7]) * o.ih2x;
-            double ce = 0.5 * (seps[__ldg(cd + row + o.nxy * k + ip) & 7] + ec) * o.ih2x;
-            double cs = 0.5 * (ec + seps[__ldg(cd + c + dso) & 7]) * o.ih2y;
-            double cn = 0.5 * (seps[__ldg(cd + c + dno) & 7] + ec) * o.ih2y;
-            if (k > 0) cb = 0.5 * (ec + em) * o.ih2z;
-            else { cb = 0.0; extra += 2.0 * ec * o.ih2z; bcv += 2.0 * ec * o.ih2z * o.vlo; }
-            if (k < o.nz - 1) ct = 0.5 * (ep + ec) * o.ih2z;
-            else { ct = 0.0; extra += 2.0 * ec * o.ih2z; bcv += 2.0 * ec * o.ih2z * o.vhi; }
+            double extra = 0.0, bcv = 0.0, cb, ct, cw, ce, cs, cn;
+            double ep = 0.0;
+            if constexpr (KIND == CK_PLANES) {
+                // a layered stack: the same face values per z plane, as the
+                // setup formed them from the codes (same operations)
+                cw = ce = __ldg(o.zc + k) * o.ih2x;
+                cs = cn = __ldg(o.zc + o.nz + k) * o.ih2y;
+                const double fb = __ldg(o.zc + 2 * o.nz + k), ft = __ldg(o.zc + 2 * o.nz + k + 1);
+                if (k > 0) cb = fb * o.ih2z;
+                else { cb = 0.0; extra += 2.0 * fb * o.ih2z; bcv += 2.0 * fb * o.ih2z * o.vlo; }
+                if (k < o.nz - 1) ct = ft * o.ih2z;
+                else { ct = 0.0; extra += 2.0 * ft * o.ih2z; bcv += 2.0 * ft * o.ih2z * o.vhi; }
+            } else {
+                ep = seps[__ldg(cd + c + o.nxy) & 7];
+                cw = 0.5 * (ec + seps[__ldg(cd + row + o.nxy * k + im) & 7]) * o.ih2x;
+                ce = 0.5 * (seps[__ldg(cd + row + o.nxy * k + ip) & 7] + ec) * o.ih2x;
+                cs = 0.5 * (ec + seps[__ldg(cd + c + dso) & 7]) * o.ih2y;
+                cn = 0.5 * (seps[__ldg(cd + c + dno) & 7] + ec) * o.ih2y;
+                if (k > 0) cb = 0.5 * (ec + em) * o.ih2z;
+                else { cb = 0.0; extra += 2.0 * ec * o.ih2z; bcv += 2.0 * ec * o.ih2z * o.vlo; }
+                if (k < o.nz - 1) ct = 0.5 * (ep + ec) * o.ih2z;
+                else { ct = 0.0; extra += 2.0 * ec * o.ih2z; bcv += 2.0 * ec * o.ih2z * o.vhi; }
+            }
             if (o.nx == 1) { cw = 0.0; ce = 0.0; }
             if (o.ny == 1) { cs = 0.0; cn = 0.0; }
             const double a = o.a ? o.a[c] : 0.0;
@@ -378,6 +391,14 @@ __global__ void __launch_bounds__(256) k_resid64(Op<double> o, const double* __r
             *rc.counter = 0;
         }
     }
+}
+
+// k_resid64 with the face coefficients by plane when level 0 has them
+template <bool CORR>
+void launch_resid64(const Op<double>& o, dim3 g, dim3 b, cudaStream_t s, const double* x, const float* e,
+                    const double* rhs, double* xout, float* r32, double* norm, const ResidCtl& rc) {
+    if (o.zc) launch_k(k_resid64<CORR, CK_PLANES>, g, b, 0, s, o, x, e, rhs, xout, r32, norm, rc);
+    else launch_k(k_resid64<CORR, CK_FINE>, g, b, 0, s, o, x, e, rhs, xout, r32, norm, rc);
 }
 
 // prolongation in the coarsened directions with the per-cell resistor-chain
@@ -1505,7 +1526,7 @@ int Multigrid::residual64(const DevParams& p, const uint8_t* code, const double*
     dim3 b2(32, 8), g2((L.n[0] + 31) / 32, (L.n[1] + 7) / 8, L.n[2]);
     (void)r;
     if (prof) prof->begin(PROF_RESID64, s);
-    { ++g_launches; launch_k(k_resid64<false>, dim3(g2.x, g2.y, (L.n[2] + R64_ZP - 1) / R64_ZP), b2, 0, s, o, phi, nullptr, rhs, nullptr, nullptr, d_norm_, ResidCtl{}); }
+    { ++g_launches; launch_resid64<false>(o, dim3(g2.x, g2.y, (L.n[2] + R64_ZP - 1) / R64_ZP), b2, s, phi, nullptr, rhs, nullptr, nullptr, d_norm_, ResidCtl{}); }
     if (prof) prof->end(s);
     cudaMemcpyAsync(h_norm_, d_norm_, NORM_SLOTS * 8, cudaMemcpyDeviceToHost, s);
     cudaError_t e = cudaStreamSynchronize(s);
@@ -1589,7 +1610,7 @@ int Multigrid::solve_mixed(const DevParams& p, const uint8_t* code, double* phi,
     cudaMemsetAsync(d_norm_, 0, NORM_SLOTS * 8, s);
     if (prof) prof->begin(PROF_RESID64, s);
     ++g_launches;
-    launch_k(k_resid64<false>, g2, b2, 0, s, o64, phi, nullptr, rhs, nullptr, r32_, d_norm_, ResidCtl{});
+    launch_resid64<false>(o64, g2, b2, s, phi, nullptr, rhs, nullptr, r32_, d_norm_, ResidCtl{});
     if (prof) prof->end(s);
     cudaMemcpyAsync(h_norm_, d_norm_, NORM_SLOTS * 8, cudaMemcpyDeviceToHost, s);
     int e = (int)cudaStreamSynchronize(s);
@@ -1608,7 +1629,7 @@ int Multigrid::solve_mixed(const DevParams& p, const uint8_t* code, double* phi,
             cudaMemsetAsync(d_norm_, 0, NORM_SLOTS * 8, s);
             if (prof) prof->begin(PROF_RESID64, s);
             ++g_launches;
-            launch_k(k_resid64<true>, g2, b2, 0, s, o64, xin, e32_, rhs, xout, r32_, d_norm_, ResidCtl{});
+            launch_resid64<true>(o64, g2, b2, s, xin, e32_, rhs, xout, r32_, d_norm_, ResidCtl{});
             if (prof) prof->end(s);
             cudaMemcpyAsync(h_norm_, d_norm_, NORM_SLOTS * 8, cudaMemcpyDeviceToHost, s);
         });
@@ -1648,14 +1669,14 @@ void Multigrid::enqueue_solve64_ctl(const DevParams& p, const uint8_t* code, dou
     // the norm slots are zero between uses
     ResidCtl rb = {ctl, RC_BEGIN, nb, rtol, maxit, 0, 0, 0, hw, hw, rc_counter_};
     ++g_launches;
-    launch_k(k_resid64<false>, g2, b2, 0, s, o, phi, nullptr, rhs, nullptr, nullptr, d_norm_, rb);
+    launch_resid64<false>(o, g2, b2, s, phi, nullptr, rhs, nullptr, nullptr, d_norm_, rb);
     cap.node(s, cudaGraphCondTypeWhile, hw, KIND_MG_CYCLE, [&](cudaStream_t b) {
         vcycle<double>(p, code, 0, phi, rhs, true, b, false);
         ++g_launches;
         launch_k(k_mg_mid, 1, 1, 0, b, d_norm_, single, maxit, ctl, hw);
         ResidCtl rr = {ctl, RC_RN, nullptr, 0.0, maxit, 0, 0, 0, hw, hw, rc_counter_};
         ++g_launches;
-        launch_k(k_resid64<false>, g2, b2, 0, b, o, phi, nullptr, rhs, nullptr, nullptr, d_norm_, rr);
+        launch_resid64<false>(o, g2, b2, b, phi, nullptr, rhs, nullptr, nullptr, d_norm_, rr);
     });
     if (!end_in_next) {
         ++g_launches;
@@ -1678,11 +1699,11 @@ void Multigrid::enqueue_solve_mixed_ctl(const DevParams& p, const uint8_t* code,
     const cudaGraphConditionalHandle hw = cap.handle(s);
     ResidCtl rb = {ctl, RC_BEGIN, nb, rtol, maxit, 0, 0, 0, hw, hw, rc_counter_};
     ++g_launches;
-    launch_k(k_resid64<false>, g2, b2, 0, s, o64, phi, nullptr, rhs, nullptr, r32_, d_norm_, rb);
+    launch_resid64<false>(o64, g2, b2, s, phi, nullptr, rhs, nullptr, r32_, d_norm_, rb);
     auto refine = [&](cudaStream_t q, const double* xin, double* xout, const ResidCtl& rc) {
         for (int k = 0; k < inner; ++k) vcycle<float>(p, code, 0, e32_, r32_, false, q, k == 0);
         ++g_launches;
-        launch_k(k_resid64<true>, g2, b2, 0, q, o64, xin, e32_, rhs, xout, r32_, d_norm_, rc);
+        launch_resid64<true>(o64, g2, b2, q, xin, e32_, rhs, xout, r32_, d_norm_, rc);
     };
     cap.node(s, cudaGraphCondTypeWhile, hw, KIND_MX_FIRST, [&](cudaStream_t b) {
         const cudaGraphConditionalHandle hif = cap.handle(b);
