@@ -253,7 +253,30 @@ __global__ void __launch_bounds__(256) k_rhs_p(DevParams p, const uint8_t* __res
 
 // one Newton linearisation pass (FP64): alpha = (rho(phi+delta) - rho)/delta
 // by the reference's LinComb, rhs = RHS - alpha phi; alpha is also written in
-// FP32 for the mixed-precision multigrid
+// FP32 for the mixed-precision multigrid.  One cell's arithmetic:
+__device__ __forceinline__ void newton_cell(const DevParams& p, const double* seps, int m, double ph, double r0,
+                                            double rp, long long c, double& a, double& v, double& bp) {
+    const int mask = m & 3;
+    a = 0.0;
+    if (mask >= 2) {
+        double e, h;
+        const double rho_pd = sc_charge(p, ph + p.delta, e, h);
+        a = p.inv_delta * rho_pd + p.neg_inv_delta * r0;
+        v = r0 - a * ph;
+    } else if (mask == 1) {
+        v = 0.0;
+    } else {
+        v = rp;
+    }
+    bp = v;
+    if (c < p.nxy) bp += 2.0 * seps[m & 7] * p.ih2[2] * p.V_lo;             // k == 0
+    if (c >= p.N - p.nxy) bp += 2.0 * seps[m & 7] * p.ih2[2] * p.V_hi;      // k == nz - 1
+}
+
+// PAIR: each thread takes two neighbouring cells with vector loads and
+// stores, every load issued before the arithmetic (N and nx ny even); the
+// charge arithmetic is latency bound, so the loads of both cells overlap it
+template <bool PAIR>
 __global__ void __launch_bounds__(256) k_newton(DevParams p, const uint8_t* __restrict__ code,
                                                 const double* __restrict__ phi, const double* __restrict__ rho,
                                                 const double* __restrict__ rhs_p, double* __restrict__ alpha,
@@ -268,31 +291,35 @@ __global__ void __launch_bounds__(256) k_newton(DevParams p, const uint8_t* __re
         for (int q = 0; q < 8; ++q) seps[q] = p.eps[q];
     __syncthreads();
     double nb = 0.0, nbp = 0.0;
-#pragma unroll 4
-    for (long long c = (long long)blockIdx.x * 256 + tid; c < p.N; c += (long long)gridDim.x * 256) {
-        // the code array carries one z ghost layer below: cell c is at c + nxy
-        const int m = __ldg(code + c + p.nxy);
-        const int mask = m & 3;
-        double a = 0.0, v;
-        if (mask >= 2) {
-            double e, h;
-            const double rho_pd = sc_charge(p, phi[c] + p.delta, e, h);
-            const double r0 = rho[c];
-            a = p.inv_delta * rho_pd + p.neg_inv_delta * r0;
-            v = r0 - a * phi[c];
-        } else if (mask == 1) {
-            v = 0.0;
-        } else {
-            v = rhs_p[c];
+    if (PAIR) {
+        const long long np = p.N / 2;
+        for (long long q = (long long)blockIdx.x * 256 + tid; q < np; q += (long long)gridDim.x * 256) {
+            const long long c = 2 * q;
+            // the code array carries one z ghost layer below: cell c is at c + nxy
+            const uchar2 m2 = __ldg(reinterpret_cast<const uchar2*>(code + p.nxy + c));
+            const double2 ph = __ldg(reinterpret_cast<const double2*>(phi + c));
+            const double2 r0 = __ldg(reinterpret_cast<const double2*>(rho + c));
+            const double2 rp = __ldg(reinterpret_cast<const double2*>(rhs_p + c));
+            double a0, v0, bp0, a1, v1, bp1;
+            newton_cell(p, seps, m2.x, ph.x, r0.x, rp.x, c, a0, v0, bp0);
+            newton_cell(p, seps, m2.y, ph.y, r0.y, rp.y, c + 1, a1, v1, bp1);
+            *reinterpret_cast<double2*>(alpha + c) = make_double2(a0, a1);
+            *reinterpret_cast<float2*>(alpha32 + c) = make_float2((float)a0, (float)a1);
+            *reinterpret_cast<double2*>(rhs + c) = make_double2(v0, v1);
+            nb = fmax(nb, fmax(fabs(v0), fabs(v1)));
+            nbp = fmax(nbp, fmax(fabs(bp0), fabs(bp1)));
         }
-        alpha[c] = a;
-        alpha32[c] = (float)a;
-        rhs[c] = v;
-        nb = fmax(nb, fabs(v));
-        double bp = v;
-        if (c < p.nxy) bp += 2.0 * seps[m & 7] * p.ih2[2] * p.V_lo;             // k == 0
-        if (c >= p.N - p.nxy) bp += 2.0 * seps[m & 7] * p.ih2[2] * p.V_hi;      // k == nz - 1
-        nbp = fmax(nbp, fabs(bp));
+    } else {
+        for (long long c = (long long)blockIdx.x * 256 + tid; c < p.N; c += (long long)gridDim.x * 256) {
+            const int m = __ldg(code + c + p.nxy);
+            double a, v, bp;
+            newton_cell(p, seps, m, phi[c], rho[c], rhs_p[c], c, a, v, bp);
+            alpha[c] = a;
+            alpha32[c] = (float)a;
+            rhs[c] = v;
+            nb = fmax(nb, fabs(v));
+            nbp = fmax(nbp, fabs(bp));
+        }
     }
     const double x = block_max(nb, sh);
     const double y = block_max(nbp, sh);
@@ -304,6 +331,7 @@ __global__ void __launch_bounds__(256) k_newton(DevParams p, const uint8_t* __re
 
 // ComputeRho at the new phi + the Newton error norms; partial sums go to
 // part[2*block], the last block folds them in block order (deterministic)
+template <bool PAIR>
 __global__ void __launch_bounds__(256) k_rho(DevParams p, const uint8_t* __restrict__ code,
                                              const double* __restrict__ phi, double* __restrict__ phi_prev,
                                              double* __restrict__ rho, double* __restrict__ e_den,
@@ -314,27 +342,52 @@ __global__ void __launch_bounds__(256) k_rho(DevParams p, const uint8_t* __restr
     __shared__ double sh[32];
     __shared__ bool last;
     double s1 = 0.0, s2 = 0.0;
-    // all loads of a cell are issued before its exponentials, and four cells
-    // are in flight per thread, so the memory rounds overlap
-#pragma unroll 4
-    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < p.N; c += (long long)gridDim.x * blockDim.x) {
-        const int m = __ldg(code + c + p.nxy) & 3;   // code has one z ghost layer below
-        const double ph = phi[c];
-        const double pp = track ? phi_prev[c] : 0.0;
-        if (m >= 2) {
-            double e, h;
-            rho[c] = sc_charge(p, ph, e, h);
+    if (PAIR) {
+        // two neighbouring cells per thread with vector loads and stores,
+        // every load issued before the exponentials (N and nx ny even)
+        const long long np = p.N / 2;
+        for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < np; q += (long long)gridDim.x * blockDim.x) {
+            const long long c = 2 * q;
+            const uchar2 m2 = __ldg(reinterpret_cast<const uchar2*>(code + p.nxy + c));   // one z ghost layer below
+            const double2 ph = __ldg(reinterpret_cast<const double2*>(phi + c));
+            const double2 pp = track ? *reinterpret_cast<const double2*>(phi_prev + c) : make_double2(0.0, 0.0);
+            double e0 = 0.0, h0 = 0.0, e1 = 0.0, h1 = 0.0;
+            const bool sc0 = (m2.x & 3) >= 2, sc1 = (m2.y & 3) >= 2;
+            const double r0 = sc0 ? sc_charge(p, ph.x, e0, h0) : 0.0;
+            const double r1 = sc1 ? sc_charge(p, ph.y, e1, h1) : 0.0;
+            *reinterpret_cast<double2*>(rho + c) = make_double2(r0, r1);
             if (carriers) {
-                e_den[c] = e;
-                h_den[c] = h;
+                if (sc0) { e_den[c] = e0; h_den[c] = h0; }
+                if (sc1) { e_den[c + 1] = e1; h_den[c + 1] = h1; }
             }
-        } else {
-            rho[c] = 0.0;
+            if (track) {
+                s1 += fabs(ph.x - pp.x);
+                s2 += fabs(ph.x);
+                s1 += fabs(ph.y - pp.y);
+                s2 += fabs(ph.y);
+                *reinterpret_cast<double2*>(phi_prev + c) = ph;
+            }
         }
-        if (track) {
-            s1 += fabs(ph - pp);
-            s2 += fabs(ph);
-            phi_prev[c] = ph;
+    } else {
+        for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < p.N; c += (long long)gridDim.x * blockDim.x) {
+            const int m = __ldg(code + c + p.nxy) & 3;   // code has one z ghost layer below
+            const double ph = phi[c];
+            const double pp = track ? phi_prev[c] : 0.0;
+            if (m >= 2) {
+                double e, h;
+                rho[c] = sc_charge(p, ph, e, h);
+                if (carriers) {
+                    e_den[c] = e;
+                    h_den[c] = h;
+                }
+            } else {
+                rho[c] = 0.0;
+            }
+            if (track) {
+                s1 += fabs(ph - pp);
+                s2 += fabs(ph);
+                phi_prev[c] = ph;
+            }
         }
     }
     if (!track) return;
@@ -504,9 +557,14 @@ int launch_rhs_p(const DevParams& p, const uint8_t* code, const uint8_t* var, co
     return (int)cudaGetLastError();
 }
 
+// the paired kernels need whole cell pairs that start on an even cell of
+// every array, the code array included (offset nx ny)
+static bool pairs_ok(const DevParams& p) { return p.N % 2 == 0 && p.nxy % 2 == 0; }
+
 int launch_newton(const DevParams& p, const uint8_t* code, const double* phi, const double* rho,
                   const double* rhs_p, double* alpha, float* alpha32, double* rhs, double* norms, cudaStream_t s) {
-    launch_k(k_newton, p.ngrid_red, dim3(256), 0, s, p, code, phi, rho, rhs_p, alpha, alpha32, rhs, norms);
+    if (pairs_ok(p)) launch_k(k_newton<true>, p.ngrid_red, dim3(256), 0, s, p, code, phi, rho, rhs_p, alpha, alpha32, rhs, norms);
+    else launch_k(k_newton<false>, p.ngrid_red, dim3(256), 0, s, p, code, phi, rho, rhs_p, alpha, alpha32, rhs, norms);
     return (int)cudaGetLastError();
 }
 
@@ -514,8 +572,12 @@ int launch_rho(const DevParams& p, const uint8_t* code, const double* phi, doubl
                double* e_den, double* h_den, double* part, unsigned int* counter, double* out, int track,
                int carriers, cudaStream_t s, const RhoCtl* rc) {
     RhoCtl none = {};
-    launch_k(k_rho, p.ngrid_red, RED_THREADS, 0, s, p, code, phi, phi_prev, rho, e_den, h_den, part, counter, out, track,
-             carriers, rc ? *rc : none);
+    if (pairs_ok(p))
+        launch_k(k_rho<true>, p.ngrid_red, RED_THREADS, 0, s, p, code, phi, phi_prev, rho, e_den, h_den, part, counter,
+                 out, track, carriers, rc ? *rc : none);
+    else
+        launch_k(k_rho<false>, p.ngrid_red, RED_THREADS, 0, s, p, code, phi, phi_prev, rho, e_den, h_den, part, counter,
+                 out, track, carriers, rc ? *rc : none);
     return (int)cudaGetLastError();
 }
 
