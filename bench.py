@@ -361,6 +361,9 @@ def main() -> None:
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    # the same kernels driven by the host loop (a synchronisation per loop
+    # test) instead of one graph per step; ncu profiles kernels only there
+    ap.add_argument("--host-loop", action="store_true")
     ap.add_argument("--adjoint-steps-per-leg", type=int, default=400)
     ap.add_argument("--adjoint-scale-steps", type=int, default=0,
                     help="also run the polycrystal adjoint (FP64 and mixed) over this many steps")
@@ -392,6 +395,8 @@ def main() -> None:
     f = api.FerroX(text, precision=args.precision)
     if grains is not None:
         f.set_grains(grains["id"], grains["angles"], grains["tphase"])
+    if args.host_loop:
+        f.set_param("fx.step_graph", 0)
     # a dedicated stream: the library's work and the timing events share it
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
@@ -503,7 +508,9 @@ def main() -> None:
             "config": {"workload": f"{args.workload}-{'x'.join(map(str, nz1))}-{args.precision}",
                        "description": WORKLOADS[args.workload]["label"], "cells": N,
                        "l2": f"inputs larger than L2: device working set {f.stats()['device_bytes'] / 1e6:.0f} MB per step",
-                       "mg_rtol": f.param("fx.mg_rtol"), "parallelism": "replicas"},
+                       "mg_rtol": f.param("fx.mg_rtol"), "parallelism": "replicas",
+                       "step": "one CUDA graph per step, loop tests on the device" if f.param("step_graph_ran")
+                       else "host-driven loop"},
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d,
