@@ -414,6 +414,11 @@ template <typename T>
 int dmalloc(fx_ctx* c, T** p, size_t n) {
     cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(n, 1) * sizeof(T));
     if (e != cudaSuccess) return set_err(c, FX_ERR_OUT_OF_MEMORY, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    // zeroed on the context's stream: nothing may depend on what an earlier
+    // allocation left there
+    e = c->s ? cudaMemsetAsync(*p, 0, std::max<size_t>(n, 1) * sizeof(T), c->s)
+             : cudaMemset(*p, 0, std::max<size_t>(n, 1) * sizeof(T));
+    if (e != cudaSuccess) return set_err(c, FX_ERR_CUDA, std::string("cudaMemset: ") + cudaGetErrorString(e));
     c->dev_bytes += n * sizeof(T);
     return 0;
 }

@@ -38,15 +38,19 @@ __device__ __forceinline__ double warp_max(double v) {
     return v;
 }
 
-// block sum in a fixed order (deterministic for a fixed launch shape)
+// block sum in a fixed order (deterministic for a fixed launch shape); the
+// result is valid in the block's first thread.  Warps are numbered by the
+// linear thread index, so 2-D and 3-D blocks reduce every warp.
 __device__ double block_sum(double v, double* sh) {
     v = warp_sum(v);
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int t = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int nw = (blockDim.x * blockDim.y * blockDim.z + 31) >> 5;
+    const int lane = t & 31, w = t >> 5;
     if (lane == 0) sh[w] = v;
     __syncthreads();
     double r = 0.0;
     if (w == 0) {
-        r = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
+        r = lane < nw ? sh[lane] : 0.0;
         r = warp_sum(r);
     }
     __syncthreads();
@@ -54,12 +58,14 @@ __device__ double block_sum(double v, double* sh) {
 }
 __device__ double block_max(double v, double* sh) {
     v = warp_max(v);
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int t = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int nw = (blockDim.x * blockDim.y * blockDim.z + 31) >> 5;
+    const int lane = t & 31, w = t >> 5;
     if (lane == 0) sh[w] = v;
     __syncthreads();
     double r = 0.0;
     if (w == 0) {
-        r = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
+        r = lane < nw ? sh[lane] : 0.0;
         r = warp_max(r);
     }
     __syncthreads();

@@ -880,6 +880,8 @@ T* dalloc(size_t n, size_t& bytes) {
     T* p = nullptr;
     if (n == 0) return nullptr;
     if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) return nullptr;
+    // zeroed: nothing may depend on what an earlier allocation left there
+    if (cudaMemset(p, 0, n * sizeof(T)) != cudaSuccess) { cudaFree(p); return nullptr; }
     bytes += n * sizeof(T);
     return p;
 }
@@ -1209,6 +1211,7 @@ int Multigrid::setup(const DevParams& p, const std::vector<uint8_t>& code, bool 
         }
     }
     if (cudaMalloc(&d_norm_, NORM_SLOTS * 8) != cudaSuccess) return -2;
+    if (cudaMemset(d_norm_, 0, NORM_SLOTS * 8) != cudaSuccess) return -1;   // zero between uses
     if (cudaMemset(d_norm_, 0, NORM_SLOTS * 8) != cudaSuccess) return -1;
     if (cudaMalloc(&rc_counter_, sizeof(unsigned int)) != cudaSuccess) return -2;
     if (cudaMemset(rc_counter_, 0, sizeof(unsigned int)) != cudaSuccess) return -1;

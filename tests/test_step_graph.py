@@ -162,3 +162,18 @@ def test_coarse_alpha_tiles_bit_identical(precision):
     for n in FIELDS:
         assert np.array_equal(out[0][0][n], out[1][0][n]), n
     assert out[0][1] == out[1][1]
+
+
+def test_fresh_contexts_bit_identical():
+    # two contexts of the same deck give the same fields and cycle counts:
+    # every reduction is order-fixed (the right-hand-side norms that set the
+    # multigrid target on stacks without a semiconductor included)
+    out = []
+    for _ in range(2):
+        f = api.FerroX(decks.mfim(32, 32, 12))
+        f.step(60)
+        out.append(({n: f.field(n) for n in FIELDS}, f.stats()["mg_cycles_total"]))
+        f.close()
+    for n in FIELDS:
+        assert np.array_equal(out[0][0][n], out[1][0][n]), n
+    assert out[0][1] == out[1][1]
