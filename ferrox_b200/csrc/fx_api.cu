@@ -89,6 +89,9 @@ struct FxError {
 
 }  // namespace
 
+// highest order of the time extrapolation of a step's first solve
+constexpr int kMaxExtrap = 6;
+
 struct fx_ctx {
     Params par;
     Inputs in;
@@ -153,7 +156,7 @@ struct fx_ctx {
     bool carriers_stale = false;
     // phi of the previous step's first solve, for the extrapolated initial
     // iterate; valid only while nothing but time steps changed the state
-    double* d_phi_hist[3] = {nullptr, nullptr, nullptr};   // phi of the last steps' first solves
+    double* d_phi_hist[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};   // phi of the last steps' first solves
     int hist_n = 0;                                // how many of them are current
     bool hist_valid = false;
     double hist_vlo = 0.0, hist_vhi = 0.0;
@@ -536,7 +539,7 @@ int mg_solve(fx_ctx* c, const double* rhs, double nb, double nbp) {
 // multigrid's initial iterate only: the Newton linearisation point stays
 // phi^n); skipped after a voltage change or any other change of the state
 int start_guess(fx_ctx* c) {
-    const int order = std::min(3, c->par.phi_extrapolate);
+    const int order = std::min(kMaxExtrap, c->par.phi_extrapolate);
     if (order <= 0 || !c->par.warm_start) return FX_OK;
     for (int q = 0; q < order; ++q)
         if (!c->d_phi_hist[q]) {
@@ -548,7 +551,8 @@ int start_guess(fx_ctx* c) {
     const int use = std::min(order, c->hist_n);   // steps of history available
     if (use > 0) {
         // the histories kept are those of `order`; shift all of them
-        double* h[3] = {c->d_phi_hist[0], order >= 2 ? c->d_phi_hist[1] : nullptr, order >= 3 ? c->d_phi_hist[2] : nullptr};
+        double* h[6];
+        for (int m = 0; m < 6; ++m) h[m] = m < order ? c->d_phi_hist[m] : nullptr;
         ++g_launches;
         int r = k_status(c, launch_phi_extrap(c->dp, use, c->d_phi, h, c->s));
         if (r) return r;
@@ -713,7 +717,7 @@ void steady_update(fx_ctx* c, int step, double phi_max, double dmax) {
 
 int sg_hist_before(fx_ctx* c, int* use) {
     *use = 0;
-    const int order = std::min(3, c->par.phi_extrapolate);
+    const int order = std::min(kMaxExtrap, c->par.phi_extrapolate);
     if (order <= 0 || !c->par.warm_start) return FX_OK;
     for (int q = 0; q < order; ++q)
         if (!c->d_phi_hist[q]) {
@@ -727,7 +731,7 @@ int sg_hist_before(fx_ctx* c, int* use) {
 }
 
 void sg_hist_after(fx_ctx* c) {
-    const int order = std::min(3, c->par.phi_extrapolate);
+    const int order = std::min(kMaxExtrap, c->par.phi_extrapolate);
     if (order <= 0 || !c->par.warm_start) return;
     c->hist_n = std::min(order, c->hist_n + 1);
     c->hist_valid = true;
@@ -737,10 +741,11 @@ void sg_hist_after(fx_ctx* c) {
 
 // start_guess's launches for `use` steps of history (bookkeeping on the host)
 void sg_start_guess(fx_ctx* c, cudaStream_t q, int use) {
-    const int order = std::min(3, c->par.phi_extrapolate);
+    const int order = std::min(kMaxExtrap, c->par.phi_extrapolate);
     if (order <= 0 || !c->par.warm_start) return;
     if (use > 0) {
-        double* h[3] = {c->d_phi_hist[0], order >= 2 ? c->d_phi_hist[1] : nullptr, order >= 3 ? c->d_phi_hist[2] : nullptr};
+        double* h[6];
+        for (int m = 0; m < 6; ++m) h[m] = m < order ? c->d_phi_hist[m] : nullptr;
         ++g_launches;
         launch_phi_extrap(c->dp, use, c->d_phi, h, q);
     } else {
@@ -868,7 +873,7 @@ std::vector<unsigned char> sg_key(const fx_ctx* c, int use) {
     const double dv[] = {c->par.mg_rtol, c->par.newton_tol};
     put(dv, sizeof(dv));
     const void* pv[] = {c->s, c->d_var, c->d_vt, c->d_f[0], c->d_f[1], c->d_f[2], c->d_phi_hist[0], c->d_phi_hist[1],
-                        c->d_phi_hist[2]};
+                        c->d_phi_hist[2], c->d_phi_hist[3], c->d_phi_hist[4], c->d_phi_hist[5]};
     put(pv, sizeof(pv));
     return k;
 }
@@ -1466,7 +1471,8 @@ void fx_destroy(fx_ctx* c) {
             for (int d = 0; d < 3; ++d) cudaFree(c->d_P[b][d]);
         for (double* a : {c->d_phi, c->d_phi_old, c->d_phi_prev, c->d_rho, c->d_e, c->d_h, c->d_alpha, c->d_rhs,
                           c->d_rhsP, c->d_dphi, c->d_E[0], c->d_E[1], c->d_E[2], c->d_f[0], c->d_f[1], c->d_f[2],
-                          c->d_part, c->d_out, c->d_phi_hist[0], c->d_phi_hist[1], c->d_phi_hist[2]})
+                          c->d_part, c->d_out, c->d_phi_hist[0], c->d_phi_hist[1], c->d_phi_hist[2], c->d_phi_hist[3],
+                          c->d_phi_hist[4], c->d_phi_hist[5]})
             cudaFree(a);
         cudaFree(c->d_alpha32);
         cudaFree(c->d_counter);

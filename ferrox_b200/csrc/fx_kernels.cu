@@ -668,29 +668,48 @@ int launch_mean_p(const DevParams& p, const uint8_t* code, const double* const P
 
 // initial iterate of a step's first Poisson solve, extrapolated in time from
 // the last steps' phi (h[0] the previous step's, h[1] the one before, ...):
-// order 1: 2 phi - h0; order 2: 3 phi - 3 h0 + h1; order 3: 4 phi - 6 h0 +
-// 4 h1 - h2.  The histories shift by one step.
+// the polynomial of degree ORDER through the last ORDER + 1 steps, evaluated
+// one step ahead, sum_m (-1)^m C(ORDER + 1, m + 1) phi^(n-m): order 1: 2 phi - h0;
+// 2: 3 phi - 3 h0 + h1; 3: 4 phi - 6 h0 + 4 h1 - h2; 4: 5 phi - 10 h0 + 10 h1 -
+// 5 h2 + h3; 5: 6, 15, 20, 15, 6, 1; 6: 7, 21, 35, 35, 21, 7, 1.  The
+// histories shift by one step (the ones beyond ORDER take zeros).
+struct PhiHist {
+    double* h[6];   // null beyond the configured order
+};
+
 template <int ORDER>
-__global__ void __launch_bounds__(256) k_phi_extrap(double* __restrict__ phi, double* __restrict__ h0,
-                                                    double* __restrict__ h1, double* __restrict__ h2,
-                                                    long long n) {
+__global__ void __launch_bounds__(256) k_phi_extrap(double* __restrict__ phi, PhiHist H, long long n) {
     pdl_entry();
     for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
-        const double t = phi[c], a = h0[c];
-        const double b = ORDER >= 2 ? h1[c] : 0.0;
+        const double t = phi[c];
+        double v[6];
+#pragma unroll
+        for (int m = 0; m < 6; ++m) v[m] = m < ORDER ? H.h[m][c] : 0.0;
+        const double a = v[0], b = v[1], d = v[2], e = v[3], f = v[4], g = v[5];
         if (ORDER == 1) phi[c] = 2.0 * t - a;
         if (ORDER == 2) phi[c] = 3.0 * t - 3.0 * a + b;
-        if (ORDER == 3) phi[c] = 4.0 * t - 6.0 * a + 4.0 * b - h2[c];
-        if (h2) h2[c] = b;
-        if (h1) h1[c] = a;
-        h0[c] = t;
+        if (ORDER == 3) phi[c] = 4.0 * t - 6.0 * a + 4.0 * b - d;
+        if (ORDER == 4) phi[c] = 5.0 * t - 10.0 * a + 10.0 * b - 5.0 * d + e;
+        if (ORDER == 5) phi[c] = 6.0 * t - 15.0 * a + 20.0 * b - 15.0 * d + 6.0 * e - f;
+        if (ORDER == 6) phi[c] = 7.0 * t - 21.0 * a + 35.0 * b - 35.0 * d + 21.0 * e - 7.0 * f + g;
+#pragma unroll
+        for (int m = 5; m >= 1; --m)
+            if (H.h[m]) H.h[m][c] = v[m - 1];
+        H.h[0][c] = t;
     }
 }
 
-int launch_phi_extrap(const DevParams& p, int order, double* phi, double* const h[3], cudaStream_t s) {
-    if (order >= 3) launch_k(k_phi_extrap<3>, p.ngrid_red, RED_THREADS, 0, s, phi, h[0], h[1], h[2], p.N);
-    else if (order == 2) launch_k(k_phi_extrap<2>, p.ngrid_red, RED_THREADS, 0, s, phi, h[0], h[1], h[2], p.N);
-    else launch_k(k_phi_extrap<1>, p.ngrid_red, RED_THREADS, 0, s, phi, h[0], h[1], h[2], p.N);
+int launch_phi_extrap(const DevParams& p, int order, double* phi, double* const h[6], cudaStream_t s) {
+    PhiHist H;
+    for (int m = 0; m < 6; ++m) H.h[m] = h[m];
+    switch (order >= 6 ? 6 : order) {
+    case 6: launch_k(k_phi_extrap<6>, p.ngrid_red, RED_THREADS, 0, s, phi, H, p.N); break;
+    case 5: launch_k(k_phi_extrap<5>, p.ngrid_red, RED_THREADS, 0, s, phi, H, p.N); break;
+    case 4: launch_k(k_phi_extrap<4>, p.ngrid_red, RED_THREADS, 0, s, phi, H, p.N); break;
+    case 3: launch_k(k_phi_extrap<3>, p.ngrid_red, RED_THREADS, 0, s, phi, H, p.N); break;
+    case 2: launch_k(k_phi_extrap<2>, p.ngrid_red, RED_THREADS, 0, s, phi, H, p.N); break;
+    default: launch_k(k_phi_extrap<1>, p.ngrid_red, RED_THREADS, 0, s, phi, H, p.N); break;
+    }
     return (int)cudaGetLastError();
 }
 

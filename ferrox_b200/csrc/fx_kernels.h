@@ -28,7 +28,9 @@ int launch_steady(const DevParams& p, const double* phi, double* phi_old, double
                   cudaStream_t s, const int* skip = nullptr);
 int launch_mean_p(const DevParams& p, const uint8_t* code, const double* const P[3], double* part,
                   unsigned int* counter, double* out, cudaStream_t s);
-int launch_phi_extrap(const DevParams& p, int order, double* phi, double* const h[3], cudaStream_t s);
+// h: the history buffers, null beyond the configured order; order: the steps of
+// history in use (1-6)
+int launch_phi_extrap(const DevParams& p, int order, double* phi, double* const h[6], cudaStream_t s);
 int launch_efield(const DevParams& p, const uint8_t* var, const Variant* vt, const double* phi, double* E[3],
                   cudaStream_t s);
 

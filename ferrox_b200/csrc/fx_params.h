@@ -57,7 +57,7 @@ struct Params {
     int mg_max_iter = 200;
     int precision = 0;           // 0 fp64, 1 mixed
     int warm_start = 1;
-    int phi_extrapolate = 3;       // first solve of a step starts from phi extrapolated in time (order 0-3)
+    int phi_extrapolate = 4;       // first solve of a step starts from phi extrapolated in time (order 0-6)
     int step_graph = 1;            // a step runs as one CUDA graph with its loop tests on the device
     int verbose = 0;
     std::string plot_dir = ".";
