@@ -11,8 +11,10 @@ Function-valued keys (``tphase_geom.tphase_geom_function(x,y,z)``,
 ``angle_alpha.alpha_function(x,y,z)``, ...; Initialization.cpp:227-365) are
 evaluated with numpy over cell centres.  The AMReX Parser itself is a
 third-party component absent from the reference tree; this evaluator covers
-the grammar the example decks use (arithmetic, ``^``, comparisons, ``if``,
-the usual functions, ``my_constants.*``), so its parity is unpinned.
+the grammar the example decks use (arithmetic, ``^``, comparisons, ``and`` /
+``or``, ``if``, ``heaviside``, the usual functions, ``my_constants.*``) with
+AMReX Parser's C-like precedence.  With no AMReX Parser to run, it is pinned by
+closed-form known answers, not by the parser's own outputs.
 
 The product library has its own C++ reader; tests compare the two.
 """
@@ -94,16 +96,132 @@ _FUNCS = {
     "min": np.minimum, "max": np.maximum,
     "_if": lambda c, a, b: np.where(np.asarray(c) != 0, a, b),
     "heaviside": lambda x, h0=0.0: np.where(np.asarray(x) > 0, 1.0, np.where(np.asarray(x) < 0, 0.0, h0)),
+    "_f": lambda v: np.asarray(v, dtype=np.float64),
+    "_pow": lambda a, b: np.power(np.asarray(a, dtype=np.float64), b),
+    "_and": lambda a, b: np.asarray((np.asarray(a) != 0) & (np.asarray(b) != 0), dtype=np.float64),
+    "_or": lambda a, b: np.asarray((np.asarray(a) != 0) | (np.asarray(b) != 0), dtype=np.float64),
 }
+
+_EXPR_TOKEN = re.compile(r"\s*(?:(\d+\.?\d*(?:[eE][+-]?\d+)?|\.\d+(?:[eE][+-]?\d+)?)|([A-Za-z_]\w*)"
+                         r"|(\*\*|<=|>=|==|!=|&&|\|\||[-+*/^<>(),]))")
+
+
+class _ExprToPython:
+    """Rewrites an AMReX Parser expression as fully parenthesised numpy code.
+
+    Precedence, loosest first, as in AMReX Parser's C-like grammar:
+    ``or ||`` < ``and &&`` < comparisons < ``+ -`` < ``* /`` < unary ``- +``
+    < ``^ **`` (right-associative, its exponent may carry a unary sign, so
+    ``-2^2 = -4`` and ``2^-1 = 0.5``).  Comparisons and the logical operators
+    give 0.0 / 1.0; ``if(c, a, b)`` selects per cell.
+    """
+
+    def __init__(self, expr: str):
+        self.toks: list[str] = []
+        s, pos = expr.strip(), 0
+        while pos < len(s):
+            m = _EXPR_TOKEN.match(s, pos)
+            if m is None or m.end() == pos:
+                raise SyntaxError(f"expression {expr!r}: unexpected {s[pos:pos + 8]!r}")
+            self.toks.append(m.group(m.lastindex))
+            pos = m.end()
+        self.i = 0
+        self.expr = expr
+
+    def run(self) -> str:
+        code = self.p_or()
+        if self.i != len(self.toks):
+            raise SyntaxError(f"expression {self.expr!r}: unexpected {self.toks[self.i]!r}")
+        return code
+
+    def peek(self):
+        return self.toks[self.i] if self.i < len(self.toks) else None
+
+    def eat(self, *ops) -> bool:
+        if self.peek() in ops:
+            self.i += 1
+            return True
+        return False
+
+    def want(self, op: str) -> None:
+        if not self.eat(op):
+            raise SyntaxError(f"expression {self.expr!r}: missing {op!r}")
+
+    def p_or(self) -> str:
+        a = self.p_and()
+        while self.eat("||", "or"):
+            a = f"_or({a}, {self.p_and()})"
+        return a
+
+    def p_and(self) -> str:
+        a = self.p_cmp()
+        while self.eat("&&", "and"):
+            a = f"_and({a}, {self.p_cmp()})"
+        return a
+
+    def p_cmp(self) -> str:
+        a = self.p_add()
+        while self.peek() in ("<", ">", "<=", ">=", "==", "!="):
+            op = self.toks[self.i]
+            self.i += 1
+            a = f"_f({a} {op} {self.p_add()})"
+        return a
+
+    def p_add(self) -> str:
+        a = self.p_mul()
+        while self.peek() in ("+", "-"):
+            op = self.toks[self.i]
+            self.i += 1
+            a = f"({a} {op} {self.p_mul()})"
+        return a
+
+    def p_mul(self) -> str:
+        a = self.p_unary()
+        while self.peek() in ("*", "/"):
+            op = self.toks[self.i]
+            self.i += 1
+            a = f"({a} {op} {self.p_unary()})"
+        return a
+
+    def p_unary(self) -> str:
+        if self.eat("-"):
+            return f"(-{self.p_unary()})"
+        if self.eat("+"):
+            return self.p_unary()
+        return self.p_pow()
+
+    def p_pow(self) -> str:
+        b = self.p_primary()
+        if self.eat("^", "**"):
+            return f"_pow({b}, {self.p_unary()})"
+        return b
+
+    def p_primary(self) -> str:
+        t = self.peek()
+        if t is None:
+            raise SyntaxError(f"expression {self.expr!r}: unexpected end")
+        self.i += 1
+        if t == "(":
+            e = self.p_or()
+            self.want(")")
+            return f"({e})"
+        if t[0].isdigit() or t[0] == ".":
+            return repr(float(t))
+        if t[0].isalpha() or t[0] == "_":
+            if self.eat("("):
+                args = []
+                if not self.eat(")"):
+                    args.append(self.p_or())
+                    while self.eat(","):
+                        args.append(self.p_or())
+                    self.want(")")
+                return f"{'_if' if t == 'if' else t}({', '.join(args)})"
+            return t
+        raise SyntaxError(f"expression {self.expr!r}: unexpected {t!r}")
 
 
 def _to_python(expr: str) -> str:
-    e = expr.replace("^", "**")
-    e = re.sub(r"\bif\s*\(", "_if(", e)
-    e = e.replace("&&", " & ").replace("||", " | ")
-    e = re.sub(r"\band\b", " & ", e)
-    e = re.sub(r"\bor\b", " | ", e)
-    return e
+    return _ExprToPython(expr).run()
 
 
 def constants(table: dict[str, list[str]]) -> dict[str, float]:
@@ -127,7 +245,6 @@ def eval_expr(expr: str, consts: dict[str, float], x=None, y=None, z=None):
     if x is not None:
         env.update(x=x, y=y, z=z)
     code = _to_python(" ".join(expr.split()))
-    # comparisons yield booleans; arithmetic on them gives 0/1 as in AMReX Parser
     val = eval(code, {"__builtins__": {}}, env)  # noqa: S307 - trusted test decks
     return np.asarray(val, dtype=np.float64) * 1.0
 
