@@ -90,6 +90,25 @@ def test_setup_matches_oracle(text):
     assert f.param("V_hi") == o.scalar("V_hi") and f.param("V_lo") == o.scalar("V_lo")
 
 
+def test_reader_last_definition_comments_and_file(tmp_path):
+    """ParmParse behaviour of the library's own reader: the last definition of a key wins,
+    '#' starts a comment (whole line or after a value), `key=value` needs no spaces, and
+    fx_create reads the same deck from a file path."""
+    text = (decks.mfim(8, 8, 12) + "\ndt = 1.0e-13\n# dt = 9.0\nlambda=2.5e-9   # trailing comment\n"
+            "dt = 3.0e-13\n")
+    f = api.FerroX(text)
+    assert f.param("dt") == 3.0e-13 and f.param("lambda") == 2.5e-9
+    f.close()
+    deck = tmp_path / "inputs"
+    deck.write_text(text)
+    g = api.FerroX(str(deck), is_text=False)
+    assert g.param("dt") == 3.0e-13 and g.param("lambda") == 2.5e-9
+    g.close()
+    with pytest.raises(api.FxError) as e:
+        api.FerroX(str(tmp_path / "missing"), is_text=False)
+    assert "cannot open" in str(e.value)
+
+
 def test_grains_setup_matches_oracle():
     text, g = decks.polycrystal(16, 16, 24, ngrains=6, seed=3)
     f = api.FerroX(text)
