@@ -1566,6 +1566,17 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
     if (!c || !key) return FX_ERR_INVALID_ARGUMENT;
     const std::string k(key);
     Params& p = c->par;
+    // the ranges the inputs reader applies to the same keys; checked before any state changes
+    if (k == "fx.phi_extrapolate" && !(v >= 0 && v <= 6))
+        return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx.phi_extrapolate must be 0..6");
+    if (k == "fx.phi_ghost_mode" && !(v == 0 || v == 1 || v == 2))
+        return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx.phi_ghost_mode must be 0 (extrap), 1 (face) or 2 (zero)");
+    if ((k == "fx.mg_max_iter" || k == "fx.newton_max_iter") && !(v >= 1))
+        return set_err(c, FX_ERR_INVALID_ARGUMENT, k + " must be at least 1");
+    if ((k == "fx.mg_nu1" || k == "fx.mg_nu2") && !(v >= 0))
+        return set_err(c, FX_ERR_INVALID_ARGUMENT, k + " must not be negative");
+    if (k == "fx.mg_rtol" && !(v > 0))
+        return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx.mg_rtol must be positive");
     if (k != "fx.profile" && k != "fx.verbose" && k != "fx.graphs" && k != "fx.step_graph" && k != "fx.pdl" &&
         k != "fx.alpha_tiles")
         ++c->gen;

@@ -478,6 +478,11 @@ Params make_params(const Inputs& in) {
             throw std::runtime_error("inputs: P_BC_flag_lo/hi entries must be 0..4 (DerivativeAlgorithm.H:71-73)");
     if (p.prob_type < 1 || p.prob_type > 3) throw std::runtime_error("inputs: prob_type must be 1, 2 or 3 (Initialization.cpp:37-43)");
     if (p.TimeIntegratorOrder != 1 && p.TimeIntegratorOrder != 2) throw std::runtime_error("inputs: TimeIntegratorOrder must be 1 or 2");
+    // the solver settings of this library (fx_set_param applies the same ranges)
+    if (p.phi_extrapolate < 0 || p.phi_extrapolate > 6) throw std::runtime_error("inputs: fx.phi_extrapolate must be 0..6");
+    if (p.mg_max_iter < 1) throw std::runtime_error("inputs: fx.mg_max_iter must be at least 1");
+    if (p.newton_max_iter < 1) throw std::runtime_error("inputs: fx.newton_max_iter must be at least 1");
+    if (!(p.mg_rtol > 0.0)) throw std::runtime_error("inputs: fx.mg_rtol must be positive");
     return p;
 }
 

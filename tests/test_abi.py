@@ -109,6 +109,31 @@ def test_reader_last_definition_comments_and_file(tmp_path):
     assert "cannot open" in str(e.value)
 
 
+@pytest.mark.parametrize("key,bad,good", [
+    ("fx.phi_extrapolate", 7, 6), ("fx.phi_extrapolate", -1, 0), ("fx.phi_ghost_mode", 3, 1),
+    ("fx.mg_max_iter", 0, 1), ("fx.newton_max_iter", 0, 1), ("fx.mg_nu1", -1, 0), ("fx.mg_nu2", -1, 0),
+    ("fx.mg_rtol", 0.0, 1e-12),
+])
+def test_solver_settings_out_of_range_are_rejected(key, bad, good):
+    """fx_set_param refuses what the inputs reader refuses, and a refused call changes nothing."""
+    f = api.FerroX(decks.mfim(8, 8, 12))
+    readable = key not in ("fx.mg_nu1", "fx.mg_nu2")
+    before = f.param(key) if readable else None
+    with pytest.raises(api.FxError) as e:
+        f.set_param(key, bad)
+    assert e.value.code == -1 and key in str(e.value)
+    if readable:
+        assert f.param(key) == before
+    f.set_param(key, good)
+    if readable:
+        assert f.param(key) == good
+    f.close()
+    if key in ("fx.phi_extrapolate", "fx.mg_max_iter", "fx.newton_max_iter", "fx.mg_rtol"):
+        with pytest.raises(api.FxError) as e:
+            api.FerroX(decks.mfim(8, 8, 12) + f"\n{key} = {bad}\n")
+        assert e.value.code == -2 and key in str(e.value)
+
+
 def test_grains_setup_matches_oracle():
     text, g = decks.polycrystal(16, 16, 24, ngrains=6, seed=3)
     f = api.FerroX(text)
