@@ -220,3 +220,22 @@ def test_uniform_stream_is_splitmix64():
         return z ^ (z >> 31)
     for n in [1, 2, 1000]:
         assert O.uniform(7, n) == (mix((7 + n * golden) & M) >> 11) * 2.0 ** -53
+
+
+def test_oracle_is_independent_of_its_thread_count():
+    """Every reduction of the oracle folds in a fixed order, so its fields do not depend
+    on the OpenMP thread count (5 Newton-coupled steps of a small MFISM stack)."""
+    L = O.lib()
+    before = L.ofx_set_threads(0)       # 0 reads the current count without changing it
+    try:
+        runs = []
+        for th in (1, 3, 8):
+            o = make(decks.mfism(16, 16, 48), threads=th)
+            for s in range(1, 6):
+                o.step(s)
+            runs.append({n: o.field(n).copy() for n in ["Pz", "Phi", "charge"]})
+        for r in runs[1:]:
+            for n in r:
+                assert np.array_equal(r[n], runs[0][n]), n
+    finally:
+        L.ofx_set_threads(before)
