@@ -1528,10 +1528,12 @@ int fx_get_param(const fx_ctx* c, const char* key, double* v) {
         {"adjoint_mg_cycles", (double)c->adj.mg_cycles}, {"adjoint_forward_ms", c->adj.fwd_ms},
         {"adjoint_backward_ms", c->adj.bwd_ms}, {"adjoint_bytes", (double)c->adj.bytes},
         {"adjoint_loss", c->adj.loss},
+        {"fx.mg_nu1", (double)c->mg.nu1}, {"fx.mg_nu2", (double)c->mg.nu2},
+        {"fx.mg_mixed_cycles", (double)c->mg.mixed_cycles}, {"fx.alpha_tiles", c->mg.alpha_tiles ? 1.0 : 0.0},
+        {"step_graph_ran", c->sg_ran ? 1.0 : 0.0}, {"fx.pdl", g_pdl ? 1.0 : 0.0},
         // 1 when level 0's face coefficients depend on z only and its smoother
         // reads them by plane instead of from the material codes
-        {"step_graph_ran", c->sg_ran ? 1.0 : 0.0}, {"fx.pdl", g_pdl ? 1.0 : 0.0},
-        {"mg_level0_planes", !c->mg.levels().empty() && (c->mg.levels()[0].zc64 || c->mg.levels()[0].zc32) ? 1.0 : 0.0}};
+        {"mg_level0_planes",!c->mg.levels().empty() && (c->mg.levels()[0].zc64 || c->mg.levels()[0].zc32) ? 1.0 : 0.0}};
     auto it = m.find(k);
     if (it != m.end()) { *v = it->second; return FX_OK; }
     // "FE_lo[2]" style access to the 3-vectors

@@ -117,21 +117,25 @@ def test_reader_last_definition_comments_and_file(tmp_path):
 def test_solver_settings_out_of_range_are_rejected(key, bad, good):
     """fx_set_param refuses what the inputs reader refuses, and a refused call changes nothing."""
     f = api.FerroX(decks.mfim(8, 8, 12))
-    readable = key not in ("fx.mg_nu1", "fx.mg_nu2")
-    before = f.param(key) if readable else None
+    before = f.param(key)
     with pytest.raises(api.FxError) as e:
         f.set_param(key, bad)
     assert e.value.code == -1 and key in str(e.value)
-    if readable:
-        assert f.param(key) == before
+    assert f.param(key) == before
     f.set_param(key, good)
-    if readable:
-        assert f.param(key) == good
+    assert f.param(key) == good
     f.close()
     if key in ("fx.phi_extrapolate", "fx.mg_max_iter", "fx.newton_max_iter", "fx.mg_rtol"):
         with pytest.raises(api.FxError) as e:
             api.FerroX(decks.mfim(8, 8, 12) + f"\n{key} = {bad}\n")
         assert e.value.code == -2 and key in str(e.value)
+
+
+def test_multigrid_defaults_read_back():
+    f = api.FerroX(decks.mfim(8, 8, 12))
+    assert (f.param("fx.mg_nu1"), f.param("fx.mg_nu2"), f.param("fx.mg_mixed_cycles")) == (2, 1, 2)
+    assert f.param("fx.alpha_tiles") == 1 and f.param("fx.phi_extrapolate") == 4
+    f.close()
 
 
 def test_grains_setup_matches_oracle():
