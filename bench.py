@@ -3,20 +3,28 @@
 A step is one pass of FerroX's time loop (Source/main.cpp:261-621): the
 semiconductor-charge Newton loop with its Poisson multigrid solves, the fused
 TDGL update with E from phi, and the steady-state check.  The default workload
-is the 128x128x144 MFISM stack (5 nm HZO / 1 nm SiO2 / 30 nm p-Si, Boltzmann
-carriers, Newton-coupled Poisson to 1e-10 relative residual, FP64), with
-seeded synthetic initial polarization.
+is the 64-grain polycrystalline film, 256x256x128 cells (5 nm HZO in 64
+seeded Voronoi grains, 70% ferroelectric with random polar axes, on 4 nm
+Al2O3), in the mixed-precision form (FP32 stencils and multigrid inside FP64
+iterative refinement, FP64 P state), Poisson to 1e-10 relative residual, with
+seeded synthetic initial polarization.  The line's "mixed_vs_fp64" times the
+plain FP64 step beside it on the same deck and gives every output field's max
+relative difference.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload mfism|mfim|polycrystal] [--precision fp64|mixed]
-                    [--no-adjoint] [--adjoint-steps-per-leg S]
+                    [--workload polycrystal|mfism|mfim] [--precision mixed|fp64]
+                    [--no-adjoint] [--adjoint-steps-per-leg S] [--adjoint-scale-steps S]
 
-With --precision mixed the line carries "mixed_vs_fp64": the FP64 and mixed
-steps timed side by side on the same deck and the per-field max relative
-difference after the run.  At N = 1 the line also carries "adjoint": the time of fx_backward over
-fx_forward_record for the hysteresis loss on the 128x128x48 MFIM stack
-(800 steps, checkpoints every 50, gradients in alpha, beta, gamma, g11, g44
-and the voltage amplitude).
+At N = 1 the line also carries "adjoint": the time of fx_backward over
+fx_forward_record for the hysteresis loss on the 128x128x48 MFIM stack (800
+steps, checkpoints every 50, gradients in alpha, beta, gamma, g11, g44 and
+the voltage amplitude), and "adjoint_polycrystal": the same on the 256x256x128
+polycrystal with the 64 per-grain alphas, in FP64 and in mixed precision.
+
+The first solve of a step starts from phi extrapolated in time from the last
+steps (order 4 by default), so a run's first steps take more V-cycles; the
+config names the order and the steps of history at the start of the timed
+region.
 
 Multi-GPU runs are independent replicas (one process per GPU, weak scaling):
 the path has no data exchange between devices.  Rank 0 prints one JSON line.
@@ -43,9 +51,8 @@ WORKLOADS = {
 METRIC = "coupled-step cell-updates/s"
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum, one ncu
 # capture, cold cache) of the dominant bandwidth-bound kernel class, by
-# (workload, precision, class): the level-0 half sweep of the layered MFISM
-# stack, coefficients by z plane (profiles/k_rbgs_l0_mfism_128x128x144.txt)
-TRAFFIC = {("mfism", "fp64", "smooth_l0"): 56.76e6}
+# (workload, precision, class), with the profile that holds the capture
+TRAFFIC = {("mfism", "fp64", "smooth_l0"): (56.76e6, "profiles/k_rbgs_l0_mfism_128x128x144.txt")}
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -74,6 +81,20 @@ def deck(name: str):
     if name == "mfim":
         return decks.mfim(nx, ny, nz), None
     return decks.polycrystal(nx, ny, nz, ngrains=64, seed=1)
+
+
+def run_config(args, cells: int) -> dict:
+    """The workload the line is quoted on; the same dict on both arms."""
+    shape = WORKLOADS[args.workload]["shape"]
+    return {"workload": f"{args.workload}-{'x'.join(map(str, shape))}-{args.precision}",
+            "description": WORKLOADS[args.workload]["label"], "cells": cells, "mg_rtol": 1e-10,
+            "parallelism": "replicas",
+            "l2": "inputs larger than L2 (126 MB): every field of the deck is >= 19 MB and the step touches "
+                  "hundreds of MB",
+            # the run-length dependence: the first solve of a step starts from
+            # phi extrapolated in time through the first solves of the last steps
+            "phi_extrapolate_order": 4,
+            "history_steps_at_timed_start": min(args.warmup, 4)}
 
 
 def peaks():
@@ -341,11 +362,12 @@ def run_reference(args) -> None:
     line = {"metric": METRIC, "value": v, "unit": "cell-updates/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": f"{args.workload}-{'x'.join(map(str, WORKLOADS[args.workload]['shape']))}-fp64",
-                       "cells": n, "parallelism": "replicas"},
+            "config": run_config(args, n),
+            "reference_precision": "fp64 (the reference has no mixed-precision path)",
             "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": threads, "kind": "port",
                              "sample": f"{args.steps} full coupled steps after {args.warmup} warm-up steps "
-                                       f"(restated CPU oracle, OpenMP {threads} threads)"},
+                                       f"(restated CPU oracle in FP64, OpenMP {threads} threads; the reference "
+                                       "build needs AMReX, absent)"},
             "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -353,11 +375,11 @@ def run_reference(args) -> None:
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="mfism", choices=list(WORKLOADS))
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--workload", default="polycrystal", choices=list(WORKLOADS))
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
@@ -365,7 +387,7 @@ def main() -> None:
     # test) instead of one graph per step; ncu profiles kernels only there
     ap.add_argument("--host-loop", action="store_true")
     ap.add_argument("--adjoint-steps-per-leg", type=int, default=400)
-    ap.add_argument("--adjoint-scale-steps", type=int, default=0,
+    ap.add_argument("--adjoint-scale-steps", type=int, default=400,
                     help="also run the polycrystal adjoint (FP64 and mixed) over this many steps")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -419,48 +441,48 @@ def main() -> None:
     clocks = sampler.stop()
     ms = ev0.elapsed_time(ev1)
     st1 = f.stats()
-    # per-launch kernel durations: the same K steps again with CUDA events
-    # around every launch (kept out of the timed region, whose cost they raise)
-    f.set_param("fx.profile", 1)
-    f.reset_kernel_times()
-    f.step(args.steps)
-    kt = f.kernel_times()
-    f.set_param("fx.profile", 0)
     if done != args.steps:
         raise RuntimeError(f"the reference loop ended after {done} of {args.steps} steps")
     ms_max = max_over_ranks(ms, world)
     value = whole_job_rate(N, args.steps, world, ms_max)
 
-    # end to end through the public API with host buffers: the initial P
-    # uploaded from pinned host memory, per step the applied voltage in and the
-    # mean polarization out, the final P and phi read back
+    # end to end through the public API, K more steps right after the timed
+    # ones (the same stretch of the run): the state stays resident in HBM, as
+    # the reference's MultiFabs stay on its device; per step the host sets the
+    # electrode voltage (fx_set_param, the step's input), runs fx_step(1) and
+    # reads the mean polarization back (fx_mean_P, the step's result); at the
+    # end P and phi are read into pinned host buffers (fx_get_field)
     ke = args.e2e_steps or args.steps
-    Pz_host = torch.empty(f.shape, dtype=torch.float64, pin_memory=True).numpy()
-    Pz_host[...] = f.field("Pz")
-    out_P = torch.empty(f.shape, dtype=torch.float64, pin_memory=True).numpy()
-    out_phi = torch.empty(f.shape, dtype=torch.float64, pin_memory=True).numpy()
-    V0 = f.param("Phi_Bc_hi")
+    comps = ["Pz"] if f.param("is_polarization_scalar") == 1.0 else ["Px", "Py", "Pz"]
+    outs = {n: torch.empty(f.shape, dtype=torch.float64, pin_memory=True).numpy() for n in comps + ["Phi"]}
     barrier()
     torch.cuda.synchronize()
     se0 = f.stats()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    f.set_initial_P(None, None, Pz_host)
     means = []
     for q in range(ke):
-        f.set_param("Phi_Bc_hi", V0)
+        f.set_param("Phi_Bc_hi", f.stats()["Phi_Bc_hi"])
         f.step(1)
         means.append(f.mean_P()[2])
-    out_P[...] = f.field("Pz")
-    out_phi[...] = f.field("Phi")
+    for n, buf in outs.items():
+        f.field(n, out=buf)
     e1.record(stream)
     torch.cuda.synchronize()
     barrier()
     se1 = f.stats()
     ems = max_over_ranks(e0.elapsed_time(e1), world)
     e2e_value = whole_job_rate(N, ke, world, ems)
-    h2d = (3 * N * 8 + ke * 8) / ke
-    d2h = (ke * 24 + 2 * N * 8) / ke
+    h2d = 8.0
+    d2h = (ke * 24 + len(outs) * N * 8) / ke
+
+    # per-launch kernel durations: K more steps with CUDA events around every
+    # launch (kept out of the timed region, whose cost they raise)
+    f.set_param("fx.profile", 1)
+    f.reset_kernel_times()
+    f.step(args.steps)
+    kt = f.kernel_times()
+    f.set_param("fx.profile", 0)
 
     if rank == 0:
         peak, peak_src = peaks()
@@ -472,18 +494,18 @@ def main() -> None:
         bw_classes = ["smooth_l0", "restrict_l0", "prolong_l0", "tdgl", "newton", "rho", "resid64", "rhs_p", "steady"]
         dom = max((k for k in bw_classes if kt[k][1]), key=lambda k: kt[k][0])
         dms, dcnt = kt[dom]
-        nz1 = WORKLOADS[args.workload]["shape"]
         Nc1 = N // 2  # level 1 halves z on these stacks (dz < dx)
         fp = 4 if args.precision == "mixed" and dom in ("smooth_l0", "restrict_l0", "prolong_l0") else 8
         planes = f.param("mg_level0_planes") == 1.0
         per_launch = algorithmic_bytes(dom, N, Nc1, sc, True, rot, fp, planes)
+        tkey = (args.workload, args.precision, dom)
         achieved = per_launch / (dms / dcnt / 1e3) / 1e9 if dcnt else None
         total_ms = sum(v[0] for v in kt.values())
         roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak if achieved else None,
-                "traffic": TRAFFIC.get((args.workload, args.precision, dom)),
-                "traffic_source": "ncu dram bytes per launch, profiles/k_rbgs_l0_mfism_128x128x144.txt"
-                if (args.workload, args.precision, dom) in TRAFFIC else None,
+                "traffic": TRAFFIC[tkey][0] if tkey in TRAFFIC else None,
+                "traffic_source": f"ncu dram bytes per launch, {TRAFFIC[tkey][1]}" if tkey in TRAFFIC
+                else "no ncu capture of this kernel class on this workload and precision",
                 "peak_source": f"{peak_src} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured"
                 else "fallback 6.65 TB/s",
                 "algorithmic_bytes_per_launch": per_launch, "launches": dcnt, "avg_launch_us": 1e3 * dms / dcnt,
@@ -505,18 +527,16 @@ def main() -> None:
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
             "data": "synthetic (seeded initial P, synthetic device stack)",
-            "config": {"workload": f"{args.workload}-{'x'.join(map(str, nz1))}-{args.precision}",
-                       "description": WORKLOADS[args.workload]["label"], "cells": N,
-                       "l2": f"inputs larger than L2: device working set {f.stats()['device_bytes'] / 1e6:.0f} MB per step",
-                       "mg_rtol": f.param("fx.mg_rtol"), "parallelism": "replicas",
-                       "step": "one CUDA graph per step, loop tests on the device" if f.param("step_graph_ran")
-                       else "host-driven loop"},
+            "config": run_config(args, N),
+            "run": {"device_bytes": f.stats()["device_bytes"],
+                    "step": "one CUDA graph per step, loop tests on the device" if f.param("step_graph_ran")
+                    else "host-driven loop"},
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": ke,
-                    # the leg continues the sweep after the timed and the per-launch passes
-                    "after_steps": args.warmup + 2 * args.steps,
+                    # the leg continues the run right after the timed steps
+                    "after_steps": args.warmup + args.steps,
                     "mg_cycles_per_step": (se1["mg_cycles_total"] - se0["mg_cycles_total"]) / ke},
             "gpu_launches": int(st1["kernel_launches"] - st0["kernel_launches"]),
             "clocks": clocks,

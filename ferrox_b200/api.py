@@ -164,8 +164,14 @@ class FerroX:
     def set_param(self, key: str, value: float) -> None:
         self._check(lib().fx_set_param(self.h, key.encode(), float(value)))
 
-    def field(self, name: str) -> np.ndarray:
-        out = np.empty(self.shape)
+    def field(self, name: str, out: np.ndarray | None = None) -> np.ndarray:
+        """The field as a (nz, ny, nx) FP64 array; with `out` (C-contiguous
+        float64 of nx*ny*nz values, e.g. a pinned buffer) the library copies
+        straight into it."""
+        if out is None:
+            out = np.empty(self.shape)
+        elif out.dtype != np.float64 or not out.flags.c_contiguous or out.size != self.N:
+            raise ValueError("out must be a C-contiguous float64 array of nx*ny*nz values")
         self._check(lib().fx_get_field(self.h, FIELD_ID[name], _dp(out), self.N))
         return out
 

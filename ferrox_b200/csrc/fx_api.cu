@@ -623,6 +623,11 @@ int compute_phi_rho_P(fx_ctx* c, int buf, bool step_start) {
         r = read_out(c, 2);
         if (r) return r;
         if (iter > 0) err = c->h_out[0] / c->h_out[1];
+        if (!std::isfinite(err)) {
+            std::ostringstream o;
+            o << "Phi-rho Newton iteration: the change of phi is not finite after " << passes << " passes";
+            return set_err(c, FX_ERR_NONFINITE, o.str());
+        }
         iter = iter + 1;
         if (c->par.verbose) printf("%d iterations :: err = %g\n", iter, err);
     }
@@ -1568,7 +1573,18 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
     if (!c || !key) return FX_ERR_INVALID_ARGUMENT;
     const std::string k(key);
     Params& p = c->par;
-    // the ranges the inputs reader applies to the same keys; checked before any state changes
+    // every refusal comes before any state changes: a refused call leaves the
+    // context (the step graphs, the phi history, the adjoint record) as it was
+    static const char* const known[] = {
+        "Phi_Bc_hi", "Phi_Bc_lo", "fx.mg_rtol", "fx.mg_max_iter", "fx.newton_max_iter", "fx.warm_start",
+        "fx.phi_extrapolate", "fx.step_graph", "fx.pdl", "fx.verbose", "fx.profile", "fx.mg_nu1", "fx.graphs",
+        "fx.mg_nu2", "fx.alpha_tiles", "fx.mg_mixed_cycles", "fx.phi_ghost_mode", "dt", "alpha", "fx.newton_tol",
+        "beta", "gamma", "g11", "g44", "BigGamma", "inc_step"};
+    bool is_known = false;
+    for (const char* q : known) is_known = is_known || k == q;
+    if (!is_known) return set_err(c, FX_ERR_INVALID_ARGUMENT, "parameter '" + k + "' cannot be set after creation");
+    if (!std::isfinite(v)) return set_err(c, FX_ERR_INVALID_ARGUMENT, k + " must be finite");
+    // the ranges the inputs reader applies to the same keys
     if (k == "fx.phi_extrapolate" && !(v >= 0 && v <= 6))
         return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx.phi_extrapolate must be 0..6");
     if (k == "fx.phi_ghost_mode" && !(v == 0 || v == 1 || v == 2))
@@ -1579,6 +1595,10 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
         return set_err(c, FX_ERR_INVALID_ARGUMENT, k + " must not be negative");
     if (k == "fx.mg_rtol" && !(v > 0))
         return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx.mg_rtol must be positive");
+    if (k == "fx.mg_mixed_cycles" && !(v >= 1))
+        return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx.mg_mixed_cycles must be at least 1");
+    if (k == "fx.newton_tol" && !(v > 0.0))
+        return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx.newton_tol must be positive");
     if (k != "fx.profile" && k != "fx.verbose" && k != "fx.graphs" && k != "fx.step_graph" && k != "fx.pdl" &&
         k != "fx.alpha_tiles")
         ++c->gen;
@@ -1602,11 +1622,7 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
     if (k == "fx.graphs") { c->mg.set_graphs(v != 0.0); return FX_OK; }
     if (k == "fx.mg_nu2") { c->mg.nu2 = (int)v; return FX_OK; }
     if (k == "fx.alpha_tiles") { c->mg.alpha_tiles = v != 0.0; return FX_OK; }
-    if (k == "fx.mg_mixed_cycles") {
-        if (v < 1) return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx.mg_mixed_cycles must be at least 1");
-        c->mg.mixed_cycles = (int)v;
-        return FX_OK;
-    }
+    if (k == "fx.mg_mixed_cycles") { c->mg.mixed_cycles = (int)v; return FX_OK; }
     if (k == "fx.phi_ghost_mode") { p.phi_ghost_mode = (int)v; c->dp.ghost_mode = (int)v; c->E_valid = false; return FX_OK; }
     if (k == "dt") { p.dt = v; c->dp.dt = v; return FX_OK; }
     if (k == "alpha") {
@@ -1624,11 +1640,7 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
         }
         return FX_OK;
     }
-    if (k == "fx.newton_tol") {
-        if (!(v > 0.0)) return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx.newton_tol must be positive");
-        p.newton_tol = v;
-        return FX_OK;
-    }
+    if (k == "fx.newton_tol") { p.newton_tol = v; return FX_OK; }
     if (k == "beta") { p.beta = v; c->dp.beta = v; return FX_OK; }
     if (k == "gamma") { p.gamma = v; c->dp.gamma = v; return FX_OK; }
     if (k == "g11") { p.g11 = v; c->dp.g11 = v; return FX_OK; }
@@ -1640,32 +1652,44 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
 
 int fx_set_precision(fx_ctx* c, int mode) {
     if (!c || (mode != 0 && mode != 1)) return FX_ERR_INVALID_ARGUMENT;
-    if (c) { ++c->gen; c->hist_valid = false; }
     if (c->dev && mode != c->par.precision)
         return set_err(c, FX_ERR_INVALID_ARGUMENT, "precision must be chosen before the first device call");
+    ++c->gen;
+    c->hist_valid = false;
     c->par.precision = mode;
     return FX_OK;
 }
 
 int fx_set_initial_P(fx_ctx* c, const double* Px, const double* Py, const double* Pz, size_t n) {
-    if (c) { ++c->gen; c->hist_valid = false; }
     if (!c || !Pz || n != c->N) return c ? set_err(c, FX_ERR_INVALID_ARGUMENT, "P arrays must hold nx*ny*nz values") : FX_ERR_INVALID_ARGUMENT;
     const double* src[3] = {Px, Py, Pz};
     bool zero_xy = true;
-    for (int d = 0; d < 2; ++d)
+    for (int d = 0; d < 2 && zero_xy; ++d)
         if (src[d]) for (size_t q = 0; q < n; ++q) if (src[d][q] != 0.0) { zero_xy = false; break; }
-    for (int d = 0; d < 3; ++d) {
-        if (src[d]) c->P0[d].assign(src[d], src[d] + n);
-        else c->P0[d].assign(n, 0.0);
-    }
+    const bool scalar = c->par.is_polarization_scalar == 1 && zero_xy;
+    ++c->gen;
+    c->hist_valid = false;
     c->user_P = true;
-    c->scalarP = c->par.is_polarization_scalar == 1 && zero_xy;
-    if (c->dev) {
-        for (int b = 0; b < 2; ++b)
-            for (int d = 0; d < 3; ++d)
-                FX_CUDA(c, cudaMemcpyAsync(c->d_P[b][d], c->P0[d].data(), n * 8, cudaMemcpyHostToDevice, c->s));
-        FX_CUDA(c, cudaStreamSynchronize(c->s));
+    c->scalarP = scalar;
+    if (!c->dev) {
+        // kept on the host until the device state is made (ensure_device uploads it)
+        for (int d = 0; d < 3; ++d) {
+            if (src[d]) c->P0[d].assign(src[d], src[d] + n);
+            else c->P0[d].assign(n, 0.0);
+        }
+        return FX_OK;
     }
+    // on the device: each component crosses the bus once, straight from the
+    // caller's buffer (a pinned buffer makes it a DMA transfer); the second
+    // ping-pong buffer is filled on the device; missing components are zero
+    const int other = 1 - c->cur;
+    for (int d = 0; d < 3; ++d) {
+        if (src[d]) FX_CUDA(c, cudaMemcpyAsync(c->d_P[c->cur][d], src[d], n * 8, cudaMemcpyHostToDevice, c->s));
+        else FX_CUDA(c, cudaMemsetAsync(c->d_P[c->cur][d], 0, n * 8, c->s));
+        FX_CUDA(c, cudaMemcpyAsync(c->d_P[other][d], c->d_P[c->cur][d], n * 8, cudaMemcpyDeviceToDevice, c->s));
+    }
+    FX_CUDA(c, cudaStreamSynchronize(c->s));
+    c->E_valid = false;
     return FX_OK;
 }
 
@@ -1700,8 +1724,9 @@ int fx_set_grains(fx_ctx* c, const uint8_t* gid, size_t n, const double* ang, co
 
 int fx_set_grain_alpha(fx_ctx* c, const double* alpha, int ng) {
     if (!c || !alpha || ng <= 0) return FX_ERR_INVALID_ARGUMENT;
-    if (c) { ++c->gen; c->hist_valid = false; }
     if (!c->grains_set) return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx_set_grains must come first");
+    ++c->gen;
+    c->hist_valid = false;
     c->galpha.assign(alpha, alpha + ng);
     try {
         build_variants(c, &c->gid, &c->galpha);
@@ -1728,17 +1753,18 @@ int fx_get_field(fx_ctx* c, int f, double* out, size_t n) {
 
 int fx_set_field(fx_ctx* c, int f, const double* in, size_t n) {
     if (!c || !in) return FX_ERR_INVALID_ARGUMENT;
-    ++c->gen; c->hist_valid = false;
     if (n != c->N) return set_err(c, FX_ERR_INVALID_ARGUMENT, "field buffers hold nx*ny*nz values");
+    if (f != FX_FIELD_PX && f != FX_FIELD_PY && f != FX_FIELD_PZ && f != FX_FIELD_PHI)
+        return set_err(c, FX_ERR_INVALID_ARGUMENT, "only Px, Py, Pz and Phi can be set");
+    bool nonzero_xy = false;
+    if ((f == FX_FIELD_PX || f == FX_FIELD_PY) && c->scalarP) {
+        for (size_t q = 0; q < n; ++q) if (in[q] != 0.0) { nonzero_xy = true; break; }
+        if (nonzero_xy && c->dev)
+            return set_err(c, FX_ERR_INVALID_ARGUMENT, "nonzero Px/Py must be set before the first device call");
+    }
+    ++c->gen; c->hist_valid = false;
     if (f == FX_FIELD_PX || f == FX_FIELD_PY || f == FX_FIELD_PZ) {
-        if (f != FX_FIELD_PZ && c->scalarP) {
-            bool nz = false;
-            for (size_t q = 0; q < n; ++q) if (in[q] != 0.0) { nz = true; break; }
-            if (nz) {
-                if (c->dev) return set_err(c, FX_ERR_INVALID_ARGUMENT, "nonzero Px/Py must be set before the first device call");
-                c->scalarP = false;
-            }
-        }
+        if (nonzero_xy) c->scalarP = false;
         if (!c->dev) { c->P0[f].assign(in, in + n); c->user_P = true; return FX_OK; }
         FX_CUDA(c, cudaMemcpyAsync(c->d_P[c->cur][f], in, n * 8, cudaMemcpyHostToDevice, c->s));
         FX_CUDA(c, cudaStreamSynchronize(c->s));

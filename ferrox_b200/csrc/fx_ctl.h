@@ -96,7 +96,9 @@ __device__ __forceinline__ void ctl_mg_end(StepCtl* ctl) {
     ctl->mg_cycles_step += it;
     ctl->mg_resid_last = rn;
     ctl->mg_target_last = t;
-    if (!(rn <= t) && ctl->status == CTL_OK) {
+    // a non-finite residual fails even against a non-finite target (a NaN in
+    // the right-hand side makes both +inf)
+    if ((!(rn <= t) || !isfinite(rn)) && ctl->status == CTL_OK) {
         ctl->status = isfinite(rn) ? CTL_MG_NO_CONV : CTL_MG_NONFINITE;
         ctl->status_n = it;
         ctl->status_val = rn;
@@ -119,6 +121,11 @@ __device__ __forceinline__ void ctl_newton(StepCtl* ctl, double s1, double s2, d
     ctl->iter += 1;
     bool go = err > tol;
     if (ctl->status != CTL_OK) {
+        go = false;
+    } else if (!isfinite(err)) {
+        ctl->status = CTL_NEWTON_NONFINITE;
+        ctl->status_n = passes;
+        ctl->status_val = err;
         go = false;
     } else if (go && passes >= max_iter) {
         ctl->status = isfinite(err) ? CTL_NEWTON_NO_CONV : CTL_NEWTON_NONFINITE;

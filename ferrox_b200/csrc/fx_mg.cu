@@ -281,11 +281,11 @@ __device__ void resid_ctl(const ResidCtl& rc, double* slots) {
         ctl->rn = rn;
         ctl->it = 0;
         ctl->parity = 0;
-        cudaGraphSetConditional(rc.h, (!(rn <= target) && 0 < rc.maxit) ? 1u : 0u);
+        cudaGraphSetConditional(rc.h, (!(rn <= target) && isfinite(rn) && 0 < rc.maxit) ? 1u : 0u);
     } else if (rc.mode == RC_RN) {
         // the exact residual after a V-cycle
         ctl->rn = rn;
-        cudaGraphSetConditional(rc.h, (!(rn <= ctl->target) && ctl->it < rc.maxit) ? 1u : 0u);
+        cudaGraphSetConditional(rc.h, (!(rn <= ctl->target) && isfinite(rn) && ctl->it < rc.maxit) ? 1u : 0u);
     } else {
         // a mixed refinement step: `inner` FP32 cycles spent; h is the
         // condition of the next step in the same body (the IF node) or the
@@ -295,7 +295,7 @@ __device__ void resid_ctl(const ResidCtl& rc, double* slots) {
         ctl->rn = rn;
         ctl->it = it;
         ctl->parity = rc.parity;
-        cudaGraphSetConditional(rc.h, (!(rn <= ctl->target) && it < rc.maxit) ? 1u : 0u);
+        cudaGraphSetConditional(rc.h, (!(rn <= ctl->target) && isfinite(rn) && it < rc.maxit) ? 1u : 0u);
         if (rc.h2 != rc.h) cudaGraphSetConditional(rc.h2, 0u);
     }
 }
@@ -946,7 +946,9 @@ __global__ void k_mg_mid(double* __restrict__ slots, int single_level, int maxit
     for (int q = 0; q < NORM_SLOTS; ++q) slots[q] = 0.0;
     const int it = ctl->it + 1;
     ctl->it = it;
-    const bool need = single_level || mid <= ctl->target;
+    // a non-finite norm (a NaN reaches the slots as +inf) ends the loop: the
+    // exact residual then records the failure
+    const bool need = single_level || mid <= ctl->target || !isfinite(mid);
     if (!need) ctl->rn = mid;
     ctl->need = need ? 1 : 0;
     cudaGraphSetConditional(hw, (!need && it < maxit) ? 1u : 0u);
@@ -1573,7 +1575,7 @@ int Multigrid::solve64(const DevParams& p, const uint8_t* code, double* phi, con
     double rn = 0.0;
     int e = residual64(p, code, phi, rhs, nullptr, s, &rn);
     if (e) return e;
-    while (!(rn <= target) && it < maxit) {
+    while (!(rn <= target) && std::isfinite(rn) && it < maxit) {
         // one V-cycle; the level-0 residual norm after pre-smoothing bounds
         // the residual after the cycle, so it is the loop test; the exact
         // final residual is checked before returning
@@ -1589,7 +1591,7 @@ int Multigrid::solve64(const DevParams& p, const uint8_t* code, double* phi, con
         const double mid = slots_max();
         if (verbose > 1) printf("  mg cycle %d: |r|/target after pre-smoothing = %.3e\n", it, mid / target);
         if (lev_.size() == 1) { e = residual64(p, code, phi, rhs, nullptr, s, &rn); if (e) return e; continue; }
-        if (mid <= target) {
+        if (mid <= target || !std::isfinite(mid)) {
             e = residual64(p, code, phi, rhs, nullptr, s, &rn);
             if (e) return e;
         } else {
@@ -1598,7 +1600,7 @@ int Multigrid::solve64(const DevParams& p, const uint8_t* code, double* phi, con
     }
     if (st) { st->cycles = it; st->resid = rn; }
     cudaMemsetAsync(d_norm_, 0, NORM_SLOTS * 8, s);
-    return rn <= target ? 0 : -3;
+    return (rn <= target && std::isfinite(rn)) ? 0 : -3;
 }
 
 int Multigrid::solve_mixed(const DevParams& p, const uint8_t* code, double* phi, const double* rhs, double target,
@@ -1622,7 +1624,7 @@ int Multigrid::solve_mixed(const DevParams& p, const uint8_t* code, double* phi,
     int it = 0, cycles = 0;
     const int inner = std::max(1, mixed_cycles);
     if (verbose > 1) printf("  refinement %d: |r|/target = %.3e\n", it, rn / target);
-    while (!(rn <= target) && cycles < maxit) {
+    while (!(rn <= target) && std::isfinite(rn) && cycles < maxit) {
         // FP32 correction cycles on the FP32 residual, then the FP64 update
         // fused with the FP64 residual of the updated iterate
         double* xin = buf[cur];
@@ -1651,7 +1653,7 @@ int Multigrid::solve_mixed(const DevParams& p, const uint8_t* code, double* phi,
     }
     if (st) { st->cycles = cycles; st->resid = rn; }
     cudaMemsetAsync(d_norm_, 0, NORM_SLOTS * 8, s);
-    return rn <= target ? 0 : -3;
+    return (rn <= target && std::isfinite(rn)) ? 0 : -3;
 }
 
 // The loop of solve64 with its tests on the device: a WHILE node runs one

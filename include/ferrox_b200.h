@@ -211,8 +211,11 @@ int fx_get_grad_P0(fx_ctx* ctx, double* dPx, double* dPy, double* dPz, size_t n)
  * 16,777,216 cells (larger n returns FX_ERR_INVALID_ARGUMENT).  The first call
  * on a device looks up that array's device address, so make the first call
  * before any stream capture.  Calls that overlap on the GPU share the scratch
- * and race: order them on one stream.  Errors are reported through the
- * return code and fx_create_error(). */
+ * and race: order them on one stream.  The looked-up address is kept for the
+ * life of the process: do not call this after cudaDeviceReset (or after the
+ * device's primary context was destroyed and made again) in the same
+ * process, since the kept address then no longer names the array.  Errors are
+ * reported through the return code and fx_create_error(). */
 int fx_mean_P_noalloc(const double* d_Px, const double* d_Py, const double* d_Pz, const uint8_t* d_mask, size_t n,
                       double* d_out, void* cuda_stream);
 

@@ -32,7 +32,11 @@ def test_reference_line_keys_and_values():
     assert d["impl"] == "reference" and d["metric"] == "coupled-step cell-updates/s"
     assert d["unit"] == "cell-updates/s" and d["higher_is_better"] is True
     assert d["n_gpus"] == 1 and d["steps"] == 2 and d["warmup"] == 3 and d["dtype"] == "f64"
-    assert d["config"]["workload"] == "mfim-64x64x36-fp64" and d["config"]["cells"] == 64 * 64 * 36
+    # the reference arm names the same workload as the GPU arm (mixed precision
+    # by default) and says that it computes in FP64
+    assert d["config"]["workload"] == "mfim-64x64x36-mixed" and d["config"]["cells"] == 64 * 64 * 36
+    assert d["reference_precision"].startswith("fp64")
+    assert d["config"]["history_steps_at_timed_start"] == 3 and d["config"]["phi_extrapolate_order"] == 4
     assert d["value"] > 0 and abs(d["value"] - 64 * 64 * 36 / (d["ms_per_step"] * 1e-3)) <= 1e-6 * d["value"]
     cb = d["cpu_baseline"]
     assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]

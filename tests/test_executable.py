@@ -15,6 +15,9 @@ EXE = os.path.join(ROOT, "ferrox_b200", "ferrox_b200")
 
 
 def _run(*args):
+    # the executable is a build output (not tracked): build it from the current sources
+    from ferrox_b200 import build
+    build.build()
     if not os.path.exists(EXE):
         pytest.fail("ferrox_b200 executable not built")
     return subprocess.run([EXE, *args], capture_output=True, text=True, timeout=120)
