@@ -441,6 +441,7 @@ def main() -> None:
     clocks = sampler.stop()
     ms = ev0.elapsed_time(ev1)
     st1 = f.stats()
+    graph_ran = f.param("step_graph_ran") == 1.0
     if done != args.steps:
         raise RuntimeError(f"the reference loop ended after {done} of {args.steps} steps")
     ms_max = max_over_ranks(ms, world)
@@ -529,7 +530,7 @@ def main() -> None:
             "data": "synthetic (seeded initial P, synthetic device stack)",
             "config": run_config(args, N),
             "run": {"device_bytes": f.stats()["device_bytes"],
-                    "step": "one CUDA graph per step, loop tests on the device" if f.param("step_graph_ran")
+                    "step": "one CUDA graph per step, loop tests on the device" if graph_ran
                     else "host-driven loop"},
             "roofline": roof,
             "cpu_baseline": cpu,

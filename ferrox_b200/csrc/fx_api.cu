@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <iterator>
 #include <map>
 #include <memory>
 #include <sstream>
@@ -1391,6 +1392,61 @@ const char* fx_version(void) { return "ferrox_b200 0.1 (sm_100a)"; }
 
 const char* fx_create_error(void) { return t_create_error.c_str(); }
 
+// ---- input files named by fx.initial_P_file and fx.grain_file ----
+
+static std::vector<char> read_binary(const std::string& path, const char* what) {
+    std::ifstream f(path, std::ios::binary);
+    if (!f) throw FxError{FX_ERR_IO, std::string("cannot open ") + what + " '" + path + "'"};
+    return std::vector<char>((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+}
+
+// fx.initial_P_file: raw little-endian FP64, x fastest; N values (Pz, with
+// Px = Py = 0) or 3N values (the Px, Py and Pz blocks in that order)
+static void load_P_file(fx_ctx* c, const std::string& path) {
+    const std::vector<char> b = read_binary(path, "fx.initial_P_file");
+    const size_t N = c->N;
+    if (b.size() != N * 8 && b.size() != 3 * N * 8)
+        throw FxError{FX_ERR_INPUTS, "fx.initial_P_file '" + path + "' holds " + std::to_string(b.size()) +
+                                         " bytes; expected 8*N (Pz) or 24*N (Px, Py, Pz) for N = " + std::to_string(N)};
+    std::vector<double> v(b.size() / 8);
+    std::memcpy(v.data(), b.data(), b.size());
+    const bool three = v.size() == 3 * N;
+    const int r = fx_set_initial_P(c, three ? v.data() : nullptr, three ? v.data() + N : nullptr,
+                                   v.data() + (three ? 2 * N : 0), N);
+    if (r) throw FxError{r, c->err};
+}
+
+// fx.grain_file: "FXGRAIN1", int32 nx, ny, nz, ngrains (little-endian), then
+// per grain four FP64 (Euler angles alpha, beta, theta in degrees, t-phase
+// flag 0/1), then N uint8 grain ids, x fastest (255: no grain)
+static void load_grain_file(fx_ctx* c, const std::string& path) {
+    const std::vector<char> b = read_binary(path, "fx.grain_file");
+    const std::string bad = "fx.grain_file '" + path + "': ";
+    if (b.size() < 24 || std::memcmp(b.data(), "FXGRAIN1", 8) != 0) throw FxError{FX_ERR_INPUTS, bad + "not a grain file"};
+    int32_t h[4];
+    std::memcpy(h, b.data() + 8, 16);
+    if (h[0] != c->nx || h[1] != c->ny || h[2] != c->nz)
+        throw FxError{FX_ERR_INPUTS, bad + "grid " + std::to_string(h[0]) + "x" + std::to_string(h[1]) + "x" +
+                                         std::to_string(h[2]) + " differs from domain.n_cell"};
+    const int ng = h[3];
+    if (ng < 1 || ng > 255) throw FxError{FX_ERR_INPUTS, bad + "ngrains must be 1..255"};
+    const size_t need = 24 + (size_t)ng * 32 + c->N;
+    if (b.size() != need) throw FxError{FX_ERR_INPUTS, bad + "size " + std::to_string(b.size()) + ", expected " + std::to_string(need)};
+    std::vector<double> per((size_t)ng * 4);
+    std::memcpy(per.data(), b.data() + 24, per.size() * 8);
+    std::vector<double> ang((size_t)ng * 3);
+    std::vector<uint8_t> tph(ng);
+    for (int g = 0; g < ng; ++g) {
+        for (int d = 0; d < 3; ++d) ang[3 * g + d] = per[4 * g + d];
+        const double t = per[4 * g + 3];
+        if (t != 0.0 && t != 1.0) throw FxError{FX_ERR_INPUTS, bad + "t-phase flags must be 0 or 1"};
+        tph[g] = t == 1.0 ? 1 : 0;
+    }
+    const uint8_t* gid = reinterpret_cast<const uint8_t*>(b.data() + 24 + (size_t)ng * 32);
+    const int r = fx_set_grains(c, gid, c->N, ang.data(), tph.data(), ng);
+    if (r) throw FxError{r, c->err};
+}
+
 int fx_create(const char* inputs, int is_text, fx_ctx** out) {
     if (!out) return FX_ERR_INVALID_ARGUMENT;
     *out = nullptr;
@@ -1454,6 +1510,13 @@ int fx_create(const char* inputs, int is_text, fx_ctx** out) {
         build_P0(c.get());
         c->Phi_Bc_hi = p.Phi_Bc_hi;
         c->inc_step = p.inc_step;
+        if (!p.grain_file.empty()) {
+            if (p.Coordinate_Transformation != 1)
+                throw FxError{FX_ERR_INPUTS, "fx.grain_file needs Coordinate_Transformation = 1 (the grains carry "
+                                             "the tphase mask and Euler angles)"};
+            load_grain_file(c.get(), p.grain_file);
+        }
+        if (!p.initial_P_file.empty()) load_P_file(c.get(), p.initial_P_file);
         fill_devparams(c.get());
     } catch (FxError& e) {
         t_create_error = e.msg;

@@ -61,6 +61,10 @@ struct Params {
     int step_graph = 1;            // a step runs as one CUDA graph with its loop tests on the device
     int verbose = 0;
     std::string plot_dir = ".";
+    // input files (raw formats in include/ferrox_b200.h): the initial P, and
+    // the grains of a polycrystal (per-cell grain id, per-grain Euler angles
+    // and t-phase flag)
+    std::string initial_P_file, grain_file;
 };
 
 // Expression over x, y, z (and my_constants) from a function-valued key.

@@ -471,6 +471,8 @@ Params make_params(const Inputs& in) {
     r.query("fx.step_graph", p.step_graph);
     r.query("fx.verbose", p.verbose);
     if (r.has("fx.plot_dir")) p.plot_dir = r.vals("fx.plot_dir")[0];
+    if (r.has("fx.initial_P_file")) p.initial_P_file = r.vals("fx.initial_P_file")[0];
+    if (r.has("fx.grain_file")) p.grain_file = r.vals("fx.grain_file")[0];
 
     // validation the reference does by amrex::Abort / assertions
     for (int d = 0; d < 3; ++d)

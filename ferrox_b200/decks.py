@@ -169,6 +169,62 @@ def grain_fields(grains: dict):
     return tph, ang
 
 
+GRAIN_MAGIC = b"FXGRAIN1"
+
+
+def write_grain_file(path: str, grains: dict) -> None:
+    """The fx.grain_file format: b"FXGRAIN1", int32 nx, ny, nz, ngrains
+    (little-endian), per grain four float64 (Euler angles alpha, beta, theta
+    in degrees, t-phase flag 0/1), then nx*ny*nz uint8 grain ids, x fastest
+    (255: no grain)."""
+    gid = np.ascontiguousarray(grains["id"], dtype=np.uint8)
+    nz, ny, nx = gid.shape
+    ng = len(grains["tphase"])
+    per = np.zeros((ng, 4), dtype="<f8")
+    per[:, :3] = grains["angles"]
+    per[:, 3] = np.asarray(grains["tphase"], dtype=np.float64)
+    with open(path, "wb") as f:
+        f.write(GRAIN_MAGIC)
+        f.write(np.array([nx, ny, nz, ng], dtype="<i4").tobytes())
+        f.write(per.tobytes())
+        f.write(gid.tobytes())
+
+
+def read_grain_file(path: str) -> dict:
+    """The grains of a file written by write_grain_file."""
+    with open(path, "rb") as f:
+        b = f.read()
+    if b[:8] != GRAIN_MAGIC:
+        raise ValueError(f"{path}: not a grain file")
+    nx, ny, nz, ng = (int(v) for v in np.frombuffer(b, dtype="<i4", count=4, offset=8))
+    per = np.frombuffer(b, dtype="<f8", count=4 * ng, offset=24).reshape(ng, 4)
+    gid = np.frombuffer(b, dtype=np.uint8, count=nx * ny * nz, offset=24 + 32 * ng).reshape(nz, ny, nx)
+    if len(b) != 24 + 32 * ng + nx * ny * nz:
+        raise ValueError(f"{path}: wrong size")
+    return dict(id=gid.copy(), angles=per[:, :3].copy(), tphase=per[:, 3].astype(np.uint8))
+
+
+def write_P_file(path: str, Pz, Px=None, Py=None) -> None:
+    """The fx.initial_P_file format: raw little-endian float64, x fastest;
+    Pz alone, or the Px, Py and Pz blocks in that order."""
+    with open(path, "wb") as f:
+        if Px is not None or Py is not None:
+            for a in (Px, Py):
+                f.write(np.ascontiguousarray(np.zeros_like(Pz) if a is None else a, dtype="<f8").tobytes())
+        f.write(np.ascontiguousarray(Pz, dtype="<f8").tobytes())
+
+
+def read_P_file(path: str, shape) -> tuple:
+    """(Px, Py, Pz) from an fx.initial_P_file (Px, Py None when it holds Pz only)."""
+    v = np.fromfile(path, dtype="<f8")
+    N = int(np.prod(shape))
+    if v.size == N:
+        return None, None, v.reshape(shape)
+    if v.size == 3 * N:
+        return tuple(v[q * N:(q + 1) * N].reshape(shape) for q in range(3))
+    raise ValueError(f"{path}: {v.size} values, expected {N} or {3 * N}")
+
+
 def triangular_sweep(v_amp: float, steps_per_leg: int) -> np.ndarray:
     """Phi_Bc_hi per step: a leg of steps_per_leg steps from -v_amp to
     +v_amp, then one back to -v_amp (2 * steps_per_leg values)."""

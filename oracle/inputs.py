@@ -365,6 +365,14 @@ def function_fields(table: dict[str, list[str]], p: dict):
     Coordinate_Transformation == 1 (Source/main.cpp:178-181)."""
     n = p["n_cell"]
     shape = (n[2], n[1], n[0])
+    if "fx.grain_file" in table and p["Coordinate_Transformation"] == 1:
+        # the polycrystal input file (format: ferrox_b200.decks.write_grain_file)
+        from ferrox_b200 import decks
+        g = decks.read_grain_file(table["fx.grain_file"][0])
+        if g["id"].shape != shape:
+            raise ValueError("inputs: fx.grain_file grid differs from domain.n_cell")
+        tph, ang = decks.grain_fields(g)
+        return (tph,) + tuple(ang)
     if p["Coordinate_Transformation"] != 1:
         z0 = np.zeros(shape)
         return z0, z0.copy(), z0.copy(), z0.copy()

@@ -130,7 +130,14 @@ class Oracle:
         table = _inputs.parse_table(text)
         p = _inputs.ferrox_params(table)
         tph, a, b, t = _inputs.function_fields(table, p)
-        return cls(p, tph, (a, b, t), **kw)
+        o = cls(p, tph, (a, b, t), **kw)
+        if "fx.initial_P_file" in table:
+            # the initial P file (format: ferrox_b200.decks.write_P_file)
+            from ferrox_b200 import decks
+            P = decks.read_P_file(table["fx.initial_P_file"][0], o.shape)
+            for name, comp in zip(["Px", "Py", "Pz"], P):
+                o.set_field(name, np.zeros(o.shape) if comp is None else comp)
+        return o
 
     def __del__(self):
         if getattr(self, "h", None):

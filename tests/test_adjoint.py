@@ -225,23 +225,22 @@ def test_checkpoint_interval_does_not_change_gradient():
 
 def test_refused_calls_keep_the_recorded_run():
     """A refused fx_set_param / fx_set_precision / fx_set_field changes nothing:
-    the recorded run stays valid for fx_backward, whose gradient is the one a
-    run without the refused calls gives."""
+    the recorded run stays valid for fx_backward, whose gradient is the one
+    the same record gave before the refused calls (to the last bits that the
+    block sums' atomic accumulation order may move)."""
     text = decks.hysteresis(16, 16, 12, v_amp=1.0, steps_per_leg=6)
     shape, target = sweep(12)
-    grads = []
-    for refuse in (False, True):
-        f = api.FerroX(text)
-        f.forward_record(target, 1.0, shape, 4)
-        if refuse:
-            for key, v in [("no_such_key", 1.0), ("fx.mg_rtol", -1.0), ("fx.newton_tol", 0.0),
-                           ("fx.mg_mixed_cycles", 0.0), ("alpha", float("nan"))]:
-                with pytest.raises(api.FxError):
-                    f.set_param(key, v)
-            with pytest.raises(api.FxError):
-                f._check(api.lib().fx_set_precision(f.h, 1))
-            with pytest.raises(api.FxError):
-                f._check(api.lib().fx_set_field(f.h, api.FIELD_ID["Ex"], api._dp(np.zeros(f.N)), f.N))
-        grads.append(f.backward())
-        f.close()
-    assert np.array_equal(grads[0], grads[1])
+    f = api.FerroX(text)
+    f.forward_record(target, 1.0, shape, 4)
+    g0 = f.backward()
+    for key, v in [("no_such_key", 1.0), ("fx.mg_rtol", -1.0), ("fx.newton_tol", 0.0),
+                   ("fx.mg_mixed_cycles", 0.0), ("alpha", float("nan"))]:
+        with pytest.raises(api.FxError):
+            f.set_param(key, v)
+    with pytest.raises(api.FxError):
+        f._check(api.lib().fx_set_precision(f.h, 1))
+    with pytest.raises(api.FxError):
+        f._check(api.lib().fx_set_field(f.h, api.FIELD_ID["Ex"], api._dp(np.zeros(f.N)), f.N))
+    g1 = f.backward()
+    assert np.allclose(g1, g0, rtol=1e-12, atol=0.0), (g0, g1)
+    f.close()
