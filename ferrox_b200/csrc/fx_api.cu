@@ -427,6 +427,23 @@ int dmalloc(fx_ctx* c, T** p, size_t n) {
     return 0;
 }
 
+// InitializePandRho's charge (Initialization.cpp:134-160): intrinsic carrier
+// densities n = p = n_i in the semiconductor and rho = q (p - n - N_A + N_D)
+int upload_initial_charge(fx_ctx* c) {
+    const size_t N = c->N;
+    std::vector<double> rho0(N, 0.0), e0(N, 0.0);
+    const double ni = std::sqrt(kNc * kNv) * exp(-0.5 * kQ * kEg / (kKb * kT));
+    for (size_t q = 0; q < N; ++q)
+        if ((c->code[q + c->nxy] & 3) >= 2) {
+            e0[q] = ni;
+            rho0[q] = kQ * (ni - ni - c->par.acceptor_doping + c->par.donor_doping);
+        }
+    FX_CUDA(c, cudaMemcpy(c->d_rho, rho0.data(), N * 8, cudaMemcpyHostToDevice));
+    FX_CUDA(c, cudaMemcpy(c->d_e, e0.data(), N * 8, cudaMemcpyHostToDevice));
+    FX_CUDA(c, cudaMemcpy(c->d_h, e0.data(), N * 8, cudaMemcpyHostToDevice));
+    return FX_OK;
+}
+
 int ensure_device(fx_ctx* c) {
     if (c->dev) return FX_OK;
     int ndev = 0;
@@ -460,16 +477,8 @@ int ensure_device(fx_ctx* c) {
     for (int b = 0; b < 2; ++b)
         for (int d = 0; d < 3; ++d) FX_CUDA(c, cudaMemcpy(c->d_P[b][d], c->P0[d].data(), N * 8, cudaMemcpyHostToDevice));
     // main.cpp:157-173 zero fields; InitializePandRho's intrinsic carriers in SC
-    std::vector<double> rho0(N, 0.0), e0(N, 0.0);
-    const double ni = std::sqrt(kNc * kNv) * exp(-0.5 * kQ * kEg / (kKb * kT));
-    for (size_t q = 0; q < N; ++q)
-        if ((c->code[q + c->nxy] & 3) >= 2) {
-            e0[q] = ni;
-            rho0[q] = kQ * (ni - ni - c->par.acceptor_doping + c->par.donor_doping);
-        }
-    FX_CUDA(c, cudaMemcpy(c->d_rho, rho0.data(), N * 8, cudaMemcpyHostToDevice));
-    FX_CUDA(c, cudaMemcpy(c->d_e, e0.data(), N * 8, cudaMemcpyHostToDevice));
-    FX_CUDA(c, cudaMemcpy(c->d_h, e0.data(), N * 8, cudaMemcpyHostToDevice));
+    r = upload_initial_charge(c);
+    if (r) return r;
     for (double* a : {c->d_phi, c->d_phi_old, c->d_phi_prev, c->d_alpha, c->d_rhs, c->d_rhsP, c->d_dphi})
         FX_CUDA(c, cudaMemset(a, 0, N * 8));
     FX_CUDA(c, cudaMemset(c->d_alpha32, 0, N * 4));
@@ -995,7 +1004,7 @@ int step_graph(fx_ctx* c, int step, bool* ran) {
 }
 
 // one pass of main.cpp:261-621; returns 1 when the loop breaks
-int step_once(fx_ctx* c) {
+int step_once_impl(fx_ctx* c) {
     const int step = c->step + 1;
     bool ran = false;
     int r = step_graph(c, step, &ran);
@@ -1038,6 +1047,46 @@ int step_once(fx_ctx* c) {
     return brk ? 1 : 0;
 }
 
+// A step whose solve failed (a non-finite residual, or no convergence within
+// the caps) has left P as it was (the TDGL update and the steady-state check
+// did not run); phi and the charge density go back to their values at the
+// end of the last completed step, so the caller can change the input and
+// step again.  phi_old holds that phi: CheckSteadyState copies phi into it at
+// the end of every step (before the first step both are zero).
+int restore_after_failure(fx_ctx* c) {
+    if (!c->dev) return FX_OK;
+    FX_CUDA(c, cudaMemcpyAsync(c->d_phi, c->d_phi_old, c->N * 8, cudaMemcpyDeviceToDevice, c->s));
+    if (c->contains_sc) {
+        if (c->step == 0) {
+            FX_CUDA(c, cudaStreamSynchronize(c->s));
+            int r = upload_initial_charge(c);
+            if (r) return r;
+            c->carriers_stale = false;
+        } else {
+            ++g_launches;
+            int r = k_status(c, launch_rho(c->dp, c->d_code, c->d_phi, c->d_phi_prev, c->d_rho, c->d_e, c->d_h,
+                                           c->d_part, c->d_counter, c->d_out, 0, 0, c->s));
+            if (r) return r;
+            c->carriers_stale = true;
+        }
+    }
+    c->E_valid = false;
+    c->hist_valid = false;
+    FX_CUDA(c, cudaStreamSynchronize(c->s));
+    return FX_OK;
+}
+
+int step_once(fx_ctx* c) {
+    const int r = step_once_impl(c);
+    if (r == FX_ERR_NONFINITE || r == FX_ERR_NO_CONVERGENCE) {
+        const std::string msg = c->err;
+        const int q = restore_after_failure(c);
+        if (q) return q;
+        c->err = msg;
+    }
+    return r;
+}
+
 int materialize_E(fx_ctx* c) {
     int r = ensure_device(c);
     if (r) return r;
@@ -1055,7 +1104,11 @@ int materialize_E(fx_ctx* c) {
 
 int host_field(fx_ctx* c, int f, std::vector<double>& out) {
     const size_t N = c->N;
-    out.assign(N, 0.0);
+    switch (f) {
+    case FX_FIELD_EPSILON: case FX_FIELD_MASK: case FX_FIELD_GAMMA: out.assign(N, 0.0); break;
+    case FX_FIELD_TPHASE: case FX_FIELD_ANGLE_ALPHA: case FX_FIELD_ANGLE_BETA: case FX_FIELD_ANGLE_THETA: break;
+    default: return 0;   // a device field: nothing allocated here
+    }
     switch (f) {
     case FX_FIELD_EPSILON:
         for (size_t q = 0; q < N; ++q) out[q] = eps_of_code(c->par, c->code[q + c->nxy]);

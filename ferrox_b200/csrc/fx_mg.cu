@@ -97,9 +97,13 @@ __device__ __forceinline__ void atomic_max_nonneg(double* addr, double v) {
     atomicMax(reinterpret_cast<unsigned long long*>(addr), (unsigned long long)__double_as_longlong(v));
 }
 
+// max that keeps a NaN (fmax would drop it): a NaN anywhere in a residual
+// must reach the loop test, where it ends the solve as a failure
+__device__ __forceinline__ double nan_max(double a, double b) { return (a > b || a != a) ? a : b; }
+
 __device__ double block_max_all(double v) {
     __shared__ double sh[32];
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    for (int o = 16; o > 0; o >>= 1) v = nan_max(v, __shfl_down_sync(0xffffffffu, v, o));
     const int t = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
     const int nt = blockDim.x * blockDim.y * blockDim.z;
     if ((t & 31) == 0) sh[t >> 5] = v;
@@ -107,7 +111,7 @@ __device__ double block_max_all(double v) {
     double r = 0.0;
     if (t < 32) {
         r = t < (nt + 31) / 32 ? sh[t] : 0.0;
-        for (int o = 16; o > 0; o >>= 1) r = fmax(r, __shfl_down_sync(0xffffffffu, r, o));
+        for (int o = 16; o > 0; o >>= 1) r = nan_max(r, __shfl_down_sync(0xffffffffu, r, o));
     }
     return r;
 }
@@ -241,7 +245,7 @@ __global__ void __launch_bounds__(256) k_resid_restrict(Op<T> o, const T* __rest
                     if (k < o.nz - 1) off += ct * x[c + o.nxy];
                     const T r = (b[c] + bcv) - (diag * x[c] - off);
                     s += r;
-                    mx = fmax(mx, fabs((double)r));
+                    mx = nan_max(mx, fabs((double)r));
                 }
         bc[I + ncx * (J + ncy * K)] = s / T(RX * RY * RZ);
     }
@@ -369,7 +373,7 @@ __global__ void __launch_bounds__(256) k_resid64(Op<double> o, const double* __r
             const double r = (b[c] + bcv) - (diag * xc - off);
             if (r32) r32[c] = (float)r;
             if (CORR) xout[c] = xc;
-            mx = fmax(mx, fabs(r));
+            mx = nan_max(mx, fabs(r));
             xm = xc; xc = xp;
             em = ec; ec = ep;
         }

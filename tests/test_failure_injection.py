@@ -5,7 +5,9 @@ The reference has no such check: a NaN in P reaches the Poisson right-hand
 side, MLMG never meets its tolerance and ComputePhi_Rho's Newton loop
 (ElectrostaticSolver.cpp:703-744) has no iteration cap.  Here every solve loop
 stops at the first non-finite residual norm, the step's TDGL update and
-steady-state check are skipped, and the status names the failure.  The
+steady-state check are skipped, the status names the failure, and phi and
+the charge density return to their values at the end of the last completed
+step, so the same context can step again once the input is fixed.  The
 poison is planted from the host (fx_set_field) between steps, in the step
 graph and in the host-driven loop, on a dielectric stack (one Poisson solve)
 and on a semiconductor stack (the Newton loop)."""
@@ -32,6 +34,7 @@ def test_nan_in_state_is_reported_and_state_kept(kind, graph, where):
     f = api.FerroX(_deck(kind))
     f.set_param("fx.step_graph", graph)
     f.step(2)
+    phi_before, rho_before = f.field("Phi"), f.field("charge")
     poisoned = f.field(where)
     fe = np.argwhere(f.field("mask") == 0)
     k, j, i = fe[len(fe) // 2]
@@ -45,6 +48,9 @@ def test_nan_in_state_is_reported_and_state_kept(kind, graph, where):
     # the failed step changed neither P nor the step count
     assert np.array_equal(f.field("Pz"), P0, equal_nan=True)
     assert f.stats()["step"] == step0
+    # phi and the charge are those of the end of the last completed step
+    assert np.array_equal(f.field("Phi"), phi_before)
+    assert np.array_equal(f.field("charge"), rho_before)
     # with the poison removed the same context steps again
     clean = f.field(where)
     clean[k, j, i] = 0.0
