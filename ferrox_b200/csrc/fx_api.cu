@@ -139,6 +139,8 @@ struct fx_ctx {
     bool own_stream = true;
     Prof prof;
     uint8_t *d_code = nullptr, *d_var = nullptr;
+    uint8_t* d_interior = nullptr;       // DevParams::interior flags
+    bool use_interior = true;            // fx.interior
     Variant* d_vt = nullptr;
     double* d_P[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
     int cur = 0;
@@ -411,6 +413,7 @@ void fill_devparams(fx_ctx* c) {
     d.sc_Cd = 2.0 * std::exp((kQ * kEd + kQ * kChi) / kbT);
     d.delta = p.delta; d.inv_delta = 1. / p.delta; d.neg_inv_delta = -1. / p.delta;
     d.ghost_mode = p.phi_ghost_mode;
+    d.interior = c->use_interior ? c->d_interior : nullptr;
     electrode_values(c);
 }
 
@@ -474,6 +477,32 @@ int ensure_device(fx_ctx* c) {
         FX_CUDA(c, cudaMemcpy(c->d_vt, c->variants.data(), c->variants.size() * sizeof(Variant), cudaMemcpyHostToDevice));
     }
     FX_CUDA(c, cudaMemcpy(c->d_code, c->code.data(), c->code.size(), cudaMemcpyHostToDevice));
+    {
+        // interior cells: the cell and its 18 face and edge neighbours are
+        // ferroelectric and 1 <= k <= nz - 2 (every P stencil takes its
+        // central form there, and every z index it reads is in range)
+        std::vector<uint8_t> in(N, 0);
+        const int nx = c->nx, ny = c->ny, nz = c->nz;
+        auto fe = [&](int i, int j, int k) {
+            i = (i % nx + nx) % nx;
+            j = (j % ny + ny) % ny;
+            return (c->code[(size_t)i + nx * ((size_t)j + (size_t)ny * (k + 1))] & 3) == 0;
+        };
+        for (int k = 1; k + 1 < nz; ++k)
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < nx; ++i) {
+                    bool ok = true;
+                    for (int dk = -1; dk <= 1 && ok; ++dk)
+                        for (int dj = -1; dj <= 1 && ok; ++dj)
+                            for (int di = -1; di <= 1 && ok; ++di)
+                                if (std::abs(di) + std::abs(dj) + std::abs(dk) <= 2) ok = fe(i + di, j + dj, k + dk);
+                    in[(size_t)i + nx * ((size_t)j + (size_t)ny * k)] = ok ? 1 : 0;
+                }
+        r = dmalloc(c, &c->d_interior, N);
+        if (r) return r;
+        FX_CUDA(c, cudaMemcpy(c->d_interior, in.data(), N, cudaMemcpyHostToDevice));
+        c->dp.interior = c->use_interior ? c->d_interior : nullptr;
+    }
     for (int b = 0; b < 2; ++b)
         for (int d = 0; d < 3; ++d) FX_CUDA(c, cudaMemcpy(c->d_P[b][d], c->P0[d].data(), N * 8, cudaMemcpyHostToDevice));
     // main.cpp:157-173 zero fields; InitializePandRho's intrinsic carriers in SC
@@ -1587,7 +1616,7 @@ void fx_destroy(fx_ctx* c) {
     if (c->dev) {
         cudaStreamSynchronize(c->s);
         adj_free(c);
-        cudaFree(c->d_code); cudaFree(c->d_var); cudaFree(c->d_vt);
+        cudaFree(c->d_code); cudaFree(c->d_var); cudaFree(c->d_vt); cudaFree(c->d_interior);
         for (int b = 0; b < 2; ++b)
             for (int d = 0; d < 3; ++d) cudaFree(c->d_P[b][d]);
         for (double* a : {c->d_phi, c->d_phi_old, c->d_phi_prev, c->d_rho, c->d_e, c->d_h, c->d_alpha, c->d_rhs,
@@ -1651,6 +1680,7 @@ int fx_get_param(const fx_ctx* c, const char* key, double* v) {
         {"adjoint_loss", c->adj.loss},
         {"fx.mg_nu1", (double)c->mg.nu1}, {"fx.mg_nu2", (double)c->mg.nu2},
         {"fx.mg_mixed_cycles", (double)c->mg.mixed_cycles}, {"fx.alpha_tiles", c->mg.alpha_tiles ? 1.0 : 0.0},
+        {"fx.interior", c->use_interior ? 1.0 : 0.0},
         {"step_graph_ran", c->sg_ran ? 1.0 : 0.0}, {"fx.pdl", g_pdl ? 1.0 : 0.0},
         // 1 when level 0's face coefficients depend on z only and its smoother
         // reads them by plane instead of from the material codes
@@ -1694,7 +1724,7 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
     static const char* const known[] = {
         "Phi_Bc_hi", "Phi_Bc_lo", "fx.mg_rtol", "fx.mg_max_iter", "fx.newton_max_iter", "fx.warm_start",
         "fx.phi_extrapolate", "fx.step_graph", "fx.pdl", "fx.verbose", "fx.profile", "fx.mg_nu1", "fx.graphs",
-        "fx.mg_nu2", "fx.alpha_tiles", "fx.mg_mixed_cycles", "fx.phi_ghost_mode", "dt", "alpha", "fx.newton_tol",
+        "fx.mg_nu2", "fx.alpha_tiles", "fx.interior", "fx.mg_mixed_cycles", "fx.phi_ghost_mode", "dt", "alpha", "fx.newton_tol",
         "beta", "gamma", "g11", "g44", "BigGamma", "inc_step"};
     bool is_known = false;
     for (const char* q : known) is_known = is_known || k == q;
@@ -1716,7 +1746,7 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
     if (k == "fx.newton_tol" && !(v > 0.0))
         return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx.newton_tol must be positive");
     if (k != "fx.profile" && k != "fx.verbose" && k != "fx.graphs" && k != "fx.step_graph" && k != "fx.pdl" &&
-        k != "fx.alpha_tiles")
+        k != "fx.alpha_tiles" && k != "fx.interior")
         ++c->gen;
     // the time history of phi only seeds the next solve's initial iterate;
     // electrode values are compared on their own, solver settings leave the
@@ -1738,6 +1768,11 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
     if (k == "fx.graphs") { c->mg.set_graphs(v != 0.0); return FX_OK; }
     if (k == "fx.mg_nu2") { c->mg.nu2 = (int)v; return FX_OK; }
     if (k == "fx.alpha_tiles") { c->mg.alpha_tiles = v != 0.0; return FX_OK; }
+    if (k == "fx.interior") {
+        c->use_interior = v != 0.0;
+        c->dp.interior = c->use_interior ? c->d_interior : nullptr;
+        return FX_OK;
+    }
     if (k == "fx.mg_mixed_cycles") { c->mg.mixed_cycles = (int)v; return FX_OK; }
     if (k == "fx.phi_ghost_mode") { p.phi_ghost_mode = (int)v; c->dp.ghost_mode = (int)v; c->E_valid = false; return FX_OK; }
     if (k == "dt") { p.dt = v; c->dp.dt = v; return FX_OK; }

@@ -51,6 +51,10 @@ struct DevParams {
     // z Dirichlet values of phi held by the solver and the ghost mode
     double V_lo, V_hi;
     int ghost_mode;
+    // one byte per cell: 1 where the cell and its 18 face and edge neighbours
+    // are ferroelectric and 1 <= k <= nz - 2, so that every mask test of the
+    // P stencils passes (their central forms apply); null: none flagged
+    const uint8_t* interior;
 };
 
 __device__ __forceinline__ int wrap(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
@@ -95,9 +99,27 @@ struct MView {
     __device__ __forceinline__ int operator()(int i, int j, int k) const { return mcode(code, *p, i, j, k) & 3; }
 };
 
+// The mask seen from an interior cell (DevParams::interior): every cell its
+// stencils test is ferroelectric, so each derivative takes its central form.
+// Evaluating the same stencil functions with this view gives the same
+// arithmetic as with MView, without the mask loads and branches.
+struct MInterior {
+    __device__ __forceinline__ int operator()(int, int, int) const { return 0; }
+};
+
+// P read from an interior cell: every z index it reads is inside [0, nz)
+template <typename T>
+struct PViewIn {
+    const double* __restrict__ a;
+    const DevParams* p;
+    __device__ __forceinline__ T operator()(int i, int j, int k) const {
+        return T(__ldg(a + cidx(*p, wrap(i, p->nx), wrap(j, p->ny), k)));
+    }
+};
+
 // DPDx / DPDy / DPDz, DerivativeAlgorithm.H:45-252 (direction D)
-template <int D, typename T, typename FV>
-__device__ __forceinline__ T dpd(const FV& F, const MView& M, int i, int j, int k) {
+template <int D, typename T, typename FV, typename MV>
+__device__ __forceinline__ T dpd(const FV& F, const MV& M, int i, int j, int k) {
     constexpr int ox = D == 0, oy = D == 1, oz = D == 2;
     const DevParams& p = *F.p;
     const T h = T(p.dx[D]);
@@ -126,8 +148,8 @@ __device__ __forceinline__ T dpd(const FV& F, const MView& M, int i, int j, int 
 }
 
 // DoubleDPDx / y / z, DerivativeAlgorithm.H:256-467 (direction D)
-template <int D, typename T, typename FV>
-__device__ __forceinline__ T ddpd(const FV& F, const MView& M, int i, int j, int k) {
+template <int D, typename T, typename FV, typename MV>
+__device__ __forceinline__ T ddpd(const FV& F, const MV& M, int i, int j, int k) {
     constexpr int ox = D == 0, oy = D == 1, oz = D == 2;
     const DevParams& p = *F.p;
     const T h = T(p.dx[D]);
@@ -162,16 +184,16 @@ __device__ __forceinline__ T ddpd(const FV& F, const MView& M, int i, int j, int
 }
 
 // DoubleDPDxDy / DxDz / DyDz, DerivativeAlgorithm.H:471-497
-template <typename T, typename FV>
-__device__ __forceinline__ T dxdy(const FV& F, const MView& M, int i, int j, int k) {
+template <typename T, typename FV, typename MV>
+__device__ __forceinline__ T dxdy(const FV& F, const MV& M, int i, int j, int k) {
     return (dpd<1, T>(F, M, i + 1, j, k) - dpd<1, T>(F, M, i - 1, j, k)) / T(2.) / T(F.p->dx[0]);
 }
-template <typename T, typename FV>
-__device__ __forceinline__ T dxdz(const FV& F, const MView& M, int i, int j, int k) {
+template <typename T, typename FV, typename MV>
+__device__ __forceinline__ T dxdz(const FV& F, const MV& M, int i, int j, int k) {
     return (dpd<2, T>(F, M, i + 1, j, k) - dpd<2, T>(F, M, i - 1, j, k)) / T(2.) / T(F.p->dx[0]);
 }
-template <typename T, typename FV>
-__device__ __forceinline__ T dydz(const FV& F, const MView& M, int i, int j, int k) {
+template <typename T, typename FV, typename MV>
+__device__ __forceinline__ T dydz(const FV& F, const MV& M, int i, int j, int k) {
     return (dpd<2, T>(F, M, i, j + 1, k) - dpd<2, T>(F, M, i, j - 1, k)) / T(2.) / T(F.p->dx[1]);
 }
 
@@ -255,8 +277,8 @@ __device__ __forceinline__ T landau(const DevParams& p, T alpha, T a, T b, T c) 
 template <typename T>
 struct Hess { T xx, yy, zz, xy, yz, xz; };
 
-template <typename T, bool ROT, typename FV>
-__device__ __forceinline__ Hess<T> hess(const FV& F, const MView& M, int i, int j, int k) {
+template <typename T, bool ROT, typename FV, typename MV>
+__device__ __forceinline__ Hess<T> hess(const FV& F, const MV& M, int i, int j, int k) {
     Hess<T> h;
     h.xx = ddpd<0, T>(F, M, i, j, k);
     h.yy = ddpd<1, T>(F, M, i, j, k);

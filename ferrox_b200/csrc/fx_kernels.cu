@@ -72,6 +72,33 @@ __device__ double block_max(double v, double* sh) {
     return r;
 }
 
+// The gradient-energy terms of CalculateTDGL_RHS (TotalEnergyDensity.cpp:
+// 133-251) at cell (i, j, k): gr for the r (z) component and, with vector P,
+// gp and gq.  M and the P views decide how neighbours are read: MView / PView
+// in general, MInterior / PViewIn at interior cells (same arithmetic).
+template <typename T, bool SCALAR, bool ROT, typename MV, typename PV>
+__device__ __forceinline__ void grad_terms(const DevParams& p, const T* R, const MV& M, const PV& Fp, const PV& Fq,
+                                           const PV& Fr, int i, int j, int k, T& gr, T& gp, T& gq) {
+    const T g11 = T(p.g11), g44 = T(p.g44), g44p = T(p.g44p), g12 = T(p.g12);
+    Hess<T> H = hess<T, ROT>(Fr, M, i, j, k);
+    T g;
+    if (ROT) {
+        g = -g11 * rot_quad(R, 2, H) - (g44 - g44p) * rot_quad(R, 0, H) - (g44 - g44p) * rot_quad(R, 1, H);
+    } else {
+        g = -g11 * H.zz - (g44 - g44p) * H.xx - (g44 - g44p) * H.yy;
+    }
+    if (!SCALAR) g = g - (g44 + g44p + g12) * dydz<T>(Fq, M, i, j, k) - (g44 + g44p + g12) * dxdz<T>(Fp, M, i, j, k);
+    gr = g;
+    if (!SCALAR) {
+        gp = -g11 * ddpd<0, T>(Fp, M, i, j, k) - (g44 + g44p) * ddpd<1, T>(Fp, M, i, j, k) -
+             (g44 + g44p) * ddpd<2, T>(Fp, M, i, j, k) - (g12 + g44 - g44p) * dxdy<T>(Fq, M, i, j, k) -
+             (g12 + g44 - g44p) * dxdz<T>(Fr, M, i, j, k);
+        gq = -g11 * ddpd<1, T>(Fq, M, i, j, k) - (g44 - g44p) * ddpd<0, T>(Fq, M, i, j, k) -
+             (g44 - g44p) * ddpd<2, T>(Fq, M, i, j, k) - (g12 + g44 + g44p) * dxdy<T>(Fp, M, i, j, k) -
+             (g12 + g44 - g44p) * dydz<T>(Fr, M, i, j, k);
+    }
+}
+
 // One forward-Euler TDGL update.  T is the stencil arithmetic (double for the
 // FP64 path, float for the mixed path); the P state is read and written in
 // FP64.  SCALAR: is_polarization_scalar == 1 with Px = Py = 0, so only Pz is
@@ -127,9 +154,17 @@ __global__ void __launch_bounds__(256) k_tdgl(DevParams p, const uint8_t* __rest
         alpha = T(v.alpha);
     }
     const T Gam = T(p.BigGamma);
-    MView M{code, &p};
-    PView<T> Fr{Pr, &p};
-    const T g11 = T(p.g11), g44 = T(p.g44), g44p = T(p.g44p), g12 = T(p.g12);
+    // the gradient terms, through the interior views where the cell's whole
+    // stencil is ferroelectric
+    T g_r = T(0), g_p = T(0), g_q = T(0);
+    if (p.incl_G) {
+        if (p.interior && __ldg(p.interior + c))
+            grad_terms<T, SCALAR, ROT>(p, R, MInterior{}, PViewIn<T>{Pp, &p}, PViewIn<T>{Pq, &p}, PViewIn<T>{Pr, &p},
+                                       i, j, k, g_r, g_p, g_q);
+        else
+            grad_terms<T, SCALAR, ROT>(p, R, MView{code, &p}, PView<T>{Pp, &p}, PView<T>{Pq, &p}, PView<T>{Pr, &p},
+                                       i, j, k, g_r, g_p, g_q);
+    }
 
     // electric field from phi, ElectrostaticSolver.cpp:195-197
     T gx = T(0), gy = T(0), gz = T(0);
@@ -139,20 +174,7 @@ __global__ void __launch_bounds__(256) k_tdgl(DevParams p, const uint8_t* __rest
     const T r = T(pr0), pp = T(pp0), pq = T(pq0);
     T fr = T(0);
     if (p.incl_L) fr += T(-1.0) * Gam * landau<T>(p, alpha, r, pp, pq);
-    if (p.incl_G) {
-        Hess<T> H = hess<T, ROT>(Fr, M, i, j, k);
-        T g;
-        if (ROT) {
-            g = -g11 * rot_quad(R, 2, H) - (g44 - g44p) * rot_quad(R, 0, H) - (g44 - g44p) * rot_quad(R, 1, H);
-        } else {
-            g = -g11 * H.zz - (g44 - g44p) * H.xx - (g44 - g44p) * H.yy;
-        }
-        if (!SCALAR) {
-            PView<T> Fp{Pp, &p}, Fq{Pq, &p};
-            g = g - (g44 + g44p + g12) * dydz<T>(Fq, M, i, j, k) - (g44 + g44p + g12) * dxdz<T>(Fp, M, i, j, k);
-        }
-        fr += T(-1.0) * Gam * g;
-    }
+    if (p.incl_G) fr += T(-1.0) * Gam * g_r;
     if (p.incl_E) {
         const T Er = -(R[6] * gx + R[7] * gy + R[8] * gz);
         fr += T(-1.0) * Gam * (-Er);
@@ -162,21 +184,14 @@ __global__ void __launch_bounds__(256) k_tdgl(DevParams p, const uint8_t* __rest
     if (MODE == 2) Pr_out[c] = 1.0 * Pr_old[c] + p.dt * (0.5 * fbr[c] + 0.5 * (double)fr);
 
     if (!SCALAR) {
-        PView<T> Fp{Pp, &p}, Fq{Pq, &p};
         T fp = T(0), fq = T(0);
         if (p.incl_L) {
             fp += T(-1.0) * Gam * landau<T>(p, alpha, pp, pq, r);
             fq += T(-1.0) * Gam * landau<T>(p, alpha, pq, pp, r);
         }
         if (p.incl_G) {
-            T gp = -g11 * ddpd<0, T>(Fp, M, i, j, k) - (g44 + g44p) * ddpd<1, T>(Fp, M, i, j, k) -
-                   (g44 + g44p) * ddpd<2, T>(Fp, M, i, j, k) - (g12 + g44 - g44p) * dxdy<T>(Fq, M, i, j, k) -
-                   (g12 + g44 - g44p) * dxdz<T>(Fr, M, i, j, k);
-            T gq = -g11 * ddpd<1, T>(Fq, M, i, j, k) - (g44 - g44p) * ddpd<0, T>(Fq, M, i, j, k) -
-                   (g44 - g44p) * ddpd<2, T>(Fq, M, i, j, k) - (g12 + g44 + g44p) * dxdy<T>(Fp, M, i, j, k) -
-                   (g12 + g44 - g44p) * dydz<T>(Fr, M, i, j, k);
-            fp += T(-1.0) * Gam * gp;
-            fq += T(-1.0) * Gam * gq;
+            fp += T(-1.0) * Gam * g_p;
+            fq += T(-1.0) * Gam * g_q;
         }
         if (p.incl_E) {
             const T Ep = -(R[0] * gx + R[1] * gy + R[2] * gz);
@@ -200,6 +215,17 @@ __global__ void __launch_bounds__(256) k_tdgl(DevParams p, const uint8_t* __rest
             Pq_out[c] = 1.0 * oq + p.dt * (0.5 * fbq[c] + 0.5 * (double)fq);
         }
     }
+}
+
+// -sum_ab R_ab dP_a/dx_b at a ferroelectric cell, ElectrostaticSolver.cpp:65-77
+template <bool SCALAR, typename MV, typename PV>
+__device__ __forceinline__ double rhs_fe(const double* R, const MV& M, const PV& Fp, const PV& Fq, const PV& Fr,
+                                         int i, int j, int k) {
+    const double r3 = R[6] * dpd<0, double>(Fr, M, i, j, k) + R[7] * dpd<1, double>(Fr, M, i, j, k) + R[8] * dpd<2, double>(Fr, M, i, j, k);
+    if (SCALAR) return -r3;
+    const double r1 = R[0] * dpd<0, double>(Fp, M, i, j, k) + R[1] * dpd<1, double>(Fp, M, i, j, k) + R[2] * dpd<2, double>(Fp, M, i, j, k);
+    const double r2 = R[3] * dpd<0, double>(Fq, M, i, j, k) + R[4] * dpd<1, double>(Fq, M, i, j, k) + R[5] * dpd<2, double>(Fq, M, i, j, k);
+    return -(r1) - (r2) - (r3);
 }
 
 // FE branch of ComputePoissonRHS, ElectrostaticSolver.cpp:65-77 (DE -> 0; the
@@ -227,17 +253,14 @@ __global__ void __launch_bounds__(256) k_rhs_p(DevParams p, const uint8_t* __res
                 const Variant& vv = vt[__ldg(var + c)];
                 for (int q = 0; q < 9; ++q) R[q] = vv.R[q];
             }
-            MView M{code, &p};
-            PView<double> Fr{Pr, &p};
-            const double r3 = R[6] * dpd<0, double>(Fr, M, i, j, k) + R[7] * dpd<1, double>(Fr, M, i, j, k) + R[8] * dpd<2, double>(Fr, M, i, j, k);
-            if (SCALAR) {
-                v = -r3;
-            } else {
-                PView<double> Fp{Pp, &p}, Fq{Pq, &p};
-                const double r1 = R[0] * dpd<0, double>(Fp, M, i, j, k) + R[1] * dpd<1, double>(Fp, M, i, j, k) + R[2] * dpd<2, double>(Fp, M, i, j, k);
-                const double r2 = R[3] * dpd<0, double>(Fq, M, i, j, k) + R[4] * dpd<1, double>(Fq, M, i, j, k) + R[5] * dpd<2, double>(Fq, M, i, j, k);
-                v = -(r1) - (r2) - (r3);
-            }
+            // through the interior views where the cell's whole stencil is
+            // ferroelectric (same arithmetic, no mask tests)
+            if (p.interior && __ldg(p.interior + c))
+                v = rhs_fe<SCALAR>(R, MInterior{}, PViewIn<double>{Pp, &p}, PViewIn<double>{Pq, &p},
+                                   PViewIn<double>{Pr, &p}, i, j, k);
+            else
+                v = rhs_fe<SCALAR>(R, MView{code, &p}, PView<double>{Pp, &p}, PView<double>{Pq, &p},
+                                   PView<double>{Pr, &p}, i, j, k);
         }
         rhs[c] = v;
         nb = fabs(v);

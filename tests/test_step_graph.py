@@ -177,3 +177,47 @@ def test_fresh_contexts_bit_identical():
     for n in FIELDS:
         assert np.array_equal(out[0][0][n], out[1][0][n]), n
     assert out[0][1] == out[1][1]
+
+
+INTERIOR_CASES = {
+    # rotated scalar P in grains (the Hessian with its mixed derivatives)
+    "polycrystal_fp64": dict(grains=True, precision=None, vector=False),
+    "polycrystal_mixed": dict(grains=True, precision="mixed", vector=False),
+    # vector P in rotated grains
+    "polycrystal_vector": dict(grains=True, precision=None, vector=True),
+    # layered stacks, scalar P, with the Newton-coupled semiconductor
+    "mfism_fp64": dict(text=decks.mfism(32, 32, 48, steps_per_voltage=3, v_step=0.1), shape=(48, 32, 32)),
+    "mfim_mixed": dict(text=decks.mfim(32, 32, 24, Phi_Bc_hi=0.8), shape=(24, 32, 32), precision="mixed"),
+}
+
+
+@pytest.mark.parametrize("case", sorted(INTERIOR_CASES))
+def test_interior_fast_path_bit_identical(case):
+    """Cells whose whole stencil is ferroelectric evaluate the TDGL gradient
+    terms and the Poisson right-hand side through the interior views
+    (fx.interior = 1, the default): the same stencil code with the mask tests
+    known to pass.  Fields and cycle counts agree bit for bit with every cell
+    taking the general path (fx.interior = 0)."""
+    cfg = INTERIOR_CASES[case]
+    grains = None
+    if cfg.get("grains"):
+        extra = {"Phi_Bc_hi": 0.7}
+        if cfg.get("vector"):
+            extra.update({"is_polarization_scalar": 0, "g12": 2.0e-11})
+        text, grains = decks.polycrystal(32, 32, 48, ngrains=6, seed=4, nsteps=10, extra=extra)
+        shape = (48, 32, 32)
+    else:
+        text, shape = cfg["text"], cfg["shape"]
+    P = start_P(shape, 5, vector=cfg.get("vector", False))
+    runs = []
+    for interior in (0, 1):
+        f = make(text, P, 1, precision=cfg.get("precision"), grains=grains, params={"fx.interior": interior})
+        f.step(6)
+        f.compute_E()
+        runs.append(({n: f.field(n) for n in FIELDS + ["PoissonRHS"]}, f.stats()["mg_cycles_total"],
+                     f.stats()["newton_iters_total"]))
+        f.close()
+    (a, ca, na), (b, cb, nb) = runs
+    assert (ca, na) == (cb, nb)
+    for n in a:
+        assert np.array_equal(a[n], b[n]), n
