@@ -498,6 +498,20 @@ int ensure_device(fx_ctx* c) {
                                 if (std::abs(di) + std::abs(dj) + std::abs(dk) <= 2) ok = fe(i + di, j + dj, k + dk);
                     in[(size_t)i + nx * ((size_t)j + (size_t)ny * k)] = ok ? 1 : 0;
                 }
+        // the planes of the cells the TDGL update changes (one plane when
+        // there are none: the launch then changes nothing)
+        c->dp.fe_k0 = nz;
+        c->dp.fe_k1 = -1;
+        for (int k = 0; k < nz; ++k)
+            for (size_t q = 0; q < c->nxy; ++q) {
+                const uint8_t m = c->code[q + c->nxy * (size_t)(k + 1)];
+                if ((m & 3) == 0 && (m & 4) == 0) {
+                    c->dp.fe_k0 = std::min(c->dp.fe_k0, k);
+                    c->dp.fe_k1 = std::max(c->dp.fe_k1, k);
+                    break;
+                }
+            }
+        if (c->dp.fe_k1 < 0) c->dp.fe_k0 = c->dp.fe_k1 = 0;
         r = dmalloc(c, &c->d_interior, N);
         if (r) return r;
         FX_CUDA(c, cudaMemcpy(c->d_interior, in.data(), N, cudaMemcpyHostToDevice));
@@ -1918,6 +1932,9 @@ int fx_set_field(fx_ctx* c, int f, const double* in, size_t n) {
         if (nonzero_xy) c->scalarP = false;
         if (!c->dev) { c->P0[f].assign(in, in + n); c->user_P = true; return FX_OK; }
         FX_CUDA(c, cudaMemcpyAsync(c->d_P[c->cur][f], in, n * 8, cudaMemcpyHostToDevice, c->s));
+        // both ping-pong buffers: cells the TDGL update leaves alone are read
+        // from either
+        FX_CUDA(c, cudaMemcpyAsync(c->d_P[1 - c->cur][f], c->d_P[c->cur][f], n * 8, cudaMemcpyDeviceToDevice, c->s));
         FX_CUDA(c, cudaStreamSynchronize(c->s));
         c->E_valid = false;
         return FX_OK;

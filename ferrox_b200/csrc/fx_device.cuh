@@ -55,6 +55,9 @@ struct DevParams {
     // are ferroelectric and 1 <= k <= nz - 2, so that every mask test of the
     // P stencils passes (their central forms apply); null: none flagged
     const uint8_t* interior;
+    // the planes holding every cell the TDGL update changes (ferroelectric,
+    // not t-phase); P elsewhere never changes and both ping-pong buffers hold it
+    int fe_k0, fe_k1;
 };
 
 __device__ __forceinline__ int wrap(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
@@ -147,6 +150,12 @@ __device__ __forceinline__ T dpd(const FV& F, const MV& M, int i, int j, int k) 
     return (F(i + ox, j + oy, k + oz) - F(i - ox, j - oy, k - oz)) / (T(2.) * h);
 }
 
+// a product that the compiler may not fuse into a neighbouring add: the
+// second-derivative forms round 2 F the same way whichever branches survive
+// inlining (and as the oracle, built without contraction, does)
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+
 // DoubleDPDx / y / z, DerivativeAlgorithm.H:256-467 (direction D)
 template <int D, typename T, typename FV, typename MV>
 __device__ __forceinline__ T ddpd(const FV& F, const MV& M, int i, int j, int k) {
@@ -164,12 +173,12 @@ __device__ __forceinline__ T ddpd(const FV& F, const MV& M, int i, int j, int k)
         if (f == 2) return (-F0 + F1) / h / h;
         if (f == 3) {
             const T Fm = F(i - ox, j - oy, k - oz);
-            if (D == 2) return (Fm - T(2.) * F0 + F1) / h / h;
-            return (F1 - T(2.) * F0 + Fm) / h / h;
+            if (D == 2) return (Fm - mul_rn(T(2.), F0) + F1) / h / h;
+            return (F1 - mul_rn(T(2.), F0) + Fm) / h / h;
         }
         const T F2 = F(i + 2 * ox, j + 2 * oy, k + 2 * oz);
-        if (D == 2) return (F0 - T(2.) * F1 + F2) / h / h;
-        return (F2 - T(2.) * F1 + F0) / h / h;
+        if (D == 2) return (F0 - mul_rn(T(2.), F1) + F2) / h / h;
+        return (F2 - mul_rn(T(2.), F1) + F0) / h / h;
     }
     if (M(i + ox, j + oy, k + oz) != 0) {
         const int f = p.fhi[D];
@@ -177,10 +186,10 @@ __device__ __forceinline__ T ddpd(const FV& F, const MV& M, int i, int j, int k)
         if (f == 0) { T F_hi = T(0); return T(4.) * (T(2.) * F_hi - T(3.) * F0 + Fm) / T(3.) / h / h; }
         if (f == 1) { T F_hi = F0 / (T(1) - h / T(2) / lam); return (h * F_hi / lam - F0 + Fm) / h / h; }
         if (f == 2) return (-F0 + Fm) / h / h;
-        if (f == 3) return (F(i + ox, j + oy, k + oz) - T(2.) * F0 + Fm) / h / h;
-        return (F0 - T(2.) * Fm + F(i - 2 * ox, j - 2 * oy, k - 2 * oz)) / h / h;
+        if (f == 3) return (F(i + ox, j + oy, k + oz) - mul_rn(T(2.), F0) + Fm) / h / h;
+        return (F0 - mul_rn(T(2.), Fm) + F(i - 2 * ox, j - 2 * oy, k - 2 * oz)) / h / h;
     }
-    return (F(i + ox, j + oy, k + oz) - T(2.) * F0 + F(i - ox, j - oy, k - oz)) / (h * h);
+    return (F(i + ox, j + oy, k + oz) - mul_rn(T(2.), F0) + F(i - ox, j - oy, k - oz)) / (h * h);
 }
 
 // DoubleDPDxDy / DxDz / DyDz, DerivativeAlgorithm.H:471-497

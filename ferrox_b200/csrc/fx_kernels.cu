@@ -123,29 +123,18 @@ __global__ void __launch_bounds__(256) k_tdgl(DevParams p, const uint8_t* __rest
     if (skip && *skip) return;   // a step graph whose ComputePhi_Rho failed
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int k = blockIdx.z;
+    const int k = blockIdx.z + p.fe_k0;   // the launch covers planes fe_k0 .. fe_k1
     if (i >= p.nx || j >= p.ny) return;
     const size_t c = cidx(p, i, j, k);
     const int m = mcode(code, p, i, j, k);
+    // Gamma = 0 outside FE (Initialization.cpp:113, :125) and the t-phase
+    // zeroing (TotalEnergyDensity.cpp:123-127) leave P unchanged there: both
+    // ping-pong buffers already hold it (every write of P from the host fills
+    // both), and the predictor's f buffer is zero there from its allocation
+    if ((m & 3) != 0 || (m & 4) != 0) return;
     const double pr0 = Pr[c];
     const double pp0 = SCALAR ? 0.0 : Pp[c];
     const double pq0 = SCALAR ? 0.0 : Pq[c];
-    // Gamma = 0 outside FE (Initialization.cpp:113, :125) and the t-phase
-    // zeroing (TotalEnergyDensity.cpp:123-127) leave P unchanged there
-    if ((m & 3) != 0 || (m & 4) != 0) {
-        if (MODE == 2) {
-            Pr_out[c] = Pr_old[c];
-            if (!SCALAR) { Pp_out[c] = Pp_old[c]; Pq_out[c] = Pq_old[c]; }
-            return;
-        }
-        if (MODE == 1) {
-            fbr[c] = 0.0;
-            if (!SCALAR) { fbp[c] = 0.0; fbq[c] = 0.0; }
-        }
-        Pr_out[c] = pr0;
-        if (!SCALAR) { Pp_out[c] = pp0; Pq_out[c] = pq0; }
-        return;
-    }
     T R[9] = {T(1), T(0), T(0), T(0), T(1), T(0), T(0), T(0), T(1)};
     T alpha = T(p.alpha);
     if (ROT) {
@@ -552,7 +541,9 @@ dim3 cell_grid(const DevParams& p) { return dim3((p.nx + 31) / 32, (p.ny + 7) / 
 int launch_tdgl(const DevParams& p, int mixed, int mode, const uint8_t* code, const uint8_t* var, const Variant* vt,
                 const double* const Pin[3], double* const Pout[3], const double* phi, double* const fbuf[3],
                 const double* const Pold[3], cudaStream_t s, const int* skip) {
-    const dim3 g = cell_grid(p), b(32, 8);
+    dim3 g = cell_grid(p);
+    const dim3 b(32, 8);
+    g.z = (unsigned)(p.fe_k1 - p.fe_k0 + 1);
     const bool scal = p.scalar && Pin[0] == nullptr;
     const bool rot = var != nullptr;
     double* fb[3] = {fbuf ? fbuf[0] : nullptr, fbuf ? fbuf[1] : nullptr, fbuf ? fbuf[2] : nullptr};
