@@ -447,31 +447,42 @@ def main() -> None:
     ms_max = max_over_ranks(ms, world)
     value = whole_job_rate(N, args.steps, world, ms_max)
 
-    # end to end through the public API, K more steps right after the timed
-    # ones (the same stretch of the run): the state stays resident in HBM, as
-    # the reference's MultiFabs stay on its device; per step the host sets the
-    # electrode voltage (fx_set_param, the step's input), runs fx_step(1) and
-    # reads the mean polarization back (fx_mean_P, the step's result); at the
-    # end P and phi are read into pinned host buffers (fx_get_field)
+    # end to end through the public API: a second context of the same deck
+    # runs the same W warm-up steps (untimed) and then the same K steps as the
+    # timed leg, so both legs cover the same stretch of the run with the same
+    # history of phi.  The state stays resident in HBM, as the reference's
+    # MultiFabs stay on its device; per step the host sets the electrode
+    # voltage (fx_set_param, the step's input), runs fx_step(1) and reads the
+    # mean polarization back (fx_mean_P, the step's result); at the end P and
+    # phi are read into pinned host buffers (fx_get_field)
     ke = args.e2e_steps or args.steps
-    comps = ["Pz"] if f.param("is_polarization_scalar") == 1.0 else ["Px", "Py", "Pz"]
-    outs = {n: torch.empty(f.shape, dtype=torch.float64, pin_memory=True).numpy() for n in comps + ["Phi"]}
+    g = api.FerroX(text, precision=args.precision)
+    if grains is not None:
+        g.set_grains(grains["id"], grains["angles"], grains["tphase"])
+    if args.host_loop:
+        g.set_param("fx.step_graph", 0)
+    g.set_stream(stream.cuda_stream)
+    g.step(args.warmup)
+    g.sync()
+    comps = ["Pz"] if g.param("is_polarization_scalar") == 1.0 else ["Px", "Py", "Pz"]
+    outs = {n: torch.empty(g.shape, dtype=torch.float64, pin_memory=True).numpy() for n in comps + ["Phi"]}
     barrier()
     torch.cuda.synchronize()
-    se0 = f.stats()
+    se0 = g.stats()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     means = []
     for q in range(ke):
-        f.set_param("Phi_Bc_hi", f.stats()["Phi_Bc_hi"])
-        f.step(1)
-        means.append(f.mean_P()[2])
+        g.set_param("Phi_Bc_hi", g.stats()["Phi_Bc_hi"])
+        g.step(1)
+        means.append(g.mean_P()[2])
     for n, buf in outs.items():
-        f.field(n, out=buf)
+        g.field(n, out=buf)
     e1.record(stream)
     torch.cuda.synchronize()
     barrier()
-    se1 = f.stats()
+    se1 = g.stats()
+    g.close()
     ems = max_over_ranks(e0.elapsed_time(e1), world)
     e2e_value = whole_job_rate(N, ke, world, ems)
     h2d = 8.0
@@ -536,8 +547,8 @@ def main() -> None:
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": ke,
-                    # the leg continues the run right after the timed steps
-                    "after_steps": args.warmup + args.steps,
+                    # a second context: the same warm-up and the same steps as the timed leg
+                    "after_steps": args.warmup,
                     "mg_cycles_per_step": (se1["mg_cycles_total"] - se0["mg_cycles_total"]) / ke},
             "gpu_launches": int(st1["kernel_launches"] - st0["kernel_launches"]),
             "clocks": clocks,

@@ -141,6 +141,7 @@ struct fx_ctx {
     uint8_t *d_code = nullptr, *d_var = nullptr;
     uint8_t* d_interior = nullptr;       // DevParams::interior flags
     bool use_interior = true;            // fx.interior
+    bool adj_store_phi = true;           // fx.adjoint_store_phi
     Variant* d_vt = nullptr;
     double* d_P[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
     int cur = 0;
@@ -201,6 +202,7 @@ struct fx_ctx {
         double* finP[3] = {nullptr, nullptr, nullptr};
         double *finPhi = nullptr, *finRho = nullptr;
         std::vector<double*> segP, segPhi;         // 3 per segment step, 1 (semiconductor only)
+        double* phiAll = nullptr;                  // phi^n of every recorded step (n = 1..T), when it fits
         double* lam[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
         int lcur = 0;
         double *mu = nullptr, *psi = nullptr, *drho = nullptr, *grad = nullptr, *dV = nullptr, *hist = nullptr;
@@ -696,6 +698,21 @@ int compute_phi_rho(fx_ctx* c) { return compute_phi_rho_P(c, c->cur, false); }
 // main.cpp:280-348: Order 1 is one fused Euler pass; Order 2 is a predictor
 // pass (f^n kept, P* into the other buffer), ComputePhi_Rho at P*, and a
 // corrector pass P^{n+1} = P^n + dt (0.5 f^n + 0.5 f*) written over P^n
+// one Order-1 Euler update of P with a given phi (the segment recompute of
+// the gradient, from the recorded phi of that step)
+int tdgl_euler_with_phi(fx_ctx* c, const double* phi) {
+    const double* Pin[3];
+    P_in(c, Pin);
+    const int nb = 1 - c->cur;
+    double* Pout[3] = {c->scalarP ? nullptr : c->d_P[nb][0], c->scalarP ? nullptr : c->d_P[nb][1], c->d_P[nb][2]};
+    ++g_launches;
+    int r = k_status(c, launch_tdgl(c->dp, c->par.precision == 1, 0, c->d_code, c->d_var, c->d_vt, Pin, Pout, phi,
+                                    nullptr, nullptr, c->s));
+    if (r) return r;
+    c->cur = nb;
+    return FX_OK;
+}
+
 int tdgl_update(fx_ctx* c) {
     int r = ensure_device(c);
     if (r) return r;
@@ -1317,10 +1334,22 @@ int forward_record(fx_ctx* c, const fx_loss_spec* sp, double* loss) {
     if ((r = adj_alloc(c, &A.finPhi, c->N))) return r;
     if (sc && (r = adj_alloc(c, &A.finRho, c->N))) return r;
     if ((r = adj_alloc(c, &A.hist, 3 * (size_t)T))) return r;
+    // phi of every step, when it fits in three quarters of the free device
+    // memory: the backward's segment recompute is then the TDGL updates
+    // alone, with no Poisson or Newton solve (else it repeats the solves)
+    if (c->adj_store_phi) {
+        size_t freeb = 0, totalb = 0;
+        const size_t need = (size_t)T * c->N * sizeof(double);
+        if (cudaMemGetInfo(&freeb, &totalb) == cudaSuccess && need <= freeb / 4 * 3) {
+            if ((r = adj_alloc(c, &A.phiAll, (size_t)T * c->N))) return r;
+        }
+    }
 
     if ((r = adj_save(c, &A.ckP[0], A.ckPhi[0], A.ckRho[0]))) return r;
     for (int n = 1; n <= T; ++n) {
         if ((r = adj_step(c, A.V[n - 1]))) return r;
+        if (A.phiAll)
+            FX_CUDA(c, cudaMemcpyAsync(A.phiAll + (size_t)(n - 1) * c->N, c->d_phi, c->N * 8, cudaMemcpyDeviceToDevice, c->s));
         const double* Pin[3];
         P_in(c, Pin);
         ++g_launches;
@@ -1365,7 +1394,7 @@ int backward(fx_ctx* c, double* grads, int ngrads) {
         A.segPhi.assign(k, nullptr);
         for (int q = 0; q < k; ++q) {
             for (int d = d0; d < 3; ++d) if ((r = adj_alloc(c, &A.segP[3 * q + d], c->N))) return r;
-            if (sc && (r = adj_alloc(c, &A.segPhi[q], c->N))) return r;
+            if (sc && !A.phiAll && (r = adj_alloc(c, &A.segPhi[q], c->N))) return r;
         }
         for (int b = 0; b < 2; ++b)
             for (int d = d0; d < 3; ++d) if ((r = adj_alloc(c, &A.lam[b][d], c->N))) return r;
@@ -1401,9 +1430,14 @@ int backward(fx_ctx* c, double* grads, int ngrads) {
                 if ((r = dcopy(c, A.segP[3 * idx + d], c->d_P[c->cur][d]))) return r;
             c->Phi_Bc_hi = A.V[n - 1];
             electrode_values(c);
-            if ((r = compute_phi_rho(c))) return r;
-            if (sc && (r = dcopy(c, A.segPhi[idx], c->d_phi))) return r;
-            if ((r = tdgl_update(c))) return r;
+            if (A.phiAll) {
+                // the recorded phi^n: the same TDGL update as the forward's
+                if ((r = tdgl_euler_with_phi(c, A.phiAll + (size_t)(n - 1) * c->N))) return r;
+            } else {
+                if ((r = compute_phi_rho(c))) return r;
+                if (sc && (r = dcopy(c, A.segPhi[idx], c->d_phi))) return r;
+                if ((r = tdgl_update(c))) return r;
+            }
             c->prof.collect();
         }
         for (int n = end; n >= start + 1; --n) {
@@ -1421,7 +1455,8 @@ int backward(fx_ctx* c, double* grads, int ngrads) {
                 if (nmu > 0.0) {
                     if (sc) {
                         ++g_launches;
-                        r = k_status(c, launch_drho(c->dp, c->d_code, A.segPhi[idx], A.drho, A.drho32, c->s));
+                        const double* phin = A.phiAll ? A.phiAll + (size_t)(n - 1) * c->N : A.segPhi[idx];
+                        r = k_status(c, launch_drho(c->dp, c->d_code, phin, A.drho, A.drho32, c->s));
                         if (r) return r;
                         c->mg.set_alpha(A.drho, A.drho32, true, c->s);
                     } else {
@@ -1694,7 +1729,8 @@ int fx_get_param(const fx_ctx* c, const char* key, double* v) {
         {"adjoint_loss", c->adj.loss},
         {"fx.mg_nu1", (double)c->mg.nu1}, {"fx.mg_nu2", (double)c->mg.nu2},
         {"fx.mg_mixed_cycles", (double)c->mg.mixed_cycles}, {"fx.alpha_tiles", c->mg.alpha_tiles ? 1.0 : 0.0},
-        {"fx.interior", c->use_interior ? 1.0 : 0.0},
+        {"fx.interior", c->use_interior ? 1.0 : 0.0}, {"fx.adjoint_store_phi", c->adj_store_phi ? 1.0 : 0.0},
+        {"adjoint_phi_stored", c->adj.phiAll ? 1.0 : 0.0},
         {"step_graph_ran", c->sg_ran ? 1.0 : 0.0}, {"fx.pdl", g_pdl ? 1.0 : 0.0},
         // 1 when level 0's face coefficients depend on z only and its smoother
         // reads them by plane instead of from the material codes
@@ -1738,7 +1774,7 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
     static const char* const known[] = {
         "Phi_Bc_hi", "Phi_Bc_lo", "fx.mg_rtol", "fx.mg_max_iter", "fx.newton_max_iter", "fx.warm_start",
         "fx.phi_extrapolate", "fx.step_graph", "fx.pdl", "fx.verbose", "fx.profile", "fx.mg_nu1", "fx.graphs",
-        "fx.mg_nu2", "fx.alpha_tiles", "fx.interior", "fx.mg_mixed_cycles", "fx.phi_ghost_mode", "dt", "alpha", "fx.newton_tol",
+        "fx.mg_nu2", "fx.alpha_tiles", "fx.interior", "fx.adjoint_store_phi", "fx.mg_mixed_cycles", "fx.phi_ghost_mode", "dt", "alpha", "fx.newton_tol",
         "beta", "gamma", "g11", "g44", "BigGamma", "inc_step"};
     bool is_known = false;
     for (const char* q : known) is_known = is_known || k == q;
@@ -1760,7 +1796,7 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
     if (k == "fx.newton_tol" && !(v > 0.0))
         return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx.newton_tol must be positive");
     if (k != "fx.profile" && k != "fx.verbose" && k != "fx.graphs" && k != "fx.step_graph" && k != "fx.pdl" &&
-        k != "fx.alpha_tiles" && k != "fx.interior")
+        k != "fx.alpha_tiles" && k != "fx.interior" && k != "fx.adjoint_store_phi")
         ++c->gen;
     // the time history of phi only seeds the next solve's initial iterate;
     // electrode values are compared on their own, solver settings leave the
@@ -1782,6 +1818,7 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
     if (k == "fx.graphs") { c->mg.set_graphs(v != 0.0); return FX_OK; }
     if (k == "fx.mg_nu2") { c->mg.nu2 = (int)v; return FX_OK; }
     if (k == "fx.alpha_tiles") { c->mg.alpha_tiles = v != 0.0; return FX_OK; }
+    if (k == "fx.adjoint_store_phi") { c->adj_store_phi = v != 0.0; return FX_OK; }
     if (k == "fx.interior") {
         c->use_interior = v != 0.0;
         c->dp.interior = c->use_interior ? c->d_interior : nullptr;

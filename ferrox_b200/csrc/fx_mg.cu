@@ -126,19 +126,12 @@ __device__ __forceinline__ float sdiv(float a, float b) { return __fdividef(a, b
 // ZERO: the first half sweep (colour 0) from x = 0: the colour-0 value is
 // (b + electrode terms) / diag and the colour-1 cell of the same x pair is
 // set to 0, so the caller need not clear x first (even nx only)
-template <typename T, int KIND, bool ZERO = false>
-__global__ void __launch_bounds__(256) k_rbgs(Op<T> o, T* __restrict__ x, const T* __restrict__ b, int color) {
-    pdl_entry();
-    __shared__ T seps[8];
-    if (KIND == CK_FINE) {
-        if (threadIdx.x == 0 && threadIdx.y == 0)
-#pragma unroll
-            for (int q = 0; q < 8; ++q) seps[q] = o.eps[q];
-        __syncthreads();
-    }
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int k = blockIdx.z;
-    const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((j + k + color) & 1);
+// the update of one cell of a red-black half sweep: t indexes the x pair,
+// the cell is the pair's one of this colour
+template <typename T, int KIND, bool ZERO>
+__device__ __forceinline__ void rbgs_update(const Op<T>& o, T* __restrict__ x, const T* __restrict__ b, int color,
+                                            int t, int j, int k, const T* seps) {
+    const int i = 2 * t + ((j + k + color) & 1);
     if (j >= o.ny || i >= o.nx) return;
     const int c = i + o.nx * (j + o.ny * k);
     int im, ip, jm, jp;
@@ -157,6 +150,20 @@ __global__ void __launch_bounds__(256) k_rbgs(Op<T> o, T* __restrict__ x, const 
     if (k > 0) s += cb * x[c - o.nxy];
     if (k < o.nz - 1) s += ct * x[c + o.nxy];
     x[c] = sdiv(s, diag);
+}
+
+template <typename T, int KIND, bool ZERO = false>
+__global__ void __launch_bounds__(256) k_rbgs(Op<T> o, T* __restrict__ x, const T* __restrict__ b, int color) {
+    pdl_entry();
+    __shared__ T seps[8];
+    if (KIND == CK_FINE) {
+        if (threadIdx.x == 0 && threadIdx.y == 0)
+#pragma unroll
+            for (int q = 0; q < 8; ++q) seps[q] = o.eps[q];
+        __syncthreads();
+    }
+    rbgs_update<T, KIND, ZERO>(o, x, b, color, blockIdx.x * blockDim.x + threadIdx.x,
+                               blockIdx.y * blockDim.y + threadIdx.y, blockIdx.z, seps);
 }
 
 // red-black z-line Gauss-Seidel half sweep: color = parity of i + j; each
@@ -207,6 +214,42 @@ __global__ void __launch_bounds__(128) k_line(Op<T> o, T* __restrict__ x, const 
 // residual b - A x at the children of each coarse cell, averaged into the
 // coarse right-hand side; optionally the |r|_inf of the level.  RX, RY, RZ
 // are the coarsening ratios (1 or 2).
+// residual b - A x at the children of coarse cell (I, J, K), averaged into
+// bc; returns the largest |r| among them
+template <typename T, int KIND, int RX, int RY, int RZ>
+__device__ __forceinline__ double rr_cell(const Op<T>& o, const T* __restrict__ x, const T* __restrict__ b,
+                                          T* __restrict__ bc, int I, int J, int K, int ncx, int ncy, const T* seps) {
+    double mx = 0.0;
+    T s = T(0);
+#pragma unroll
+    for (int dk = 0; dk < RZ; ++dk)
+#pragma unroll
+        for (int dj = 0; dj < RY; ++dj)
+#pragma unroll
+            for (int di = 0; di < RX; ++di) {
+                const int i = RX * I + di, j = RY * J + dj, k = RZ * K + dk;
+                const int c = i + o.nx * (j + o.ny * k);
+                int im, ip, jm, jp;
+                nbr(i, o.nx, im, ip);
+                nbr(j, o.ny, jm, jp);
+                T cw, ce, cs, cn, cb, ct, diag, bcv;
+                coeffs<T, KIND>(o, i, j, k, c, im, ip, jm, jp, cw, ce, cs, cn, cb, ct, diag, bcv, seps);
+                const int row = c - i;
+                T off = cw * x[row + im] + ce * x[row + ip] + cs * x[c + (jm - j) * o.nx] +
+                        cn * x[c + (jp - j) * o.nx];
+                if (k > 0) off += cb * x[c - o.nxy];
+                if (k < o.nz - 1) off += ct * x[c + o.nxy];
+                const T r = (b[c] + bcv) - (diag * x[c] - off);
+                s += r;
+                mx = nan_max(mx, fabs((double)r));
+            }
+    bc[I + ncx * (J + ncy * K)] = s / T(RX * RY * RZ);
+    return mx;
+}
+
+// residual b - A x at the children of each coarse cell, averaged into the
+// coarse right-hand side; optionally the |r|_inf of the level.  RX, RY, RZ
+// are the coarsening ratios (1 or 2).
 template <typename T, int KIND, int RX, int RY, int RZ>
 __global__ void __launch_bounds__(256) k_resid_restrict(Op<T> o, const T* __restrict__ x, const T* __restrict__ b,
                                                         T* __restrict__ bc, int ncx, int ncy, int ncz,
@@ -223,32 +266,7 @@ __global__ void __launch_bounds__(256) k_resid_restrict(Op<T> o, const T* __rest
         __syncthreads();
     }
     double mx = 0.0;
-    if (I < ncx && J < ncy) {
-        T s = T(0);
-#pragma unroll
-        for (int dk = 0; dk < RZ; ++dk)
-#pragma unroll
-            for (int dj = 0; dj < RY; ++dj)
-#pragma unroll
-                for (int di = 0; di < RX; ++di) {
-                    const int i = RX * I + di, j = RY * J + dj, k = RZ * K + dk;
-                    const int c = i + o.nx * (j + o.ny * k);
-                    int im, ip, jm, jp;
-                    nbr(i, o.nx, im, ip);
-                    nbr(j, o.ny, jm, jp);
-                    T cw, ce, cs, cn, cb, ct, diag, bcv;
-                    coeffs<T, KIND>(o, i, j, k, c, im, ip, jm, jp, cw, ce, cs, cn, cb, ct, diag, bcv, seps);
-                    const int row = c - i;
-                    T off = cw * x[row + im] + ce * x[row + ip] + cs * x[c + (jm - j) * o.nx] +
-                            cn * x[c + (jp - j) * o.nx];
-                    if (k > 0) off += cb * x[c - o.nxy];
-                    if (k < o.nz - 1) off += ct * x[c + o.nxy];
-                    const T r = (b[c] + bcv) - (diag * x[c] - off);
-                    s += r;
-                    mx = nan_max(mx, fabs((double)r));
-                }
-        bc[I + ncx * (J + ncy * K)] = s / T(RX * RY * RZ);
-    }
+    if (I < ncx && J < ncy) mx = rr_cell<T, KIND, RX, RY, RZ>(o, x, b, bc, I, J, K, ncx, ncy, seps);
     if (norm) {
         const double m = block_max_all(mx);
         const int slot = (blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)) & (NORM_SLOTS - 1);
@@ -410,13 +428,9 @@ void launch_resid64(const Op<double>& o, dim3 g, dim3 b, cudaStream_t s, const d
 // far neighbour is the homogeneous Dirichlet value 0.  RX, RY, RZ are the
 // coarsening ratios (1 or 2), fixed at compile time.
 template <typename T, int RX, int RY, int RZ>
-__global__ void __launch_bounds__(256) k_prolong(T* __restrict__ xf, const T* __restrict__ xc, const float* __restrict__ wx,
-                                                 const float* __restrict__ wy, const float* __restrict__ wz, int nx, int ny,
-                                                 int nz, int ncx, int ncy, int ncz) {
-    pdl_entry();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int k = blockIdx.z;
+__device__ __forceinline__ void prolong_cell(T* __restrict__ xf, const T* __restrict__ xc, const float* __restrict__ wx,
+                                             const float* __restrict__ wy, const float* __restrict__ wz, int i, int j,
+                                             int k, int nx, int ny, int nz, int ncx, int ncy, int ncz) {
     if (i >= nx || j >= ny) return;
     const int fc = i + nx * (j + ny * k);
     const int I0 = RX == 2 ? (i >> 1) : i, J0 = RY == 2 ? (j >> 1) : j, K0 = RZ == 2 ? (k >> 1) : k;
@@ -461,6 +475,16 @@ __global__ void __launch_bounds__(256) k_prolong(T* __restrict__ xf, const T* __
         s = acc;
     }
     xf[fc] += s;
+}
+
+// the coarse correction interpolated into the finer level and added
+template <typename T, int RX, int RY, int RZ>
+__global__ void __launch_bounds__(256) k_prolong(T* __restrict__ xf, const T* __restrict__ xc, const float* __restrict__ wx,
+                                                 const float* __restrict__ wy, const float* __restrict__ wz, int nx, int ny,
+                                                 int nz, int ncx, int ncy, int ncz) {
+    pdl_entry();
+    prolong_cell<T, RX, RY, RZ>(xf, xc, wx, wy, wz, blockIdx.x * blockDim.x + threadIdx.x,
+                                blockIdx.y * blockDim.y + threadIdx.y, blockIdx.z, nx, ny, nz, ncx, ncy, ncz);
 }
 
 // ---------------------------------------------------------------------
@@ -688,10 +712,10 @@ __device__ __forceinline__ void cp_async_el(E* dst, const E* src) {
     else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
 }
 
+// The V-cycle of the shared-memory levels, run by one CTA on the shared
+// memory smraw.
 template <typename T>
-__global__ void __launch_bounds__(1024) k_coarse_vcycle(CoarseArgs A) {
-    pdl_entry();
-    extern __shared__ __align__(16) unsigned char smraw[];
+__device__ void coarse_cta_cycle(const CoarseArgs& A, unsigned char* smraw) {
     __shared__ int s_valid;
     T* sm = reinterpret_cast<T*>(smraw);
     float* sw = reinterpret_cast<float*>(smraw + A.wbase);
@@ -766,6 +790,13 @@ __global__ void __launch_bounds__(1024) k_coarse_vcycle(CoarseArgs A) {
     }
     T* x_out = (T*)A.x_out;
     for (int c = threadIdx.x; c < A.L[0].N; c += blockDim.x) x_out[c] = sm[A.L[0].ox + c];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(1024) k_coarse_vcycle(CoarseArgs A) {
+    pdl_entry();
+    extern __shared__ __align__(16) unsigned char smraw[];
+    coarse_cta_cycle<T>(A, smraw);
 }
 
 template <typename Tin, typename T>
@@ -1354,22 +1385,24 @@ void Multigrid::plan_coarse(bool want64, bool want32) {
 template <> int Multigrid::coarse_top<double>() const { return coarse_top64_; }
 template <> int Multigrid::coarse_top<float>() const { return coarse_top32_; }
 
+// the arguments of the one-CTA cycle for levels top .. bottom
 template <typename T>
-void Multigrid::launch_coarse(int top, cudaStream_t s) {
+static CoarseArgs make_coarse_args(const std::vector<MGLevel>& lev_, int top, int nu1, int nu2, int nu_bottom,
+                                   bool has_alpha_, int* d_fvalid_) {
     CoarseArgs A;
     std::memset(&A, 0, sizeof(A));
     const size_t es = sizeof(T);
     size_t wbase = 0;
-    const size_t bytes = coarse_bytes(lev_, top, es, &wbase);
+    coarse_bytes(lev_, top, es, &wbase);
     A.nlev = (int)lev_.size() - top;
     A.nu1 = nu1; A.nu2 = nu2; A.nu_bottom = nu_bottom;
     A.wbase = (long long)wbase;
-    A.b_in = lb<T>(lev_[top]);
-    A.x_out = lx<T>(lev_[top]);
+    A.b_in = lb<T>(const_cast<MGLevel&>(lev_[top]));
+    A.x_out = lx<T>(const_cast<MGLevel&>(lev_[top]));
     A.fvalid = d_fvalid_ + (sizeof(T) == 8 ? 0 : 1);
     long long off = 0, woff = 0;
     for (int q = 0; q < A.nlev; ++q) {
-        MGLevel& L = lev_[top + q];
+        const MGLevel& L = lev_[top + q];
         CoarseLevelDesc& d = A.L[q];
         const long long N = (long long)L.N, nxy = (long long)L.n[0] * L.n[1];
         d.nx = L.n[0]; d.ny = L.n[1]; d.nz = L.n[2]; d.N = (int)N; d.line = L.line;
@@ -1401,6 +1434,13 @@ void Multigrid::launch_coarse(int top, cudaStream_t s) {
             d.rx = d.ry = d.rz = 1;
         }
     }
+    return A;
+}
+
+template <typename T>
+void Multigrid::launch_coarse(int top, cudaStream_t s) {
+    const CoarseArgs A = make_coarse_args<T>(lev_, top, nu1, nu2, nu_bottom, has_alpha_, d_fvalid_);
+    const size_t bytes = coarse_bytes(lev_, top, sizeof(T), nullptr);
     if (prof) prof->begin(PROF_COARSE_CTA, s);
     ++g_launches;
     launch_k(k_coarse_vcycle<T>, 1, 1024, bytes, s, A);

@@ -124,6 +124,7 @@ public:
     int nu1 = 2, nu2 = 1, nu_bottom = 40;
     int mixed_cycles = 2;    // FP32 V-cycles per FP64 refinement step
     bool alpha_tiles = true; // coarse alphas below level 1 in one launch (k_alpha_tiles)
+
     static constexpr int kMaxLev = 24;
     Prof* prof = nullptr;
     int verbose = 0;
@@ -159,6 +160,7 @@ private:
     bool use_graphs_ = true;
     template <typename F> int replay(GraphCache& g, const void* x, const void* rhs, const DevParams& p, cudaStream_t s, F&& enqueue);
     int coarse_top64_ = -1, coarse_top32_ = -1;   // first level run by the one-CTA kernel
+
     int* d_fvalid_ = nullptr;    // [0] FP64, [1] FP32: the one-CTA factors in global memory are current
     // k_alpha_tiles: tile level (0: per-level launches), level-l cells per
     // tile, the largest staged tile, and the last-block counter

@@ -244,3 +244,27 @@ def test_refused_calls_keep_the_recorded_run():
     g1 = f.backward()
     assert np.allclose(g1, g0, rtol=1e-12, atol=0.0), (g0, g1)
     f.close()
+
+
+@pytest.mark.parametrize("sc", [False, True], ids=["mfim", "mfism"])
+def test_stored_phi_recompute_matches_solve_recompute(sc):
+    """With phi of every recorded step kept in device memory
+    (fx.adjoint_store_phi = 1, when it fits), the backward recomputes each
+    segment's P with the TDGL updates alone; without it, with the Newton and
+    Poisson solves as well.  The recomputed states are the recorded ones
+    either way, so the gradients agree (to the order in which the parameter
+    sums' atomic additions land)."""
+    if sc:
+        text = decks.mfism(16, 16, 48, extra={"Phi_Bc_hi": 0.3, "fx.newton_tol": 1e-11})
+    else:
+        text = decks.hysteresis(16, 16, 12, v_amp=1.0, steps_per_leg=8)
+    shape, target = sweep(16)
+    out = []
+    for store in (0, 1):
+        f = api.FerroX(text)
+        f.set_param("fx.adjoint_store_phi", store)
+        f.forward_record(target, 1.0 if not sc else 0.3, shape, 5)
+        assert f.param("adjoint_phi_stored") == store
+        out.append(f.backward())
+        f.close()
+    assert np.allclose(out[0], out[1], rtol=1e-11, atol=0.0), out
