@@ -142,6 +142,8 @@ struct fx_ctx {
     uint8_t* d_interior = nullptr;       // DevParams::interior flags
     bool use_interior = true;            // fx.interior
     bool adj_store_phi = true;           // fx.adjoint_store_phi
+    double* adj_phi_store = nullptr;     // the record's phi of every step; kept between records
+    size_t adj_phi_store_n = 0;          // its length in doubles
     Variant* d_vt = nullptr;
     double* d_P[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
     int cur = 0;
@@ -943,7 +945,7 @@ std::vector<unsigned char> sg_key(const fx_ctx* c, int use) {
     const int iv[] = {c->cur, use, c->par.TimeIntegratorOrder, c->par.precision, c->par.warm_start,
                       c->par.phi_extrapolate, c->par.newton_max_iter, c->par.mg_max_iter, c->mg.nu1, c->mg.nu2,
                       c->mg.mixed_cycles, c->scalarP ? 1 : 0, c->contains_sc ? 1 : 0, g_pdl ? 1 : 0,
-                      c->mg.alpha_tiles ? 1 : 0};
+                      c->mg.alpha_tiles ? 1 : 0, c->mg.nu1c, c->mg.nu2c};
     put(iv, sizeof(iv));
     const double dv[] = {c->par.mg_rtol, c->par.newton_tol};
     put(dv, sizeof(dv));
@@ -1338,11 +1340,24 @@ int forward_record(fx_ctx* c, const fx_loss_spec* sp, double* loss) {
     // memory: the backward's segment recompute is then the TDGL updates
     // alone, with no Poisson or Newton solve (else it repeats the solves)
     if (c->adj_store_phi) {
-        size_t freeb = 0, totalb = 0;
-        const size_t need = (size_t)T * c->N * sizeof(double);
-        if (cudaMemGetInfo(&freeb, &totalb) == cudaSuccess && need <= freeb / 4 * 3) {
-            if ((r = adj_alloc(c, &A.phiAll, (size_t)T * c->N))) return r;
+        const size_t need = (size_t)T * c->N;
+        if (c->adj_phi_store && c->adj_phi_store_n < need) {
+            cudaStreamSynchronize(c->s);
+            cudaFree(c->adj_phi_store);
+            c->adj_phi_store = nullptr;
+            c->adj_phi_store_n = 0;
         }
+        if (!c->adj_phi_store) {
+            size_t freeb = 0, totalb = 0;
+            if (cudaMemGetInfo(&freeb, &totalb) == cudaSuccess && need * sizeof(double) <= freeb / 4 * 3 &&
+                cudaMalloc(&c->adj_phi_store, need * sizeof(double)) == cudaSuccess)
+                c->adj_phi_store_n = need;
+            else
+                c->adj_phi_store = nullptr;
+            cudaGetLastError();
+        }
+        A.phiAll = c->adj_phi_store;
+        if (A.phiAll) A.bytes += need * sizeof(double);
     }
 
     if ((r = adj_save(c, &A.ckP[0], A.ckPhi[0], A.ckRho[0]))) return r;
@@ -1590,6 +1605,13 @@ int fx_create(const char* inputs, int is_text, fx_ctx** out) {
         c->in = parse_inputs(text);
         c->par = make_params(c->in);
         Params& p = c->par;
+        {
+            // the AMReX cut-cell Poisson path (ElectrostaticSolver.cpp:613-676) is not restated
+            auto it = c->in.table.find("domain.embedded_boundary");
+            if (it != c->in.table.end() && !it->second.empty() && eval_number(it->second[0], c->in.constants) != 0.0)
+                throw FxError{FX_ERR_UNSUPPORTED, "domain.embedded_boundary = 1 (the cut-cell Poisson solver of "
+                                                  "AMReX MLEBABecLap) is not supported"};
+        }
         if (!p.is_periodic[0] || !p.is_periodic[1] || p.is_periodic[2])
             throw FxError{FX_ERR_UNSUPPORTED, "only domain.is_periodic = 1 1 0 (periodic x/y, electrodes in z) is supported"};
         for (int d = 0; d < 2; ++d)
@@ -1665,6 +1687,7 @@ void fx_destroy(fx_ctx* c) {
     if (c->dev) {
         cudaStreamSynchronize(c->s);
         adj_free(c);
+        cudaFree(c->adj_phi_store);
         cudaFree(c->d_code); cudaFree(c->d_var); cudaFree(c->d_vt); cudaFree(c->d_interior);
         for (int b = 0; b < 2; ++b)
             for (int d = 0; d < 3; ++d) cudaFree(c->d_P[b][d]);
@@ -1774,7 +1797,7 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
     static const char* const known[] = {
         "Phi_Bc_hi", "Phi_Bc_lo", "fx.mg_rtol", "fx.mg_max_iter", "fx.newton_max_iter", "fx.warm_start",
         "fx.phi_extrapolate", "fx.step_graph", "fx.pdl", "fx.verbose", "fx.profile", "fx.mg_nu1", "fx.graphs",
-        "fx.mg_nu2", "fx.alpha_tiles", "fx.interior", "fx.adjoint_store_phi", "fx.mg_mixed_cycles", "fx.phi_ghost_mode", "dt", "alpha", "fx.newton_tol",
+        "fx.mg_nu2", "fx.alpha_tiles", "fx.interior", "fx.adjoint_store_phi", "fx.mg_zline", "fx.mg_nu1_coarse", "fx.mg_nu2_coarse", "fx.mg_mixed_cycles", "fx.phi_ghost_mode", "dt", "alpha", "fx.newton_tol",
         "beta", "gamma", "g11", "g44", "BigGamma", "inc_step"};
     bool is_known = false;
     for (const char* q : known) is_known = is_known || k == q;
@@ -1787,6 +1810,10 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
         return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx.phi_ghost_mode must be 0 (extrap), 1 (face) or 2 (zero)");
     if ((k == "fx.mg_max_iter" || k == "fx.newton_max_iter") && !(v >= 1))
         return set_err(c, FX_ERR_INVALID_ARGUMENT, k + " must be at least 1");
+    if (k == "fx.mg_nu1_coarse" && !(v == -1 || v >= 1))
+        return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx.mg_nu1_coarse must be -1 (as fx.mg_nu1) or at least 1");
+    if (k == "fx.mg_nu2_coarse" && !(v >= -1))
+        return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx.mg_nu2_coarse must be -1 (as fx.mg_nu2) or at least 0");
     if ((k == "fx.mg_nu1" || k == "fx.mg_nu2") && !(v >= 0))
         return set_err(c, FX_ERR_INVALID_ARGUMENT, k + " must not be negative");
     if (k == "fx.mg_rtol" && !(v > 0))
@@ -1795,6 +1822,8 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
         return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx.mg_mixed_cycles must be at least 1");
     if (k == "fx.newton_tol" && !(v > 0.0))
         return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx.newton_tol must be positive");
+    if (k == "fx.mg_zline" && c->dev)
+        return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx.mg_zline must be set before the first device call");
     if (k != "fx.profile" && k != "fx.verbose" && k != "fx.graphs" && k != "fx.step_graph" && k != "fx.pdl" &&
         k != "fx.alpha_tiles" && k != "fx.interior" && k != "fx.adjoint_store_phi")
         ++c->gen;
@@ -1819,6 +1848,9 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
     if (k == "fx.mg_nu2") { c->mg.nu2 = (int)v; return FX_OK; }
     if (k == "fx.alpha_tiles") { c->mg.alpha_tiles = v != 0.0; return FX_OK; }
     if (k == "fx.adjoint_store_phi") { c->adj_store_phi = v != 0.0; return FX_OK; }
+    if (k == "fx.mg_zline") { c->mg.zline_first = v != 0.0; return FX_OK; }
+    if (k == "fx.mg_nu1_coarse") { c->mg.nu1c = (int)v; return FX_OK; }
+    if (k == "fx.mg_nu2_coarse") { c->mg.nu2c = (int)v; return FX_OK; }
     if (k == "fx.interior") {
         c->use_interior = v != 0.0;
         c->dp.interior = c->use_interior ? c->d_interior : nullptr;

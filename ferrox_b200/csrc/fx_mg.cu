@@ -1049,7 +1049,12 @@ int Multigrid::setup(const DevParams& p, const std::vector<uint8_t>& code, bool 
     while (true) {
         MGLevel& f = lev_.back();
         const double hmin = std::min(f.h[0], std::min(f.h[1], f.h[2]));
-        const bool cz = f.n[2] % 2 == 0 && f.h[2] <= 1.5 * hmin;
+        // zline_first: where z is the strongly coupled direction, keep z and
+        // smooth with z-lines while x and y coarsen (instead of coarsening z
+        // until the spacings meet)
+        const bool zstrong = 1.5 * f.h[2] < std::min(f.h[0], f.h[1]);
+        const bool cz = f.n[2] % 2 == 0 && f.h[2] <= 1.5 * hmin && !(zline_first && zstrong &&
+                                                                       (coarsenable_xy(f.n[0]) || coarsenable_xy(f.n[1])));
         int cr[3] = {1, 1, 1};
         if (cz) {
             cr[2] = 2;
@@ -1513,7 +1518,7 @@ void Multigrid::vcycle(const DevParams& p, const uint8_t* code, int l, T* x, con
         return;
     }
     if (zero && !zero_first_ok(L)) cudaMemsetAsync(x, 0, L.N * sizeof(T), s);
-    smooth<T>(p, code, l, x, b, inhom, nu1, s, zero && zero_first_ok(L));
+    smooth<T>(p, code, l, x, b, inhom, (l > 0 && nu1c >= 0) ? nu1c : nu1, s, zero && zero_first_ok(L));
     MGLevel& C = lev_[l + 1];
     const T* a = nullptr;
     if (has_alpha_) {
@@ -1564,7 +1569,7 @@ void Multigrid::vcycle(const DevParams& p, const uint8_t* code, int l, T* x, con
 #undef FX_PR
     }
     if (prof) prof->end(s);
-    smooth<T>(p, code, l, x, b, inhom, nu2, s, false);
+    smooth<T>(p, code, l, x, b, inhom, (l > 0 && nu2c >= 0) ? nu2c : nu2, s, false);
 }
 
 int Multigrid::residual64(const DevParams& p, const uint8_t* code, const double* phi, const double* rhs, double* r,
@@ -1592,7 +1597,7 @@ int Multigrid::replay(GraphCache& g, const void* x, const void* rhs, const DevPa
         return (int)cudaGetLastError();
     }
     if (!g.exec || g.x != x || g.rhs != rhs || g.has_alpha != has_alpha_ || g.vlo != p.V_lo || g.vhi != p.V_hi ||
-        g.nu1 != nu1 || g.nu2 != nu2 || g.pdl != g_pdl) {
+        g.nu1 != nu1 || g.nu2 != nu2 || g.nu1c != nu1c || g.nu2c != nu2c || g.pdl != g_pdl) {
         if (g.exec) { cudaGraphExecDestroy(g.exec); g.exec = nullptr; }
         cudaGraph_t graph;
         const long long l0 = g_launches.load();
@@ -1607,6 +1612,7 @@ int Multigrid::replay(GraphCache& g, const void* x, const void* rhs, const DevPa
         cudaGraphDestroy(graph);
         if (e) return (int)e;
         g.x = x; g.rhs = rhs; g.has_alpha = has_alpha_; g.vlo = p.V_lo; g.vhi = p.V_hi; g.nu1 = nu1; g.nu2 = nu2;
+        g.nu1c = nu1c; g.nu2c = nu2c;
         g.pdl = g_pdl;
     }
     g_launches += g.launches;

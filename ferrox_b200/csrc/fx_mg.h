@@ -122,8 +122,10 @@ public:
     size_t bytes() const { return bytes_; }
     const std::vector<MGLevel>& levels() const { return lev_; }
     int nu1 = 2, nu2 = 1, nu_bottom = 40;
+    int nu1c = -1, nu2c = -1;   // sweeps on the levels below level 0 (-1: nu1 / nu2); the one-CTA levels use nu1 / nu2
     int mixed_cycles = 2;    // FP32 V-cycles per FP64 refinement step
     bool alpha_tiles = true; // coarse alphas below level 1 in one launch (k_alpha_tiles)
+    bool zline_first = false; // z-line smoothing with x/y coarsening where z is strongly coupled (set before setup)
 
     static constexpr int kMaxLev = 24;
     Prof* prof = nullptr;
@@ -152,7 +154,7 @@ private:
         const void* rhs = nullptr;
         bool has_alpha = false;
         double vlo = 0, vhi = 0;
-        int nu1 = 0, nu2 = 0;
+        int nu1 = 0, nu2 = 0, nu1c = 0, nu2c = 0;
         bool pdl = false;
         long long launches = 0;
     };
