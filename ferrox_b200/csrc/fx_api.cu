@@ -536,6 +536,7 @@ int ensure_device(fx_ctx* c) {
     if (st == -2) return set_err(c, FX_ERR_OUT_OF_MEMORY, "multigrid allocation failed");
     if (st != 0) return set_err(c, FX_ERR_CUDA, "multigrid setup failed");
     c->dev_bytes += c->mg.bytes();
+    c->mg.prepare_lines(c->dp, c->d_code, c->s);
     c->mg_ready = true;
     c->dev = true;
     FX_CUDA(c, cudaDeviceSynchronize());

@@ -97,6 +97,9 @@ public:
     ~Multigrid();
     // builds the hierarchy and uploads the coarse face coefficients
     int setup(const DevParams& p, const std::vector<uint8_t>& code_host, bool want64, bool want32);
+    // the device material codes and parameters for the z-line factors (after
+    // setup, before the first solve); forms the factors of the launched z-line levels
+    void prepare_lines(const DevParams& p, const uint8_t* code, cudaStream_t s);
     // alpha changed on level 0 (device, FP64 and FP32 copies): average down
     int set_alpha(const double* a64, const float* a32, bool has_alpha, cudaStream_t s);
     // FP64 solve of A phi = rhs (+ electrode terms) to |r|_inf <= target
@@ -134,6 +137,10 @@ public:
 
 private:
     std::vector<MGLevel> lev_;
+    const uint8_t* code_dev_ = nullptr;   // level 0's material codes (device), for the z-line factors
+    DevParams dp_lines_{};
+    size_t line_smem_max_ = 0;            // dynamic shared memory the z-line tile kernel may take
+    void factor_lines(cudaStream_t s);
     double eps_[8];
     const double* a0_64 = nullptr;
     const float* a0_32 = nullptr;
