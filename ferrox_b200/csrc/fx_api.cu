@@ -536,7 +536,6 @@ int ensure_device(fx_ctx* c) {
     if (st == -2) return set_err(c, FX_ERR_OUT_OF_MEMORY, "multigrid allocation failed");
     if (st != 0) return set_err(c, FX_ERR_CUDA, "multigrid setup failed");
     c->dev_bytes += c->mg.bytes();
-    c->mg.prepare_lines(c->dp, c->d_code, c->s);
     c->mg_ready = true;
     c->dev = true;
     FX_CUDA(c, cudaDeviceSynchronize());
@@ -1798,7 +1797,7 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
     static const char* const known[] = {
         "Phi_Bc_hi", "Phi_Bc_lo", "fx.mg_rtol", "fx.mg_max_iter", "fx.newton_max_iter", "fx.warm_start",
         "fx.phi_extrapolate", "fx.step_graph", "fx.pdl", "fx.verbose", "fx.profile", "fx.mg_nu1", "fx.graphs",
-        "fx.mg_nu2", "fx.alpha_tiles", "fx.interior", "fx.adjoint_store_phi", "fx.mg_zline", "fx.mg_nu1_coarse", "fx.mg_nu2_coarse", "fx.mg_mixed_cycles", "fx.phi_ghost_mode", "dt", "alpha", "fx.newton_tol",
+        "fx.mg_nu2", "fx.alpha_tiles", "fx.interior", "fx.adjoint_store_phi", "fx.mg_nu1_coarse", "fx.mg_nu2_coarse", "fx.mg_mixed_cycles", "fx.phi_ghost_mode", "dt", "alpha", "fx.newton_tol",
         "beta", "gamma", "g11", "g44", "BigGamma", "inc_step"};
     bool is_known = false;
     for (const char* q : known) is_known = is_known || k == q;
@@ -1823,8 +1822,6 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
         return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx.mg_mixed_cycles must be at least 1");
     if (k == "fx.newton_tol" && !(v > 0.0))
         return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx.newton_tol must be positive");
-    if (k == "fx.mg_zline" && c->dev)
-        return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx.mg_zline must be set before the first device call");
     if (k != "fx.profile" && k != "fx.verbose" && k != "fx.graphs" && k != "fx.step_graph" && k != "fx.pdl" &&
         k != "fx.alpha_tiles" && k != "fx.interior" && k != "fx.adjoint_store_phi")
         ++c->gen;
@@ -1849,7 +1846,6 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
     if (k == "fx.mg_nu2") { c->mg.nu2 = (int)v; return FX_OK; }
     if (k == "fx.alpha_tiles") { c->mg.alpha_tiles = v != 0.0; return FX_OK; }
     if (k == "fx.adjoint_store_phi") { c->adj_store_phi = v != 0.0; return FX_OK; }
-    if (k == "fx.mg_zline") { c->mg.zline_first = v != 0.0; return FX_OK; }
     if (k == "fx.mg_nu1_coarse") { c->mg.nu1c = (int)v; return FX_OK; }
     if (k == "fx.mg_nu2_coarse") { c->mg.nu2c = (int)v; return FX_OK; }
     if (k == "fx.interior") {

@@ -211,116 +211,9 @@ __global__ void __launch_bounds__(128) k_line(Op<T> o, T* __restrict__ x, const 
     }
 }
 
-// The z-line smoother in factored form.  A level's z-line systems
-// (diag_k x_k - cb_k x_{k-1} - ct_k x_{k+1} = r_k) depend only on the
-// operator, so their elimination factors are formed once, one column per
-// thread: den_k = diag_k - cb_k q_{k-1}, q_k = ct_k / den_k, inv_k = 1 / den_k,
-// p_k = cb_k / den_k (again only when alpha changes).  A half sweep is then
-// (1) every cell of the colour's columns: x_k = r_k inv_k from its x/y
-// neighbours (the other colour), in parallel; (2) per column the recurrences
-// d_k = x_k + p_k d_{k-1}, x_k = d_k + q_k x_{k+1}.
-template <typename T, int KIND>
-__global__ void __launch_bounds__(128) k_line_factor(Op<T> o, T* __restrict__ q, T* __restrict__ inv,
-                                                     T* __restrict__ p) {
-    pdl_entry();
-    __shared__ T seps[8];
-    if (KIND == CK_FINE) {
-        if (threadIdx.x == 0 && threadIdx.y == 0)
-#pragma unroll
-            for (int e = 0; e < 8; ++e) seps[e] = o.eps[e];
-        __syncthreads();
-    }
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= o.nx || j >= o.ny) return;
-    int im, ip, jm, jp;
-    nbr(i, o.nx, im, ip);
-    nbr(j, o.ny, jm, jp);
-    T qprev = T(0);
-    int c = i + o.nx * j;
-    for (int k = 0; k < o.nz; ++k, c += o.nxy) {
-        T cw, ce, cs, cn, cb, ct, diag, bcv;
-        coeffs<T, KIND>(o, i, j, k, c, im, ip, jm, jp, cw, ce, cs, cn, cb, ct, diag, bcv, seps);
-        const T iv = T(1) / (diag - cb * qprev);
-        const T qk = ct * iv;
-        q[c] = qk;
-        inv[c] = iv;
-        p[c] = cb * iv;
-        qprev = qk;
-    }
-}
-
-// One factored z-line half sweep per launch: a block takes LT columns of the
-// colour in one row (x pairs t0 .. t0 + LT - 1) over all nz planes.  (1) All
-// its threads form g_k = r_k inv_k for the tile's cells from their x/y
-// neighbours (the other colour, which this half sweep does not change) into
-// shared memory, with the factors p and q beside them; (2) LT threads run the
-// column recurrences d_k = g_k + p_k d_{k-1}, x_k = d_k + q_k x_{k+1} in
-// shared memory; (3) all threads write the tile back.  Shared memory:
-// 3 nz LT elements of T (dynamic).
-constexpr int LT = 32;
-
-template <typename T, int KIND>
-__global__ void __launch_bounds__(256) k_line_tile(Op<T> o, T* __restrict__ x, const T* __restrict__ b,
-                                                   const T* __restrict__ q, const T* __restrict__ inv,
-                                                   const T* __restrict__ p, int color) {
-    pdl_entry();
-    extern __shared__ __align__(16) unsigned char lsm[];
-    T* sg = reinterpret_cast<T*>(lsm);
-    T* sp = sg + o.nz * LT;
-    T* sq = sp + o.nz * LT;
-    __shared__ T seps[8];
-    if (KIND == CK_FINE) {
-        if (threadIdx.x == 0)
-#pragma unroll
-            for (int e = 0; e < 8; ++e) seps[e] = o.eps[e];
-        __syncthreads();
-    }
-    const int j = blockIdx.y;
-    const int t0 = blockIdx.x * LT;
-    const int hx = o.nx / 2;
-    const int par = (j + color) & 1;
-    int jm, jp;
-    nbr(j, o.ny, jm, jp);
-    const int nel = o.nz * LT;
-    for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-        const int w = e % LT, k = e / LT, t = t0 + w;
-        if (t >= hx) continue;
-        const int i = 2 * t + par;
-        const int c = i + o.nx * (j + o.ny * k);
-        int im, ip;
-        nbr(i, o.nx, im, ip);
-        T cw, ce, cs, cn, cb, ct, diag, bcv;
-        coeffs<T, KIND>(o, i, j, k, c, im, ip, jm, jp, cw, ce, cs, cn, cb, ct, diag, bcv, seps);
-        const int row = c - i;
-        const T r = b[c] + bcv + cw * x[row + im] + ce * x[row + ip] + cs * x[c + (jm - j) * o.nx] +
-                    cn * x[c + (jp - j) * o.nx];
-        sg[e] = r * inv[c];
-        sp[e] = p[c];
-        sq[e] = q[c];
-    }
-    __syncthreads();
-    if (threadIdx.x < LT && t0 + (int)threadIdx.x < hx) {
-        const int w = threadIdx.x;
-        T d = sg[w];
-        for (int k = 1; k < o.nz; ++k) {
-            d = sg[k * LT + w] + sp[k * LT + w] * d;
-            sg[k * LT + w] = d;
-        }
-        T xn = d;
-        for (int k = o.nz - 2; k >= 0; --k) {
-            xn = sg[k * LT + w] + sq[k * LT + w] * xn;
-            sg[k * LT + w] = xn;
-        }
-    }
-    __syncthreads();
-    for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-        const int w = e % LT, k = e / LT, t = t0 + w;
-        if (t >= hx) continue;
-        x[2 * t + par + o.nx * (j + o.ny * k)] = sg[e];
-    }
-}
-
+// residual b - A x at the children of each coarse cell, averaged into the
+// coarse right-hand side; optionally the |r|_inf of the level.  RX, RY, RZ
+// are the coarsening ratios (1 or 2).
 // residual b - A x at the children of coarse cell (I, J, K), averaged into
 // bc; returns the largest |r| among them
 template <typename T, int KIND, int RX, int RY, int RZ>
@@ -1156,12 +1049,7 @@ int Multigrid::setup(const DevParams& p, const std::vector<uint8_t>& code, bool 
     while (true) {
         MGLevel& f = lev_.back();
         const double hmin = std::min(f.h[0], std::min(f.h[1], f.h[2]));
-        // zline_first: where z is the strongly coupled direction, keep z and
-        // smooth with z-lines while x and y coarsen (instead of coarsening z
-        // until the spacings meet)
-        const bool zstrong = 1.5 * f.h[2] < std::min(f.h[0], f.h[1]);
-        const bool cz = f.n[2] % 2 == 0 && f.h[2] <= 1.5 * hmin && !(zline_first && zstrong &&
-                                                                       (coarsenable_xy(f.n[0]) || coarsenable_xy(f.n[1])));
+        const bool cz = f.n[2] % 2 == 0 && f.h[2] <= 1.5 * hmin;
         int cr[3] = {1, 1, 1};
         if (cz) {
             cr[2] = 2;
@@ -1406,51 +1294,15 @@ int Multigrid::setup(const DevParams& p, const std::vector<uint8_t>& code, bool 
     return 0;
 }
 
-// the elimination factors of the launched z-line levels for the current
-// operator (alpha included)
-void Multigrid::factor_lines(cudaStream_t s) {
-    for (int l = 0; l < (int)lev_.size(); ++l) {
-        MGLevel& L = lev_[l];
-        if (!L.line) continue;
-        dim3 b(32, 4), g((L.n[0] + 31) / 32, (L.n[1] + 3) / 4);
-        auto run = [&](auto tag, auto** fac, int top) {
-            using T = decltype(tag);
-            if (!fac[0] || (top > 0 && l >= top)) return;
-            const T* a = nullptr;
-            if (has_alpha_) {
-                if (l == 0) { if constexpr (sizeof(T) == 8) a = (const T*)a0_64; else a = (const T*)a0_32; }
-                else a = la<T>(L);
-            }
-            Op<T> o = make_op<T>(L, l, code_dev_, eps_, a, false, dp_lines_);
-            ++g_launches;
-            if (o.zc) launch_k(k_line_factor<T, CK_PLANES>, g, b, 0, s, o, (T*)fac[0], (T*)fac[1], (T*)fac[2]);
-            else if (l == 0) launch_k(k_line_factor<T, CK_FINE>, g, b, 0, s, o, (T*)fac[0], (T*)fac[1], (T*)fac[2]);
-            else launch_k(k_line_factor<T, CK_ARRAYS>, g, b, 0, s, o, (T*)fac[0], (T*)fac[1], (T*)fac[2]);
-        };
-        run(double(0), L.fac64, coarse_top64_);
-        run(float(0), L.fac32, coarse_top32_);
-    }
-}
-
-void Multigrid::prepare_lines(const DevParams& p, const uint8_t* code, cudaStream_t s) {
-    code_dev_ = code;
-    dp_lines_ = p;
-    factor_lines(s);
-}
-
 int Multigrid::set_alpha(const double* a64, const float* a32, bool has_alpha, cudaStream_t s) {
     // the one-CTA factors depend on alpha: recompute them at the next call
     // (the tile kernel below clears the flags itself)
     const bool tiles = has_alpha && at_T_ >= 2 && alpha_tiles;
     if ((has_alpha || has_alpha_) && d_fvalid_ && !tiles) cudaMemsetAsync(d_fvalid_, 0, 2 * sizeof(int), s);
-    const bool had_alpha = has_alpha_;
     a0_64 = a64;
     a0_32 = a32;
     has_alpha_ = has_alpha;
-    if (!has_alpha) {
-        if (had_alpha && code_dev_) factor_lines(s);   // back to the operator without alpha
-        return 0;
-    }
+    if (!has_alpha) return 0;
     const size_t lmax = tiles ? 2 : lev_.size();   // per-level launches below this level
     for (size_t l = 1; l < lmax; ++l) {
         MGLevel& L = lev_[l];
@@ -1482,7 +1334,6 @@ int Multigrid::set_alpha(const double* a64, const float* a32, bool has_alpha, cu
         ++g_launches;
         launch_k(k_alpha_tiles, (unsigned)LT.N, 256, (size_t)at_cap_ * 24, s, A);
     }
-    if (code_dev_) factor_lines(s);
     return (int)cudaGetLastError();
 }
 
@@ -1518,14 +1369,6 @@ void Multigrid::plan_coarse(bool want64, bool want32) {
         cudaFuncSetAttribute(k_coarse_vcycle<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coarse_smem64_);
     if (coarse_top32_ > 0)
         cudaFuncSetAttribute(k_coarse_vcycle<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coarse_smem32_);
-    // the z-line tile kernel: up to the per-block maximum of shared memory
-    line_smem_max_ = budget;
-    for (auto f : {(const void*)k_line_tile<double, CK_FINE>, (const void*)k_line_tile<double, CK_PLANES>,
-                   (const void*)k_line_tile<double, CK_ARRAYS>, (const void*)k_line_tile<float, CK_FINE>,
-                   (const void*)k_line_tile<float, CK_PLANES>, (const void*)k_line_tile<float, CK_ARRAYS>})
-        if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)budget) != cudaSuccess)
-            line_smem_max_ = 0;
-    cudaGetLastError();
     // global copies of the one-CTA levels' smoother factors (q and p only on
     // z-line levels), and the flags that say whether they are current
     for (int l = 0; l < (int)lev_.size(); ++l) {
@@ -1535,11 +1378,6 @@ void Multigrid::plan_coarse(bool want64, bool want32) {
             if (coarse_top64_ > 0 && l >= coarse_top64_ && n[k]) L.fac64[k] = dalloc<double>(n[k], bytes_);
             if (coarse_top32_ > 0 && l >= coarse_top32_ && n[k]) L.fac32[k] = dalloc<float>(n[k], bytes_);
         }
-        // the launched z-line levels keep their factors too (k_line_factor)
-        if (L.line && (l < coarse_top64_ || coarse_top64_ < 0) && want64 && !L.fac64[0])
-            for (int k = 0; k < 3; ++k) L.fac64[k] = dalloc<double>(L.N, bytes_);
-        if (L.line && (l < coarse_top32_ || coarse_top32_ < 0) && want32 && !L.fac32[0])
-            for (int k = 0; k < 3; ++k) L.fac32[k] = dalloc<float>(L.N, bytes_);
     }
     if (cudaMalloc(&d_fvalid_, 2 * sizeof(int)) == cudaSuccess) cudaMemset(d_fvalid_, 0, 2 * sizeof(int));
 }
@@ -1623,24 +1461,7 @@ void Multigrid::smooth(const DevParams& p, const uint8_t* code, int l, T* x, con
         else a = la<T>(L);
     }
     Op<T> o = make_op<T>(L, l, code, eps_, a, inhom, p);
-    T* const* fac = nullptr;
-    if constexpr (sizeof(T) == 8) fac = (T* const*)L.fac64; else fac = (T* const*)L.fac32;
-    const int top = coarse_top<T>();
-    if (L.line && fac[0] && code_dev_ && !(top > 0 && l >= top) && L.n[0] % 2 == 0 &&
-        (size_t)3 * L.n[2] * LT * sizeof(T) <= line_smem_max_) {
-        // factored z-line half sweeps, one tile kernel each (k_line_tile)
-        const size_t sm = (size_t)3 * L.n[2] * LT * sizeof(T);
-        dim3 g1((L.n[0] / 2 + LT - 1) / LT, L.n[1]);
-        for (int it = 0; it < sweeps; ++it)
-            for (int color = 0; color < 2; ++color) {
-                if (prof) prof->begin(l == 0 ? PROF_SMOOTH_L0 : l == 1 ? PROF_MG_L1 : l == 2 ? PROF_MG_L2 : PROF_MG_COARSE, s);
-                ++g_launches;
-                if (o.zc) launch_k(k_line_tile<T, CK_PLANES>, g1, 256, sm, s, o, x, b, (const T*)fac[0], (const T*)fac[1], (const T*)fac[2], color);
-                else if (l == 0) launch_k(k_line_tile<T, CK_FINE>, g1, 256, sm, s, o, x, b, (const T*)fac[0], (const T*)fac[1], (const T*)fac[2], color);
-                else launch_k(k_line_tile<T, CK_ARRAYS>, g1, 256, sm, s, o, x, b, (const T*)fac[0], (const T*)fac[1], (const T*)fac[2], color);
-                if (prof) prof->end(s);
-            }
-    } else if (L.line) {
+    if (L.line) {
         T* q = lq<T>(L);
         dim3 b2(32, 4), g2(((L.n[0] + 1) / 2 + 31) / 32, (L.n[1] + 3) / 4, 1);
         for (int it = 0; it < sweeps; ++it)

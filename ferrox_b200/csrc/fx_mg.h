@@ -97,9 +97,6 @@ public:
     ~Multigrid();
     // builds the hierarchy and uploads the coarse face coefficients
     int setup(const DevParams& p, const std::vector<uint8_t>& code_host, bool want64, bool want32);
-    // the device material codes and parameters for the z-line factors (after
-    // setup, before the first solve); forms the factors of the launched z-line levels
-    void prepare_lines(const DevParams& p, const uint8_t* code, cudaStream_t s);
     // alpha changed on level 0 (device, FP64 and FP32 copies): average down
     int set_alpha(const double* a64, const float* a32, bool has_alpha, cudaStream_t s);
     // FP64 solve of A phi = rhs (+ electrode terms) to |r|_inf <= target
@@ -128,7 +125,6 @@ public:
     int nu1c = -1, nu2c = -1;   // sweeps on the levels below level 0 (-1: nu1 / nu2); the one-CTA levels use nu1 / nu2
     int mixed_cycles = 2;    // FP32 V-cycles per FP64 refinement step
     bool alpha_tiles = true; // coarse alphas below level 1 in one launch (k_alpha_tiles)
-    bool zline_first = false; // z-line smoothing with x/y coarsening where z is strongly coupled (set before setup)
 
     static constexpr int kMaxLev = 24;
     Prof* prof = nullptr;
@@ -137,10 +133,6 @@ public:
 
 private:
     std::vector<MGLevel> lev_;
-    const uint8_t* code_dev_ = nullptr;   // level 0's material codes (device), for the z-line factors
-    DevParams dp_lines_{};
-    size_t line_smem_max_ = 0;            // dynamic shared memory the z-line tile kernel may take
-    void factor_lines(cudaStream_t s);
     double eps_[8];
     const double* a0_64 = nullptr;
     const float* a0_32 = nullptr;
