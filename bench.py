@@ -87,7 +87,8 @@ def deck(name: str):
 def run_config(args, cells: int) -> dict:
     """The workload the line is quoted on; the same dict on both arms."""
     shape = WORKLOADS[args.workload]["shape"]
-    return {"workload": f"{args.workload}-{'x'.join(map(str, shape))}-{args.precision}",
+    extra = {"settings": list(args.set)} if getattr(args, "set", None) else {}
+    return {**extra, "workload": f"{args.workload}-{'x'.join(map(str, shape))}-{args.precision}",
             "description": WORKLOADS[args.workload]["label"], "cells": cells, "mg_rtol": 1e-10,
             "parallelism": "replicas",
             "l2": "inputs larger than L2 (126 MB): every field of the deck is >= 19 MB and the step touches "
@@ -343,6 +344,13 @@ def adjoint_scale(stream, steps: int, k: int = 50) -> dict:
     return out
 
 
+def apply_settings(ctx, args):
+    """The --set KEY=VALUE solver settings, applied to a measured context."""
+    for kv in args.set:
+        key, _, val = kv.partition("=")
+        ctx.set_param(key.strip(), float(val))
+
+
 def e2e_leg(args, api, text, grains, stream, N, world, ke, barrier, torch) -> dict:
     """The metric end to end through the public API: a second context of the
     same deck runs the same W warm-up steps (untimed) and then the same K
@@ -357,6 +365,7 @@ def e2e_leg(args, api, text, grains, stream, N, world, ke, barrier, torch) -> di
         g.set_grains(grains["id"], grains["angles"], grains["tphase"])
     if args.host_loop:
         g.set_param("fx.step_graph", 0)
+    apply_settings(g, args)
     g.set_stream(stream.cuda_stream)
     g.step(args.warmup)
     g.sync()
@@ -442,6 +451,8 @@ def main() -> None:
     # the same kernels driven by the host loop (a synchronisation per loop
     # test) instead of one graph per step; ncu profiles kernels only there
     ap.add_argument("--host-loop", action="store_true")
+    # a solver setting of the measured contexts (fx_set_param), e.g. --set fx.mg_seg=16
+    ap.add_argument("--set", action="append", default=[], metavar="KEY=VALUE")
     ap.add_argument("--adjoint-steps-per-leg", type=int, default=400)
     ap.add_argument("--adjoint-scale-steps", type=int, default=400,
                     help="also run the polycrystal adjoint (FP64 and mixed) over this many steps")
@@ -475,6 +486,7 @@ def main() -> None:
         f.set_grains(grains["id"], grains["angles"], grains["tphase"])
     if args.host_loop:
         f.set_param("fx.step_graph", 0)
+    apply_settings(f, args)
     # a dedicated stream: the library's work and the timing events share it
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)

@@ -155,6 +155,10 @@ __device__ __forceinline__ T dpd(const FV& F, const MV& M, int i, int j, int k) 
 // inlining (and as the oracle, built without contraction, does)
 __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
 
 // DoubleDPDx / y / z, DerivativeAlgorithm.H:256-467 (direction D)
 template <int D, typename T, typename FV, typename MV>

@@ -38,6 +38,53 @@ struct Op {
 // CK_PLANES coarse face beta by plane (laterally uniform)
 constexpr int CK_ARRAYS = 0, CK_FINE = 1, CK_PLANES = 2;
 
+// The per-cell arithmetic of the operator, every rounding written out (no
+// product left for the compiler to fuse into a neighbouring add), so that
+// each form of the smoother and residual that uses these helpers gives the
+// same bits for a cell whatever surrounds it after inlining.
+// a face coupling from the two cells' eps: 0.5 (e0 + e1) / h^2
+template <typename T>
+__device__ __forceinline__ T face_avg(T e0, T e1, T ih2) { return mul_rn(mul_rn(T(0.5), add_rn(e0, e1)), ih2); }
+// a face coupling from a stored face beta
+template <typename T>
+__device__ __forceinline__ T face_beta(T f, T ih2) { return mul_rn(f, ih2); }
+// an electrode face (maxorder-2 ghost 2 V - phi_0): 2 beta / h^2 into the
+// diagonal, 2 beta V / h^2 into the right-hand side
+template <typename T>
+__device__ __forceinline__ void electrode(T beta, T ih2, T v, T& extra, T& bcv) {
+    const T e2 = mul_rn(mul_rn(T(2), beta), ih2);
+    extra = add_rn(extra, e2);
+    bcv = add_rn(bcv, mul_rn(e2, v));
+}
+// the same on a coarse level (homogeneous electrode values: no right-hand-side term)
+template <typename T>
+__device__ __forceinline__ void electrode0(T beta, T ih2, T& extra) {
+    extra = add_rn(extra, mul_rn(mul_rn(T(2), beta), ih2));
+}
+template <typename T>
+__device__ __forceinline__ T diag_sum(T a, T cw, T ce, T cs, T cn, T cb, T ct, T extra) {
+    T d = add_rn(-a, cw);
+    d = add_rn(d, ce);
+    d = add_rn(d, cs);
+    d = add_rn(d, cn);
+    d = add_rn(d, cb);
+    d = add_rn(d, ct);
+    return add_rn(d, extra);
+}
+// b + electrode terms + the off-diagonal couplings times the neighbours
+template <typename T>
+__device__ __forceinline__ T gs_rhs(T b, T bcv, T cw, T xw, T ce, T xe, T cs, T xs, T cn, T xn, bool lo, T cb, T xb,
+                                    bool hi, T ct, T xt) {
+    T s = add_rn(b, bcv);
+    s = fma_rn(cw, xw, s);
+    s = fma_rn(ce, xe, s);
+    s = fma_rn(cs, xs, s);
+    s = fma_rn(cn, xn, s);
+    if (lo) s = fma_rn(cb, xb, s);
+    if (hi) s = fma_rn(ct, xt, s);
+    return s;
+}
+
 template <typename T, int KIND>
 __device__ __forceinline__ void coeffs(const Op<T>& o, int i, int j, int k, int c, int im, int ip, int jm, int jp,
                                        T& cw, T& ce, T& cs, T& cn, T& cb, T& ct, T& diag, T& bcv, const T* eps) {
@@ -47,40 +94,41 @@ __device__ __forceinline__ void coeffs(const Op<T>& o, int i, int j, int k, int 
         const uint8_t* cd = o.code + o.nxy;   // skip the k = -1 ghost layer
         const int row = c - i;
         const T ec = eps[__ldg(cd + c) & 7];
-        cw = T(0.5) * (ec + eps[__ldg(cd + row + im) & 7]) * o.ih2x;
-        ce = T(0.5) * (eps[__ldg(cd + row + ip) & 7] + ec) * o.ih2x;
-        cs = T(0.5) * (ec + eps[__ldg(cd + c + (jm - j) * o.nx) & 7]) * o.ih2y;
-        cn = T(0.5) * (eps[__ldg(cd + c + (jp - j) * o.nx) & 7] + ec) * o.ih2y;
-        if (k > 0) cb = T(0.5) * (ec + eps[__ldg(cd + c - o.nxy) & 7]) * o.ih2z;
-        else { cb = T(0); extra += T(2) * ec * o.ih2z; bcv += T(2) * ec * o.ih2z * o.vlo; }
-        if (k < o.nz - 1) ct = T(0.5) * (eps[__ldg(cd + c + o.nxy) & 7] + ec) * o.ih2z;
-        else { ct = T(0); extra += T(2) * ec * o.ih2z; bcv += T(2) * ec * o.ih2z * o.vhi; }
+        cw = face_avg(ec, eps[__ldg(cd + row + im) & 7], o.ih2x);
+        ce = face_avg(ec, eps[__ldg(cd + row + ip) & 7], o.ih2x);
+        cs = face_avg(ec, eps[__ldg(cd + c + (jm - j) * o.nx) & 7], o.ih2y);
+        cn = face_avg(ec, eps[__ldg(cd + c + (jp - j) * o.nx) & 7], o.ih2y);
+        if (k > 0) cb = face_avg(ec, eps[__ldg(cd + c - o.nxy) & 7], o.ih2z);
+        else { cb = T(0); electrode(ec, o.ih2z, o.vlo, extra, bcv); }
+        if (k < o.nz - 1) ct = face_avg(ec, eps[__ldg(cd + c + o.nxy) & 7], o.ih2z);
+        else { ct = T(0); electrode(ec, o.ih2z, o.vhi, extra, bcv); }
     } else if constexpr (KIND == CK_PLANES) {
         // a layered stack: every face of a plane has the same beta
-        cw = ce = __ldg(o.zc + k) * o.ih2x;
-        cs = cn = __ldg(o.zc + o.nz + k) * o.ih2y;
+        cw = ce = face_beta(__ldg(o.zc + k), o.ih2x);
+        cs = cn = face_beta(__ldg(o.zc + o.nz + k), o.ih2y);
         // (level 0: bb[0], bb[nz] are the eps of the electrode-layer cells)
         const T fb = __ldg(o.zc + 2 * o.nz + k), ft = __ldg(o.zc + 2 * o.nz + k + 1);
-        if (k > 0) cb = fb * o.ih2z;
-        else { cb = T(0); extra += T(2) * fb * o.ih2z; bcv += T(2) * fb * o.ih2z * o.vlo; }
-        if (k < o.nz - 1) ct = ft * o.ih2z;
-        else { ct = T(0); extra += T(2) * ft * o.ih2z; bcv += T(2) * ft * o.ih2z * o.vhi; }
+        if (k > 0) cb = face_beta(fb, o.ih2z);
+        else { cb = T(0); electrode(fb, o.ih2z, o.vlo, extra, bcv); }
+        if (k < o.nz - 1) ct = face_beta(ft, o.ih2z);
+        else { ct = T(0); electrode(ft, o.ih2z, o.vhi, extra, bcv); }
     } else {
+        // coarse levels: homogeneous electrode conditions (no right-hand-side term)
         const int row = c - i;
-        cw = __ldg(o.bw + c) * o.ih2x;
-        ce = __ldg(o.bw + row + ip) * o.ih2x;
-        cs = __ldg(o.bs + c) * o.ih2y;
-        cn = __ldg(o.bs + c + (jp - j) * o.nx) * o.ih2y;
+        cw = face_beta(__ldg(o.bw + c), o.ih2x);
+        ce = face_beta(__ldg(o.bw + row + ip), o.ih2x);
+        cs = face_beta(__ldg(o.bs + c), o.ih2y);
+        cn = face_beta(__ldg(o.bs + c + (jp - j) * o.nx), o.ih2y);
         const T fb = __ldg(o.bb + c), ft = __ldg(o.bb + c + o.nxy);
-        if (k > 0) cb = fb * o.ih2z;
-        else { cb = T(0); extra += T(2) * fb * o.ih2z; }
-        if (k < o.nz - 1) ct = ft * o.ih2z;
-        else { ct = T(0); extra += T(2) * ft * o.ih2z; }
+        if (k > 0) cb = face_beta(fb, o.ih2z);
+        else { cb = T(0); electrode0(fb, o.ih2z, extra); }
+        if (k < o.nz - 1) ct = face_beta(ft, o.ih2z);
+        else { ct = T(0); electrode0(ft, o.ih2z, extra); }
     }
     if (o.nx == 1) { cw = T(0); ce = T(0); }
     if (o.ny == 1) { cs = T(0); cn = T(0); }
     const T a = o.a ? o.a[c] : T(0);
-    diag = -a + cw + ce + cs + cn + cb + ct + extra;
+    diag = diag_sum(a, cw, ce, cs, cn, cb, ct, extra);
 }
 
 __device__ __forceinline__ void nbr(int i, int n, int& m, int& p) {
@@ -141,14 +189,13 @@ __device__ __forceinline__ void rbgs_update(const Op<T>& o, T* __restrict__ x, c
     coeffs<T, KIND>(o, i, j, k, c, im, ip, jm, jp, cw, ce, cs, cn, cb, ct, diag, bcv, seps);
     const int row = c - i;
     if (ZERO) {
-        x[c] = sdiv(b[c] + bcv, diag);
+        x[c] = sdiv(add_rn(b[c], bcv), diag);
         x[c + ((i & 1) ? -1 : 1)] = T(0);
         return;
     }
-    T s = b[c] + bcv + cw * x[row + im] + ce * x[row + ip] + cs * x[c + (jm - j) * o.nx] +
-          cn * x[c + (jp - j) * o.nx];
-    if (k > 0) s += cb * x[c - o.nxy];
-    if (k < o.nz - 1) s += ct * x[c + o.nxy];
+    const bool lo = k > 0, hi = k < o.nz - 1;
+    const T s = gs_rhs(b[c], bcv, cw, x[row + im], ce, x[row + ip], cs, x[c + (jm - j) * o.nx], cn,
+                       x[c + (jp - j) * o.nx], lo, cb, lo ? x[c - o.nxy] : T(0), hi, ct, hi ? x[c + o.nxy] : T(0));
     x[c] = sdiv(s, diag);
 }
 
@@ -164,6 +211,199 @@ __global__ void __launch_bounds__(256) k_rbgs(Op<T> o, T* __restrict__ x, const 
     }
     rbgs_update<T, KIND, ZERO>(o, x, b, color, blockIdx.x * blockDim.x + threadIdx.x,
                                blockIdx.y * blockDim.y + threadIdx.y, blockIdx.z, seps);
+}
+
+// ---- row-segment form of the point red-black half sweep
+//
+// Each thread owns a 32-byte segment of one x row (SEG = 8 FP32 or 4 FP64
+// cells starting at a multiple of SEG) and updates the SEG / 2 cells of the
+// colour in it.  Every row it needs -- the segment itself, the rows j - 1 and
+// j + 1, the planes k - 1 and k + 1, b, alpha, the material codes or face
+// coefficients -- arrives in two 16-byte loads (codes: one 8- or 4-byte load),
+// and the index, wrap and plane tests are paid once per segment instead of
+// once per cell.  The segment is written back whole: the other colour's
+// cells with the bits they were read with (no thread of this half sweep
+// writes them), so the result is bit-identical to k_rbgs, whose per-cell
+// operations it repeats in the same order.  A warp never mixes the two
+// parities of (j + k + colour): with fewer than 32 segments per row the
+// block's rows are ordered even offsets first, so each warp's rows share one.
+template <typename T, int SB> struct SegW { static constexpr int n = SB / (int)sizeof(T); };
+
+// 16-byte vector accesses written as PTX: one 128-bit load or store per
+// call (through float4 / double2 copies, ncu counted two load instructions
+// per 16 bytes in this kernel).  The x accesses are volatile and the store
+// clobbers memory, so they keep their order; the read-only loads (.nc) may move.
+__device__ __forceinline__ void ld16(const float* p, float* v) {
+    asm volatile("ld.global.v4.f32 {%0, %1, %2, %3}, [%4];"
+                 : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]) : "l"(p));
+}
+__device__ __forceinline__ void ld16(const double* p, double* v) {
+    asm volatile("ld.global.v2.f64 {%0, %1}, [%2];" : "=d"(v[0]), "=d"(v[1]) : "l"(p));
+}
+__device__ __forceinline__ void ldg16(const float* p, float* v) {
+    asm("ld.global.nc.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]) : "l"(p));
+}
+__device__ __forceinline__ void ldg16(const double* p, double* v) {
+    asm("ld.global.nc.v2.f64 {%0, %1}, [%2];" : "=d"(v[0]), "=d"(v[1]) : "l"(p));
+}
+__device__ __forceinline__ void st16(float* p, const float* v) {
+    asm volatile("st.global.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3])
+                 : "memory");
+}
+__device__ __forceinline__ void st16(double* p, const double* v) {
+    asm volatile("st.global.v2.f64 [%0], {%1, %2};" ::"l"(p), "d"(v[0]), "d"(v[1]) : "memory");
+}
+
+template <typename T, int SB>
+__device__ __forceinline__ void ld_seg(const T* p, T (&v)[SegW<T, SB>::n]) {
+    constexpr int H = 16 / (int)sizeof(T);
+    ld16(p, v);
+    if constexpr (SB == 32) ld16(p + H, v + H);
+}
+
+template <typename T, int SB>
+__device__ __forceinline__ void ldg_seg(const T* p, T (&v)[SegW<T, SB>::n]) {
+    constexpr int H = 16 / (int)sizeof(T);
+    ldg16(p, v);
+    if constexpr (SB == 32) ldg16(p + H, v + H);
+}
+
+template <typename T, int SB>
+__device__ __forceinline__ void st_seg(T* p, const T (&v)[SegW<T, SB>::n]) {
+    constexpr int H = 16 / (int)sizeof(T);
+    st16(p, v);
+    if constexpr (SB == 32) st16(p + H, v + H);
+}
+
+// the material codes of a segment, one byte per cell
+template <int SEG>
+__device__ __forceinline__ unsigned long long ld_codes(const uint8_t* p) {
+    if constexpr (SEG == 8) return __ldg(reinterpret_cast<const unsigned long long*>(p));
+    else if constexpr (SEG == 4) return (unsigned long long)__ldg(reinterpret_cast<const unsigned int*>(p));
+    else return (unsigned long long)__ldg(reinterpret_cast<const unsigned short*>(p));
+}
+
+__device__ __forceinline__ int code_at(unsigned long long w, int m) { return (int)(w >> (8 * m)) & 7; }
+
+// the half sweep of one segment; PAR: the in-segment offset of this colour's cells
+template <typename T, int SB, int KIND, bool ZERO, int PAR>
+__device__ __forceinline__ void seg_update(const Op<T>& o, T* __restrict__ x, const T* __restrict__ b, int i0, int j,
+                                           int k, const T* seps) {
+    constexpr int SEG = SegW<T, SB>::n;
+    const int row = o.nx * (j + o.ny * k);
+    const int c0 = row + i0;
+    int jm, jp;
+    nbr(j, o.ny, jm, jp);
+    const int so = (jm - j) * o.nx, no = (jp - j) * o.nx;
+    const bool lo = k > 0, hi = k < o.nz - 1;
+    // the x neighbour outside the segment: left of cell 0 (PAR 0) or right of cell SEG - 1 (PAR 1)
+    const int ih = PAR == 0 ? (i0 == 0 ? o.nx - 1 : i0 - 1) : (i0 + SEG == o.nx ? 0 : i0 + SEG);
+    T xc[SEG], bv[SEG];
+    T xs[SEG], xn[SEG], xb[SEG], xt[SEG];
+    ld_seg<T, SB>(x + c0, xc);
+    ldg_seg<T, SB>(b + c0, bv);
+    T xh = T(0);
+    if (!ZERO) {
+        xh = x[row + ih];
+        ld_seg<T, SB>(x + c0 + so, xs);
+        ld_seg<T, SB>(x + c0 + no, xn);
+        if (lo) ld_seg<T, SB>(x + c0 - o.nxy, xb);
+        if (hi) ld_seg<T, SB>(x + c0 + o.nxy, xt);
+    }
+    T av[SEG];
+    if (o.a) ldg_seg<T, SB>(o.a + c0, av);
+    // face coefficients: per cell (codes, arrays) or per plane
+    T pw = T(0), ps = T(0), pb = T(0), pt = T(0);
+    unsigned long long wc = 0, ws = 0, wn = 0, wb = 0, wt = 0;
+    int chalo = 0;
+    T fw[SEG], fs[SEG], fn[SEG], fb[SEG], ft[SEG];
+    T fh = T(0);
+    if constexpr (KIND == CK_FINE) {
+        const uint8_t* cd = o.code + o.nxy;   // skip the k = -1 ghost layer
+        wc = ld_codes<SEG>(cd + c0);
+        ws = ld_codes<SEG>(cd + c0 + so);
+        wn = ld_codes<SEG>(cd + c0 + no);
+        if (lo) wb = ld_codes<SEG>(cd + c0 - o.nxy);
+        if (hi) wt = ld_codes<SEG>(cd + c0 + o.nxy);
+        chalo = __ldg(cd + row + ih) & 7;
+    } else if constexpr (KIND == CK_PLANES) {
+        pw = __ldg(o.zc + k);
+        ps = __ldg(o.zc + o.nz + k);
+        pb = __ldg(o.zc + 2 * o.nz + k);
+        pt = __ldg(o.zc + 2 * o.nz + k + 1);
+    } else {
+        ldg_seg<T, SB>(o.bw + c0, fw);
+        ldg_seg<T, SB>(o.bs + c0, fs);
+        ldg_seg<T, SB>(o.bs + c0 + no, fn);
+        ldg_seg<T, SB>(o.bb + c0, fb);
+        ldg_seg<T, SB>(o.bb + c0 + o.nxy, ft);
+        if (PAR == 1) fh = __ldg(o.bw + row + ih);
+    }
+#pragma unroll
+    for (int u = 0; u < SEG / 2; ++u) {
+        const int m = 2 * u + PAR;
+        T cw, ce, cs, cn, cb, ct, extra = T(0), bcv = T(0);
+        if constexpr (KIND == CK_FINE) {
+            const T ec = seps[code_at(wc, m)];
+            cw = face_avg(ec, seps[m == 0 ? chalo : code_at(wc, m - 1)], o.ih2x);
+            ce = face_avg(ec, seps[m == SEG - 1 ? chalo : code_at(wc, m + 1)], o.ih2x);
+            cs = face_avg(ec, seps[code_at(ws, m)], o.ih2y);
+            cn = face_avg(ec, seps[code_at(wn, m)], o.ih2y);
+            if (lo) cb = face_avg(ec, seps[code_at(wb, m)], o.ih2z);
+            else { cb = T(0); electrode(ec, o.ih2z, o.vlo, extra, bcv); }
+            if (hi) ct = face_avg(ec, seps[code_at(wt, m)], o.ih2z);
+            else { ct = T(0); electrode(ec, o.ih2z, o.vhi, extra, bcv); }
+        } else if constexpr (KIND == CK_PLANES) {
+            cw = ce = face_beta(pw, o.ih2x);
+            cs = cn = face_beta(ps, o.ih2y);
+            if (lo) cb = face_beta(pb, o.ih2z);
+            else { cb = T(0); electrode(pb, o.ih2z, o.vlo, extra, bcv); }
+            if (hi) ct = face_beta(pt, o.ih2z);
+            else { ct = T(0); electrode(pt, o.ih2z, o.vhi, extra, bcv); }
+        } else {
+            cw = face_beta(fw[m], o.ih2x);
+            ce = face_beta(m == SEG - 1 ? fh : fw[m + 1], o.ih2x);
+            cs = face_beta(fs[m], o.ih2y);
+            cn = face_beta(fn[m], o.ih2y);
+            if (lo) cb = face_beta(fb[m], o.ih2z);
+            else { cb = T(0); electrode0(fb[m], o.ih2z, extra); }
+            if (hi) ct = face_beta(ft[m], o.ih2z);
+            else { ct = T(0); electrode0(ft[m], o.ih2z, extra); }
+        }
+        if (o.ny == 1) { cs = T(0); cn = T(0); }
+        const T diag = diag_sum(o.a ? av[m] : T(0), cw, ce, cs, cn, cb, ct, extra);
+        if (ZERO) {
+            xc[m] = sdiv(add_rn(bv[m], bcv), diag);
+            xc[m ^ 1] = T(0);
+            continue;
+        }
+        const T s = gs_rhs(bv[m], bcv, cw, m == 0 ? xh : xc[m - 1], ce, m == SEG - 1 ? xh : xc[m + 1], cs, xs[m], cn,
+                           xn[m], lo, cb, xb[m], hi, ct, xt[m]);
+        xc[m] = sdiv(s, diag);
+    }
+    st_seg<T, SB>(x + c0, xc);
+}
+
+template <typename T, int SB, int KIND, bool ZERO = false>
+__global__ void __launch_bounds__(256) k_rbgs_seg(Op<T> o, T* __restrict__ x, const T* __restrict__ b, int color) {
+    pdl_entry();
+    __shared__ T seps[8];
+    if (KIND == CK_FINE) {
+        if (threadIdx.x == 0 && threadIdx.y == 0)
+#pragma unroll
+            for (int q = 0; q < 8; ++q) seps[q] = o.eps[q];
+        __syncthreads();
+    }
+    constexpr int SEG = SegW<T, SB>::n;
+    // rows of the block: even offsets first, so that a warp's rows share a parity
+    const int h = blockDim.y / 2;
+    const int ty = threadIdx.y;
+    const int j = blockIdx.y * blockDim.y + (ty < h ? 2 * ty : 2 * (ty - h) + 1);
+    const int k = blockIdx.z;
+    const int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * SEG;
+    if (j >= o.ny) return;
+    if (((j + k + color) & 1) == 0) seg_update<T, SB, KIND, ZERO, 0>(o, x, b, i0, j, k, seps);
+    else seg_update<T, SB, KIND, ZERO, 1>(o, x, b, i0, j, k, seps);
 }
 
 // red-black z-line Gauss-Seidel half sweep: color = parity of i + j; each
@@ -1447,6 +1687,49 @@ void Multigrid::launch_coarse(int top, cudaStream_t s) {
     if (prof) prof->end(s);
 }
 
+// a level the row-segment half sweep (k_rbgs_seg) can take with SB-byte
+// segments: rows of whole segments, a segment count per row that divides 32
+// or is a multiple of it, and every array it reads 16-byte aligned (segment
+// starts are then SB-byte aligned, the codes' loads aligned to their width)
+template <typename T, int SB>
+static bool seg_shape(const MGLevel& L, int l, const Op<T>& o, const T* x, const T* b) {
+    constexpr int SEG = SegW<T, SB>::n;
+    if (L.line || SEG < 2 || L.n[0] % SEG != 0) return false;
+    const int gx = L.n[0] / SEG;
+    if (!(gx % 32 == 0 || 32 % gx == 0)) return false;
+    auto al = [](const void* p, uintptr_t a) { return ((uintptr_t)p % a) == 0; };
+    if (!al(x, 16) || !al(b, 16) || !al(o.a, 16)) return false;
+    if (o.zc) return true;
+    if (l == 0) return al(o.code + o.nxy, SEG);   // the codes past the ghost layer
+    return al(o.bw, 16) && al(o.bs, 16) && al(o.bb, 16);
+}
+
+// the half sweeps of one smoothing pass by SB-byte row segments
+template <typename T, int SB>
+static void seg_sweeps(const MGLevel& L, int l, const Op<T>& o, T* x, const T* b, int sweeps, bool zero, int cat,
+                       Prof* prof, cudaStream_t s) {
+    // bx segments of a row per block row, 256 / bx rows per block
+    const int gx = L.n[0] / SegW<T, SB>::n, bx = gx < 32 ? gx : 32, by = 256 / bx;
+    dim3 b2(bx, by), g2(gx / bx, (L.n[1] + by - 1) / by, L.n[2]);
+    for (int it = 0; it < sweeps; ++it)
+        for (int color = 0; color < 2; ++color) {
+            if (prof) prof->begin(cat, s);
+            const bool z = zero && it == 0 && color == 0;
+            ++g_launches;
+            if (l == 0 && !o.zc) {
+                if (z) launch_k(k_rbgs_seg<T, SB, CK_FINE, true>, g2, b2, 0, s, o, x, b, color);
+                else launch_k(k_rbgs_seg<T, SB, CK_FINE>, g2, b2, 0, s, o, x, b, color);
+            } else if (o.zc) {
+                if (z) launch_k(k_rbgs_seg<T, SB, CK_PLANES, true>, g2, b2, 0, s, o, x, b, color);
+                else launch_k(k_rbgs_seg<T, SB, CK_PLANES>, g2, b2, 0, s, o, x, b, color);
+            } else {
+                if (z) launch_k(k_rbgs_seg<T, SB, CK_ARRAYS, true>, g2, b2, 0, s, o, x, b, color);
+                else launch_k(k_rbgs_seg<T, SB, CK_ARRAYS>, g2, b2, 0, s, o, x, b, color);
+            }
+            if (prof) prof->end(s);
+        }
+}
+
 // a level whose first half sweep can start from an uncleared x (point
 // red-black with x / colour pairs)
 static bool zero_first_ok(const MGLevel& L) { return !L.line && L.n[0] % 2 == 0; }
@@ -1473,6 +1756,12 @@ void Multigrid::smooth(const DevParams& p, const uint8_t* code, int l, T* x, con
                 else launch_k(k_line<T, CK_ARRAYS>, g2, b2, 0, s, o, x, b, q, color);
                 if (prof) prof->end(s);
             }
+    } else if (seg_bytes == 32 && (long long)L.N >= seg_min_cells && seg_shape<T, 32>(L, l, o, x, b)) {
+        seg_sweeps<T, 32>(L, l, o, x, b, sweeps, zero,
+                          l == 0 ? PROF_SMOOTH_L0 : l == 1 ? PROF_MG_L1 : l == 2 ? PROF_MG_L2 : PROF_MG_COARSE, prof, s);
+    } else if (seg_bytes == 16 && (long long)L.N >= seg_min_cells && seg_shape<T, 16>(L, l, o, x, b)) {
+        seg_sweeps<T, 16>(L, l, o, x, b, sweeps, zero,
+                          l == 0 ? PROF_SMOOTH_L0 : l == 1 ? PROF_MG_L1 : l == 2 ? PROF_MG_L2 : PROF_MG_COARSE, prof, s);
     } else {
         dim3 b2(32, 8), g2(((L.n[0] + 1) / 2 + 31) / 32, (L.n[1] + 7) / 8, L.n[2]);
         for (int it = 0; it < sweeps; ++it)
@@ -1592,7 +1881,8 @@ int Multigrid::replay(GraphCache& g, const void* x, const void* rhs, const DevPa
         return (int)cudaGetLastError();
     }
     if (!g.exec || g.x != x || g.rhs != rhs || g.has_alpha != has_alpha_ || g.vlo != p.V_lo || g.vhi != p.V_hi ||
-        g.nu1 != nu1 || g.nu2 != nu2 || g.nu1c != nu1c || g.nu2c != nu2c || g.pdl != g_pdl) {
+        g.nu1 != nu1 || g.nu2 != nu2 || g.nu1c != nu1c || g.nu2c != nu2c || g.pdl != g_pdl ||
+        g.seg != seg_bytes || g.seg_min != seg_min_cells) {
         if (g.exec) { cudaGraphExecDestroy(g.exec); g.exec = nullptr; }
         cudaGraph_t graph;
         const long long l0 = g_launches.load();
@@ -1608,7 +1898,7 @@ int Multigrid::replay(GraphCache& g, const void* x, const void* rhs, const DevPa
         if (e) return (int)e;
         g.x = x; g.rhs = rhs; g.has_alpha = has_alpha_; g.vlo = p.V_lo; g.vhi = p.V_hi; g.nu1 = nu1; g.nu2 = nu2;
         g.nu1c = nu1c; g.nu2c = nu2c;
-        g.pdl = g_pdl;
+        g.pdl = g_pdl; g.seg = seg_bytes; g.seg_min = seg_min_cells;
     }
     g_launches += g.launches;
     return (int)cudaGraphLaunch(g.exec, s);

@@ -125,6 +125,8 @@ public:
     int nu1c = -1, nu2c = -1;   // sweeps on the levels below level 0 (-1: nu1 / nu2); the one-CTA levels use nu1 / nu2
     int mixed_cycles = 2;    // FP32 V-cycles per FP64 refinement step
     bool alpha_tiles = true; // coarse alphas below level 1 in one launch (k_alpha_tiles)
+    int seg_bytes = 16;      // point red-black half sweeps by row segments of 16 or 32 bytes where the shape allows (k_rbgs_seg); 0: one cell per thread
+    long long seg_min_cells = 0;  // ... on levels of at least this many cells
 
     static constexpr int kMaxLev = 24;
     Prof* prof = nullptr;
@@ -155,6 +157,8 @@ private:
         double vlo = 0, vhi = 0;
         int nu1 = 0, nu2 = 0, nu1c = 0, nu2c = 0;
         bool pdl = false;
+        int seg = 0;
+        long long seg_min = 0;
         long long launches = 0;
     };
     GraphCache g64_, g32_, g32b_;   // g32b_: the refinement step from the second FP64 buffer

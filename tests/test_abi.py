@@ -112,7 +112,8 @@ def test_reader_last_definition_comments_and_file(tmp_path):
 @pytest.mark.parametrize("key,bad,good", [
     ("fx.phi_extrapolate", 7, 6), ("fx.phi_extrapolate", -1, 0), ("fx.phi_ghost_mode", 3, 1),
     ("fx.mg_max_iter", 0, 1), ("fx.newton_max_iter", 0, 1), ("fx.mg_nu1", -1, 0), ("fx.mg_nu2", -1, 0),
-    ("fx.mg_rtol", 0.0, 1e-12),
+    ("fx.mg_rtol", 0.0, 1e-12), ("fx.mg_seg", 8, 16), ("fx.mg_seg_min", -1, 1000),
+    ("fx.mg_nu1_coarse", 0, 1), ("fx.mg_nu2_coarse", -2, 0),
 ])
 def test_solver_settings_out_of_range_are_rejected(key, bad, good):
     """fx_set_param refuses what the inputs reader refuses, and a refused call changes nothing."""

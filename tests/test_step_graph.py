@@ -224,3 +224,50 @@ def test_interior_fast_path_bit_identical(case):
     for n in a:
         scale = np.abs(b[n]).max()
         assert np.abs(a[n] - b[n]).max() <= 1e-12 * scale, (n, np.abs(a[n] - b[n]).max() / scale)
+
+
+SEG_CASES = {
+    # level 0 from the material codes, coarse levels from face-beta arrays;
+    # 256-cell rows: 32 FP32 segments per row, one row per warp
+    "polycrystal_fp64": dict(grains=(256, 32, 24), precision=None),
+    "polycrystal_mixed": dict(grains=(256, 32, 24), precision="mixed"),
+    # 64-cell rows: several rows per warp (the even-offsets-first row order)
+    "polycrystal_mixed_64": dict(grains=(64, 64, 48), precision="mixed"),
+    # layered stacks: face beta by plane, alpha from the Newton-coupled semiconductor
+    "mfism_fp64": dict(text=decks.mfism(32, 32, 48, steps_per_voltage=3, v_step=0.1), shape=(48, 32, 32)),
+    "mfism_mixed": dict(text=decks.mfism(32, 32, 48, steps_per_voltage=3, v_step=0.1), shape=(48, 32, 32),
+                        precision="mixed"),
+    "mfim_mixed": dict(text=decks.mfim(64, 64, 24, Phi_Bc_hi=0.8), shape=(24, 64, 64), precision="mixed"),
+}
+
+
+@pytest.mark.parametrize("case", sorted(SEG_CASES))
+def test_segment_smoother_bit_identical(case):
+    """The row-segment red-black half sweep (fx.mg_seg = 16 or 32 bytes per
+    thread; every level whose rows it can take, fx.mg_seg_min = 0) repeats the
+    per-cell operations of the one-cell-per-thread sweep (fx.mg_seg = 0) with
+    the same roundings: fields and V-cycle counts are bit-identical, in the
+    step graph and in the host-driven loop."""
+    cfg = SEG_CASES[case]
+    grains = None
+    if cfg.get("grains"):
+        nx, ny, nz = cfg["grains"]
+        text, grains = decks.polycrystal(nx, ny, nz, ngrains=6, seed=4, nsteps=10, extra={"Phi_Bc_hi": 0.7})
+        shape = (nz, ny, nx)
+    else:
+        text, shape = cfg["text"], cfg["shape"]
+    P = start_P(shape, 7)
+    for graph in (1, 0):
+        runs = []
+        for seg in (0, 16, 32):
+            f = make(text, P, graph, precision=cfg.get("precision"), grains=grains,
+                     params={"fx.mg_seg": seg, "fx.mg_seg_min": 0})
+            f.step(5)
+            runs.append(({n: f.field(n) for n in FIELDS}, f.stats()["mg_cycles_total"],
+                         f.stats()["newton_iters_total"]))
+            f.close()
+        a, ca, na = runs[0]
+        for seg, (b, cb, nb) in zip((16, 32), runs[1:]):
+            assert (ca, na) == (cb, nb), (graph, seg, ca, cb, na, nb)
+            for n in FIELDS:
+                assert np.array_equal(a[n], b[n]), (graph, seg, n, np.abs(a[n] - b[n]).max())
