@@ -85,6 +85,19 @@ __device__ __forceinline__ T gs_rhs(T b, T bcv, T cw, T xw, T ce, T xe, T cs, T 
     return s;
 }
 
+// the residual b + electrode terms - (diag x - the off-diagonal couplings times the neighbours)
+template <typename T>
+__device__ __forceinline__ T res_val(T b, T bcv, T diag, T xc, T cw, T xw, T ce, T xe, T cs, T xs, T cn, T xn, bool lo,
+                                     T cb, T xb, bool hi, T ct, T xt) {
+    T off = mul_rn(cw, xw);
+    off = fma_rn(ce, xe, off);
+    off = fma_rn(cs, xs, off);
+    off = fma_rn(cn, xn, off);
+    if (lo) off = fma_rn(cb, xb, off);
+    if (hi) off = fma_rn(ct, xt, off);
+    return add_rn(add_rn(b, bcv), -fma_rn(diag, xc, -off));
+}
+
 template <typename T, int KIND>
 __device__ __forceinline__ void coeffs(const Op<T>& o, int i, int j, int k, int c, int im, int ip, int jm, int jp,
                                        T& cw, T& ce, T& cs, T& cn, T& cb, T& ct, T& diag, T& bcv, const T* eps) {
@@ -285,68 +298,56 @@ __device__ __forceinline__ unsigned long long ld_codes(const uint8_t* p) {
 
 __device__ __forceinline__ int code_at(unsigned long long w, int m) { return (int)(w >> (8 * m)) & 7; }
 
-// the half sweep of one segment; PAR: the in-segment offset of this colour's cells
-template <typename T, int SB, int KIND, bool ZERO, int PAR>
-__device__ __forceinline__ void seg_update(const Op<T>& o, T* __restrict__ x, const T* __restrict__ b, int i0, int j,
-                                           int k, const T* seps) {
-    constexpr int SEG = SegW<T, SB>::n;
-    const int row = o.nx * (j + o.ny * k);
-    const int c0 = row + i0;
-    int jm, jp;
-    nbr(j, o.ny, jm, jp);
-    const int so = (jm - j) * o.nx, no = (jp - j) * o.nx;
-    const bool lo = k > 0, hi = k < o.nz - 1;
-    // the x neighbour outside the segment: left of cell 0 (PAR 0) or right of cell SEG - 1 (PAR 1)
-    const int ih = PAR == 0 ? (i0 == 0 ? o.nx - 1 : i0 - 1) : (i0 + SEG == o.nx ? 0 : i0 + SEG);
-    T xc[SEG], bv[SEG];
-    T xs[SEG], xn[SEG], xb[SEG], xt[SEG];
-    ld_seg<T, SB>(x + c0, xc);
-    ldg_seg<T, SB>(b + c0, bv);
-    T xh = T(0);
-    if (!ZERO) {
-        xh = x[row + ih];
-        ld_seg<T, SB>(x + c0 + so, xs);
-        ld_seg<T, SB>(x + c0 + no, xn);
-        if (lo) ld_seg<T, SB>(x + c0 - o.nxy, xb);
-        if (hi) ld_seg<T, SB>(x + c0 + o.nxy, xt);
+// The operator coefficients of one row segment: the material codes of the
+// segment's row and of its four neighbour rows (level 0), the stored face
+// beta (coarse levels) or the plane's face beta (layered stacks).  NL / NR:
+// the cells left of the segment's first / right of its last are needed.
+template <typename T, int SB, int KIND, bool NL, bool NR>
+struct SegCoef {
+    static constexpr int SEG = SegW<T, SB>::n;
+    unsigned long long wc = 0, ws = 0, wn = 0, wb = 0, wt = 0;   // codes, one byte per cell
+    int hl = 0, hr = 0;                                           // halo codes
+    T pw = T(0), ps = T(0), pb = T(0), pt = T(0);                 // plane values
+    T fw[SEG], fs[SEG], fn[SEG], fb[SEG], ft[SEG];                // face arrays
+    T fr = T(0);                                                  // low-x face beta right of the segment
+
+    // row: first cell of the row; c0 = row + i0; so / no: offsets of the rows j - 1 / j + 1;
+    // il / ir: x index left of the segment / right of it
+    __device__ __forceinline__ void load(const Op<T>& o, int row, int c0, int so, int no, int k, bool lo, bool hi,
+                                         int il, int ir) {
+        if constexpr (KIND == CK_FINE) {
+            const uint8_t* cd = o.code + o.nxy;   // skip the k = -1 ghost layer
+            wc = ld_codes<SEG>(cd + c0);
+            ws = ld_codes<SEG>(cd + c0 + so);
+            wn = ld_codes<SEG>(cd + c0 + no);
+            if (lo) wb = ld_codes<SEG>(cd + c0 - o.nxy);
+            if (hi) wt = ld_codes<SEG>(cd + c0 + o.nxy);
+            if (NL) hl = __ldg(cd + row + il) & 7;
+            if (NR) hr = __ldg(cd + row + ir) & 7;
+        } else if constexpr (KIND == CK_PLANES) {
+            pw = __ldg(o.zc + k);
+            ps = __ldg(o.zc + o.nz + k);
+            pb = __ldg(o.zc + 2 * o.nz + k);
+            pt = __ldg(o.zc + 2 * o.nz + k + 1);
+        } else {
+            ldg_seg<T, SB>(o.bw + c0, fw);
+            ldg_seg<T, SB>(o.bs + c0, fs);
+            ldg_seg<T, SB>(o.bs + c0 + no, fn);
+            ldg_seg<T, SB>(o.bb + c0, fb);
+            ldg_seg<T, SB>(o.bb + c0 + o.nxy, ft);
+            if (NR) fr = __ldg(o.bw + row + ir);
+        }
     }
-    T av[SEG];
-    if (o.a) ldg_seg<T, SB>(o.a + c0, av);
-    // face coefficients: per cell (codes, arrays) or per plane
-    T pw = T(0), ps = T(0), pb = T(0), pt = T(0);
-    unsigned long long wc = 0, ws = 0, wn = 0, wb = 0, wt = 0;
-    int chalo = 0;
-    T fw[SEG], fs[SEG], fn[SEG], fb[SEG], ft[SEG];
-    T fh = T(0);
-    if constexpr (KIND == CK_FINE) {
-        const uint8_t* cd = o.code + o.nxy;   // skip the k = -1 ghost layer
-        wc = ld_codes<SEG>(cd + c0);
-        ws = ld_codes<SEG>(cd + c0 + so);
-        wn = ld_codes<SEG>(cd + c0 + no);
-        if (lo) wb = ld_codes<SEG>(cd + c0 - o.nxy);
-        if (hi) wt = ld_codes<SEG>(cd + c0 + o.nxy);
-        chalo = __ldg(cd + row + ih) & 7;
-    } else if constexpr (KIND == CK_PLANES) {
-        pw = __ldg(o.zc + k);
-        ps = __ldg(o.zc + o.nz + k);
-        pb = __ldg(o.zc + 2 * o.nz + k);
-        pt = __ldg(o.zc + 2 * o.nz + k + 1);
-    } else {
-        ldg_seg<T, SB>(o.bw + c0, fw);
-        ldg_seg<T, SB>(o.bs + c0, fs);
-        ldg_seg<T, SB>(o.bs + c0 + no, fn);
-        ldg_seg<T, SB>(o.bb + c0, fb);
-        ldg_seg<T, SB>(o.bb + c0 + o.nxy, ft);
-        if (PAR == 1) fh = __ldg(o.bw + row + ih);
-    }
-#pragma unroll
-    for (int u = 0; u < SEG / 2; ++u) {
-        const int m = 2 * u + PAR;
-        T cw, ce, cs, cn, cb, ct, extra = T(0), bcv = T(0);
+
+    // the couplings of cell m of the segment (the operations of coeffs<T, KIND>)
+    __device__ __forceinline__ void cell(const Op<T>& o, const T* seps, int m, bool lo, bool hi, T& cw, T& ce, T& cs,
+                                         T& cn, T& cb, T& ct, T& extra, T& bcv) const {
+        extra = T(0);
+        bcv = T(0);
         if constexpr (KIND == CK_FINE) {
             const T ec = seps[code_at(wc, m)];
-            cw = face_avg(ec, seps[m == 0 ? chalo : code_at(wc, m - 1)], o.ih2x);
-            ce = face_avg(ec, seps[m == SEG - 1 ? chalo : code_at(wc, m + 1)], o.ih2x);
+            cw = face_avg(ec, seps[m == 0 ? hl : code_at(wc, m - 1)], o.ih2x);
+            ce = face_avg(ec, seps[m == SEG - 1 ? hr : code_at(wc, m + 1)], o.ih2x);
             cs = face_avg(ec, seps[code_at(ws, m)], o.ih2y);
             cn = face_avg(ec, seps[code_at(wn, m)], o.ih2y);
             if (lo) cb = face_avg(ec, seps[code_at(wb, m)], o.ih2z);
@@ -362,7 +363,7 @@ __device__ __forceinline__ void seg_update(const Op<T>& o, T* __restrict__ x, co
             else { ct = T(0); electrode(pt, o.ih2z, o.vhi, extra, bcv); }
         } else {
             cw = face_beta(fw[m], o.ih2x);
-            ce = face_beta(m == SEG - 1 ? fh : fw[m + 1], o.ih2x);
+            ce = face_beta(m == SEG - 1 ? fr : fw[m + 1], o.ih2x);
             cs = face_beta(fs[m], o.ih2y);
             cn = face_beta(fn[m], o.ih2y);
             if (lo) cb = face_beta(fb[m], o.ih2z);
@@ -371,6 +372,43 @@ __device__ __forceinline__ void seg_update(const Op<T>& o, T* __restrict__ x, co
             else { ct = T(0); electrode0(ft[m], o.ih2z, extra); }
         }
         if (o.ny == 1) { cs = T(0); cn = T(0); }
+    }
+};
+
+// the half sweep of one segment; PAR: the in-segment offset of this colour's cells
+template <typename T, int SB, int KIND, bool ZERO, int PAR>
+__device__ __forceinline__ void seg_update(const Op<T>& o, T* __restrict__ x, const T* __restrict__ b, int i0, int j,
+                                           int k, const T* seps) {
+    constexpr int SEG = SegW<T, SB>::n;
+    const int row = o.nx * (j + o.ny * k);
+    const int c0 = row + i0;
+    int jm, jp;
+    nbr(j, o.ny, jm, jp);
+    const int so = (jm - j) * o.nx, no = (jp - j) * o.nx;
+    const bool lo = k > 0, hi = k < o.nz - 1;
+    // the x neighbour outside the segment: left of cell 0 (PAR 0) or right of cell SEG - 1 (PAR 1)
+    const int il = i0 == 0 ? o.nx - 1 : i0 - 1, ir = i0 + SEG == o.nx ? 0 : i0 + SEG;
+    T xc[SEG], bv[SEG];
+    T xs[SEG], xn[SEG], xb[SEG], xt[SEG];
+    ld_seg<T, SB>(x + c0, xc);
+    ldg_seg<T, SB>(b + c0, bv);
+    T xh = T(0);
+    if (!ZERO) {
+        xh = x[row + (PAR == 0 ? il : ir)];
+        ld_seg<T, SB>(x + c0 + so, xs);
+        ld_seg<T, SB>(x + c0 + no, xn);
+        if (lo) ld_seg<T, SB>(x + c0 - o.nxy, xb);
+        if (hi) ld_seg<T, SB>(x + c0 + o.nxy, xt);
+    }
+    T av[SEG];
+    if (o.a) ldg_seg<T, SB>(o.a + c0, av);
+    SegCoef<T, SB, KIND, PAR == 0, PAR == 1> cf;
+    cf.load(o, row, c0, so, no, k, lo, hi, il, ir);
+#pragma unroll
+    for (int u = 0; u < SEG / 2; ++u) {
+        const int m = 2 * u + PAR;
+        T cw, ce, cs, cn, cb, ct, extra, bcv;
+        cf.cell(o, seps, m, lo, hi, cw, ce, cs, cn, cb, ct, extra, bcv);
         const T diag = diag_sum(o.a ? av[m] : T(0), cw, ce, cs, cn, cb, ct, extra);
         if (ZERO) {
             xc[m] = sdiv(add_rn(bv[m], bcv), diag);
@@ -382,6 +420,40 @@ __device__ __forceinline__ void seg_update(const Op<T>& o, T* __restrict__ x, co
         xc[m] = sdiv(s, diag);
     }
     st_seg<T, SB>(x + c0, xc);
+}
+
+// the residual b - A x of the SEG cells of one row segment (every cell; both
+// halo cells read)
+template <typename T, int SB, int KIND>
+__device__ __forceinline__ void seg_resid_row(const Op<T>& o, const T* __restrict__ x, const T* __restrict__ b,
+                                              int i0, int j, int k, const T* seps, T (&r)[SegW<T, SB>::n]) {
+    constexpr int SEG = SegW<T, SB>::n;
+    const int row = o.nx * (j + o.ny * k);
+    const int c0 = row + i0;
+    int jm, jp;
+    nbr(j, o.ny, jm, jp);
+    const int so = (jm - j) * o.nx, no = (jp - j) * o.nx;
+    const bool lo = k > 0, hi = k < o.nz - 1;
+    const int il = i0 == 0 ? o.nx - 1 : i0 - 1, ir = i0 + SEG == o.nx ? 0 : i0 + SEG;
+    T xc[SEG], bv[SEG], xs[SEG], xn[SEG], xb[SEG], xt[SEG], av[SEG];
+    ld_seg<T, SB>(x + c0, xc);
+    ldg_seg<T, SB>(b + c0, bv);
+    const T xl = x[row + il], xr = x[row + ir];
+    ld_seg<T, SB>(x + c0 + so, xs);
+    ld_seg<T, SB>(x + c0 + no, xn);
+    if (lo) ld_seg<T, SB>(x + c0 - o.nxy, xb);
+    if (hi) ld_seg<T, SB>(x + c0 + o.nxy, xt);
+    if (o.a) ldg_seg<T, SB>(o.a + c0, av);
+    SegCoef<T, SB, KIND, true, true> cf;
+    cf.load(o, row, c0, so, no, k, lo, hi, il, ir);
+#pragma unroll
+    for (int m = 0; m < SEG; ++m) {
+        T cw, ce, cs, cn, cb, ct, extra, bcv;
+        cf.cell(o, seps, m, lo, hi, cw, ce, cs, cn, cb, ct, extra, bcv);
+        const T diag = diag_sum(o.a ? av[m] : T(0), cw, ce, cs, cn, cb, ct, extra);
+        r[m] = res_val(bv[m], bcv, diag, xc[m], cw, m == 0 ? xl : xc[m - 1], ce, m == SEG - 1 ? xr : xc[m + 1], cs,
+                       xs[m], cn, xn[m], lo, cb, xb[m], hi, ct, xt[m]);
+    }
 }
 
 template <typename T, int SB, int KIND, bool ZERO = false>
@@ -475,12 +547,11 @@ __device__ __forceinline__ double rr_cell(const Op<T>& o, const T* __restrict__ 
                 T cw, ce, cs, cn, cb, ct, diag, bcv;
                 coeffs<T, KIND>(o, i, j, k, c, im, ip, jm, jp, cw, ce, cs, cn, cb, ct, diag, bcv, seps);
                 const int row = c - i;
-                T off = cw * x[row + im] + ce * x[row + ip] + cs * x[c + (jm - j) * o.nx] +
-                        cn * x[c + (jp - j) * o.nx];
-                if (k > 0) off += cb * x[c - o.nxy];
-                if (k < o.nz - 1) off += ct * x[c + o.nxy];
-                const T r = (b[c] + bcv) - (diag * x[c] - off);
-                s += r;
+                const bool lo = k > 0, hi = k < o.nz - 1;
+                const T r = res_val(b[c], bcv, diag, x[c], cw, x[row + im], ce, x[row + ip], cs, x[c + (jm - j) * o.nx],
+                                    cn, x[c + (jp - j) * o.nx], lo, cb, lo ? x[c - o.nxy] : T(0), hi, ct,
+                                    hi ? x[c + o.nxy] : T(0));
+                s = add_rn(s, r);
                 mx = nan_max(mx, fabs((double)r));
             }
     bc[I + ncx * (J + ncy * K)] = s / T(RX * RY * RZ);
@@ -667,6 +738,15 @@ void launch_resid64(const Op<double>& o, dim3 g, dim3 b, cudaStream_t s, const d
 // weights (near parent, far neighbour), added to x; beyond an electrode the
 // far neighbour is the homogeneous Dirichlet value 0.  RX, RY, RZ are the
 // coarsening ratios (1 or 2), fixed at compile time.
+// the z-only prolongation of one fine cell: (1 - w) x(K0) + w x(K1), the far
+// term absent beyond an electrode (roundings written out: both launch forms
+// give the same bits)
+template <typename T>
+__device__ __forceinline__ T prolong_z_val(T w, T x0, T x1, bool zin) {
+    const T t0 = mul_rn(add_rn(T(1), -w), x0);
+    return zin ? fma_rn(w, x1, t0) : t0;
+}
+
 template <typename T, int RX, int RY, int RZ>
 __device__ __forceinline__ void prolong_cell(T* __restrict__ xf, const T* __restrict__ xc, const float* __restrict__ wx,
                                              const float* __restrict__ wy, const float* __restrict__ wz, int i, int j,
@@ -696,7 +776,7 @@ __device__ __forceinline__ void prolong_cell(T* __restrict__ xf, const T* __rest
         const T wxn = T(1) - wxf, wyn = T(1) - wyf;
         s = wyn * (wxn * X(I0, J0, K0) + wxf * X(I1, J0, K0)) + wyf * (wxn * X(I0, J1, K0) + wxf * X(I1, J1, K0));
     } else if (RZ == 2 && RX == 1 && RY == 1) {
-        s = (T(1) - wzf) * X(I0, J0, K0) + (zin ? wzf * X(I0, J0, K1) : T(0));
+        s = prolong_z_val(wzf, X(I0, J0, K0), X(I0, J0, K1), zin);
     } else {
         // remaining ratio patterns (single x or y direction, x-z, y-z)
         T acc = T(0);
@@ -714,7 +794,7 @@ __device__ __forceinline__ void prolong_cell(T* __restrict__ xf, const T* __rest
         }
         s = acc;
     }
-    xf[fc] += s;
+    xf[fc] = RZ == 2 && RX == 1 && RY == 1 ? add_rn(xf[fc], s) : xf[fc] + s;
 }
 
 // the coarse correction interpolated into the finer level and added
@@ -725,6 +805,89 @@ __global__ void __launch_bounds__(256) k_prolong(T* __restrict__ xf, const T* __
     pdl_entry();
     prolong_cell<T, RX, RY, RZ>(xf, xc, wx, wy, wz, blockIdx.x * blockDim.x + threadIdx.x,
                                 blockIdx.y * blockDim.y + threadIdx.y, blockIdx.z, nx, ny, nz, ncx, ncy, ncz);
+}
+
+// ---- row-segment forms of the z-semicoarsening transfers (ratios 1, 1, 2),
+// one 16- or 32-byte segment of a row per thread, as k_rbgs_seg
+
+// residual at the two fine cells of each coarse cell of a segment (fine
+// planes 2K and 2K + 1, same x and y), averaged into the coarse right-hand
+// side; optionally the |r|_inf of the level.  Same operations as
+// k_resid_restrict<T, KIND, 1, 1, 2>.
+template <typename T, int SB, int KIND>
+__global__ void __launch_bounds__(256) k_rr_z_seg(Op<T> o, const T* __restrict__ x, const T* __restrict__ b,
+                                                  T* __restrict__ bc, double* __restrict__ norm) {
+    pdl_entry();
+    __shared__ T seps[8];
+    if (KIND == CK_FINE) {
+        if (threadIdx.x == 0 && threadIdx.y == 0)
+#pragma unroll
+            for (int q = 0; q < 8; ++q) seps[q] = o.eps[q];
+        __syncthreads();
+    }
+    constexpr int SEG = SegW<T, SB>::n;
+    const int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * SEG;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int K = blockIdx.z;
+    double mx = 0.0;
+    if (j < o.ny) {
+        T acc[SEG], r[SEG];
+#pragma unroll
+        for (int m = 0; m < SEG; ++m) acc[m] = T(0);
+#pragma unroll
+        for (int dk = 0; dk < 2; ++dk) {
+            seg_resid_row<T, SB, KIND>(o, x, b, i0, j, 2 * K + dk, seps, r);
+#pragma unroll
+            for (int m = 0; m < SEG; ++m) {
+                acc[m] = add_rn(acc[m], r[m]);
+                mx = nan_max(mx, fabs((double)r[m]));
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < SEG; ++m) acc[m] = acc[m] / T(2);
+        st_seg<T, SB>(bc + i0 + o.nx * (j + o.ny * K), acc);
+    }
+    if (norm) {
+        const double m = block_max_all(mx);
+        const int slot = (blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)) & (NORM_SLOTS - 1);
+        if (threadIdx.x == 0 && threadIdx.y == 0) atomic_max_nonneg(norm + slot, m);
+    }
+}
+
+// the z-only prolongation of a row segment of fine plane k, added to xf
+// (same operations as k_prolong<T, 1, 1, 2>)
+template <typename T, int SB>
+__global__ void __launch_bounds__(256) k_prolong_z_seg(T* __restrict__ xf, const T* __restrict__ xc,
+                                                       const float* __restrict__ wz, int nx, int ny, int ncz) {
+    pdl_entry();
+    constexpr int SEG = SegW<T, SB>::n;
+    const int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * SEG;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (j >= ny) return;
+    const int K0 = k >> 1;
+    int K1 = (k & 1) ? K0 + 1 : K0 - 1;
+    const bool zin = K1 >= 0 && K1 < ncz;
+    if (!zin) K1 = K0;
+    const int fc = i0 + nx * (j + ny * k);
+    const int cc = i0 + nx * j;
+    T v[SEG], x0[SEG], x1[SEG];
+    float w[SEG];
+    ld_seg<T, SB>(xf + fc, v);
+    ldg_seg<T, SB>(xc + cc + nx * ny * K0, x0);
+    if (zin) ldg_seg<T, SB>(xc + cc + nx * ny * K1, x1);
+    if constexpr (SEG == 4) {
+        ldg16(wz + fc, w);
+    } else if constexpr (SEG == 8) {
+        ldg16(wz + fc, w);
+        ldg16(wz + fc + 4, w + 4);
+    } else {
+        const float2 q = __ldg(reinterpret_cast<const float2*>(wz + fc));
+        w[0] = q.x; w[1] = q.y;
+    }
+#pragma unroll
+    for (int m = 0; m < SEG; ++m) v[m] = add_rn(v[m], prolong_z_val(T(w[m]), x0[m], zin ? x1[m] : T(0), zin));
+    st_seg<T, SB>(xf + fc, v);
 }
 
 // ---------------------------------------------------------------------
@@ -1828,7 +1991,21 @@ void Multigrid::vcycle(const DevParams& p, const uint8_t* code, int l, T* x, con
         case 6: FX_RR(F, 2, 2, 1); break;             \
         default: FX_RR(F, 2, 2, 2); break;            \
         }
-        if (o.zc) { FX_RR_ALL(CK_PLANES) } else if (l == 0) { FX_RR_ALL(CK_FINE) } else { FX_RR_ALL(CK_ARRAYS) }
+        const int sb = key == 1 && (long long)L.N >= seg_min_cells && ((uintptr_t)bc % 16) == 0
+                           ? (seg_bytes == 32 && seg_shape<T, 32>(L, l, o, x, b) ? 32
+                              : seg_bytes == 16 && seg_shape<T, 16>(L, l, o, x, b) ? 16 : 0)
+                           : 0;
+        if (sb) {
+            // z-semicoarsening by row segments
+            const int gx = L.n[0] / (sb / (int)sizeof(T)), bx = gx < 32 ? gx : 32, by = 256 / bx;
+            dim3 bs(bx, by), gs(gx / bx, (L.n[1] + by - 1) / by, C.n[2]);
+#define FX_RRS(SB) \
+            if (o.zc) launch_k(k_rr_z_seg<T, SB, CK_PLANES>, gs, bs, 0, s, o, x, b, bc, norm); \
+            else if (l == 0) launch_k(k_rr_z_seg<T, SB, CK_FINE>, gs, bs, 0, s, o, x, b, bc, norm); \
+            else launch_k(k_rr_z_seg<T, SB, CK_ARRAYS>, gs, bs, 0, s, o, x, b, bc, norm);
+            if (sb == 32) { FX_RRS(32) } else { FX_RRS(16) }
+#undef FX_RRS
+        } else if (o.zc) { FX_RR_ALL(CK_PLANES) } else if (l == 0) { FX_RR_ALL(CK_FINE) } else { FX_RR_ALL(CK_ARRAYS) }
 #undef FX_RR_ALL
 #undef FX_RR
     }
@@ -1841,6 +2018,17 @@ void Multigrid::vcycle(const DevParams& p, const uint8_t* code, int l, T* x, con
         const int key = (C.cr[0] == 2) * 4 + (C.cr[1] == 2) * 2 + (C.cr[2] == 2);
         T* xc = lx<T>(C);
 #define FX_PR(RX, RY, RZ) launch_k(k_prolong<T, RX, RY, RZ>, g3, b2, 0, s, x, xc, C.wf[0], C.wf[1], C.wf[2], L.n[0], L.n[1], L.n[2], C.n[0], C.n[1], C.n[2])
+        auto al16 = [](const void* q) { return ((uintptr_t)q % 16) == 0; };
+        const int sb = key == 1 && (long long)L.N >= seg_min_cells && al16(xc) && al16(C.wf[2])
+                           ? (seg_bytes == 32 && seg_shape<T, 32>(L, l, o, x, b) ? 32
+                              : seg_bytes == 16 && seg_shape<T, 16>(L, l, o, x, b) ? 16 : 0)
+                           : 0;
+        if (sb) {
+            const int gx = L.n[0] / (sb / (int)sizeof(T)), bx = gx < 32 ? gx : 32, by = 256 / bx;
+            dim3 bs(bx, by), gs(gx / bx, (L.n[1] + by - 1) / by, L.n[2]);
+            if (sb == 32) launch_k(k_prolong_z_seg<T, 32>, gs, bs, 0, s, x, xc, C.wf[2], L.n[0], L.n[1], C.n[2]);
+            else launch_k(k_prolong_z_seg<T, 16>, gs, bs, 0, s, x, xc, C.wf[2], L.n[0], L.n[1], C.n[2]);
+        } else
         switch (key) {
         case 1: FX_PR(1, 1, 2); break;
         case 2: FX_PR(1, 2, 1); break;
