@@ -640,7 +640,7 @@ __global__ void __launch_bounds__(256) k_resid64(Op<double> o, const double* __r
     pdl_entry();
     // a step graph's exact residual after a V-cycle, not needed this time
     if (rc.mode == RC_RN && !rc.ctl->need) return;
-    auto X = [&](int n) -> double { return CORR ? x[n] + (double)e[n] : x[n]; };
+    auto X = [&](int n) -> double { return CORR ? add_rn(x[n], (double)e[n]) : x[n]; };
     __shared__ double seps[8];
     if (threadIdx.x == 0 && threadIdx.y == 0)
 #pragma unroll
@@ -673,33 +673,30 @@ __global__ void __launch_bounds__(256) k_resid64(Op<double> o, const double* __r
             if constexpr (KIND == CK_PLANES) {
                 // a layered stack: the same face values per z plane, as the
                 // setup formed them from the codes (same operations)
-                cw = ce = __ldg(o.zc + k) * o.ih2x;
-                cs = cn = __ldg(o.zc + o.nz + k) * o.ih2y;
+                cw = ce = face_beta(__ldg(o.zc + k), o.ih2x);
+                cs = cn = face_beta(__ldg(o.zc + o.nz + k), o.ih2y);
                 const double fb = __ldg(o.zc + 2 * o.nz + k), ft = __ldg(o.zc + 2 * o.nz + k + 1);
-                if (k > 0) cb = fb * o.ih2z;
-                else { cb = 0.0; extra += 2.0 * fb * o.ih2z; bcv += 2.0 * fb * o.ih2z * o.vlo; }
-                if (k < o.nz - 1) ct = ft * o.ih2z;
-                else { ct = 0.0; extra += 2.0 * ft * o.ih2z; bcv += 2.0 * ft * o.ih2z * o.vhi; }
+                if (k > 0) cb = face_beta(fb, o.ih2z);
+                else { cb = 0.0; electrode(fb, o.ih2z, o.vlo, extra, bcv); }
+                if (k < o.nz - 1) ct = face_beta(ft, o.ih2z);
+                else { ct = 0.0; electrode(ft, o.ih2z, o.vhi, extra, bcv); }
             } else {
                 ep = seps[__ldg(cd + c + o.nxy) & 7];
-                cw = 0.5 * (ec + seps[__ldg(cd + row + o.nxy * k + im) & 7]) * o.ih2x;
-                ce = 0.5 * (seps[__ldg(cd + row + o.nxy * k + ip) & 7] + ec) * o.ih2x;
-                cs = 0.5 * (ec + seps[__ldg(cd + c + dso) & 7]) * o.ih2y;
-                cn = 0.5 * (seps[__ldg(cd + c + dno) & 7] + ec) * o.ih2y;
-                if (k > 0) cb = 0.5 * (ec + em) * o.ih2z;
-                else { cb = 0.0; extra += 2.0 * ec * o.ih2z; bcv += 2.0 * ec * o.ih2z * o.vlo; }
-                if (k < o.nz - 1) ct = 0.5 * (ep + ec) * o.ih2z;
-                else { ct = 0.0; extra += 2.0 * ec * o.ih2z; bcv += 2.0 * ec * o.ih2z * o.vhi; }
+                cw = face_avg(ec, seps[__ldg(cd + row + o.nxy * k + im) & 7], o.ih2x);
+                ce = face_avg(ec, seps[__ldg(cd + row + o.nxy * k + ip) & 7], o.ih2x);
+                cs = face_avg(ec, seps[__ldg(cd + c + dso) & 7], o.ih2y);
+                cn = face_avg(ec, seps[__ldg(cd + c + dno) & 7], o.ih2y);
+                if (k > 0) cb = face_avg(ec, em, o.ih2z);
+                else { cb = 0.0; electrode(ec, o.ih2z, o.vlo, extra, bcv); }
+                if (k < o.nz - 1) ct = face_avg(ec, ep, o.ih2z);
+                else { ct = 0.0; electrode(ec, o.ih2z, o.vhi, extra, bcv); }
             }
             if (o.nx == 1) { cw = 0.0; ce = 0.0; }
             if (o.ny == 1) { cs = 0.0; cn = 0.0; }
-            const double a = o.a ? o.a[c] : 0.0;
-            const double diag = -a + cw + ce + cs + cn + cb + ct + extra;
+            const double diag = diag_sum(o.a ? o.a[c] : 0.0, cw, ce, cs, cn, cb, ct, extra);
             const int rk = row + o.nxy * k;
-            double off = cw * X(rk + im) + ce * X(rk + ip) + cs * X(c + dso) + cn * X(c + dno);
-            if (k > 0) off += cb * xm;
-            if (k < o.nz - 1) off += ct * xp;
-            const double r = (b[c] + bcv) - (diag * xc - off);
+            const double r = res_val(b[c], bcv, diag, xc, cw, X(rk + im), ce, X(rk + ip), cs, X(c + dso), cn, X(c + dno),
+                                     k > 0, cb, xm, k < o.nz - 1, ct, xp);
             if (r32) r32[c] = (float)r;
             if (CORR) xout[c] = xc;
             mx = nan_max(mx, fabs(r));
@@ -726,10 +723,138 @@ __global__ void __launch_bounds__(256) k_resid64(Op<double> o, const double* __r
     }
 }
 
-// k_resid64 with the face coefficients by plane when level 0 has them
+// the FP32 copies of a segment's residuals (SEG floats: 8 or 16 bytes)
+template <int SEG>
+__device__ __forceinline__ void st_r32(float* p, const double (&r)[SEG]) {
+    if constexpr (SEG == 2) {
+        *reinterpret_cast<float2*>(p) = make_float2((float)r[0], (float)r[1]);
+    } else {
+        float v[4] = {(float)r[0], (float)r[1], (float)r[2], (float)r[3]};
+        asm volatile("st.global.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3])
+                     : "memory");
+    }
+}
+
+// the iterate of a segment: x, or x + e (the FP32 correction added in FP64)
+template <bool CORR, int SB>
+__device__ __forceinline__ void ld_iter(const double* x, const float* e, int c, double (&v)[SegW<double, SB>::n]) {
+    constexpr int SEG = SegW<double, SB>::n;
+    ldg_seg<double, SB>(x + c, v);
+    if constexpr (CORR) {
+        float f[SEG];
+        if constexpr (SEG == 2) {
+            const float2 q = __ldg(reinterpret_cast<const float2*>(e + c));
+            f[0] = q.x; f[1] = q.y;
+        } else {
+            ldg16(e + c, f);
+        }
+#pragma unroll
+        for (int m = 0; m < SEG; ++m) v[m] = add_rn(v[m], (double)f[m]);
+    }
+}
+
+// k_resid64 by row segments: each thread takes one SB-byte segment of a row
+// (2 or 4 cells) through R64_ZP consecutive planes, the iterate of the planes
+// k - 1, k, k + 1 carried in registers.  Same operations per cell as
+// k_resid64, so the same bits.
+template <bool CORR, int KIND, int SB>
+__global__ void __launch_bounds__(256) k_resid64_seg(Op<double> o, const double* __restrict__ x,
+                                                     const float* __restrict__ e, const double* __restrict__ b,
+                                                     double* __restrict__ xout, float* __restrict__ r32,
+                                                     double* __restrict__ norm, ResidCtl rc) {
+    pdl_entry();
+    if (rc.mode == RC_RN && !rc.ctl->need) return;
+    constexpr int SEG = SegW<double, SB>::n;
+    __shared__ double seps[8];
+    if (threadIdx.x == 0 && threadIdx.y == 0)
+#pragma unroll
+        for (int q = 0; q < 8; ++q) seps[q] = o.eps[q];
+    __syncthreads();
+    const int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * SEG;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k0 = blockIdx.z * R64_ZP;
+    double mx = 0.0;
+    if (j < o.ny) {
+        int jm, jp;
+        nbr(j, o.ny, jm, jp);
+        const int so = (jm - j) * o.nx, no = (jp - j) * o.nx;
+        const int il = i0 == 0 ? o.nx - 1 : i0 - 1, ir = i0 + SEG == o.nx ? 0 : i0 + SEG;
+        auto X = [&](int n) -> double { return CORR ? add_rn(__ldg(x + n), (double)__ldg(e + n)) : __ldg(x + n); };
+        double xm[SEG], xc[SEG], xp[SEG];
+        const int col = i0 + o.nx * j;
+        if (k0 > 0) ld_iter<CORR, SB>(x, e, col + o.nxy * (k0 - 1), xm);
+        ld_iter<CORR, SB>(x, e, col + o.nxy * k0, xc);
+#pragma unroll
+        for (int q = 0; q < R64_ZP; ++q) {
+            const int k = k0 + q;
+            if (k >= o.nz) break;
+            const int row = o.nx * (j + o.ny * k);
+            const int c0 = row + i0;
+            const bool lo = k > 0, hi = k < o.nz - 1;
+            if (hi) ld_iter<CORR, SB>(x, e, c0 + o.nxy, xp);
+            double xs[SEG], xn[SEG], bv[SEG], av[SEG];
+            ld_iter<CORR, SB>(x, e, c0 + so, xs);
+            ld_iter<CORR, SB>(x, e, c0 + no, xn);
+            const double xl = X(row + il), xr = X(row + ir);
+            ldg_seg<double, SB>(b + c0, bv);
+            if (o.a) ldg_seg<double, SB>(o.a + c0, av);
+            SegCoef<double, SB, KIND, true, true> cf;
+            cf.load(o, row, c0, so, no, k, lo, hi, il, ir);
+            double r[SEG];
+#pragma unroll
+            for (int m = 0; m < SEG; ++m) {
+                double cw, ce, cs, cn, cb, ct, extra, bcv;
+                cf.cell(o, seps, m, lo, hi, cw, ce, cs, cn, cb, ct, extra, bcv);
+                const double diag = diag_sum(o.a ? av[m] : 0.0, cw, ce, cs, cn, cb, ct, extra);
+                r[m] = res_val(bv[m], bcv, diag, xc[m], cw, m == 0 ? xl : xc[m - 1], ce, m == SEG - 1 ? xr : xc[m + 1],
+                               cs, xs[m], cn, xn[m], lo, cb, xm[m], hi, ct, xp[m]);
+                mx = nan_max(mx, fabs(r[m]));
+            }
+            if (r32) st_r32<SEG>(r32 + c0, r);
+            if (CORR) st_seg<double, SB>(xout + c0, xc);
+#pragma unroll
+            for (int m = 0; m < SEG; ++m) { xm[m] = xc[m]; xc[m] = xp[m]; }
+        }
+    }
+    const double m = block_max_all(mx);
+    const int slot = (blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)) & (NORM_SLOTS - 1);
+    if (threadIdx.x == 0 && threadIdx.y == 0) atomic_max_nonneg(norm + slot, m);
+    if (rc.ctl) {
+        // a step graph: the last block tests the solve's loop on the norm
+        __shared__ bool last;
+        if (threadIdx.x == 0 && threadIdx.y == 0) {
+            __threadfence();
+            last = atomicAdd(rc.counter, 1u) == gridDim.x * gridDim.y * gridDim.z - 1;
+        }
+        __syncthreads();
+        if (last && threadIdx.x == 0 && threadIdx.y == 0) {
+            __threadfence();
+            resid_ctl(rc, norm);
+            *rc.counter = 0;
+        }
+    }
+}
+
+// k_resid64 with the face coefficients by plane when level 0 has them; by
+// row segments of sb = 32 bytes where level 0's rows and the arrays'
+// alignment allow (sb = 0: one column of cells per thread)
 template <bool CORR>
 void launch_resid64(const Op<double>& o, dim3 g, dim3 b, cudaStream_t s, const double* x, const float* e,
-                    const double* rhs, double* xout, float* r32, double* norm, const ResidCtl& rc) {
+                    const double* rhs, double* xout, float* r32, double* norm, const ResidCtl& rc, int sb = 0) {
+    if (sb == 32) {
+        const int seg = sb / 8;
+        const int gx = o.nx / seg;
+        auto al = [](const void* p, uintptr_t a) { return ((uintptr_t)p % a) == 0; };
+        const bool ok = o.nx % seg == 0 && (gx % 32 == 0 || 32 % gx == 0) && al(x, 16) && al(rhs, 16) && al(o.a, 16) &&
+                        al(e, 4 * seg) && al(xout, 16) && al(r32, 4 * seg) && (o.zc || al(o.code + o.nxy, seg));
+        if (ok) {
+            const int bx = gx < 32 ? gx : 32, by = 256 / bx;
+            dim3 bs(bx, by), gs(gx / bx, (o.ny + by - 1) / by, (o.nz + R64_ZP - 1) / R64_ZP);
+            if (o.zc) launch_k(k_resid64_seg<CORR, CK_PLANES, 32>, gs, bs, 0, s, o, x, e, rhs, xout, r32, norm, rc);
+            else launch_k(k_resid64_seg<CORR, CK_FINE, 32>, gs, bs, 0, s, o, x, e, rhs, xout, r32, norm, rc);
+            return;
+        }
+    }
     if (o.zc) launch_k(k_resid64<CORR, CK_PLANES>, g, b, 0, s, o, x, e, rhs, xout, r32, norm, rc);
     else launch_k(k_resid64<CORR, CK_FINE>, g, b, 0, s, o, x, e, rhs, xout, r32, norm, rc);
 }
@@ -2052,7 +2177,7 @@ int Multigrid::residual64(const DevParams& p, const uint8_t* code, const double*
     dim3 b2(32, 8), g2((L.n[0] + 31) / 32, (L.n[1] + 7) / 8, L.n[2]);
     (void)r;
     if (prof) prof->begin(PROF_RESID64, s);
-    { ++g_launches; launch_resid64<false>(o, dim3(g2.x, g2.y, (L.n[2] + R64_ZP - 1) / R64_ZP), b2, s, phi, nullptr, rhs, nullptr, nullptr, d_norm_, ResidCtl{}); }
+    { ++g_launches; launch_resid64<false>(o, dim3(g2.x, g2.y, (L.n[2] + R64_ZP - 1) / R64_ZP), b2, s, phi, nullptr, rhs, nullptr, nullptr, d_norm_, ResidCtl{}, res_seg()); }
     if (prof) prof->end(s);
     cudaMemcpyAsync(h_norm_, d_norm_, NORM_SLOTS * 8, cudaMemcpyDeviceToHost, s);
     cudaError_t e = cudaStreamSynchronize(s);
@@ -2138,7 +2263,7 @@ int Multigrid::solve_mixed(const DevParams& p, const uint8_t* code, double* phi,
     cudaMemsetAsync(d_norm_, 0, NORM_SLOTS * 8, s);
     if (prof) prof->begin(PROF_RESID64, s);
     ++g_launches;
-    launch_resid64<false>(o64, g2, b2, s, phi, nullptr, rhs, nullptr, r32_, d_norm_, ResidCtl{});
+    launch_resid64<false>(o64, g2, b2, s, phi, nullptr, rhs, nullptr, r32_, d_norm_, ResidCtl{}, res_seg());
     if (prof) prof->end(s);
     cudaMemcpyAsync(h_norm_, d_norm_, NORM_SLOTS * 8, cudaMemcpyDeviceToHost, s);
     int e = (int)cudaStreamSynchronize(s);
@@ -2157,7 +2282,7 @@ int Multigrid::solve_mixed(const DevParams& p, const uint8_t* code, double* phi,
             cudaMemsetAsync(d_norm_, 0, NORM_SLOTS * 8, s);
             if (prof) prof->begin(PROF_RESID64, s);
             ++g_launches;
-            launch_resid64<true>(o64, g2, b2, s, xin, e32_, rhs, xout, r32_, d_norm_, ResidCtl{});
+            launch_resid64<true>(o64, g2, b2, s, xin, e32_, rhs, xout, r32_, d_norm_, ResidCtl{}, res_seg());
             if (prof) prof->end(s);
             cudaMemcpyAsync(h_norm_, d_norm_, NORM_SLOTS * 8, cudaMemcpyDeviceToHost, s);
         });
@@ -2197,14 +2322,14 @@ void Multigrid::enqueue_solve64_ctl(const DevParams& p, const uint8_t* code, dou
     // the norm slots are zero between uses
     ResidCtl rb = {ctl, RC_BEGIN, nb, rtol, maxit, 0, 0, 0, hw, hw, rc_counter_};
     ++g_launches;
-    launch_resid64<false>(o, g2, b2, s, phi, nullptr, rhs, nullptr, nullptr, d_norm_, rb);
+    launch_resid64<false>(o, g2, b2, s, phi, nullptr, rhs, nullptr, nullptr, d_norm_, rb, res_seg());
     cap.node(s, cudaGraphCondTypeWhile, hw, KIND_MG_CYCLE, [&](cudaStream_t b) {
         vcycle<double>(p, code, 0, phi, rhs, true, b, false);
         ++g_launches;
         launch_k(k_mg_mid, 1, 1, 0, b, d_norm_, single, maxit, ctl, hw);
         ResidCtl rr = {ctl, RC_RN, nullptr, 0.0, maxit, 0, 0, 0, hw, hw, rc_counter_};
         ++g_launches;
-        launch_resid64<false>(o, g2, b2, b, phi, nullptr, rhs, nullptr, nullptr, d_norm_, rr);
+        launch_resid64<false>(o, g2, b2, b, phi, nullptr, rhs, nullptr, nullptr, d_norm_, rr, res_seg());
     });
     if (!end_in_next) {
         ++g_launches;
@@ -2227,11 +2352,11 @@ void Multigrid::enqueue_solve_mixed_ctl(const DevParams& p, const uint8_t* code,
     const cudaGraphConditionalHandle hw = cap.handle(s);
     ResidCtl rb = {ctl, RC_BEGIN, nb, rtol, maxit, 0, 0, 0, hw, hw, rc_counter_};
     ++g_launches;
-    launch_resid64<false>(o64, g2, b2, s, phi, nullptr, rhs, nullptr, r32_, d_norm_, rb);
+    launch_resid64<false>(o64, g2, b2, s, phi, nullptr, rhs, nullptr, r32_, d_norm_, rb, res_seg());
     auto refine = [&](cudaStream_t q, const double* xin, double* xout, const ResidCtl& rc) {
         for (int k = 0; k < inner; ++k) vcycle<float>(p, code, 0, e32_, r32_, false, q, k == 0);
         ++g_launches;
-        launch_resid64<true>(o64, g2, b2, q, xin, e32_, rhs, xout, r32_, d_norm_, rc);
+        launch_resid64<true>(o64, g2, b2, q, xin, e32_, rhs, xout, r32_, d_norm_, rc, res_seg());
     };
     cap.node(s, cudaGraphCondTypeWhile, hw, KIND_MX_FIRST, [&](cudaStream_t b) {
         const cudaGraphConditionalHandle hif = cap.handle(b);

@@ -135,6 +135,10 @@ public:
 
 private:
     std::vector<MGLevel> lev_;
+    // the segment width for level 0's FP64 residual: 32 bytes whenever the
+    // smoother runs by segments (measured faster than 16 for this kernel); 0:
+    // one column of cells per thread
+    int res_seg() const { return seg_bytes && !lev_.empty() && (long long)lev_[0].N >= seg_min_cells ? 32 : 0; }
     double eps_[8];
     const double* a0_64 = nullptr;
     const float* a0_32 = nullptr;
