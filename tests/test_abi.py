@@ -136,6 +136,7 @@ def test_multigrid_defaults_read_back():
     f = api.FerroX(decks.mfim(8, 8, 12))
     assert (f.param("fx.mg_nu1"), f.param("fx.mg_nu2"), f.param("fx.mg_mixed_cycles")) == (2, 1, 2)
     assert f.param("fx.alpha_tiles") == 1 and f.param("fx.phi_extrapolate") == 4
+    assert (f.param("fx.mg_nu1_coarse"), f.param("fx.mg_nu2_coarse"), f.param("fx.mg_seg")) == (1, -1, 16)
     f.close()
 
 
