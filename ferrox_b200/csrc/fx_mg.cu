@@ -1967,7 +1967,8 @@ static CoarseArgs make_coarse_args(const std::vector<MGLevel>& lev_, int top, in
 
 template <typename T>
 void Multigrid::launch_coarse(int top, cudaStream_t s) {
-    const CoarseArgs A = make_coarse_args<T>(lev_, top, nu1, nu2, nu_bottom, has_alpha_, d_fvalid_);
+    const CoarseArgs A = make_coarse_args<T>(lev_, top, nu1c >= 0 ? nu1c : nu1, nu2c >= 0 ? nu2c : nu2, nu_bottom,
+                                             has_alpha_, d_fvalid_);
     const size_t bytes = coarse_bytes(lev_, top, sizeof(T), nullptr);
     if (prof) prof->begin(PROF_COARSE_CTA, s);
     ++g_launches;

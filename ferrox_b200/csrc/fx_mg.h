@@ -122,9 +122,9 @@ public:
     size_t bytes() const { return bytes_; }
     const std::vector<MGLevel>& levels() const { return lev_; }
     int nu1 = 2, nu2 = 1, nu_bottom = 40;
-    // sweeps on the levels below level 0 (-1: nu1 / nu2); the one-CTA levels
-    // use nu1 / nu2.  One pre-smoothing sweep below level 0 measured fastest on
-    // the polycrystal (both precisions) and the MFISM stack
+    // sweeps on the levels below level 0, the one-CTA levels included (-1: nu1
+    // / nu2).  One pre-smoothing sweep below level 0 measured fastest on the
+    // polycrystal (both precisions) and the MFISM stack
     int nu1c = 1, nu2c = -1;
     int mixed_cycles = 2;    // FP32 V-cycles per FP64 refinement step
     bool alpha_tiles = true; // coarse alphas below level 1 in one launch (k_alpha_tiles)
