@@ -142,6 +142,7 @@ struct fx_ctx {
     uint8_t* d_interior = nullptr;       // DevParams::interior flags
     bool use_interior = true;            // fx.interior
     bool adj_store_phi = true;           // fx.adjoint_store_phi
+    bool adj_extrap = true;          // the adjoint solves start from psi extrapolated in reverse time
     double* adj_phi_store = nullptr;     // the record's phi of every step; kept between records
     size_t adj_phi_store_n = 0;          // its length in doubles
     Variant* d_vt = nullptr;
@@ -208,6 +209,8 @@ struct fx_ctx {
         double* lam[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
         int lcur = 0;
         double *mu = nullptr, *psi = nullptr, *drho = nullptr, *grad = nullptr, *dV = nullptr, *hist = nullptr;
+        double* psiHist[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};   // psi of the last reverse steps
+        int psi_n = 0;                             // reverse steps of psi history held
         float* drho32 = nullptr;
         uint8_t* gid = nullptr;
         bool have_P0 = false;
@@ -1416,6 +1419,8 @@ int backward(fx_ctx* c, double* grads, int ngrads) {
             for (int d = d0; d < 3; ++d) if ((r = adj_alloc(c, &A.lam[b][d], c->N))) return r;
         if ((r = adj_alloc(c, &A.mu, c->N))) return r;
         if ((r = adj_alloc(c, &A.psi, c->N))) return r;
+        for (int q = 0; q < std::min(kMaxExtrap, c->par.phi_extrapolate); ++q)
+            if ((r = adj_alloc(c, &A.psiHist[q], c->N))) return r;
         if (sc && ((r = adj_alloc(c, &A.drho, c->N)) || (r = adj_alloc(c, &A.drho32, c->N)))) return r;
         if ((r = adj_alloc(c, &A.grad, 8 + 256))) return r;
         if ((r = adj_alloc(c, &A.dV, (size_t)T))) return r;
@@ -1427,6 +1432,7 @@ int backward(fx_ctx* c, double* grads, int ngrads) {
     FX_CUDA(c, cudaMemsetAsync(A.grad, 0, (8 + 256) * 8, c->s));
     FX_CUDA(c, cudaMemsetAsync(A.dV, 0, (size_t)T * 8, c->s));
     FX_CUDA(c, cudaMemsetAsync(A.psi, 0, c->N * 8, c->s));
+    A.psi_n = 0;
     // dL/d<Pz>^n spread over the FE cells
     std::vector<double> g(T + 1, 0.0);
     for (int n = 1; n <= T; ++n) g[n] = 2.0 / T * (A.m[n - 1] - A.target[n - 1]) / (double)A.nfe;
@@ -1478,6 +1484,21 @@ int backward(fx_ctx* c, double* grads, int ngrads) {
                     } else {
                         c->mg.set_alpha(nullptr, nullptr, false, c->s);
                     }
+                    // the initial iterate: psi extrapolated in reverse time through the
+                    // solutions of the last reverse steps (the forward's phi rule); the
+                    // solve still runs to the residual bound
+                    int order = 0;
+                    while (order < 6 && A.psiHist[order]) ++order;
+                    if (order > 0 && c->par.warm_start && c->adj_extrap) {
+                        const int use = std::min(order, A.psi_n);
+                        if (use > 0) {
+                            ++g_launches;
+                            if ((r = k_status(c, launch_phi_extrap(c->dp, use, A.psi, A.psiHist, c->s)))) return r;
+                        } else {
+                            FX_CUDA(c, cudaMemcpyAsync(A.psiHist[0], A.psi, c->N * 8, cudaMemcpyDeviceToDevice, c->s));
+                        }
+                        A.psi_n = std::min(order, A.psi_n + 1);
+                    }
                     const double target = std::max(c->par.mg_rtol, 1e-16) * nmu;
                     MGStats st;
                     int e = mixed ? c->mg.solve_mixed(dp0, c->d_code, A.psi, A.mu, target, c->par.mg_max_iter, c->s, &st)
@@ -1490,6 +1511,8 @@ int backward(fx_ctx* c, double* grads, int ngrads) {
                     }
                     if (e) return set_err(c, FX_ERR_CUDA, std::string("multigrid: ") + cudaGetErrorString((cudaError_t)e));
                     psi = A.psi;
+                } else {
+                    A.psi_n = 0;   // psi = 0 this step: the history starts again
                 }
             }
             const double* Pn[3] = {A.segP[3 * idx], A.segP[3 * idx + 1], A.segP[3 * idx + 2]};
@@ -1756,6 +1779,7 @@ int fx_get_param(const fx_ctx* c, const char* key, double* v) {
         {"fx.mg_seg", (double)c->mg.seg_bytes}, {"fx.mg_seg_min", (double)c->mg.seg_min_cells},
         {"fx.mg_nu1_coarse", (double)c->mg.nu1c}, {"fx.mg_nu2_coarse", (double)c->mg.nu2c},
         {"fx.interior", c->use_interior ? 1.0 : 0.0}, {"fx.adjoint_store_phi", c->adj_store_phi ? 1.0 : 0.0},
+        {"fx.adjoint_extrapolate", c->adj_extrap ? 1.0 : 0.0},
         {"adjoint_phi_stored", c->adj.phiAll ? 1.0 : 0.0},
         {"step_graph_ran", c->sg_ran ? 1.0 : 0.0}, {"fx.pdl", g_pdl ? 1.0 : 0.0},
         // 1 when level 0's face coefficients depend on z only and its smoother
@@ -1800,7 +1824,7 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
     static const char* const known[] = {
         "Phi_Bc_hi", "Phi_Bc_lo", "fx.mg_rtol", "fx.mg_max_iter", "fx.newton_max_iter", "fx.warm_start",
         "fx.phi_extrapolate", "fx.step_graph", "fx.pdl", "fx.verbose", "fx.profile", "fx.mg_nu1", "fx.graphs",
-        "fx.mg_nu2", "fx.alpha_tiles", "fx.interior", "fx.adjoint_store_phi", "fx.mg_nu1_coarse", "fx.mg_nu2_coarse", "fx.mg_seg", "fx.mg_seg_min", "fx.mg_mixed_cycles", "fx.phi_ghost_mode", "dt", "alpha", "fx.newton_tol",
+        "fx.mg_nu2", "fx.alpha_tiles", "fx.interior", "fx.adjoint_store_phi", "fx.adjoint_extrapolate", "fx.mg_nu1_coarse", "fx.mg_nu2_coarse", "fx.mg_seg", "fx.mg_seg_min", "fx.mg_mixed_cycles", "fx.phi_ghost_mode", "dt", "alpha", "fx.newton_tol",
         "beta", "gamma", "g11", "g44", "BigGamma", "inc_step"};
     bool is_known = false;
     for (const char* q : known) is_known = is_known || k == q;
@@ -1830,7 +1854,8 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
     if (k == "fx.mg_seg_min" && !(v >= 0))
         return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx.mg_seg_min must not be negative");
     if (k != "fx.profile" && k != "fx.verbose" && k != "fx.graphs" && k != "fx.step_graph" && k != "fx.pdl" &&
-        k != "fx.alpha_tiles" && k != "fx.interior" && k != "fx.adjoint_store_phi" && k != "fx.mg_seg" &&
+        k != "fx.alpha_tiles" && k != "fx.interior" && k != "fx.adjoint_store_phi" && k != "fx.adjoint_extrapolate" &&
+        k != "fx.mg_seg" &&
         k != "fx.mg_seg_min")
         ++c->gen;
     // the time history of phi only seeds the next solve's initial iterate;
@@ -1856,6 +1881,7 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
     if (k == "fx.mg_seg") { c->mg.seg_bytes = (int)v; return FX_OK; }
     if (k == "fx.mg_seg_min") { c->mg.seg_min_cells = (long long)std::min(v, 9.0e18); return FX_OK; }
     if (k == "fx.adjoint_store_phi") { c->adj_store_phi = v != 0.0; return FX_OK; }
+    if (k == "fx.adjoint_extrapolate") { c->adj_extrap = v != 0.0; return FX_OK; }
     if (k == "fx.mg_nu1_coarse") { c->mg.nu1c = (int)v; return FX_OK; }
     if (k == "fx.mg_nu2_coarse") { c->mg.nu2c = (int)v; return FX_OK; }
     if (k == "fx.interior") {

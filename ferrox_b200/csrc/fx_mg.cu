@@ -2027,6 +2027,11 @@ template <typename T>
 void Multigrid::smooth(const DevParams& p, const uint8_t* code, int l, T* x, const T* b, bool inhom, int sweeps,
                        cudaStream_t s, bool zero) {
     MGLevel& L = lev_[l];
+    if (zero && sweeps == 0) {
+        // no sweep to start from zero (fx.mg_nu1 = 0): the correction is zero
+        cudaMemsetAsync(x, 0, L.N * sizeof(T), s);
+        return;
+    }
     const T* a = nullptr;
     if (has_alpha_) {
         if (l == 0) { if constexpr (sizeof(T) == 8) a = (const T*)a0_64; else a = (const T*)a0_32; }

@@ -271,3 +271,21 @@ def test_segment_smoother_bit_identical(case):
             assert (ca, na) == (cb, nb), (graph, seg, ca, cb, na, nb)
             for n in FIELDS:
                 assert np.array_equal(a[n], b[n]), (graph, seg, n, np.abs(a[n] - b[n]).max())
+
+
+def test_no_pre_smoothing_starts_from_a_zero_correction():
+    """fx.mg_nu1 = 0 (no pre-smoothing on level 0): the mixed path's FP32
+    correction cycle starts from zero without a sweep to clear it, so the
+    smoother clears it; the fields match the default cycle's to the solver
+    tolerance."""
+    text = decks.mfim(32, 32, 24, Phi_Bc_hi=0.8)
+    P = start_P((24, 32, 32), 3)
+    out = []
+    for nu1 in (2, 0):
+        f = make(text, P, 1, precision="mixed", params={"fx.mg_nu1": nu1})
+        f.step(4)
+        out.append({n: f.field(n) for n in ("Pz", "Phi")})
+        f.close()
+    for n in ("Pz", "Phi"):
+        scale = np.abs(out[0][n]).max()
+        assert np.abs(out[0][n] - out[1][n]).max() <= 1e-7 * scale, n
