@@ -478,6 +478,118 @@ __global__ void __launch_bounds__(256) k_rbgs_seg(Op<T> o, T* __restrict__ x, co
     else seg_update<T, SB, KIND, ZERO, 1>(o, x, b, i0, j, k, seps);
 }
 
+// ---- the split (red-black) layout of level 0's FP32 arrays in the mixed path
+//
+// The FP32 correction x and right-hand side b of level 0 hold the cells of
+// colour c = (i + j + k) & 1 at [c * N/2 + (n >> 1)], n = i + nx (j + ny k)
+// the natural index (nx even: the two cells of an x pair share n >> 1, one
+// of each colour).  A half sweep then reads only the other colour's values
+// of its neighbours and writes only its own colour, every sector it moves
+// fully used.  A thread takes 8 natural cells of a row (i0 a multiple of 8):
+// its 4 cells of one colour are 16 contiguous bytes of that colour's array.
+
+// the 8 natural-order values of cells n0 .. n0 + 7 (n0 a multiple of 8) of a
+// split array; ce: the colour of the even positions
+__device__ __forceinline__ void ld_split8(const float* a, int Nh, int n0, int ce, float (&v)[8]) {
+    float e[4], o[4];
+    ld16(a + ce * Nh + (n0 >> 1), e);
+    ld16(a + (1 - ce) * Nh + (n0 >> 1), o);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) { v[2 * u] = e[u]; v[2 * u + 1] = o[u]; }
+}
+
+// the same for 4 natural cells (n0 a multiple of 4): 8 bytes of each colour
+__device__ __forceinline__ void ld_split4(const float* a, int Nh, int n0, int ce, float (&v)[4]) {
+    const float2 e = *reinterpret_cast<const float2*>(a + ce * Nh + (n0 >> 1));
+    const float2 o = *reinterpret_cast<const float2*>(a + (1 - ce) * Nh + (n0 >> 1));
+    v[0] = e.x; v[1] = o.x; v[2] = e.y; v[3] = o.y;
+}
+template <int NC>
+__device__ __forceinline__ void ld_splitn(const float* a, int Nh, int n0, int ce, float (&v)[NC]) {
+    if constexpr (NC == 8) ld_split8(a, Nh, n0, ce, v);
+    else ld_split4(a, Nh, n0, ce, v);
+}
+
+// one natural cell n of colour c
+__device__ __forceinline__ float at_split(const float* a, int Nh, int n, int c) { return a[c * Nh + (n >> 1)]; }
+
+// the half sweep of the 4 colour-`color` cells of 8 natural cells; PAR: their
+// offset in the 8 (same operations as seg_update)
+template <int KIND, bool ZERO, int PAR>
+__device__ __forceinline__ void split_update(const Op<float>& o, float* __restrict__ x, const float* __restrict__ b,
+                                             int i0, int j, int k, int color, int Nh, const float* seps) {
+    const int row = o.nx * (j + o.ny * k);
+    const int n0 = row + i0;
+    const int m0 = n0 >> 1;
+    int jm, jp;
+    nbr(j, o.ny, jm, jp);
+    const int so = (jm - j) * o.nx, no = (jp - j) * o.nx;
+    const bool lo = k > 0, hi = k < o.nz - 1;
+    const int il = i0 == 0 ? o.nx - 1 : i0 - 1, ir = i0 + 8 == o.nx ? 0 : i0 + 8;
+    float* xo = x + color * Nh;            // this colour
+    const float* xt = x + (1 - color) * Nh;  // the other colour: every neighbour
+    float bv[4], oc[4], xs[4], xn[4], xb[4], xtp[4], av[8], nv[4];
+    ld16(b + color * Nh + m0, bv);
+    float xh = 0.f;
+    if (!ZERO) {
+        ld16(xt + m0, oc);
+        xh = xt[(row + (PAR == 0 ? il : ir)) >> 1];
+        ld16(xt + ((n0 + so) >> 1), xs);
+        ld16(xt + ((n0 + no) >> 1), xn);
+        if (lo) ld16(xt + ((n0 - o.nxy) >> 1), xb);
+        if (hi) ld16(xt + ((n0 + o.nxy) >> 1), xtp);
+    }
+    if (o.a) {
+        ldg16(o.a + n0, av);
+        ldg16(o.a + n0 + 4, av + 4);
+    }
+    SegCoef<float, 32, KIND, PAR == 0, PAR == 1> cf;
+    cf.load(o, row, n0, so, no, k, lo, hi, il, ir);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int m = 2 * u + PAR;
+        float cw, ce, cs, cn, cb, ct, extra, bcv;
+        cf.cell(o, seps, m, lo, hi, cw, ce, cs, cn, cb, ct, extra, bcv);
+        const float diag = diag_sum(o.a ? av[m] : 0.f, cw, ce, cs, cn, cb, ct, extra);
+        if (ZERO) {
+            nv[u] = sdiv(add_rn(bv[u], bcv), diag);
+            continue;
+        }
+        // the x neighbours: the other colour's cells of the 8, or the halo
+        const float xw = PAR == 0 ? (u == 0 ? xh : oc[u - 1]) : oc[u];
+        const float xe = PAR == 0 ? oc[u] : (u == 3 ? xh : oc[u + 1]);
+        const float sum = gs_rhs(bv[u], bcv, cw, xw, ce, xe, cs, xs[u], cn, xn[u], lo, cb, xb[u], hi, ct, xtp[u]);
+        nv[u] = sdiv(sum, diag);
+    }
+    st16(xo + m0, nv);
+    if (ZERO) {
+        const float z[4] = {0.f, 0.f, 0.f, 0.f};
+        st16(x + (1 - color) * Nh + m0, z);
+    }
+}
+
+template <int KIND, bool ZERO = false>
+__global__ void __launch_bounds__(256) k_rbgs_split(Op<float> o, float* __restrict__ x, const float* __restrict__ b,
+                                                    int color, int Nh) {
+    pdl_entry();
+    __shared__ float seps[8];
+    if (KIND == CK_FINE) {
+        if (threadIdx.x == 0 && threadIdx.y == 0)
+#pragma unroll
+            for (int q = 0; q < 8; ++q) seps[q] = o.eps[q];
+        __syncthreads();
+    }
+    // rows of the block: even offsets first, so that a warp's rows share a parity
+    const int h = blockDim.y / 2;
+    const int ty = threadIdx.y;
+    const int j = blockIdx.y * blockDim.y + (ty < h ? 2 * ty : 2 * (ty - h) + 1);
+    const int k = blockIdx.z;
+    const int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * 8;
+    if (j >= o.ny) return;
+    if (((j + k + color) & 1) == 0) split_update<KIND, ZERO, 0>(o, x, b, i0, j, k, color, Nh, seps);
+    else split_update<KIND, ZERO, 1>(o, x, b, i0, j, k, color, Nh, seps);
+}
+
 // red-black z-line Gauss-Seidel half sweep: color = parity of i + j; each
 // thread solves the tridiagonal system of one column (Thomas), q holds the
 // forward-elimination ratios
@@ -735,14 +847,22 @@ __device__ __forceinline__ void st_r32(float* p, const double (&r)[SEG]) {
     }
 }
 
-// the iterate of a segment: x, or x + e (the FP32 correction added in FP64)
-template <bool CORR, int SB>
-__device__ __forceinline__ void ld_iter(const double* x, const float* e, int c, double (&v)[SegW<double, SB>::n]) {
+// the iterate of a segment: x, or x + e (the FP32 correction added in FP64);
+// SPLIT: e in the split layout of level 0 (4 cells: the two of colour ce at
+// even positions, the two of the other colour at odd ones, 8 bytes each)
+template <bool CORR, int SB, bool SPLIT = false>
+__device__ __forceinline__ void ld_iter(const double* x, const float* e, int c, double (&v)[SegW<double, SB>::n],
+                                        int ce = 0, int Nh = 0) {
     constexpr int SEG = SegW<double, SB>::n;
     ldg_seg<double, SB>(x + c, v);
     if constexpr (CORR) {
         float f[SEG];
-        if constexpr (SEG == 2) {
+        if constexpr (SPLIT) {
+            static_assert(SEG == 4, "split rows of 4 cells");
+            const float2 a = __ldg(reinterpret_cast<const float2*>(e + ce * Nh + (c >> 1)));
+            const float2 q = __ldg(reinterpret_cast<const float2*>(e + (1 - ce) * Nh + (c >> 1)));
+            f[0] = a.x; f[1] = q.x; f[2] = a.y; f[3] = q.y;
+        } else if constexpr (SEG == 2) {
             const float2 q = __ldg(reinterpret_cast<const float2*>(e + c));
             f[0] = q.x; f[1] = q.y;
         } else {
@@ -753,15 +873,21 @@ __device__ __forceinline__ void ld_iter(const double* x, const float* e, int c, 
     }
 }
 
+// the FP32 copies of 4 residuals into the split layout (colour ce at the even positions)
+__device__ __forceinline__ void st_r32_split(float* p, int c, int ce, int Nh, const double (&r)[4]) {
+    *reinterpret_cast<float2*>(p + ce * Nh + (c >> 1)) = make_float2((float)r[0], (float)r[2]);
+    *reinterpret_cast<float2*>(p + (1 - ce) * Nh + (c >> 1)) = make_float2((float)r[1], (float)r[3]);
+}
+
 // k_resid64 by row segments: each thread takes one SB-byte segment of a row
 // (2 or 4 cells) through R64_ZP consecutive planes, the iterate of the planes
 // k - 1, k, k + 1 carried in registers.  Same operations per cell as
 // k_resid64, so the same bits.
-template <bool CORR, int KIND, int SB>
+template <bool CORR, int KIND, int SB, bool SPLIT = false>
 __global__ void __launch_bounds__(256) k_resid64_seg(Op<double> o, const double* __restrict__ x,
                                                      const float* __restrict__ e, const double* __restrict__ b,
                                                      double* __restrict__ xout, float* __restrict__ r32,
-                                                     double* __restrict__ norm, ResidCtl rc) {
+                                                     double* __restrict__ norm, ResidCtl rc, int Nh) {
     pdl_entry();
     if (rc.mode == RC_RN && !rc.ctl->need) return;
     constexpr int SEG = SegW<double, SB>::n;
@@ -779,11 +905,17 @@ __global__ void __launch_bounds__(256) k_resid64_seg(Op<double> o, const double*
         nbr(j, o.ny, jm, jp);
         const int so = (jm - j) * o.nx, no = (jp - j) * o.nx;
         const int il = i0 == 0 ? o.nx - 1 : i0 - 1, ir = i0 + SEG == o.nx ? 0 : i0 + SEG;
-        auto X = [&](int n) -> double { return CORR ? add_rn(__ldg(x + n), (double)__ldg(e + n)) : __ldg(x + n); };
+        // one cell n of x (+ e), cl: its colour (the split layout's array)
+        auto X = [&](int n, int cl) -> double {
+            if (!CORR) return __ldg(x + n);
+            return add_rn(__ldg(x + n), (double)__ldg(SPLIT ? e + cl * Nh + (n >> 1) : e + n));
+        };
         double xm[SEG], xc[SEG], xp[SEG];
         const int col = i0 + o.nx * j;
-        if (k0 > 0) ld_iter<CORR, SB>(x, e, col + o.nxy * (k0 - 1), xm);
-        ld_iter<CORR, SB>(x, e, col + o.nxy * k0, xc);
+        // the colour of a row's even positions at plane kk (i0 is even)
+        auto cev = [&](int jj, int kk) { return (jj + kk) & 1; };
+        if (k0 > 0) ld_iter<CORR, SB, SPLIT>(x, e, col + o.nxy * (k0 - 1), xm, cev(j, k0 - 1), Nh);
+        ld_iter<CORR, SB, SPLIT>(x, e, col + o.nxy * k0, xc, cev(j, k0), Nh);
 #pragma unroll
         for (int q = 0; q < R64_ZP; ++q) {
             const int k = k0 + q;
@@ -791,11 +923,12 @@ __global__ void __launch_bounds__(256) k_resid64_seg(Op<double> o, const double*
             const int row = o.nx * (j + o.ny * k);
             const int c0 = row + i0;
             const bool lo = k > 0, hi = k < o.nz - 1;
-            if (hi) ld_iter<CORR, SB>(x, e, c0 + o.nxy, xp);
+            if (hi) ld_iter<CORR, SB, SPLIT>(x, e, c0 + o.nxy, xp, cev(j, k + 1), Nh);
             double xs[SEG], xn[SEG], bv[SEG], av[SEG];
-            ld_iter<CORR, SB>(x, e, c0 + so, xs);
-            ld_iter<CORR, SB>(x, e, c0 + no, xn);
-            const double xl = X(row + il), xr = X(row + ir);
+            ld_iter<CORR, SB, SPLIT>(x, e, c0 + so, xs, cev(j + 1, k), Nh);
+            ld_iter<CORR, SB, SPLIT>(x, e, c0 + no, xn, cev(j + 1, k), Nh);
+            // the halo cells: il is odd, ir even (nx even)
+            const double xl = X(row + il, 1 - cev(j, k)), xr = X(row + ir, cev(j, k));
             ldg_seg<double, SB>(b + c0, bv);
             if (o.a) ldg_seg<double, SB>(o.a + c0, av);
             SegCoef<double, SB, KIND, true, true> cf;
@@ -810,7 +943,10 @@ __global__ void __launch_bounds__(256) k_resid64_seg(Op<double> o, const double*
                                cs, xs[m], cn, xn[m], lo, cb, xm[m], hi, ct, xp[m]);
                 mx = nan_max(mx, fabs(r[m]));
             }
-            if (r32) st_r32<SEG>(r32 + c0, r);
+            if (r32) {
+                if constexpr (SPLIT) st_r32_split(r32, c0, cev(j, k), Nh, r);
+                else st_r32<SEG>(r32 + c0, r);
+            }
             if (CORR) st_seg<double, SB>(xout + c0, xc);
 #pragma unroll
             for (int m = 0; m < SEG; ++m) { xm[m] = xc[m]; xc[m] = xp[m]; }
@@ -840,7 +976,8 @@ __global__ void __launch_bounds__(256) k_resid64_seg(Op<double> o, const double*
 // alignment allow (sb = 0: one column of cells per thread)
 template <bool CORR>
 void launch_resid64(const Op<double>& o, dim3 g, dim3 b, cudaStream_t s, const double* x, const float* e,
-                    const double* rhs, double* xout, float* r32, double* norm, const ResidCtl& rc, int sb = 0) {
+                    const double* rhs, double* xout, float* r32, double* norm, const ResidCtl& rc, int sb = 0,
+                    bool split = false) {
     if (sb == 32) {
         const int seg = sb / 8;
         const int gx = o.nx / seg;
@@ -850,8 +987,14 @@ void launch_resid64(const Op<double>& o, dim3 g, dim3 b, cudaStream_t s, const d
         if (ok) {
             const int bx = gx < 32 ? gx : 32, by = 256 / bx;
             dim3 bs(bx, by), gs(gx / bx, (o.ny + by - 1) / by, (o.nz + R64_ZP - 1) / R64_ZP);
-            if (o.zc) launch_k(k_resid64_seg<CORR, CK_PLANES, 32>, gs, bs, 0, s, o, x, e, rhs, xout, r32, norm, rc);
-            else launch_k(k_resid64_seg<CORR, CK_FINE, 32>, gs, bs, 0, s, o, x, e, rhs, xout, r32, norm, rc);
+            const int Nh = (o.nxy * o.nz) / 2;
+            if (split) {
+                if (o.zc) launch_k(k_resid64_seg<CORR, CK_PLANES, 32, true>, gs, bs, 0, s, o, x, e, rhs, xout, r32, norm, rc, Nh);
+                else launch_k(k_resid64_seg<CORR, CK_FINE, 32, true>, gs, bs, 0, s, o, x, e, rhs, xout, r32, norm, rc, Nh);
+            } else {
+                if (o.zc) launch_k(k_resid64_seg<CORR, CK_PLANES, 32>, gs, bs, 0, s, o, x, e, rhs, xout, r32, norm, rc, Nh);
+                else launch_k(k_resid64_seg<CORR, CK_FINE, 32>, gs, bs, 0, s, o, x, e, rhs, xout, r32, norm, rc, Nh);
+            }
             return;
         }
     }
@@ -1013,6 +1156,114 @@ __global__ void __launch_bounds__(256) k_prolong_z_seg(T* __restrict__ xf, const
 #pragma unroll
     for (int m = 0; m < SEG; ++m) v[m] = add_rn(v[m], prolong_z_val(T(w[m]), x0[m], zin ? x1[m] : T(0), zin));
     st_seg<T, SB>(xf + fc, v);
+}
+
+// the residual of NC = 4 or 8 natural cells of a row of level 0 with x and b
+// in the split layout (same operations as seg_resid_row)
+template <int KIND, int NC>
+__device__ __forceinline__ void split_resid_row(const Op<float>& o, const float* __restrict__ x,
+                                                const float* __restrict__ b, int i0, int j, int k, int Nh,
+                                                const float* seps, float (&r)[NC]) {
+    const int row = o.nx * (j + o.ny * k);
+    const int n0 = row + i0;
+    int jm, jp;
+    nbr(j, o.ny, jm, jp);
+    const int so = (jm - j) * o.nx, no = (jp - j) * o.nx;
+    const bool lo = k > 0, hi = k < o.nz - 1;
+    const int il = i0 == 0 ? o.nx - 1 : i0 - 1, ir = i0 + NC == o.nx ? 0 : i0 + NC;
+    const int ce = (j + k) & 1;   // colour of the even positions (i0 is even)
+    float xc[NC], bv[NC], xs[NC], xn[NC], xb[NC], xt[NC], av[NC];
+    ld_splitn<NC>(x, Nh, n0, ce, xc);
+    ld_splitn<NC>(b, Nh, n0, ce, bv);
+    const float xl = at_split(x, Nh, row + il, 1 - ce), xr = at_split(x, Nh, row + ir, ce);
+    ld_splitn<NC>(x, Nh, n0 + so, 1 - ce, xs);
+    ld_splitn<NC>(x, Nh, n0 + no, 1 - ce, xn);
+    if (lo) ld_splitn<NC>(x, Nh, n0 - o.nxy, 1 - ce, xb);
+    if (hi) ld_splitn<NC>(x, Nh, n0 + o.nxy, 1 - ce, xt);
+    if (o.a) {
+        ldg16(o.a + n0, av);
+        if constexpr (NC == 8) ldg16(o.a + n0 + 4, av + 4);
+    }
+    SegCoef<float, 4 * NC, KIND, true, true> cf;
+    cf.load(o, row, n0, so, no, k, lo, hi, il, ir);
+#pragma unroll
+    for (int m = 0; m < NC; ++m) {
+        float cw, ce_, cs, cn, cb, ct, extra, bcv;
+        cf.cell(o, seps, m, lo, hi, cw, ce_, cs, cn, cb, ct, extra, bcv);
+        const float diag = diag_sum(o.a ? av[m] : 0.f, cw, ce_, cs, cn, cb, ct, extra);
+        r[m] = res_val(bv[m], bcv, diag, xc[m], cw, m == 0 ? xl : xc[m - 1], ce_, m == NC - 1 ? xr : xc[m + 1], cs,
+                       xs[m], cn, xn[m], lo, cb, xb[m], hi, ct, xt[m]);
+    }
+}
+
+// level 0 -> 1 z-semicoarsening restriction from the split layout: 4 coarse
+// cells of a row per thread, written in the natural layout of level 1 (same
+// operations as k_rr_z_seg)
+template <int KIND>
+__global__ void __launch_bounds__(256) k_rr_z_split(Op<float> o, const float* __restrict__ x,
+                                                    const float* __restrict__ b, float* __restrict__ bc, int Nh) {
+    pdl_entry();
+    __shared__ float seps[8];
+    if (KIND == CK_FINE) {
+        if (threadIdx.x == 0 && threadIdx.y == 0)
+#pragma unroll
+            for (int q = 0; q < 8; ++q) seps[q] = o.eps[q];
+        __syncthreads();
+    }
+    const int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int K = blockIdx.z;
+    if (j >= o.ny) return;
+    float acc[4], r[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) acc[m] = 0.f;
+#pragma unroll
+    for (int dk = 0; dk < 2; ++dk) {
+        split_resid_row<KIND, 4>(o, x, b, i0, j, 2 * K + dk, Nh, seps, r);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) acc[m] = add_rn(acc[m], r[m]);
+    }
+#pragma unroll
+    for (int m = 0; m < 4; ++m) acc[m] = acc[m] / 2.f;
+    st16(bc + i0 + o.nx * (j + o.ny * K), acc);
+}
+
+// level 1 -> 0 z-only prolongation into the split layout: 8 natural fine
+// cells per thread (same operations as k_prolong_z_seg)
+__global__ void __launch_bounds__(256) k_prolong_z_split(float* __restrict__ xf, const float* __restrict__ xc,
+                                                         const float* __restrict__ wz, int nx, int ny, int ncz,
+                                                         int Nh) {
+    pdl_entry();
+    const int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * 8;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (j >= ny) return;
+    const int K0 = k >> 1;
+    int K1 = (k & 1) ? K0 + 1 : K0 - 1;
+    const bool zin = K1 >= 0 && K1 < ncz;
+    if (!zin) K1 = K0;
+    const int n0 = i0 + nx * (j + ny * k);
+    const int cc = i0 + nx * j;
+    const int ce = (j + k) & 1;
+    float v[8], x0[8], x1[8], w[8];
+    ld_split8(xf, Nh, n0, ce, v);
+    ldg16(xc + cc + nx * ny * K0, x0);
+    ldg16(xc + cc + nx * ny * K0 + 4, x0 + 4);
+    if (zin) {
+        ldg16(xc + cc + nx * ny * K1, x1);
+        ldg16(xc + cc + nx * ny * K1 + 4, x1 + 4);
+    }
+    ldg16(wz + n0, w);
+    ldg16(wz + n0 + 4, w + 4);
+    float e[4], o[4];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        const float t = add_rn(v[m], prolong_z_val(w[m], x0[m], zin ? x1[m] : 0.f, zin));
+        if (m & 1) o[m >> 1] = t;
+        else e[m >> 1] = t;
+    }
+    st16(xf + ce * Nh + (n0 >> 1), e);
+    st16(xf + (1 - ce) * Nh + (n0 >> 1), o);
 }
 
 // ---------------------------------------------------------------------
@@ -2019,6 +2270,27 @@ static void seg_sweeps(const MGLevel& L, int l, const Op<T>& o, T* x, const T* b
         }
 }
 
+// level 0's FP32 arrays can take the split layout for a mixed solve: rows of
+// 8-cell groups in whole warps or warp fractions, an even ny (the y wrap keeps
+// the colouring), z-only coarsening into level 1 (the split restriction and
+// prolongation), the FP64 residual by 32-byte segments, every array aligned
+bool Multigrid::split0_ok(const uint8_t* code, std::initializer_list<const void*> p64) const {
+    if (!split_mode || seg_bytes == 0 || lev_.size() < 2 || !e32_ || !r32_) return false;
+    const MGLevel& L = lev_[0];
+    const MGLevel& C = lev_[1];
+    if (L.line || (long long)L.N < seg_min_cells || L.n[0] % 8 != 0 || L.n[1] % 2 != 0) return false;
+    const int gx = L.n[0] / 8;
+    if (!(gx % 32 == 0 || 32 % gx == 0)) return false;
+    if (!(C.cr[0] == 1 && C.cr[1] == 1 && C.cr[2] == 2)) return false;
+    auto al = [](const void* q, uintptr_t a) { return ((uintptr_t)q % a) == 0; };
+    if (!al(e32_, 16) || !al(r32_, 16) || !al(a0_32, 16) || !al(a0_64, 16) || !al(C.wf[2], 16) ||
+        !al(C.x32, 16) || !al(C.b32, 16) || !al(code + (size_t)L.n[0] * L.n[1], 8))
+        return false;
+    for (const void* q : p64)
+        if (!al(q, 16)) return false;
+    return res_seg() == 32;
+}
+
 // a level whose first half sweep can start from an uncleared x (point
 // red-black with x / colour pairs)
 static bool zero_first_ok(const MGLevel& L) { return !L.line && L.n[0] % 2 == 0; }
@@ -2038,6 +2310,29 @@ void Multigrid::smooth(const DevParams& p, const uint8_t* code, int l, T* x, con
         else a = la<T>(L);
     }
     Op<T> o = make_op<T>(L, l, code, eps_, a, inhom, p);
+    if constexpr (sizeof(T) == 4) {
+        if (l == 0 && split_now_) {
+            // level 0 in the split layout: 8 natural cells (4 of one colour) per thread
+            const int gx = L.n[0] / 8, bx = gx < 32 ? gx : 32, by = 256 / bx;
+            const int Nh = (int)(L.N / 2);
+            dim3 b2(bx, by), g2(gx / bx, (L.n[1] + by - 1) / by, L.n[2]);
+            for (int it = 0; it < sweeps; ++it)
+                for (int color = 0; color < 2; ++color) {
+                    if (prof) prof->begin(PROF_SMOOTH_L0, s);
+                    const bool z = zero && it == 0 && color == 0;
+                    ++g_launches;
+                    if (o.zc) {
+                        if (z) launch_k(k_rbgs_split<CK_PLANES, true>, g2, b2, 0, s, o, x, b, color, Nh);
+                        else launch_k(k_rbgs_split<CK_PLANES>, g2, b2, 0, s, o, x, b, color, Nh);
+                    } else {
+                        if (z) launch_k(k_rbgs_split<CK_FINE, true>, g2, b2, 0, s, o, x, b, color, Nh);
+                        else launch_k(k_rbgs_split<CK_FINE>, g2, b2, 0, s, o, x, b, color, Nh);
+                    }
+                    if (prof) prof->end(s);
+                }
+            return;
+        }
+    }
     if (L.line) {
         T* q = lq<T>(L);
         dim3 b2(32, 4), g2(((L.n[0] + 1) / 2 + 31) / 32, (L.n[1] + 3) / 4, 1);
@@ -2126,7 +2421,19 @@ void Multigrid::vcycle(const DevParams& p, const uint8_t* code, int l, T* x, con
                            ? (seg_bytes == 32 && seg_shape<T, 32>(L, l, o, x, b) ? 32
                               : seg_bytes == 16 && seg_shape<T, 16>(L, l, o, x, b) ? 16 : 0)
                            : 0;
-        if (sb) {
+        bool done = false;
+        if constexpr (sizeof(T) == 4) {
+            if (l == 0 && split_now_) {
+                const int gx = L.n[0] / 4, bx = gx < 32 ? gx : 32, by = 256 / bx;
+                dim3 bs(bx, by), gs(gx / bx, (L.n[1] + by - 1) / by, C.n[2]);
+                const int Nh = (int)(L.N / 2);
+                if (o.zc) launch_k(k_rr_z_split<CK_PLANES>, gs, bs, 0, s, o, x, b, bc, Nh);
+                else launch_k(k_rr_z_split<CK_FINE>, gs, bs, 0, s, o, x, b, bc, Nh);
+                done = true;
+            }
+        }
+        if (done) {
+        } else if (sb) {
             // z-semicoarsening by row segments
             const int gx = L.n[0] / (sb / (int)sizeof(T)), bx = gx < 32 ? gx : 32, by = 256 / bx;
             dim3 bs(bx, by), gs(gx / bx, (L.n[1] + by - 1) / by, C.n[2]);
@@ -2149,12 +2456,22 @@ void Multigrid::vcycle(const DevParams& p, const uint8_t* code, int l, T* x, con
         const int key = (C.cr[0] == 2) * 4 + (C.cr[1] == 2) * 2 + (C.cr[2] == 2);
         T* xc = lx<T>(C);
 #define FX_PR(RX, RY, RZ) launch_k(k_prolong<T, RX, RY, RZ>, g3, b2, 0, s, x, xc, C.wf[0], C.wf[1], C.wf[2], L.n[0], L.n[1], L.n[2], C.n[0], C.n[1], C.n[2])
+        bool done = false;
+        if constexpr (sizeof(T) == 4) {
+            if (l == 0 && split_now_) {
+                const int gx = L.n[0] / 8, bx = gx < 32 ? gx : 32, by = 256 / bx;
+                dim3 bs(bx, by), gs(gx / bx, (L.n[1] + by - 1) / by, L.n[2]);
+                launch_k(k_prolong_z_split, gs, bs, 0, s, x, xc, C.wf[2], L.n[0], L.n[1], C.n[2], (int)(L.N / 2));
+                done = true;
+            }
+        }
         auto al16 = [](const void* q) { return ((uintptr_t)q % 16) == 0; };
-        const int sb = key == 1 && (long long)L.N >= seg_min_cells && al16(xc) && al16(C.wf[2])
+        const int sb = !done && key == 1 && (long long)L.N >= seg_min_cells && al16(xc) && al16(C.wf[2])
                            ? (seg_bytes == 32 && seg_shape<T, 32>(L, l, o, x, b) ? 32
                               : seg_bytes == 16 && seg_shape<T, 16>(L, l, o, x, b) ? 16 : 0)
                            : 0;
-        if (sb) {
+        if (done) {
+        } else if (sb) {
             const int gx = L.n[0] / (sb / (int)sizeof(T)), bx = gx < 32 ? gx : 32, by = 256 / bx;
             dim3 bs(bx, by), gs(gx / bx, (L.n[1] + by - 1) / by, L.n[2]);
             if (sb == 32) launch_k(k_prolong_z_seg<T, 32>, gs, bs, 0, s, x, xc, C.wf[2], L.n[0], L.n[1], C.n[2]);
@@ -2201,7 +2518,7 @@ int Multigrid::replay(GraphCache& g, const void* x, const void* rhs, const DevPa
     }
     if (!g.exec || g.x != x || g.rhs != rhs || g.has_alpha != has_alpha_ || g.vlo != p.V_lo || g.vhi != p.V_hi ||
         g.nu1 != nu1 || g.nu2 != nu2 || g.nu1c != nu1c || g.nu2c != nu2c || g.pdl != g_pdl ||
-        g.seg != seg_bytes || g.seg_min != seg_min_cells) {
+        g.seg != seg_bytes || g.seg_min != seg_min_cells || g.split != split_now_) {
         if (g.exec) { cudaGraphExecDestroy(g.exec); g.exec = nullptr; }
         cudaGraph_t graph;
         const long long l0 = g_launches.load();
@@ -2217,7 +2534,7 @@ int Multigrid::replay(GraphCache& g, const void* x, const void* rhs, const DevPa
         if (e) return (int)e;
         g.x = x; g.rhs = rhs; g.has_alpha = has_alpha_; g.vlo = p.V_lo; g.vhi = p.V_hi; g.nu1 = nu1; g.nu2 = nu2;
         g.nu1c = nu1c; g.nu2c = nu2c;
-        g.pdl = g_pdl; g.seg = seg_bytes; g.seg_min = seg_min_cells;
+        g.pdl = g_pdl; g.seg = seg_bytes; g.seg_min = seg_min_cells; g.split = split_now_;
     }
     g_launches += g.launches;
     return (int)cudaGraphLaunch(g.exec, s);
@@ -2266,10 +2583,11 @@ int Multigrid::solve_mixed(const DevParams& p, const uint8_t* code, double* phi,
     // step adds the FP32 correction while it forms the next residual
     double* buf[2] = {phi, alt64m_};
     int cur = 0;
+    split_now_ = split0_ok(code, {phi, rhs, alt64m_});
     cudaMemsetAsync(d_norm_, 0, NORM_SLOTS * 8, s);
     if (prof) prof->begin(PROF_RESID64, s);
     ++g_launches;
-    launch_resid64<false>(o64, g2, b2, s, phi, nullptr, rhs, nullptr, r32_, d_norm_, ResidCtl{}, res_seg());
+    launch_resid64<false>(o64, g2, b2, s, phi, nullptr, rhs, nullptr, r32_, d_norm_, ResidCtl{}, res_seg(), split_now_);
     if (prof) prof->end(s);
     cudaMemcpyAsync(h_norm_, d_norm_, NORM_SLOTS * 8, cudaMemcpyDeviceToHost, s);
     int e = (int)cudaStreamSynchronize(s);
@@ -2288,7 +2606,7 @@ int Multigrid::solve_mixed(const DevParams& p, const uint8_t* code, double* phi,
             cudaMemsetAsync(d_norm_, 0, NORM_SLOTS * 8, s);
             if (prof) prof->begin(PROF_RESID64, s);
             ++g_launches;
-            launch_resid64<true>(o64, g2, b2, s, xin, e32_, rhs, xout, r32_, d_norm_, ResidCtl{}, res_seg());
+            launch_resid64<true>(o64, g2, b2, s, xin, e32_, rhs, xout, r32_, d_norm_, ResidCtl{}, res_seg(), split_now_);
             if (prof) prof->end(s);
             cudaMemcpyAsync(h_norm_, d_norm_, NORM_SLOTS * 8, cudaMemcpyDeviceToHost, s);
         });
@@ -2357,12 +2675,13 @@ void Multigrid::enqueue_solve_mixed_ctl(const DevParams& p, const uint8_t* code,
     const int inner = std::max(1, mixed_cycles);
     const cudaGraphConditionalHandle hw = cap.handle(s);
     ResidCtl rb = {ctl, RC_BEGIN, nb, rtol, maxit, 0, 0, 0, hw, hw, rc_counter_};
+    split_now_ = split0_ok(code, {phi, rhs, alt64m_});
     ++g_launches;
-    launch_resid64<false>(o64, g2, b2, s, phi, nullptr, rhs, nullptr, r32_, d_norm_, rb, res_seg());
+    launch_resid64<false>(o64, g2, b2, s, phi, nullptr, rhs, nullptr, r32_, d_norm_, rb, res_seg(), split_now_);
     auto refine = [&](cudaStream_t q, const double* xin, double* xout, const ResidCtl& rc) {
         for (int k = 0; k < inner; ++k) vcycle<float>(p, code, 0, e32_, r32_, false, q, k == 0);
         ++g_launches;
-        launch_resid64<true>(o64, g2, b2, q, xin, e32_, rhs, xout, r32_, d_norm_, rc, res_seg());
+        launch_resid64<true>(o64, g2, b2, q, xin, e32_, rhs, xout, r32_, d_norm_, rc, res_seg(), split_now_);
     };
     cap.node(s, cudaGraphCondTypeWhile, hw, KIND_MX_FIRST, [&](cudaStream_t b) {
         const cudaGraphConditionalHandle hif = cap.handle(b);

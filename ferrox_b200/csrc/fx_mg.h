@@ -15,6 +15,7 @@
 #pragma once
 
 #include <cstdint>
+#include <initializer_list>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -130,6 +131,7 @@ public:
     bool alpha_tiles = true; // coarse alphas below level 1 in one launch (k_alpha_tiles)
     int seg_bytes = 16;      // point red-black half sweeps by row segments of 16 or 32 bytes where the shape allows (k_rbgs_seg); 0: one cell per thread
     long long seg_min_cells = 0;  // ... on levels of at least this many cells
+    bool split_mode = true;  // level 0's FP32 correction and residual in the red-black split layout (mixed path)
 
     static constexpr int kMaxLev = 24;
     Prof* prof = nullptr;
@@ -138,6 +140,13 @@ public:
 
 private:
     std::vector<MGLevel> lev_;
+    // level 0's FP32 arrays in the split layout for the solve being enqueued
+    // (split0_ok at its start; every level-0 FP32 kernel and the FP64
+    // residuals that write or read them follow it)
+    bool split0_ok(const uint8_t* code, std::initializer_list<const void*> p64) const;
+public:
+    bool split_now_ = false;   // (read back as mg_level0_split: the last mixed solve used the split layout)
+private:
     // the segment width for level 0's FP64 residual: 32 bytes whenever the
     // smoother runs by segments (measured faster than 16 for this kernel); 0:
     // one column of cells per thread
@@ -163,7 +172,7 @@ private:
         bool has_alpha = false;
         double vlo = 0, vhi = 0;
         int nu1 = 0, nu2 = 0, nu1c = 0, nu2c = 0;
-        bool pdl = false;
+        bool pdl = false, split = false;
         int seg = 0;
         long long seg_min = 0;
         long long launches = 0;

@@ -229,15 +229,18 @@ def test_interior_fast_path_bit_identical(case):
 SEG_CASES = {
     # level 0 from the material codes, coarse levels from face-beta arrays;
     # 256-cell rows: 32 FP32 segments per row, one row per warp
-    "polycrystal_fp64": dict(grains=(256, 32, 24), precision=None),
-    "polycrystal_mixed": dict(grains=(256, 32, 24), precision="mixed"),
+    "polycrystal_fp64": dict(grains=(256, 32, 48), precision=None),
+    "polycrystal_mixed": dict(grains=(256, 32, 48), precision="mixed", split=True),
     # 64-cell rows: several rows per warp (the even-offsets-first row order)
-    "polycrystal_mixed_64": dict(grains=(64, 64, 48), precision="mixed"),
+    "polycrystal_mixed_64": dict(grains=(64, 64, 48), precision="mixed", split=True),
     # layered stacks: face beta by plane, alpha from the Newton-coupled semiconductor
     "mfism_fp64": dict(text=decks.mfism(32, 32, 48, steps_per_voltage=3, v_step=0.1), shape=(48, 32, 32)),
     "mfism_mixed": dict(text=decks.mfism(32, 32, 48, steps_per_voltage=3, v_step=0.1), shape=(48, 32, 32),
                         precision="mixed"),
     "mfim_mixed": dict(text=decks.mfim(64, 64, 24, Phi_Bc_hi=0.8), shape=(24, 64, 64), precision="mixed"),
+    # level 0 -> 1 by z alone, so the mixed path takes the split layout, with alpha
+    "mfism_mixed_split": dict(text=decks.mfism(32, 32, 144, steps_per_voltage=3, v_step=0.1), shape=(144, 32, 32),
+                              precision="mixed", split=True),
 }
 
 
@@ -246,8 +249,10 @@ def test_segment_smoother_bit_identical(case):
     """The row-segment red-black half sweep (fx.mg_seg = 16 or 32 bytes per
     thread; every level whose rows it can take, fx.mg_seg_min = 0) repeats the
     per-cell operations of the one-cell-per-thread sweep (fx.mg_seg = 0) with
-    the same roundings: fields and V-cycle counts are bit-identical, in the
-    step graph and in the host-driven loop."""
+    the same roundings, and so do the kernels on level 0's red-black split
+    layout of the mixed path (fx.mg_split = 1, the default, against 0): fields
+    and V-cycle counts are bit-identical, in the step graph and in the
+    host-driven loop."""
     cfg = SEG_CASES[case]
     grains = None
     if cfg.get("grains"):
@@ -259,18 +264,21 @@ def test_segment_smoother_bit_identical(case):
     P = start_P(shape, 7)
     for graph in (1, 0):
         runs = []
-        for seg in (0, 16, 32):
+        settings = [(0, 1), (16, 1), (32, 1), (16, 0)]
+        for seg, split in settings:
             f = make(text, P, graph, precision=cfg.get("precision"), grains=grains,
-                     params={"fx.mg_seg": seg, "fx.mg_seg_min": 0})
+                     params={"fx.mg_seg": seg, "fx.mg_seg_min": 0, "fx.mg_split": split})
             f.step(5)
             runs.append(({n: f.field(n) for n in FIELDS}, f.stats()["mg_cycles_total"],
                          f.stats()["newton_iters_total"]))
+            if cfg.get("split") and seg:
+                assert f.param("mg_level0_split") == split, (seg, split)
             f.close()
         a, ca, na = runs[0]
-        for seg, (b, cb, nb) in zip((16, 32), runs[1:]):
-            assert (ca, na) == (cb, nb), (graph, seg, ca, cb, na, nb)
+        for (seg, split), (b, cb, nb) in zip(settings[1:], runs[1:]):
+            assert (ca, na) == (cb, nb), (graph, seg, split, ca, cb, na, nb)
             for n in FIELDS:
-                assert np.array_equal(a[n], b[n]), (graph, seg, n, np.abs(a[n] - b[n]).max())
+                assert np.array_equal(a[n], b[n]), (graph, seg, split, n, np.abs(a[n] - b[n]).max())
 
 
 def test_no_pre_smoothing_starts_from_a_zero_correction():
