@@ -1777,7 +1777,7 @@ int fx_get_param(const fx_ctx* c, const char* key, double* v) {
         {"fx.mg_nu1", (double)c->mg.nu1}, {"fx.mg_nu2", (double)c->mg.nu2},
         {"fx.mg_mixed_cycles", (double)c->mg.mixed_cycles}, {"fx.alpha_tiles", c->mg.alpha_tiles ? 1.0 : 0.0},
         {"fx.mg_seg", (double)c->mg.seg_bytes}, {"fx.mg_seg_min", (double)c->mg.seg_min_cells},
-        {"fx.mg_split", c->mg.split_mode ? 1.0 : 0.0}, {"mg_level0_split", c->mg.split_now_ ? 1.0 : 0.0},
+        {"fx.mg_split", c->mg.split_mode ? 1.0 : 0.0}, {"fx.mg_half", c->mg.half_coarse ? 1.0 : 0.0}, {"mg_level0_split", c->mg.split_now_ ? 1.0 : 0.0},
         {"fx.mg_nu1_coarse", (double)c->mg.nu1c}, {"fx.mg_nu2_coarse", (double)c->mg.nu2c},
         {"fx.interior", c->use_interior ? 1.0 : 0.0}, {"fx.adjoint_store_phi", c->adj_store_phi ? 1.0 : 0.0},
         {"fx.adjoint_extrapolate", c->adj_extrap ? 1.0 : 0.0},
@@ -1825,7 +1825,7 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
     static const char* const known[] = {
         "Phi_Bc_hi", "Phi_Bc_lo", "fx.mg_rtol", "fx.mg_max_iter", "fx.newton_max_iter", "fx.warm_start",
         "fx.phi_extrapolate", "fx.step_graph", "fx.pdl", "fx.verbose", "fx.profile", "fx.mg_nu1", "fx.graphs",
-        "fx.mg_nu2", "fx.alpha_tiles", "fx.interior", "fx.adjoint_store_phi", "fx.adjoint_extrapolate", "fx.mg_nu1_coarse", "fx.mg_nu2_coarse", "fx.mg_seg", "fx.mg_seg_min", "fx.mg_split", "fx.mg_mixed_cycles", "fx.phi_ghost_mode", "dt", "alpha", "fx.newton_tol",
+        "fx.mg_nu2", "fx.alpha_tiles", "fx.interior", "fx.adjoint_store_phi", "fx.adjoint_extrapolate", "fx.mg_nu1_coarse", "fx.mg_nu2_coarse", "fx.mg_seg", "fx.mg_seg_min", "fx.mg_split", "fx.mg_half", "fx.mg_mixed_cycles", "fx.phi_ghost_mode", "dt", "alpha", "fx.newton_tol",
         "beta", "gamma", "g11", "g44", "BigGamma", "inc_step"};
     bool is_known = false;
     for (const char* q : known) is_known = is_known || k == q;
@@ -1852,12 +1852,14 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
         return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx.newton_tol must be positive");
     if (k == "fx.mg_seg" && !(v == 0 || v == 16 || v == 32))
         return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx.mg_seg must be 0 (one cell per thread), 16 or 32 (segment bytes)");
+    if (k == "fx.mg_half" && c->dev)
+        return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx.mg_half must be set before the first device call");
     if (k == "fx.mg_seg_min" && !(v >= 0))
         return set_err(c, FX_ERR_INVALID_ARGUMENT, "fx.mg_seg_min must not be negative");
     if (k != "fx.profile" && k != "fx.verbose" && k != "fx.graphs" && k != "fx.step_graph" && k != "fx.pdl" &&
         k != "fx.alpha_tiles" && k != "fx.interior" && k != "fx.adjoint_store_phi" && k != "fx.adjoint_extrapolate" &&
         k != "fx.mg_seg" &&
-        k != "fx.mg_seg_min" && k != "fx.mg_split")
+        k != "fx.mg_seg_min" && k != "fx.mg_split" && k != "fx.mg_half")
         ++c->gen;
     // the time history of phi only seeds the next solve's initial iterate;
     // electrode values are compared on their own, solver settings leave the
@@ -1881,6 +1883,7 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
     if (k == "fx.alpha_tiles") { c->mg.alpha_tiles = v != 0.0; return FX_OK; }
     if (k == "fx.mg_seg") { c->mg.seg_bytes = (int)v; return FX_OK; }
     if (k == "fx.mg_split") { c->mg.split_mode = v != 0.0; return FX_OK; }
+    if (k == "fx.mg_half") { c->mg.half_coarse = v != 0.0; return FX_OK; }
     if (k == "fx.mg_seg_min") { c->mg.seg_min_cells = (long long)std::min(v, 9.0e18); return FX_OK; }
     if (k == "fx.adjoint_store_phi") { c->adj_store_phi = v != 0.0; return FX_OK; }
     if (k == "fx.adjoint_extrapolate") { c->adj_extrap = v != 0.0; return FX_OK; }

@@ -11,6 +11,8 @@
 #include <cstring>
 #include <atomic>
 
+#include <cuda_fp16.h>
+
 namespace fx {
 
 extern std::atomic<long long> g_launches;
@@ -30,13 +32,26 @@ struct Op {
     const T* a;            // alpha (may be null)
     const T* zc;           // coarse: face beta by plane (bw[nz], bs[nz], bb[nz+1]) when laterally uniform
     T vlo, vhi;            // electrode values (inhomogeneous level-0 operator only)
+    // coarse, FP32 cycle: the face beta in FP16 scaled by 1 / hscale (ih2x..z
+    // then carry hscale); null where the level keeps FP32 arrays
+    const uint16_t* bwh;
+    const uint16_t* bsh;
+    const uint16_t* bbh;
 };
+
+// one FP16 face beta (read-only path)
+__device__ __forceinline__ float hload(const uint16_t* p) { return __half2float(__ushort_as_half(__ldg(p))); }
+
+// a coarse level whose FP32 kernels read the FP16 face arrays
+template <typename T>
+static bool half_faces(const Op<T>& o) { return sizeof(T) == 4 && o.bwh != nullptr && !o.zc; }
 
 // couplings of cell (i,j,k) to its six neighbours (already divided by h^2),
 // the diagonal and the electrode contribution to the right-hand side
 // KIND: CK_FINE level 0 (material codes), CK_ARRAYS coarse face-beta arrays,
-// CK_PLANES coarse face beta by plane (laterally uniform)
-constexpr int CK_ARRAYS = 0, CK_FINE = 1, CK_PLANES = 2;
+// CK_PLANES coarse face beta by plane (laterally uniform), CK_HALF coarse
+// face-beta arrays in FP16 (FP32 cycle only)
+constexpr int CK_ARRAYS = 0, CK_FINE = 1, CK_PLANES = 2, CK_HALF = 3;
 
 // The per-cell arithmetic of the operator, every rounding written out (no
 // product left for the compiler to fuse into a neighbouring add), so that
@@ -125,6 +140,18 @@ __device__ __forceinline__ void coeffs(const Op<T>& o, int i, int j, int k, int 
         else { cb = T(0); electrode(fb, o.ih2z, o.vlo, extra, bcv); }
         if (k < o.nz - 1) ct = face_beta(ft, o.ih2z);
         else { ct = T(0); electrode(ft, o.ih2z, o.vhi, extra, bcv); }
+    } else if constexpr (KIND == CK_HALF) {
+        static_assert(sizeof(T) == 4, "FP16 faces in the FP32 cycle only");
+        const int row = c - i;
+        cw = face_beta(hload(o.bwh + c), o.ih2x);
+        ce = face_beta(hload(o.bwh + row + ip), o.ih2x);
+        cs = face_beta(hload(o.bsh + c), o.ih2y);
+        cn = face_beta(hload(o.bsh + c + (jp - j) * o.nx), o.ih2y);
+        const T fb = hload(o.bbh + c), ft = hload(o.bbh + c + o.nxy);
+        if (k > 0) cb = face_beta(fb, o.ih2z);
+        else { cb = T(0); electrode0(fb, o.ih2z, extra); }
+        if (k < o.nz - 1) ct = face_beta(ft, o.ih2z);
+        else { ct = T(0); electrode0(ft, o.ih2z, extra); }
     } else {
         // coarse levels: homogeneous electrode conditions (no right-hand-side term)
         const int row = c - i;
@@ -329,6 +356,14 @@ struct SegCoef {
             ps = __ldg(o.zc + o.nz + k);
             pb = __ldg(o.zc + 2 * o.nz + k);
             pt = __ldg(o.zc + 2 * o.nz + k + 1);
+        } else if constexpr (KIND == CK_HALF) {
+            static_assert(sizeof(T) == 4, "FP16 faces in the FP32 cycle only");
+            ldh_seg(o.bwh + c0, fw);
+            ldh_seg(o.bsh + c0, fs);
+            ldh_seg(o.bsh + c0 + no, fn);
+            ldh_seg(o.bbh + c0, fb);
+            ldh_seg(o.bbh + c0 + o.nxy, ft);
+            if (NR) fr = hload(o.bwh + row + ir);
         } else {
             ldg_seg<T, SB>(o.bw + c0, fw);
             ldg_seg<T, SB>(o.bs + c0, fs);
@@ -336,6 +371,24 @@ struct SegCoef {
             ldg_seg<T, SB>(o.bb + c0, fb);
             ldg_seg<T, SB>(o.bb + c0 + o.nxy, ft);
             if (NR) fr = __ldg(o.bw + row + ir);
+        }
+    }
+
+    // SEG FP16 face betas (2 SEG bytes) as T
+    template <int N>
+    __device__ __forceinline__ static void ldh_seg(const uint16_t* p, T (&v)[N]) {
+        auto h2f = [](unsigned w, int hi) {
+            return __half2float(__ushort_as_half((unsigned short)(hi ? w >> 16 : w & 0xffffu)));
+        };
+        if constexpr (N == 4) {
+            const uint2 q = __ldg(reinterpret_cast<const uint2*>(p));
+            v[0] = h2f(q.x, 0); v[1] = h2f(q.x, 1); v[2] = h2f(q.y, 0); v[3] = h2f(q.y, 1);
+        } else {
+            static_assert(N == 8, "4 or 8 FP16 faces");
+            const uint4 q = __ldg(reinterpret_cast<const uint4*>(p));
+            const unsigned w[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+            for (int t = 0; t < 4; ++t) { v[2 * t] = h2f(w[t], 0); v[2 * t + 1] = h2f(w[t], 1); }
         }
     }
 
@@ -362,6 +415,7 @@ struct SegCoef {
             if (hi) ct = face_beta(pt, o.ih2z);
             else { ct = T(0); electrode(pt, o.ih2z, o.vhi, extra, bcv); }
         } else {
+            // face arrays, FP32 or FP16 (already converted)
             cw = face_beta(fw[m], o.ih2x);
             ce = face_beta(m == SEG - 1 ? fr : fw[m + 1], o.ih2x);
             cs = face_beta(fs[m], o.ih2y);
@@ -1718,7 +1772,16 @@ Op<T> make_op(const MGLevel& L, int l, const uint8_t* code, const double* eps, c
     else o.zc = (const T*)L.zc32;
     o.vlo = inhom ? T(p.V_lo) : T(0);
     o.vhi = inhom ? T(p.V_hi) : T(0);
-    (void)l;
+    o.bwh = o.bsh = o.bbh = nullptr;
+    if constexpr (sizeof(T) == 4) {
+        if (l > 0 && L.bwh && !o.zc) {
+            // FP16 faces scaled by 1 / hscale: the couplings carry hscale
+            o.bwh = L.bwh; o.bsh = L.bsh; o.bbh = L.bbh;
+            o.ih2x = T(L.hscale / (L.h[0] * L.h[0]));
+            o.ih2y = T(L.hscale / (L.h[1] * L.h[1]));
+            o.ih2z = T(L.hscale / (L.h[2] * L.h[2]));
+        }
+    }
     return o;
 }
 
@@ -1797,6 +1860,7 @@ Multigrid::~Multigrid() {
         if (l > 0) { cudaFree(L.x64); cudaFree(L.b64); cudaFree(L.x32); cudaFree(L.b32); }
         cudaFree(L.bw64); cudaFree(L.bs64); cudaFree(L.bb64); cudaFree(L.a64); cudaFree(L.cp64);
         cudaFree(L.bw32); cudaFree(L.bs32); cudaFree(L.bb32); cudaFree(L.a32); cudaFree(L.cp32);
+        cudaFree(L.bwh); cudaFree(L.bsh); cudaFree(L.bbh);
         for (int d = 0; d < 3; ++d) { cudaFree(L.wf[d]); cudaFree(L.fac64[d]); cudaFree(L.fac32[d]); }
         cudaFree(L.zc64);
         cudaFree(L.zc32);
@@ -2019,6 +2083,25 @@ int Multigrid::setup(const DevParams& p, const std::vector<uint8_t>& code, bool 
                 for (size_t q = 0; q < N + lnxy; ++q) t[q] = (float)fb[q];
                 if (cudaMemcpy(L.bb32, t.data(), (N + lnxy) * 4, cudaMemcpyHostToDevice) != cudaSuccess) return -1;
                 if (cudaMemset(L.a32, 0, N * 4) != cudaSuccess) return -1;
+                if (half_coarse && !L.zc32) {
+                    // the FP32 cycle's launched kernels read the faces in FP16,
+                    // scaled into (0, 1] by the level's largest face beta
+                    double mx = 0.0;
+                    for (size_t q = 0; q < N; ++q) mx = std::max(mx, std::max(fw[q], fs[q]));
+                    for (size_t q = 0; q < N + lnxy; ++q) mx = std::max(mx, fb[q]);
+                    if (mx > 0.0 && std::isfinite(mx)) {
+                        L.hscale = mx;
+                        L.bwh = dalloc<uint16_t>(N, bytes_); L.bsh = dalloc<uint16_t>(N, bytes_);
+                        L.bbh = dalloc<uint16_t>(N + lnxy, bytes_);
+                        if (!L.bwh || !L.bsh || !L.bbh) return -2;
+                        std::vector<uint16_t> h(N + lnxy);
+                        auto put = [&](const std::vector<double>& v, uint16_t* d, size_t n) {
+                            for (size_t q = 0; q < n; ++q) h[q] = __half_as_ushort(__double2half(v[q] / mx));
+                            return cudaMemcpy(d, h.data(), n * 2, cudaMemcpyHostToDevice) == cudaSuccess;
+                        };
+                        if (!put(fw, L.bwh, N) || !put(fs, L.bsh, N) || !put(fb, L.bbh, N + lnxy)) return -1;
+                    }
+                }
             }
         }
         if (L.line) {
@@ -2241,6 +2324,7 @@ static bool seg_shape(const MGLevel& L, int l, const Op<T>& o, const T* x, const
     if (!al(x, 16) || !al(b, 16) || !al(o.a, 16)) return false;
     if (o.zc) return true;
     if (l == 0) return al(o.code + o.nxy, SEG);   // the codes past the ghost layer
+    if (o.bwh) return al(o.bwh, 2 * SEG) && al(o.bsh, 2 * SEG) && al(o.bbh, 2 * SEG);
     return al(o.bw, 16) && al(o.bs, 16) && al(o.bb, 16);
 }
 
@@ -2262,6 +2346,11 @@ static void seg_sweeps(const MGLevel& L, int l, const Op<T>& o, T* x, const T* b
             } else if (o.zc) {
                 if (z) launch_k(k_rbgs_seg<T, SB, CK_PLANES, true>, g2, b2, 0, s, o, x, b, color);
                 else launch_k(k_rbgs_seg<T, SB, CK_PLANES>, g2, b2, 0, s, o, x, b, color);
+            } else if (half_faces(o)) {
+                if constexpr (sizeof(T) == 4) {
+                    if (z) launch_k(k_rbgs_seg<T, SB, CK_HALF, true>, g2, b2, 0, s, o, x, b, color);
+                    else launch_k(k_rbgs_seg<T, SB, CK_HALF>, g2, b2, 0, s, o, x, b, color);
+                }
             } else {
                 if (z) launch_k(k_rbgs_seg<T, SB, CK_ARRAYS, true>, g2, b2, 0, s, o, x, b, color);
                 else launch_k(k_rbgs_seg<T, SB, CK_ARRAYS>, g2, b2, 0, s, o, x, b, color);
@@ -2342,7 +2431,9 @@ void Multigrid::smooth(const DevParams& p, const uint8_t* code, int l, T* x, con
                 ++g_launches;
                 if (o.zc) launch_k(k_line<T, CK_PLANES>, g2, b2, 0, s, o, x, b, q, color);
                 else if (l == 0) launch_k(k_line<T, CK_FINE>, g2, b2, 0, s, o, x, b, q, color);
-                else launch_k(k_line<T, CK_ARRAYS>, g2, b2, 0, s, o, x, b, q, color);
+                else if (half_faces(o)) {
+                    if constexpr (sizeof(T) == 4) launch_k(k_line<T, CK_HALF>, g2, b2, 0, s, o, x, b, q, color);
+                } else launch_k(k_line<T, CK_ARRAYS>, g2, b2, 0, s, o, x, b, q, color);
                 if (prof) prof->end(s);
             }
     } else if (seg_bytes == 32 && (long long)L.N >= seg_min_cells && seg_shape<T, 32>(L, l, o, x, b)) {
@@ -2366,7 +2457,12 @@ void Multigrid::smooth(const DevParams& p, const uint8_t* code, int l, T* x, con
                         if (z) launch_k(k_rbgs<T, CK_PLANES, true>, g2, b2, 0, s, o, x, b, color);
                         else launch_k(k_rbgs<T, CK_PLANES>, g2, b2, 0, s, o, x, b, color);
                     } else {
-                        if (z) launch_k(k_rbgs<T, CK_ARRAYS, true>, g2, b2, 0, s, o, x, b, color);
+                        if (half_faces(o)) {
+                            if constexpr (sizeof(T) == 4) {
+                                if (z) launch_k(k_rbgs<T, CK_HALF, true>, g2, b2, 0, s, o, x, b, color);
+                                else launch_k(k_rbgs<T, CK_HALF>, g2, b2, 0, s, o, x, b, color);
+                            }
+                        } else if (z) launch_k(k_rbgs<T, CK_ARRAYS, true>, g2, b2, 0, s, o, x, b, color);
                         else launch_k(k_rbgs<T, CK_ARRAYS>, g2, b2, 0, s, o, x, b, color);
                     }
                 }
@@ -2440,10 +2536,13 @@ void Multigrid::vcycle(const DevParams& p, const uint8_t* code, int l, T* x, con
 #define FX_RRS(SB) \
             if (o.zc) launch_k(k_rr_z_seg<T, SB, CK_PLANES>, gs, bs, 0, s, o, x, b, bc, norm); \
             else if (l == 0) launch_k(k_rr_z_seg<T, SB, CK_FINE>, gs, bs, 0, s, o, x, b, bc, norm); \
+            else if (half_faces(o)) { if constexpr (sizeof(T) == 4) launch_k(k_rr_z_seg<T, SB, CK_HALF>, gs, bs, 0, s, o, x, b, bc, norm); } \
             else launch_k(k_rr_z_seg<T, SB, CK_ARRAYS>, gs, bs, 0, s, o, x, b, bc, norm);
             if (sb == 32) { FX_RRS(32) } else { FX_RRS(16) }
 #undef FX_RRS
-        } else if (o.zc) { FX_RR_ALL(CK_PLANES) } else if (l == 0) { FX_RR_ALL(CK_FINE) } else { FX_RR_ALL(CK_ARRAYS) }
+        } else if (o.zc) { FX_RR_ALL(CK_PLANES) } else if (l == 0) { FX_RR_ALL(CK_FINE) }
+        else if (half_faces(o)) { if constexpr (sizeof(T) == 4) { FX_RR_ALL(CK_HALF) } }
+        else { FX_RR_ALL(CK_ARRAYS) }
 #undef FX_RR_ALL
 #undef FX_RR
     }

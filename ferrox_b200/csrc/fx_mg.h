@@ -43,6 +43,11 @@ struct MGLevel {
     // bw[nz], bs[nz], bb[nz + 1] in one array, else null
     double* zc64 = nullptr;
     float* zc32 = nullptr;
+    // the FP32 cycle's face beta of a launched coarse level in FP16, scaled by
+    // 1 / hscale (the largest face beta of the level); null on level 0, on
+    // layered levels (per plane) and without fx.mg_half
+    uint16_t *bwh = nullptr, *bsh = nullptr, *bbh = nullptr;
+    double hscale = 1.0;
 };
 
 // Optional per-launch timing: CUDA events around each launch of a kernel
@@ -132,6 +137,7 @@ public:
     int seg_bytes = 16;      // point red-black half sweeps by row segments of 16 or 32 bytes where the shape allows (k_rbgs_seg); 0: one cell per thread
     long long seg_min_cells = 0;  // ... on levels of at least this many cells
     bool split_mode = true;  // level 0's FP32 correction and residual in the red-black split layout (mixed path)
+    bool half_coarse = true; // the FP32 cycle's coarse face beta in FP16 (set before setup)
 
     static constexpr int kMaxLev = 24;
     Prof* prof = nullptr;

@@ -137,6 +137,7 @@ def test_multigrid_defaults_read_back():
     assert (f.param("fx.mg_nu1"), f.param("fx.mg_nu2"), f.param("fx.mg_mixed_cycles")) == (2, 1, 2)
     assert f.param("fx.alpha_tiles") == 1 and f.param("fx.phi_extrapolate") == 4
     assert (f.param("fx.mg_nu1_coarse"), f.param("fx.mg_nu2_coarse"), f.param("fx.mg_seg")) == (1, -1, 16)
+    assert (f.param("fx.mg_split"), f.param("fx.mg_half")) == (1, 1)
     f.close()
 
 

@@ -297,3 +297,27 @@ def test_no_pre_smoothing_starts_from_a_zero_correction():
     for n in ("Pz", "Phi"):
         scale = np.abs(out[0][n]).max()
         assert np.abs(out[0][n] - out[1][n]).max() <= 1e-7 * scale, n
+
+
+@pytest.mark.parametrize("graph", [1, 0], ids=["step_graph", "host_loop"])
+def test_fp16_coarse_faces_change_convergence_only(graph):
+    """The FP32 correction cycle's coarse face beta in FP16 (fx.mg_half = 1,
+    the default) against FP32 arrays (0): the coarse operators only
+    precondition the FP64 refinement, so both runs solve the same FP64
+    Poisson problem to the same residual bound; the fields agree to the
+    solver tolerance."""
+    text, grains = decks.polycrystal(64, 64, 48, ngrains=6, seed=4, nsteps=10, extra={"Phi_Bc_hi": 0.7})
+    P = start_P((48, 64, 64), 9)
+    out = []
+    for half in (0, 1):
+        f = api.FerroX(text, precision="mixed")
+        f.set_param("fx.mg_half", half)
+        f.set_grains(grains["id"], grains["angles"], grains["tphase"])
+        f.set_initial_P(*P)
+        f.set_param("fx.step_graph", graph)
+        f.step(5)
+        out.append({n: f.field(n) for n in ("Pz", "Phi", "Ez")})
+        f.close()
+    for n in out[0]:
+        scale = np.abs(out[0][n]).max()
+        assert np.abs(out[0][n] - out[1][n]).max() <= 1e-7 * scale, (n, np.abs(out[0][n] - out[1][n]).max() / scale)
