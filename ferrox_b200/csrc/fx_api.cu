@@ -33,6 +33,7 @@ thread_local std::string t_create_error;
 namespace fx {
 std::atomic<long long> g_launches{0};
 bool g_pdl = true;
+bool g_rhs_seg = true;
 // message of the last failed call that has no context (fx_create and the
 // context-free entry points)
 void set_free_error(const std::string& m) { t_create_error = m; }
@@ -947,7 +948,7 @@ std::vector<unsigned char> sg_key(const fx_ctx* c, int use) {
     put(&c->dp, sizeof(DevParams));
     const int iv[] = {c->cur, use, c->par.TimeIntegratorOrder, c->par.precision, c->par.warm_start,
                       c->par.phi_extrapolate, c->par.newton_max_iter, c->par.mg_max_iter, c->mg.nu1, c->mg.nu2,
-                      c->mg.mixed_cycles, c->scalarP ? 1 : 0, c->contains_sc ? 1 : 0, g_pdl ? 1 : 0,
+                      c->mg.mixed_cycles, c->scalarP ? 1 : 0, c->contains_sc ? 1 : 0, g_pdl ? 1 : 0, g_rhs_seg ? 1 : 0,
                       c->mg.alpha_tiles ? 1 : 0, c->mg.nu1c, c->mg.nu2c, c->mg.seg_bytes, c->mg.split_mode ? 1 : 0,
                       (int)std::min<long long>(c->mg.seg_min_cells, 2147483647LL)};
     put(iv, sizeof(iv));
@@ -1783,6 +1784,7 @@ int fx_get_param(const fx_ctx* c, const char* key, double* v) {
         {"fx.adjoint_extrapolate", c->adj_extrap ? 1.0 : 0.0},
         {"adjoint_phi_stored", c->adj.phiAll ? 1.0 : 0.0},
         {"step_graph_ran", c->sg_ran ? 1.0 : 0.0}, {"fx.pdl", g_pdl ? 1.0 : 0.0},
+        {"fx.rhs_seg", g_rhs_seg ? 1.0 : 0.0},
         // 1 when level 0's face coefficients depend on z only and its smoother
         // reads them by plane instead of from the material codes
         {"mg_level0_planes",!c->mg.levels().empty() && (c->mg.levels()[0].zc64 || c->mg.levels()[0].zc32) ? 1.0 : 0.0}};
@@ -1825,7 +1827,7 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
     static const char* const known[] = {
         "Phi_Bc_hi", "Phi_Bc_lo", "fx.mg_rtol", "fx.mg_max_iter", "fx.newton_max_iter", "fx.warm_start",
         "fx.phi_extrapolate", "fx.step_graph", "fx.pdl", "fx.verbose", "fx.profile", "fx.mg_nu1", "fx.graphs",
-        "fx.mg_nu2", "fx.alpha_tiles", "fx.interior", "fx.adjoint_store_phi", "fx.adjoint_extrapolate", "fx.mg_nu1_coarse", "fx.mg_nu2_coarse", "fx.mg_seg", "fx.mg_seg_min", "fx.mg_split", "fx.mg_half", "fx.mg_mixed_cycles", "fx.phi_ghost_mode", "dt", "alpha", "fx.newton_tol",
+        "fx.mg_nu2", "fx.alpha_tiles", "fx.interior", "fx.adjoint_store_phi", "fx.adjoint_extrapolate", "fx.mg_nu1_coarse", "fx.mg_nu2_coarse", "fx.mg_seg", "fx.mg_seg_min", "fx.mg_split", "fx.mg_half", "fx.rhs_seg", "fx.mg_mixed_cycles", "fx.phi_ghost_mode", "dt", "alpha", "fx.newton_tol",
         "beta", "gamma", "g11", "g44", "BigGamma", "inc_step"};
     bool is_known = false;
     for (const char* q : known) is_known = is_known || k == q;
@@ -1859,7 +1861,7 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
     if (k != "fx.profile" && k != "fx.verbose" && k != "fx.graphs" && k != "fx.step_graph" && k != "fx.pdl" &&
         k != "fx.alpha_tiles" && k != "fx.interior" && k != "fx.adjoint_store_phi" && k != "fx.adjoint_extrapolate" &&
         k != "fx.mg_seg" &&
-        k != "fx.mg_seg_min" && k != "fx.mg_split" && k != "fx.mg_half")
+        k != "fx.mg_seg_min" && k != "fx.mg_split" && k != "fx.mg_half" && k != "fx.rhs_seg")
         ++c->gen;
     // the time history of phi only seeds the next solve's initial iterate;
     // electrode values are compared on their own, solver settings leave the
@@ -1884,6 +1886,7 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
     if (k == "fx.mg_seg") { c->mg.seg_bytes = (int)v; return FX_OK; }
     if (k == "fx.mg_split") { c->mg.split_mode = v != 0.0; return FX_OK; }
     if (k == "fx.mg_half") { c->mg.half_coarse = v != 0.0; return FX_OK; }
+    if (k == "fx.rhs_seg") { g_rhs_seg = v != 0.0; return FX_OK; }
     if (k == "fx.mg_seg_min") { c->mg.seg_min_cells = (long long)std::min(v, 9.0e18); return FX_OK; }
     if (k == "fx.adjoint_store_phi") { c->adj_store_phi = v != 0.0; return FX_OK; }
     if (k == "fx.adjoint_extrapolate") { c->adj_extrap = v != 0.0; return FX_OK; }

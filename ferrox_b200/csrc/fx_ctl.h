@@ -31,6 +31,8 @@ extern std::atomic<long long> g_launches;
 // Without the attribute the wait returns at once, so the same kernels serve
 // both forms.
 extern bool g_pdl;
+// the scalar Poisson right-hand side by row segments (k_rhs_p_seg; process-wide like g_pdl)
+extern bool g_rhs_seg;
 
 __device__ __forceinline__ void pdl_entry() {
     asm volatile("griddepcontrol.wait;\n" ::: "memory");

@@ -206,12 +206,21 @@ __global__ void __launch_bounds__(256) k_tdgl(DevParams p, const uint8_t* __rest
     }
 }
 
+// R_z . grad Pz with every rounding fixed
+__device__ __forceinline__ double rhs_r3(double r6, double r7, double r8, double d0, double d1, double d2) {
+    return fma_rn(r8, d2, fma_rn(r7, d1, mul_rn(r6, d0)));
+}
+
 // -sum_ab R_ab dP_a/dx_b at a ferroelectric cell, ElectrostaticSolver.cpp:65-77
 template <bool SCALAR, typename MV, typename PV>
 __device__ __forceinline__ double rhs_fe(const double* R, const MV& M, const PV& Fp, const PV& Fq, const PV& Fr,
                                          int i, int j, int k) {
+    if (SCALAR) {
+        // roundings written out, shared with the row-segment kernel (k_rhs_p_seg)
+        return -rhs_r3(R[6], R[7], R[8], dpd<0, double>(Fr, M, i, j, k), dpd<1, double>(Fr, M, i, j, k),
+                       dpd<2, double>(Fr, M, i, j, k));
+    }
     const double r3 = R[6] * dpd<0, double>(Fr, M, i, j, k) + R[7] * dpd<1, double>(Fr, M, i, j, k) + R[8] * dpd<2, double>(Fr, M, i, j, k);
-    if (SCALAR) return -r3;
     const double r1 = R[0] * dpd<0, double>(Fp, M, i, j, k) + R[1] * dpd<1, double>(Fp, M, i, j, k) + R[2] * dpd<2, double>(Fp, M, i, j, k);
     const double r2 = R[3] * dpd<0, double>(Fq, M, i, j, k) + R[4] * dpd<1, double>(Fq, M, i, j, k) + R[5] * dpd<2, double>(Fq, M, i, j, k);
     return -(r1) - (r2) - (r3);
@@ -258,6 +267,101 @@ __global__ void __launch_bounds__(256) k_rhs_p(DevParams p, const uint8_t* __res
         if (k == 0) bp += 2.0 * e * p.ih2[2] * p.V_lo;
         if (k == p.nz - 1) bp += 2.0 * e * p.ih2[2] * p.V_hi;
         nbp = fabs(bp);
+    }
+    if (norms) {
+        const double a = block_max(nb, sh);
+        const double b = block_max(nbp, sh);
+        if (threadIdx.x == 0 && threadIdx.y == 0) {
+            atomic_max_nonneg(norms, a);
+            atomic_max_nonneg(norms + 1, b);
+        }
+    }
+}
+
+// k_rhs_p for scalar P by row segments: 4 cells of a row per thread.  Where
+// all 4 are interior cells (the whole stencil ferroelectric) the central
+// forms run on the segment's rows loaded once (two 16-byte loads per row);
+// otherwise each cell takes k_rhs_p's own path.  Same operations per cell,
+// so the same bits.
+template <bool ROT>
+__global__ void __launch_bounds__(256) k_rhs_p_seg(DevParams p, const uint8_t* __restrict__ code,
+                                                   const uint8_t* __restrict__ var, const Variant* __restrict__ vt,
+                                                   const double* __restrict__ Pr, double* __restrict__ rhs,
+                                                   double* __restrict__ norms) {
+    pdl_entry();
+    const int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    __shared__ double sh[32];
+    double nb = 0.0, nbp = 0.0;
+    if (j < p.ny) {
+        const size_t c0 = cidx(p, i0, j, k);
+        const unsigned cw = __ldg(reinterpret_cast<const unsigned*>(code + c0 + p.nxy));
+        const unsigned iw = p.interior ? __ldg(reinterpret_cast<const unsigned*>(p.interior + c0)) : 0u;
+        double v[4];
+        bool fast = true;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) fast = fast && ((iw >> (8 * m)) & 0xffu) != 0u && ((cw >> (8 * m)) & 3u) == 0u;
+        if (fast) {
+            const int jm = j == 0 ? p.ny - 1 : j - 1, jp = j == p.ny - 1 ? 0 : j + 1;
+            const int il = i0 == 0 ? p.nx - 1 : i0 - 1, ir = i0 + 4 == p.nx ? 0 : i0 + 4;
+            const size_t row = c0 - i0;
+            double xc[4], xs[4], xn[4], xb[4], xt[4];
+            auto ld4 = [](const double* q, double (&a)[4]) {
+                const double2 u = __ldg(reinterpret_cast<const double2*>(q));
+                const double2 w = __ldg(reinterpret_cast<const double2*>(q) + 1);
+                a[0] = u.x; a[1] = u.y; a[2] = w.x; a[3] = w.y;
+            };
+            ld4(Pr + c0, xc);
+            ld4(Pr + cidx(p, i0, jm, k), xs);
+            ld4(Pr + cidx(p, i0, jp, k), xn);
+            ld4(Pr + c0 - p.nxy, xb);   // interior cells are off the z faces
+            ld4(Pr + c0 + p.nxy, xt);
+            const double xl = __ldg(Pr + row + il), xr = __ldg(Pr + row + ir);
+            const double hx = p.dx[0], hy = p.dx[1], hz = p.dx[2];
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+                double r6 = -0.0, r7 = 0.0, r8 = 1.0;
+                if (ROT) {
+                    const Variant& vv = vt[__ldg(var + c0 + m)];
+                    r6 = vv.R[6]; r7 = vv.R[7]; r8 = vv.R[8];
+                }
+                const double d0 = ((m == 3 ? xr : xc[m + 1]) - (m == 0 ? xl : xc[m - 1])) / (2. * hx);
+                const double d1 = (xn[m] - xs[m]) / (2. * hy);
+                const double d2 = (xt[m] - xb[m]) / (2. * hz);
+                v[m] = -rhs_r3(r6, r7, r8, d0, d1, d2);
+            }
+        } else {
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+                const int i = i0 + m;
+                v[m] = 0.0;
+                if (((cw >> (8 * m)) & 3u) == 0u) {
+                    double R[9] = {1, 0, 0, 0, 1, 0, -0.0, 0, 1};
+                    if (ROT) {
+                        const Variant& vv = vt[__ldg(var + c0 + m)];
+                        for (int q = 0; q < 9; ++q) R[q] = vv.R[q];
+                    }
+                    if (p.interior && ((iw >> (8 * m)) & 0xffu))
+                        v[m] = rhs_fe<true>(R, MInterior{}, PViewIn<double>{Pr, &p}, PViewIn<double>{Pr, &p},
+                                            PViewIn<double>{Pr, &p}, i, j, k);
+                    else
+                        v[m] = rhs_fe<true>(R, MView{code, &p}, PView<double>{Pr, &p}, PView<double>{Pr, &p},
+                                            PView<double>{Pr, &p}, i, j, k);
+                }
+            }
+        }
+        *reinterpret_cast<double2*>(rhs + c0) = make_double2(v[0], v[1]);
+        *(reinterpret_cast<double2*>(rhs + c0) + 1) = make_double2(v[2], v[3]);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            nb = fmax(nb, fabs(v[m]));
+            double bp = v[m];
+            const double e = p.eps[(cw >> (8 * m)) & 7u];
+            if (k == 0) bp += 2.0 * e * p.ih2[2] * p.V_lo;
+            if (k == p.nz - 1) bp += 2.0 * e * p.ih2[2] * p.V_hi;
+            nbp = fmax(nbp, fabs(bp));
+        }
     }
     if (norms) {
         const double a = block_max(nb, sh);
@@ -567,6 +671,17 @@ int launch_rhs_p(const DevParams& p, const uint8_t* code, const uint8_t* var, co
     const dim3 g = cell_grid(p), b(32, 8);
     const bool scal = p.scalar && P[0] == nullptr;
     const bool rot = var != nullptr;
+    const int gx = p.nx / 4;
+    auto al = [](const void* q, uintptr_t a) { return ((uintptr_t)q % a) == 0; };
+    if (scal && g_rhs_seg && p.nx % 4 == 0 && (gx % 32 == 0 || 32 % gx == 0) && al(P[2], 16) && al(rhs, 16) &&
+        al(code + p.nxy, 4) && (!p.interior || al(p.interior, 4))) {
+        // 4 cells of a row per thread
+        const int bx = gx < 32 ? gx : 32, by = 256 / bx;
+        const dim3 bs(bx, by), gs(gx / bx, (p.ny + by - 1) / by, p.nz);
+        if (rot) launch_k(k_rhs_p_seg<true>, gs, bs, 0, s, p, code, var, vt, P[2], rhs, norms);
+        else launch_k(k_rhs_p_seg<false>, gs, bs, 0, s, p, code, var, vt, P[2], rhs, norms);
+        return (int)cudaGetLastError();
+    }
     if (scal) {
         if (rot) launch_k(k_rhs_p<true, true>, g, b, 0, s, p, code, var, vt, P[0], P[1], P[2], rhs, norms);
         else launch_k(k_rhs_p<true, false>, g, b, 0, s, p, code, var, vt, P[0], P[1], P[2], rhs, norms);

@@ -321,3 +321,35 @@ def test_fp16_coarse_faces_change_convergence_only(graph):
     for n in out[0]:
         scale = np.abs(out[0][n]).max()
         assert np.abs(out[0][n] - out[1][n]).max() <= 1e-7 * scale, (n, np.abs(out[0][n] - out[1][n]).max() / scale)
+
+
+@pytest.mark.parametrize("case", ["polycrystal_mixed", "polycrystal_fp64", "mfism_fp64"])
+def test_rhs_segment_kernel_bit_identical(case):
+    """The scalar Poisson right-hand side by row segments (fx.rhs_seg = 1, the
+    default, process-wide) repeats the per-cell kernel's operations: fields,
+    the right-hand side and the cycle counts are bit-identical."""
+    if case.startswith("polycrystal"):
+        text, grains = decks.polycrystal(64, 64, 48, ngrains=6, seed=4, nsteps=10, extra={"Phi_Bc_hi": 0.7})
+        shape = (48, 64, 64)
+    else:
+        text, grains = decks.mfism(32, 32, 48, steps_per_voltage=3, v_step=0.1), None
+        shape = (48, 32, 32)
+    prec = "mixed" if case.endswith("mixed") else None
+    P = start_P(shape, 5)
+    runs = []
+    try:
+        for seg in (0, 1):
+            f = make(text, P, 1, precision=prec, grains=grains)
+            f.set_param("fx.rhs_seg", seg)
+            f.step(5)
+            f.compute_E()
+            runs.append(({n: f.field(n) for n in FIELDS + ["PoissonRHS"]}, f.stats()["mg_cycles_total"]))
+            f.close()
+    finally:
+        g = api.FerroX(decks.mfim(8, 8, 12))
+        g.set_param("fx.rhs_seg", 1)
+        g.close()
+    (a, ca), (b, cb) = runs
+    assert ca == cb
+    for n in a:
+        assert np.array_equal(a[n], b[n]), (n, np.abs(a[n] - b[n]).max())
