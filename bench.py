@@ -52,7 +52,7 @@ METRIC = "coupled-step cell-updates/s"
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum, one ncu
 # capture, cold cache) of the dominant bandwidth-bound kernel class, by
 # (workload, precision, class), with the profile that holds the capture
-TRAFFIC = {("mfism", "fp64", "smooth_l0"): (56.76e6, "profiles/k_rbgs_l0_mfism_128x128x144.txt"),
+TRAFFIC = {("mfism", "fp64", "smooth_l0"): (56.72e6, "profiles/k_rbgs_seg_l0_mfism_128x128x144.txt"),
            ("polycrystal", "mixed", "smooth_l0"): (42.64e6, "profiles/k_rbgs_split_l0_polycrystal_mixed.txt")}
 FALLBACK_HBM_GBS = 6650.0
 
