@@ -949,7 +949,7 @@ std::vector<unsigned char> sg_key(const fx_ctx* c, int use) {
     const int iv[] = {c->cur, use, c->par.TimeIntegratorOrder, c->par.precision, c->par.warm_start,
                       c->par.phi_extrapolate, c->par.newton_max_iter, c->par.mg_max_iter, c->mg.nu1, c->mg.nu2,
                       c->mg.mixed_cycles, c->scalarP ? 1 : 0, c->contains_sc ? 1 : 0, g_pdl ? 1 : 0, g_rhs_seg ? 1 : 0,
-                      c->mg.alpha_tiles ? 1 : 0, c->mg.nu1c, c->mg.nu2c, c->mg.seg_bytes, c->mg.split_mode ? 1 : 0,
+                      c->mg.alpha_tiles ? 1 : 0, c->mg.nu1c, c->mg.nu2c, c->mg.seg_bytes, c->mg.dense_coarse ? 1 : 0, c->mg.split_mode ? 1 : 0,
                       (int)std::min<long long>(c->mg.seg_min_cells, 2147483647LL)};
     put(iv, sizeof(iv));
     const double dv[] = {c->par.mg_rtol, c->par.newton_tol};
@@ -1778,7 +1778,8 @@ int fx_get_param(const fx_ctx* c, const char* key, double* v) {
         {"fx.mg_nu1", (double)c->mg.nu1}, {"fx.mg_nu2", (double)c->mg.nu2},
         {"fx.mg_mixed_cycles", (double)c->mg.mixed_cycles}, {"fx.alpha_tiles", c->mg.alpha_tiles ? 1.0 : 0.0},
         {"fx.mg_seg", (double)c->mg.seg_bytes}, {"fx.mg_seg_min", (double)c->mg.seg_min_cells},
-        {"fx.mg_split", c->mg.split_mode ? 1.0 : 0.0}, {"fx.mg_half", c->mg.half_coarse ? 1.0 : 0.0}, {"mg_level0_split", c->mg.split_now_ ? 1.0 : 0.0},
+        {"fx.mg_split", c->mg.split_mode ? 1.0 : 0.0}, {"fx.mg_half", c->mg.half_coarse ? 1.0 : 0.0},
+        {"fx.mg_dense", c->mg.dense_coarse ? 1.0 : 0.0}, {"mg_level0_split", c->mg.split_now_ ? 1.0 : 0.0},
         {"fx.mg_nu1_coarse", (double)c->mg.nu1c}, {"fx.mg_nu2_coarse", (double)c->mg.nu2c},
         {"fx.interior", c->use_interior ? 1.0 : 0.0}, {"fx.adjoint_store_phi", c->adj_store_phi ? 1.0 : 0.0},
         {"fx.adjoint_extrapolate", c->adj_extrap ? 1.0 : 0.0},
@@ -1827,7 +1828,7 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
     static const char* const known[] = {
         "Phi_Bc_hi", "Phi_Bc_lo", "fx.mg_rtol", "fx.mg_max_iter", "fx.newton_max_iter", "fx.warm_start",
         "fx.phi_extrapolate", "fx.step_graph", "fx.pdl", "fx.verbose", "fx.profile", "fx.mg_nu1", "fx.graphs",
-        "fx.mg_nu2", "fx.alpha_tiles", "fx.interior", "fx.adjoint_store_phi", "fx.adjoint_extrapolate", "fx.mg_nu1_coarse", "fx.mg_nu2_coarse", "fx.mg_seg", "fx.mg_seg_min", "fx.mg_split", "fx.mg_half", "fx.rhs_seg", "fx.mg_mixed_cycles", "fx.phi_ghost_mode", "dt", "alpha", "fx.newton_tol",
+        "fx.mg_nu2", "fx.alpha_tiles", "fx.interior", "fx.adjoint_store_phi", "fx.adjoint_extrapolate", "fx.mg_nu1_coarse", "fx.mg_nu2_coarse", "fx.mg_seg", "fx.mg_seg_min", "fx.mg_split", "fx.mg_half", "fx.mg_dense", "fx.rhs_seg", "fx.mg_mixed_cycles", "fx.phi_ghost_mode", "dt", "alpha", "fx.newton_tol",
         "beta", "gamma", "g11", "g44", "BigGamma", "inc_step"};
     bool is_known = false;
     for (const char* q : known) is_known = is_known || k == q;
@@ -1861,7 +1862,7 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
     if (k != "fx.profile" && k != "fx.verbose" && k != "fx.graphs" && k != "fx.step_graph" && k != "fx.pdl" &&
         k != "fx.alpha_tiles" && k != "fx.interior" && k != "fx.adjoint_store_phi" && k != "fx.adjoint_extrapolate" &&
         k != "fx.mg_seg" &&
-        k != "fx.mg_seg_min" && k != "fx.mg_split" && k != "fx.mg_half" && k != "fx.rhs_seg")
+        k != "fx.mg_seg_min" && k != "fx.mg_split" && k != "fx.mg_half" && k != "fx.rhs_seg" && k != "fx.mg_dense")
         ++c->gen;
     // the time history of phi only seeds the next solve's initial iterate;
     // electrode values are compared on their own, solver settings leave the
@@ -1887,6 +1888,7 @@ int fx_set_param(fx_ctx* c, const char* key, double v) {
     if (k == "fx.mg_split") { c->mg.split_mode = v != 0.0; return FX_OK; }
     if (k == "fx.mg_half") { c->mg.half_coarse = v != 0.0; return FX_OK; }
     if (k == "fx.rhs_seg") { g_rhs_seg = v != 0.0; return FX_OK; }
+    if (k == "fx.mg_dense") { c->mg.dense_coarse = v != 0.0; return FX_OK; }
     if (k == "fx.mg_seg_min") { c->mg.seg_min_cells = (long long)std::min(v, 9.0e18); return FX_OK; }
     if (k == "fx.adjoint_store_phi") { c->adj_store_phi = v != 0.0; return FX_OK; }
     if (k == "fx.adjoint_extrapolate") { c->adj_extrap = v != 0.0; return FX_OK; }

@@ -1873,6 +1873,10 @@ Multigrid::~Multigrid() {
     if (g32b_.exec) cudaGraphExecDestroy(g32b_.exec);
     cudaFree(d_norm_);
     if (h_norm_) cudaFreeHost(h_norm_);
+    cudaFree(dinv64_);
+    cudaFree(dinv32_);
+    dinv64_ = nullptr;
+    dinv32_ = nullptr;
     cudaFree(e32_);
     cudaFree(alt64m_);
     cudaFree(r32_);
@@ -2124,6 +2128,7 @@ int Multigrid::setup(const DevParams& p, const std::vector<uint8_t>& code, bool 
         lev_[0].b32 = r32_;
     }
     plan_coarse(want64, want32);
+    build_dense(want64, want32);
     // the tile level of k_alpha_tiles: the deepest level whose cells cover at
     // most 4096 level-1 cells, with few cells left below it for the last block
     at_T_ = 0;
@@ -2244,6 +2249,137 @@ void Multigrid::plan_coarse(bool want64, bool want32) {
     if (cudaMalloc(&d_fvalid_, 2 * sizeof(int)) == cudaSuccess) cudaMemset(d_fvalid_, 0, 2 * sizeof(int));
 }
 
+// ---- the exact coarse solve: dense inverse of the first one-CTA level
+//
+// In-place Gauss-Jordan inversion of the level's operator (symmetric positive
+// definite: no pivoting), one column k per step in three launches: keep
+// column k, scale row k by the pivot's inverse, eliminate column k from every
+// other row.  Run once at setup.
+__global__ void k_gj_col(const double* __restrict__ A, int n, int k, double* __restrict__ col) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) col[i] = A[(size_t)i * n + k];
+}
+__global__ void k_gj_row(double* __restrict__ A, int n, int k, const double* __restrict__ col) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const double pinv = 1.0 / col[k];
+    A[(size_t)k * n + j] = j == k ? pinv : A[(size_t)k * n + j] * pinv;
+}
+__global__ void k_gj_rest(double* __restrict__ A, int n, int k, const double* __restrict__ col) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y;
+    if (j >= n || i == k) return;
+    const double ci = col[i];
+    if (j == k) A[(size_t)i * n + k] = -ci * (1.0 / col[k]);
+    else A[(size_t)i * n + j] -= ci * A[(size_t)k * n + j];
+}
+__global__ void k_to_f32(const double* __restrict__ a, float* __restrict__ b, size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = (float)a[i];
+}
+
+// x = Ainv b for the first one-CTA level (one warp per row)
+template <typename T>
+__global__ void __launch_bounds__(256) k_dense_solve(const T* __restrict__ Ainv, const T* __restrict__ b,
+                                                     T* __restrict__ x, int n) {
+    pdl_entry();
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= n) return;
+    const T* a = Ainv + (size_t)row * n;
+    T s = T(0);
+    for (int c = lane; c < n; c += 32) s += __ldg(a + c) * __ldg(b + c);
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) x[row] = s;
+}
+
+// the dense inverse of level top's operator (the one-CTA kernel's arrays and
+// arithmetic: face beta times 1/h^2, Dirichlet z faces folded into the
+// diagonal, no alpha), FP64 on the device; null when the level is too large
+static double* dense_inverse(const MGLevel& L, size_t& bytes) {
+    const int n = (int)L.N;
+    if (n <= 0 || n > Multigrid::kDenseMax) return nullptr;
+    const int nx = L.n[0], ny = L.n[1], nz = L.n[2], nxy = nx * ny;
+    std::vector<double> bw(L.N), bs(L.N), bb(L.N + nxy);
+    if (L.bw64) {
+        if (cudaMemcpy(bw.data(), L.bw64, L.N * 8, cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(bs.data(), L.bs64, L.N * 8, cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(bb.data(), L.bb64, (L.N + nxy) * 8, cudaMemcpyDeviceToHost) != cudaSuccess)
+            return nullptr;
+    } else if (L.bw32) {
+        std::vector<float> t(L.N + nxy);
+        if (cudaMemcpy(t.data(), L.bw32, L.N * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return nullptr;
+        for (size_t q = 0; q < L.N; ++q) bw[q] = t[q];
+        if (cudaMemcpy(t.data(), L.bs32, L.N * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return nullptr;
+        for (size_t q = 0; q < L.N; ++q) bs[q] = t[q];
+        if (cudaMemcpy(t.data(), L.bb32, (L.N + nxy) * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return nullptr;
+        for (size_t q = 0; q < L.N + nxy; ++q) bb[q] = t[q];
+    } else {
+        return nullptr;
+    }
+    const double ihx = 1.0 / (L.h[0] * L.h[0]), ihy = 1.0 / (L.h[1] * L.h[1]), ihz = 1.0 / (L.h[2] * L.h[2]);
+    std::vector<double> A((size_t)n * n, 0.0);
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                const int c = i + nx * (j + ny * k);
+                const int im = i == 0 ? nx - 1 : i - 1, ip = i == nx - 1 ? 0 : i + 1;
+                const int jm = j == 0 ? ny - 1 : j - 1, jp = j == ny - 1 ? 0 : j + 1;
+                const int row = c - i;
+                double cw = bw[c] * ihx, ce = bw[row + ip] * ihx;
+                double cs = bs[c] * ihy, cn = bs[c + (jp - j) * nx] * ihy;
+                double cb = 0.0, ct = 0.0, extra = 0.0;
+                if (k > 0) cb = bb[c] * ihz; else extra += 2.0 * bb[c] * ihz;
+                if (k < nz - 1) ct = bb[c + nxy] * ihz; else extra += 2.0 * bb[c + nxy] * ihz;
+                if (nx == 1) { cw = 0.0; ce = 0.0; }
+                if (ny == 1) { cs = 0.0; cn = 0.0; }
+                double* a = &A[(size_t)c * n];
+                a[c] += cw + ce + cs + cn + cb + ct + extra;
+                a[row + im] -= cw;
+                a[row + ip] -= ce;
+                a[c + (jm - j) * nx] -= cs;
+                a[c + (jp - j) * nx] -= cn;
+                if (k > 0) a[c - nxy] -= cb;
+                if (k < nz - 1) a[c + nxy] -= ct;
+            }
+    double *dA = nullptr, *col = nullptr;
+    if (cudaMalloc(&dA, A.size() * 8) != cudaSuccess) return nullptr;
+    if (cudaMalloc(&col, (size_t)n * 8) != cudaSuccess) { cudaFree(dA); return nullptr; }
+    bool ok = cudaMemcpy(dA, A.data(), A.size() * 8, cudaMemcpyHostToDevice) == cudaSuccess;
+    const int tb = 256, gb = (n + tb - 1) / tb;
+    for (int k = 0; ok && k < n; ++k) {
+        k_gj_col<<<gb, tb>>>(dA, n, k, col);
+        k_gj_row<<<gb, tb>>>(dA, n, k, col);
+        k_gj_rest<<<dim3(gb, n), tb>>>(dA, n, k, col);
+    }
+    ok = ok && cudaDeviceSynchronize() == cudaSuccess;
+    cudaFree(col);
+    if (!ok) { cudaFree(dA); return nullptr; }
+    bytes += A.size() * 8;
+    return dA;
+}
+
+// the exact coarse solves, built once at setup (after plan_coarse)
+int Multigrid::build_dense(bool want64, bool want32) {
+    if (!dense_coarse) return 0;
+    if (want64 && coarse_top64_ > 0) dinv64_ = dense_inverse(lev_[coarse_top64_], bytes_);
+    if (want32 && coarse_top32_ > 0) {
+        size_t scratch = 0;
+        double* d = (want64 && coarse_top64_ == coarse_top32_ && dinv64_) ? dinv64_
+                                                                          : dense_inverse(lev_[coarse_top32_], scratch);
+        if (d) {
+            const size_t n2 = lev_[coarse_top32_].N * lev_[coarse_top32_].N;
+            if (cudaMalloc(&dinv32_, n2 * 4) == cudaSuccess) {
+                k_to_f32<<<(unsigned)((n2 + 255) / 256), 256>>>(d, dinv32_, n2);
+                if (cudaDeviceSynchronize() != cudaSuccess) { cudaFree(dinv32_); dinv32_ = nullptr; }
+                else bytes_ += n2 * 4;
+            }
+            if (d != dinv64_) cudaFree(d);
+        }
+    }
+    return 0;
+}
+
 template <> int Multigrid::coarse_top<double>() const { return coarse_top64_; }
 template <> int Multigrid::coarse_top<float>() const { return coarse_top32_; }
 
@@ -2301,6 +2437,18 @@ static CoarseArgs make_coarse_args(const std::vector<MGLevel>& lev_, int top, in
 
 template <typename T>
 void Multigrid::launch_coarse(int top, cudaStream_t s) {
+    const T* dinv = nullptr;
+    if constexpr (sizeof(T) == 8) dinv = dinv64_;
+    else dinv = dinv32_;
+    if (dinv && dense_coarse && !has_alpha_) {
+        // the exact solve of the first one-CTA level: x = Ainv b
+        const int n = (int)lev_[top].N;
+        if (prof) prof->begin(PROF_COARSE_CTA, s);
+        ++g_launches;
+        launch_k(k_dense_solve<T>, (n * 32 + 255) / 256, 256, 0, s, dinv, (const T*)lb<T>(lev_[top]), lx<T>(lev_[top]), n);
+        if (prof) prof->end(s);
+        return;
+    }
     const CoarseArgs A = make_coarse_args<T>(lev_, top, nu1c >= 0 ? nu1c : nu1, nu2c >= 0 ? nu2c : nu2, nu_bottom,
                                              has_alpha_, d_fvalid_);
     const size_t bytes = coarse_bytes(lev_, top, sizeof(T), nullptr);
@@ -2617,7 +2765,7 @@ int Multigrid::replay(GraphCache& g, const void* x, const void* rhs, const DevPa
     }
     if (!g.exec || g.x != x || g.rhs != rhs || g.has_alpha != has_alpha_ || g.vlo != p.V_lo || g.vhi != p.V_hi ||
         g.nu1 != nu1 || g.nu2 != nu2 || g.nu1c != nu1c || g.nu2c != nu2c || g.pdl != g_pdl ||
-        g.seg != seg_bytes || g.seg_min != seg_min_cells || g.split != split_now_) {
+        g.seg != seg_bytes || g.seg_min != seg_min_cells || g.split != split_now_ || g.dense != dense_coarse) {
         if (g.exec) { cudaGraphExecDestroy(g.exec); g.exec = nullptr; }
         cudaGraph_t graph;
         const long long l0 = g_launches.load();
@@ -2633,7 +2781,7 @@ int Multigrid::replay(GraphCache& g, const void* x, const void* rhs, const DevPa
         if (e) return (int)e;
         g.x = x; g.rhs = rhs; g.has_alpha = has_alpha_; g.vlo = p.V_lo; g.vhi = p.V_hi; g.nu1 = nu1; g.nu2 = nu2;
         g.nu1c = nu1c; g.nu2c = nu2c;
-        g.pdl = g_pdl; g.seg = seg_bytes; g.seg_min = seg_min_cells; g.split = split_now_;
+        g.pdl = g_pdl; g.seg = seg_bytes; g.seg_min = seg_min_cells; g.split = split_now_; g.dense = dense_coarse;
     }
     g_launches += g.launches;
     return (int)cudaGraphLaunch(g.exec, s);

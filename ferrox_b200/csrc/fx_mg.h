@@ -138,6 +138,11 @@ public:
     long long seg_min_cells = 0;  // ... on levels of at least this many cells
     bool split_mode = true;  // level 0's FP32 correction and residual in the red-black split layout (mixed path)
     bool half_coarse = true; // the FP32 cycle's coarse face beta in FP16 (set before setup)
+    // the one-CTA levels replaced, while alpha is absent, by the exact solve
+    // with the dense inverse of the first one-CTA level's operator (built at
+    // setup when that level has at most kDenseMax cells)
+    bool dense_coarse = true;
+    static constexpr int kDenseMax = 4096;
 
     static constexpr int kMaxLev = 24;
     Prof* prof = nullptr;
@@ -178,7 +183,7 @@ private:
         bool has_alpha = false;
         double vlo = 0, vhi = 0;
         int nu1 = 0, nu2 = 0, nu1c = 0, nu2c = 0;
-        bool pdl = false, split = false;
+        bool pdl = false, split = false, dense = false;
         int seg = 0;
         long long seg_min = 0;
         long long launches = 0;
@@ -187,6 +192,9 @@ private:
     bool use_graphs_ = true;
     template <typename F> int replay(GraphCache& g, const void* x, const void* rhs, const DevParams& p, cudaStream_t s, F&& enqueue);
     int coarse_top64_ = -1, coarse_top32_ = -1;   // first level run by the one-CTA kernel
+    double* dinv64_ = nullptr;   // dense inverse of level coarse_top64_'s operator (alpha absent), or null
+    float* dinv32_ = nullptr;    // ... of level coarse_top32_'s, FP32
+    int build_dense(bool want64, bool want32);
 
     int* d_fvalid_ = nullptr;    // [0] FP64, [1] FP32: the one-CTA factors in global memory are current
     // k_alpha_tiles: tile level (0: per-level launches), level-l cells per

@@ -353,3 +353,29 @@ def test_rhs_segment_kernel_bit_identical(case):
     assert ca == cb
     for n in a:
         assert np.array_equal(a[n], b[n]), (n, np.abs(a[n] - b[n]).max())
+
+
+@pytest.mark.parametrize("case", ["polycrystal_mixed", "polycrystal_fp64", "mfim_fp64"])
+def test_dense_coarse_solve_changes_convergence_only(case):
+    """With alpha absent the one-CTA levels are replaced by the exact solve
+    with the dense inverse of their first level (fx.mg_dense = 1, the
+    default); against the one-CTA V-cycle (0) the fields agree to the solver
+    tolerance, in the step graph and in the host-driven loop."""
+    if case.startswith("polycrystal"):
+        text, grains = decks.polycrystal(64, 64, 48, ngrains=6, seed=4, nsteps=10, extra={"Phi_Bc_hi": 0.7})
+        shape = (48, 64, 64)
+    else:
+        text, grains = decks.mfim(32, 32, 24, Phi_Bc_hi=0.8), None
+        shape = (24, 32, 32)
+    prec = "mixed" if case.endswith("mixed") else None
+    P = start_P(shape, 13)
+    for graph in (1, 0):
+        out = []
+        for dense in (0, 1):
+            f = make(text, P, graph, precision=prec, grains=grains, params={"fx.mg_dense": dense})
+            f.step(5)
+            out.append({n: f.field(n) for n in ("Pz", "Phi", "Ez")})
+            f.close()
+        for n in out[0]:
+            scale = np.abs(out[0][n]).max()
+            assert np.abs(out[0][n] - out[1][n]).max() <= 1e-7 * scale, (graph, n)
