@@ -2288,7 +2288,19 @@ __global__ void __launch_bounds__(256) k_dense_solve(const T* __restrict__ Ainv,
     if (row >= n) return;
     const T* a = Ainv + (size_t)row * n;
     T s = T(0);
-    for (int c = lane; c < n; c += 32) s += __ldg(a + c) * __ldg(b + c);
+    constexpr int V = 16 / (int)sizeof(T);   // elements per 16-byte load
+    if (n % (32 * V) == 0) {
+        // 16-byte loads, the row in 32 V-element strides
+        for (int c = lane * V; c < n; c += 32 * V) {
+            T av[V], bv[V];
+            ldg16(a + c, av);
+            ldg16(b + c, bv);
+#pragma unroll
+            for (int q = 0; q < V; ++q) s += av[q] * bv[q];
+        }
+    } else {
+        for (int c = lane; c < n; c += 32) s += __ldg(a + c) * __ldg(b + c);
+    }
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
     if (lane == 0) x[row] = s;
 }
