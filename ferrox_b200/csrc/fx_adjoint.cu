@@ -587,7 +587,22 @@ __global__ void __launch_bounds__(256) k_drho(DevParams p, const uint8_t* __rest
 
 dim3 cell_grid2(const DevParams& p) { return dim3((p.nx + 31) / 32, (p.ny + 7) / 8, p.nz); }
 
+// psi = 0 when the reverse step's source is zero (max|mu| not positive):
+// the adjoint solve then starts, and ends, at the exact answer
+__global__ void __launch_bounds__(256) k_zero_if_zero(double* __restrict__ psi, const double* __restrict__ nmu,
+                                                      long long n) {
+    pdl_entry();
+    if (*nmu > 0.0) return;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x)
+        psi[c] = 0.0;
+}
+
 }  // namespace
+
+int launch_zero_if_zero(double* psi, const double* nmu, long long n, cudaStream_t s) {
+    launch_k(k_zero_if_zero, 4 * 148, 256, 0, s, psi, nmu, n);
+    return (int)cudaGetLastError();
+}
 
 int launch_adj_init(const DevParams& p, const uint8_t* code, double* lam[3], double g, cudaStream_t s) {
     k_adj_init<<<p.ngrid_red, 256, 0, s>>>(p, code, lam[0], lam[1], lam[2], g);

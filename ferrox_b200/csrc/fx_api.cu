@@ -212,6 +212,8 @@ struct fx_ctx {
         double *mu = nullptr, *psi = nullptr, *drho = nullptr, *grad = nullptr, *dV = nullptr, *hist = nullptr;
         double* psiHist[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};   // psi of the last reverse steps
         int psi_n = 0;                             // reverse steps of psi history held
+        double* nmu = nullptr;                     // max|mu| of the reverse step (device), and a zero
+        cudaGraphExec_t solve_exec = nullptr;      // the reverse step's adjoint solve as a graph (this backward)
         float* drho32 = nullptr;
         uint8_t* gid = nullptr;
         bool have_P0 = false;
@@ -1401,6 +1403,46 @@ int forward_record(fx_ctx* c, const fx_loss_spec* sp, double* loss) {
     return FX_OK;
 }
 
+// The adjoint Poisson solve of a reverse step as one graph: the coarse
+// alphas of the step's linearisation (semiconductor), psi cleared when the
+// source is zero, and the device-controlled multigrid loop with its target
+// rtol max|mu| formed on the device from A.nmu.  The loop's statistics and a
+// failure accumulate in the step control block, read once after the
+// backward.  Returns false where conditional capture is unavailable.
+bool adj_solve_graph(fx_ctx* c, const DevParams& dp0, bool sc, bool mixed) {
+    auto& A = c->adj;
+    if (!c->d_ctl) {
+        if (dmalloc(c, &c->d_ctl, 1)) return false;
+        if (cudaMallocHost(&c->h_ctl, sizeof(StepCtl)) != cudaSuccess) return false;
+        if (c->cap.init() != cudaSuccess) return false;
+    }
+    c->cap.reset();
+    const long long l0 = g_launches.load();
+    if (cudaStreamBeginCapture(c->s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return false;
+    if (sc) c->mg.set_alpha(A.drho, A.drho32, true, c->s);
+    else c->mg.set_alpha(nullptr, nullptr, false, c->s);
+    launch_zero_if_zero(A.psi, A.nmu, (long long)c->N, c->s);
+    if (mixed)
+        c->mg.enqueue_solve_mixed_ctl(dp0, c->d_code, A.psi, A.mu, A.nmu, c->par.mg_rtol, c->par.mg_max_iter, c->d_ctl,
+                                      c->cap, c->s, false);
+    else
+        c->mg.enqueue_solve64_ctl(dp0, c->d_code, A.psi, A.mu, A.nmu, c->par.mg_rtol, c->par.mg_max_iter, c->d_ctl,
+                                  c->cap, c->s, false);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(c->s, &graph);
+    g_launches -= g_launches.load() - l0;   // counted per execution by the caller's estimate
+    if (!e) e = c->cap.err;
+    if (!e) e = cudaGetLastError();
+    if (!e) e = cudaGraphInstantiate(&A.solve_exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (e) {
+        if (A.solve_exec) { cudaGraphExecDestroy(A.solve_exec); A.solve_exec = nullptr; }
+        cudaGetLastError();
+        return false;
+    }
+    return true;
+}
+
 int backward(fx_ctx* c, double* grads, int ngrads) {
     const auto t0 = std::chrono::steady_clock::now();
     auto& A = c->adj;
@@ -1422,6 +1464,7 @@ int backward(fx_ctx* c, double* grads, int ngrads) {
         if ((r = adj_alloc(c, &A.psi, c->N))) return r;
         for (int q = 0; q < std::min(kMaxExtrap, c->par.phi_extrapolate); ++q)
             if ((r = adj_alloc(c, &A.psiHist[q], c->N))) return r;
+        if ((r = adj_alloc(c, &A.nmu, 2))) return r;
         if (sc && ((r = adj_alloc(c, &A.drho, c->N)) || (r = adj_alloc(c, &A.drho32, c->N)))) return r;
         if ((r = adj_alloc(c, &A.grad, 8 + 256))) return r;
         if ((r = adj_alloc(c, &A.dV, (size_t)T))) return r;
@@ -1444,6 +1487,21 @@ int backward(fx_ctx* c, double* grads, int ngrads) {
     dp0.V_lo = 0.0;
     dp0.V_hi = 0.0;
     const int ngalpha = (int)c->galpha.size();
+    // the reverse steps without a host round trip: the adjoint solve as a
+    // device-controlled graph (fx.step_graph = 1, no per-kernel profiling)
+    bool dev_solve = false;
+    // the solve graph lives for this backward only, whatever path leaves it
+    struct ExecGuard {
+        cudaGraphExec_t* e;
+        ~ExecGuard() { if (*e) { cudaGraphExecDestroy(*e); *e = nullptr; } }
+    } guard{&A.solve_exec};
+    if (c->par.include_Elec && c->par.step_graph && !c->prof.on) {
+        dev_solve = adj_solve_graph(c, dp0, sc, mixed);
+        if (dev_solve) {
+            ++g_launches;
+            if ((r = k_status(c, launch_ctl_step_begin(c->d_ctl, A.nmu, c->s)))) return r;
+        }
+    }
     for (int s = A.nck - 1; s >= 0; --s) {
         const int start = s * k, end = std::min(T, start + k);
         if ((r = adj_restore(c, &A.ckP[3 * s], A.ckPhi[s], A.ckRho[s]))) return r;
@@ -1466,7 +1524,34 @@ int backward(fx_ctx* c, double* grads, int ngrads) {
         for (int n = end; n >= start + 1; --n) {
             const int idx = n - 1 - start;
             const double* psi = nullptr;
-            if (c->par.include_Elec) {
+            if (dev_solve) {
+                // no host round trip: the source norm, the linearisation, the
+                // initial iterate and the graph of the solve, in stream order
+                FX_CUDA(c, cudaMemsetAsync(A.nmu, 0, 2 * sizeof(double), c->s));
+                ++g_launches;
+                r = k_status(c, launch_adj_phi(c->dp, mixed, vec, c->d_code, c->d_var, c->d_vt, A.lam[cur], A.mu,
+                                               A.nmu, A.dV + (n - 1), c->s));
+                if (r) return r;
+                if (sc) {
+                    ++g_launches;
+                    const double* phin = A.phiAll ? A.phiAll + (size_t)(n - 1) * c->N : A.segPhi[idx];
+                    if ((r = k_status(c, launch_drho(c->dp, c->d_code, phin, A.drho, A.drho32, c->s)))) return r;
+                }
+                int order = 0;
+                while (order < 6 && A.psiHist[order]) ++order;
+                if (order > 0 && c->par.warm_start && c->adj_extrap) {
+                    const int use = std::min(order, A.psi_n);
+                    if (use > 0) {
+                        ++g_launches;
+                        if ((r = k_status(c, launch_phi_extrap(c->dp, use, A.psi, A.psiHist, c->s)))) return r;
+                    } else {
+                        FX_CUDA(c, cudaMemcpyAsync(A.psiHist[0], A.psi, c->N * 8, cudaMemcpyDeviceToDevice, c->s));
+                    }
+                    A.psi_n = std::min(order, A.psi_n + 1);
+                }
+                FX_CUDA(c, cudaGraphLaunch(A.solve_exec, c->s));
+                psi = A.psi;   // zero where the source is zero
+            } else if (c->par.include_Elec) {
                 FX_CUDA(c, cudaMemsetAsync(c->d_out, 0, sizeof(double), c->s));
                 ++g_launches;
                 r = k_status(c, launch_adj_phi(c->dp, mixed, vec, c->d_code, c->d_var, c->d_vt, A.lam[cur], A.mu,
@@ -1522,6 +1607,17 @@ int backward(fx_ctx* c, double* grads, int ngrads) {
                                          A.lam[cur], psi, g[n - 1], A.lam[1 - cur], A.grad, A.dV + (n - 1), c->s));
             if (r) return r;
             cur = 1 - cur;
+        }
+    }
+    if (dev_solve) {
+        FX_CUDA(c, cudaMemcpyAsync(c->h_ctl, c->d_ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, c->s));
+        FX_CUDA(c, cudaStreamSynchronize(c->s));
+        const StepCtl& t = *c->h_ctl;
+        A.mg_cycles += t.mg_cycles_step;
+        if (t.status != CTL_OK) {
+            std::ostringstream o;
+            o << "adjoint Poisson multigrid did not reach |r| <= " << t.status_target << " (|r| = " << t.status_val << ")";
+            return set_err(c, t.status == CTL_MG_NO_CONV ? FX_ERR_NO_CONVERGENCE : FX_ERR_NONFINITE, o.str());
         }
     }
     A.lcur = cur;

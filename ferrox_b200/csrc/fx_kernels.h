@@ -51,5 +51,7 @@ int launch_adj_P(const DevParams& p, int mixed, bool vec, const uint8_t* code, c
                  const uint8_t* gid, int ngalpha, const double* const P[3], double* const lam[3], const double* psi,
                  double gload, double* const lam_out[3], double* grad, double* dV, cudaStream_t s);
 int launch_drho(const DevParams& p, const uint8_t* code, const double* phi, double* a64, float* a32, cudaStream_t s);
+// psi = 0 when *nmu (the adjoint source's max) is not positive
+int launch_zero_if_zero(double* psi, const double* nmu, long long n, cudaStream_t s);
 
 }  // namespace fx
