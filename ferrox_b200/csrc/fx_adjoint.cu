@@ -366,8 +366,9 @@ __global__ void __launch_bounds__(256) k_adj_phi(DevParams p, const uint8_t* __r
         phi_visit<T, VEC, ROT>(std::make_integer_sequence<int, 7>{}, p, code, var, vt, lp, lq, lr, D, i, j, k, acc, dvacc);
         dv = p.dt * (double)(mGam * dvacc);
         const double v = p.dt * (double)(mGam * acc);
-        mu[cidx(p, i, j, k)] = v;
-        amax = fabs(v);
+        const size_t cc = cidx(p, i, j, k);
+        mu[cc] = v;
+        if ((long long)cc < p.Ns) amax = fabs(v);   // the solve reads mu on its own cells only
     }
     const double bm = block_max2(amax, sh);
     const double bs = block_sum2(dv, sh);

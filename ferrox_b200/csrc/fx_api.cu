@@ -98,6 +98,11 @@ struct fx_ctx {
     Params par;
     Inputs in;
     DevParams dp{};
+    // an embedded boundary covering the layers k >= eb_nz: the Poisson solve
+    // runs on the fluid layers below it, their top face the embedded
+    // Dirichlet surface at eb_V (read_embedded_boundary, poisson_params)
+    int eb_nz = 0;                       // 0: no embedded boundary
+    double eb_V = 0.0;
     int nx = 0, ny = 0, nz = 0;
     size_t N = 0, nxy = 0;
     double dx[3] = {0, 0, 0};
@@ -247,12 +252,102 @@ double eps_of_code(const Params& p, int code) {
 
 double phi_ref() { return kChi + 0.5 * kEg + 0.5 * kKb * kT * log(kNc / kNv) / kQ; }
 
+// Embedded boundaries (domain.embedded_boundary = 1; EmbeddedBoundaries.cpp:66-140
+// reads the objects, ElectrostaticSolver.cpp:613-676 hands them to MLEBABecLap
+// with setEBDirichlet) in the form the reference's FET decks give them: one
+// `box` object with no fluid inside that spans the periodic x / y extent and
+// covers z from a cell face up to the top of the domain (inputs_mfim_eb:
+// z >= 9 nm of 10 nm; inputs_mfis_eb: z >= 16 nm of 17 nm).  The embedded
+// surface is then the plane z = box_lo[2], a face of the grid: the cells
+// below it are whole fluid cells whose top face carries the Dirichlet value
+// surf_soln (ebgeom.specify_inhomo_dir = 1; 0 V otherwise), the cells above
+// are covered.  A cut-cell geometry -- a surface through the cells, or one
+// that does not span x / y -- needs AMReX's EB2 volume and area fractions and
+// is refused, as are planes, parser and STL objects, EB2 input and unions.
+void read_embedded_boundary(fx_ctx* c) {
+    const auto& T = c->in.table;
+    const auto& K = c->in.constants;
+    auto first = [&](const std::string& key) -> const std::string* {
+        auto it = T.find(key);
+        return (it == T.end() || it->second.empty()) ? nullptr : &it->second[0];
+    };
+    auto num = [&](const std::string& key, double dflt) {
+        const std::string* v = first(key);
+        return v ? eval_number(*v, K) : dflt;
+    };
+    if (num("domain.embedded_boundary", 0.0) == 0.0) return;
+    auto refuse = [](const std::string& why) {
+        throw FxError{FX_ERR_UNSUPPORTED, "embedded boundary: " + why +
+                                              " (only a box object spanning x / y from a cell face to the top of z, "
+                                              "whose surface lies on grid faces, is supported; cut cells are not)"};
+    };
+    if (num("ebgeom.specify_input_using_eb2", 0.0) != 0.0) refuse("ebgeom.specify_input_using_eb2 = 1");
+    auto it = T.find("ebgeom.objects");
+    if (it == T.end() || it->second.empty()) refuse("no ebgeom.objects");
+    if (it->second.size() != 1) refuse("a union of " + std::to_string(it->second.size()) + " objects");
+    const std::string name = it->second[0];
+    const std::string* type = first(name + ".geom_type");
+    if (!type) throw FxError{FX_ERR_INPUTS, "inputs: " + name + ".geom_type is missing"};
+    if (*type != "box") refuse("geom_type " + *type);
+    auto arr3 = [&](const std::string& key, double out[3]) {
+        auto a = T.find(key);
+        if (a == T.end() || a->second.size() < 3) throw FxError{FX_ERR_INPUTS, "inputs: " + key + " needs 3 entries"};
+        for (int d = 0; d < 3; ++d) out[d] = eval_number(a->second[d], K);
+    };
+    double lo[3], hi[3];
+    arr3(name + ".box_lo", lo);
+    arr3(name + ".box_hi", hi);
+    const std::string* fluid = first(name + ".has_fluid_inside");
+    if (!fluid) throw FxError{FX_ERR_INPUTS, "inputs: " + name + ".has_fluid_inside is missing"};
+    if (*fluid == "1" || *fluid == "true") refuse(name + ".has_fluid_inside = 1");
+    if (!(*fluid == "0" || *fluid == "false")) throw FxError{FX_ERR_INPUTS, "inputs: " + name + ".has_fluid_inside must be 0 or 1"};
+    const Params& p = c->par;
+    double dx[3];
+    for (int d = 0; d < 3; ++d) dx[d] = (p.prob_hi[d] - p.prob_lo[d]) / p.n_cell[d];
+    for (int d = 0; d < 2; ++d)
+        if (lo[d] > p.prob_lo[d] + 1e-6 * dx[d] || hi[d] < p.prob_hi[d] - 1e-6 * dx[d])
+            refuse(name + " does not span the domain in " + std::string(d ? "y" : "x"));
+    if (hi[2] < p.prob_hi[2] - 1e-6 * dx[2]) refuse(name + " does not reach the top of the domain");
+    const double f = (lo[2] - p.prob_lo[2]) / dx[2];
+    const long kb = std::lround(f);
+    if (std::fabs(f - (double)kb) > 1e-6) refuse(name + ".box_lo[2] is not on a cell face");
+    if (kb < 1 || kb >= p.n_cell[2]) refuse(name + " leaves no fluid layer or covers no cell");
+    c->eb_nz = (int)kb;
+    c->eb_V = 0.0;
+    if (num("ebgeom.specify_inhomo_dir", 0.0) != 0.0) {
+        const std::string* v = first(name + ".surf_soln");
+        if (!v) throw FxError{FX_ERR_INPUTS, "inputs: " + name + ".surf_soln is missing (ebgeom.specify_inhomo_dir = 1)"};
+        c->eb_V = eval_number(*v, K);
+    }
+}
+
 // SetPhiBC_z values, ElectrostaticSolver.cpp:512-519
 void electrode_values(fx_ctx* c) {
     const double pr = phi_ref();
     const double phi_m = c->par.use_work_function ? c->par.metal_work_function : pr;
     c->dp.V_lo = c->par.Phi_Bc_lo;
     c->dp.V_hi = c->Phi_Bc_hi - (phi_m - pr);
+    c->dp.Ns = c->eb_nz > 0 ? (long long)c->nxy * c->eb_nz : (long long)c->N;
+    c->dp.Vs_hi = c->eb_nz > 0 ? c->eb_V : c->dp.V_hi;
+}
+
+// The grid as the Poisson solver sees it.  With an embedded boundary the
+// solve covers the fluid layers k < eb_nz, a prefix of every cell array, and
+// their top face is the embedded surface: a Dirichlet face at surf_soln
+// (setEBDirichlet, ElectrostaticSolver.cpp:668-672, takes it as given, with
+// the cut cell's own beta_cc), at half a cell from the layer's centres like
+// an electrode.  The covered cells are not part of the solve; phi there keeps
+// the 0 that every solve of ComputePhi_Rho_EB starts from
+// (ElectrostaticSolver.cpp:787).
+DevParams poisson_params(const fx_ctx* c) {
+    DevParams d = c->dp;
+    if (c->eb_nz > 0) {
+        d.nz = c->eb_nz;
+        d.N = d.nxy * c->eb_nz;
+        d.ngrid_red = (int)std::min<long long>(std::max<long long>((d.N + 255) / 256, 1), 148 * 8);
+        d.V_hi = c->eb_V;
+    }
+    return d;
 }
 
 // InitializeMaterialMask, Initialization.cpp:184-202 at one cell centre
@@ -538,7 +633,7 @@ int ensure_device(fx_ctx* c) {
     FX_CUDA(c, cudaMemset(c->d_counter, 0, 4));
     const bool mixed = c->par.precision == 1;
     c->mg.verbose = c->par.verbose;
-    int st = c->mg.setup(c->dp, c->code, true, mixed);
+    int st = c->mg.setup(poisson_params(c), c->code, true, mixed);
     if (st == -2) return set_err(c, FX_ERR_OUT_OF_MEMORY, "multigrid allocation failed");
     if (st != 0) return set_err(c, FX_ERR_CUDA, "multigrid setup failed");
     c->dev_bytes += c->mg.bytes();
@@ -582,8 +677,8 @@ int mg_solve(fx_ctx* c, const double* rhs, double nb, double nbp) {
     if (!c->par.warm_start) FX_CUDA(c, cudaMemsetAsync(c->d_phi, 0, c->N * 8, c->s));
     MGStats st;
     int r = c->par.precision == 1
-                ? c->mg.solve_mixed(c->dp, c->d_code, c->d_phi, rhs, target, c->par.mg_max_iter, c->s, &st)
-                : c->mg.solve64(c->dp, c->d_code, c->d_phi, rhs, target, c->par.mg_max_iter, c->s, &st);
+                ? c->mg.solve_mixed(poisson_params(c), c->d_code, c->d_phi, rhs, target, c->par.mg_max_iter, c->s, &st)
+                : c->mg.solve64(poisson_params(c), c->d_code, c->d_phi, rhs, target, c->par.mg_max_iter, c->s, &st);
     c->mg_last += st.cycles;
     c->mg_total += st.cycles;
     c->mg_resid_last = st.resid;
@@ -840,10 +935,10 @@ void sg_start_guess(fx_ctx* c, cudaStream_t q, int use) {
 void sg_mg_solve(fx_ctx* c, cudaStream_t q, const double* rhs, bool end_in_next) {
     if (!c->par.warm_start) cudaMemsetAsync(c->d_phi, 0, c->N * 8, q);
     if (c->par.precision == 1)
-        c->mg.enqueue_solve_mixed_ctl(c->dp, c->d_code, c->d_phi, rhs, c->d_out, c->par.mg_rtol, c->par.mg_max_iter,
+        c->mg.enqueue_solve_mixed_ctl(poisson_params(c), c->d_code, c->d_phi, rhs, c->d_out, c->par.mg_rtol, c->par.mg_max_iter,
                                       c->d_ctl, c->cap, q, end_in_next);
     else
-        c->mg.enqueue_solve64_ctl(c->dp, c->d_code, c->d_phi, rhs, c->d_out, c->par.mg_rtol, c->par.mg_max_iter,
+        c->mg.enqueue_solve64_ctl(poisson_params(c), c->d_code, c->d_phi, rhs, c->d_out, c->par.mg_rtol, c->par.mg_max_iter,
                                   c->d_ctl, c->cap, q, end_in_next);
 }
 
@@ -1483,7 +1578,7 @@ int backward(fx_ctx* c, double* grads, int ngrads) {
     int cur = 0;
     if ((r = k_status(c, launch_adj_init(c->dp, c->d_code, A.lam[cur], g[T], c->s)))) return r;
     ++g_launches;
-    DevParams dp0 = c->dp;   // the adjoint solve: homogeneous electrode values
+    DevParams dp0 = poisson_params(c);   // the adjoint solve: homogeneous electrode values
     dp0.V_lo = 0.0;
     dp0.V_hi = 0.0;
     const int ngalpha = (int)c->galpha.size();
@@ -1726,19 +1821,18 @@ int fx_create(const char* inputs, int is_text, fx_ctx** out) {
         c->in = parse_inputs(text);
         c->par = make_params(c->in);
         Params& p = c->par;
-        {
-            // the AMReX cut-cell Poisson path (ElectrostaticSolver.cpp:613-676) is not restated
-            auto it = c->in.table.find("domain.embedded_boundary");
-            if (it != c->in.table.end() && !it->second.empty() && eval_number(it->second[0], c->in.constants) != 0.0)
-                throw FxError{FX_ERR_UNSUPPORTED, "domain.embedded_boundary = 1 (the cut-cell Poisson solver of "
-                                                  "AMReX MLEBABecLap) is not supported"};
-        }
+        read_embedded_boundary(c.get());
         if (!p.is_periodic[0] || !p.is_periodic[1] || p.is_periodic[2])
             throw FxError{FX_ERR_UNSUPPORTED, "only domain.is_periodic = 1 1 0 (periodic x/y, electrodes in z) is supported"};
         for (int d = 0; d < 2; ++d)
             if ((!p.bc_lo[d].empty() && p.bc_lo[d].substr(0, 3) != "per") || (!p.bc_hi[d].empty() && p.bc_hi[d].substr(0, 3) != "per"))
                 throw FxError{FX_ERR_INPUTS, "boundary.lo/hi must be 'per' in periodic directions (BoundaryConditions.cpp:196)"};
-        if ((!p.bc_lo[2].empty() && p.bc_lo[2].substr(0, 3) != "dir") || (!p.bc_hi[2].empty() && p.bc_hi[2].substr(0, 3) != "dir"))
+        // the top boundary lies inside the covered cells of an embedded
+        // boundary, where its type (the reference's EB decks give neu) never enters
+        const bool hi_covered = c->eb_nz > 0;
+        if ((!p.bc_lo[2].empty() && p.bc_lo[2].substr(0, 3) != "dir") ||
+            (!hi_covered && !p.bc_hi[2].empty() && p.bc_hi[2].substr(0, 3) != "dir") ||
+            (hi_covered && !p.bc_hi[2].empty() && p.bc_hi[2].substr(0, 3) == "per"))
             throw FxError{FX_ERR_UNSUPPORTED, "z boundaries must be Dirichlet electrodes (dir)"};
         c->nx = p.n_cell[0]; c->ny = p.n_cell[1]; c->nz = p.n_cell[2];
         for (int d = 0; d < 2; ++d)
@@ -1882,6 +1976,9 @@ int fx_get_param(const fx_ctx* c, const char* key, double* v) {
         {"adjoint_phi_stored", c->adj.phiAll ? 1.0 : 0.0},
         {"step_graph_ran", c->sg_ran ? 1.0 : 0.0}, {"fx.pdl", g_pdl ? 1.0 : 0.0},
         {"fx.rhs_seg", g_rhs_seg ? 1.0 : 0.0},
+        // the embedded boundary: the Poisson solve's fluid layers (0: none)
+        // and the Dirichlet value on their top face
+        {"eb_fluid_layers", (double)c->eb_nz}, {"eb_surf_soln", c->eb_V},
         // 1 when level 0's face coefficients depend on z only and its smoother
         // reads them by plane instead of from the material codes
         {"mg_level0_planes",!c->mg.levels().empty() && (c->mg.levels()[0].zc64 || c->mg.levels()[0].zc32) ? 1.0 : 0.0}};

@@ -51,6 +51,11 @@ struct DevParams {
     // z Dirichlet values of phi held by the solver and the ghost mode
     double V_lo, V_hi;
     int ghost_mode;
+    // the Poisson solve's cells, a prefix of every cell array (N, or the
+    // fluid layers below an embedded boundary), and the Dirichlet value on
+    // their top face (V_hi, or the embedded surface's)
+    long long Ns;
+    double Vs_hi;
     // one byte per cell: 1 where the cell and its 18 face and edge neighbours
     // are ferroelectric and 1 <= k <= nz - 2, so that every mask test of the
     // P stencils passes (their central forms apply); null: none flagged

@@ -261,12 +261,14 @@ __global__ void __launch_bounds__(256) k_rhs_p(DevParams p, const uint8_t* __res
                                    PView<double>{Pr, &p}, i, j, k);
         }
         rhs[c] = v;
-        nb = fabs(v);
-        double bp = v;
-        const double e = p.eps[m & 7];
-        if (k == 0) bp += 2.0 * e * p.ih2[2] * p.V_lo;
-        if (k == p.nz - 1) bp += 2.0 * e * p.ih2[2] * p.V_hi;
-        nbp = fabs(bp);
+        if ((long long)c < p.Ns) {   // the norms cover the cells of the solve
+            nb = fabs(v);
+            double bp = v;
+            const double e = p.eps[m & 7];
+            if (k == 0) bp += 2.0 * e * p.ih2[2] * p.V_lo;
+            if ((long long)c >= p.Ns - p.nxy) bp += 2.0 * e * p.ih2[2] * p.Vs_hi;
+            nbp = fabs(bp);
+        }
     }
     if (norms) {
         const double a = block_max(nb, sh);
@@ -353,14 +355,16 @@ __global__ void __launch_bounds__(256) k_rhs_p_seg(DevParams p, const uint8_t* _
         }
         *reinterpret_cast<double2*>(rhs + c0) = make_double2(v[0], v[1]);
         *(reinterpret_cast<double2*>(rhs + c0) + 1) = make_double2(v[2], v[3]);
+        if ((long long)c0 < p.Ns) {   // the norms cover the cells of the solve
 #pragma unroll
-        for (int m = 0; m < 4; ++m) {
-            nb = fmax(nb, fabs(v[m]));
-            double bp = v[m];
-            const double e = p.eps[(cw >> (8 * m)) & 7u];
-            if (k == 0) bp += 2.0 * e * p.ih2[2] * p.V_lo;
-            if (k == p.nz - 1) bp += 2.0 * e * p.ih2[2] * p.V_hi;
-            nbp = fmax(nbp, fabs(bp));
+            for (int m = 0; m < 4; ++m) {
+                nb = fmax(nb, fabs(v[m]));
+                double bp = v[m];
+                const double e = p.eps[(cw >> (8 * m)) & 7u];
+                if (k == 0) bp += 2.0 * e * p.ih2[2] * p.V_lo;
+                if ((long long)c0 >= p.Ns - p.nxy) bp += 2.0 * e * p.ih2[2] * p.Vs_hi;
+                nbp = fmax(nbp, fabs(bp));
+            }
         }
     }
     if (norms) {
@@ -392,7 +396,7 @@ __device__ __forceinline__ void newton_cell(const DevParams& p, const double* se
     }
     bp = v;
     if (c < p.nxy) bp += 2.0 * seps[m & 7] * p.ih2[2] * p.V_lo;             // k == 0
-    if (c >= p.N - p.nxy) bp += 2.0 * seps[m & 7] * p.ih2[2] * p.V_hi;      // k == nz - 1
+    if (c >= p.Ns - p.nxy) bp += 2.0 * seps[m & 7] * p.ih2[2] * p.Vs_hi;    // the solve's top layer
 }
 
 // PAIR: each thread takes two neighbouring cells with vector loads and
@@ -428,8 +432,10 @@ __global__ void __launch_bounds__(256) k_newton(DevParams p, const uint8_t* __re
             *reinterpret_cast<double2*>(alpha + c) = make_double2(a0, a1);
             *reinterpret_cast<float2*>(alpha32 + c) = make_float2((float)a0, (float)a1);
             *reinterpret_cast<double2*>(rhs + c) = make_double2(v0, v1);
-            nb = fmax(nb, fmax(fabs(v0), fabs(v1)));
-            nbp = fmax(nbp, fmax(fabs(bp0), fabs(bp1)));
+            if (c < p.Ns) {   // the norms cover the cells of the solve (Ns, nxy even)
+                nb = fmax(nb, fmax(fabs(v0), fabs(v1)));
+                nbp = fmax(nbp, fmax(fabs(bp0), fabs(bp1)));
+            }
         }
     } else {
         for (long long c = (long long)blockIdx.x * 256 + tid; c < p.N; c += (long long)gridDim.x * 256) {
@@ -439,8 +445,10 @@ __global__ void __launch_bounds__(256) k_newton(DevParams p, const uint8_t* __re
             alpha[c] = a;
             alpha32[c] = (float)a;
             rhs[c] = v;
-            nb = fmax(nb, fabs(v));
-            nbp = fmax(nbp, fabs(bp));
+            if (c < p.Ns) {
+                nb = fmax(nb, fabs(v));
+                nbp = fmax(nbp, fabs(bp));
+            }
         }
     }
     const double x = block_max(nb, sh);

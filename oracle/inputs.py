@@ -349,6 +349,53 @@ def ferrox_params(table: dict[str, list[str]]) -> dict:
     return p
 
 
+def embedded_boundary(table: dict[str, list[str]], p: dict):
+    """(fluid layers, surface value) of a grid-aligned embedded boundary, or None.
+
+    EmbeddedBoundaries.cpp:66-140 reads ``ebgeom.objects`` and each object's
+    ``geom_type``, ``box_lo`` / ``box_hi``, ``has_fluid_inside`` and, with
+    ``ebgeom.specify_inhomo_dir = 1``, ``surf_soln``.  The oracle takes the
+    form the reference's FET decks use: one box with no fluid inside spanning
+    x and y and covering z from a cell face to the top, so the embedded surface
+    is the face below layer ``kb`` and the solve runs on layers ``k < kb``.
+    Any other geometry raises ``ValueError``.
+    """
+    consts = constants(table)
+
+    def first(key, default=None):
+        return table[key][0] if key in table and table[key] else default
+
+    if float(eval_expr(first("domain.embedded_boundary", "0"), consts)) == 0.0:
+        return None
+    if float(eval_expr(first("ebgeom.specify_input_using_eb2", "0"), consts)) != 0.0:
+        raise ValueError("embedded boundary: EB2 input")
+    names = table.get("ebgeom.objects", [])
+    if len(names) != 1:
+        raise ValueError("embedded boundary: exactly one object expected")
+    name = names[0]
+    if first(name + ".geom_type") != "box":
+        raise ValueError("embedded boundary: only box objects")
+    if first(name + ".has_fluid_inside") not in ("0", "false"):
+        raise ValueError("embedded boundary: the box must have no fluid inside")
+    lo = [float(eval_expr(v, consts)) for v in table[name + ".box_lo"][:3]]
+    hi = [float(eval_expr(v, consts)) for v in table[name + ".box_hi"][:3]]
+    plo, phi_, n = p["prob_lo"], p["prob_hi"], p["n_cell"]
+    h = [(phi_[d] - plo[d]) / n[d] for d in range(3)]
+    for d in range(2):
+        if lo[d] > plo[d] + 1e-6 * h[d] or hi[d] < phi_[d] - 1e-6 * h[d]:
+            raise ValueError("embedded boundary: the box must span x and y")
+    if hi[2] < phi_[2] - 1e-6 * h[2]:
+        raise ValueError("embedded boundary: the box must reach the top")
+    f = (lo[2] - plo[2]) / h[2]
+    kb = int(round(f))
+    if abs(f - kb) > 1e-6 or not 1 <= kb < n[2]:
+        raise ValueError("embedded boundary: the surface must be an interior cell face")
+    V = 0.0
+    if float(eval_expr(first("ebgeom.specify_inhomo_dir", "0"), consts)) != 0.0:
+        V = float(eval_expr(first(name + ".surf_soln"), consts))
+    return kb, V
+
+
 def cell_centres(p: dict):
     n = p["n_cell"]
     dx = [(p["prob_hi"][d] - p["prob_lo"][d]) / n[d] for d in range(3)]

@@ -110,6 +110,11 @@ struct ofx_ctx {
     Fab beta_cc;
     Fab ang[3];
     std::vector<double> bxf, byf, bzf;   // beta on faces
+    // a grid-aligned embedded boundary covering the layers k >= eb_nz
+    // (0: none): the solve runs on the layers below it with the Dirichlet
+    // value eb_V on their top face (ofx_set_eb)
+    int eb_nz = 0;
+    double eb_V = 0.0;
     double V_lo = 0.0, V_hi = 0.0;       // Dirichlet values held by setLevelBC
     bool contains_sc = false;
 
@@ -646,9 +651,22 @@ void mg_setup(ofx_ctx* c, const double* alpha_cc_valid) {
     if (c->mg.empty()) {
         MGLevel l0;
         for (int d = 0; d < 3; ++d) { l0.n[d] = c->n[d]; l0.h[d] = c->dx[d]; }
+        if (c->eb_nz > 0) l0.n[2] = c->eb_nz;
         size_t N = l0.N();
         l0.a.assign(N, 0.0);
         l0.bx = c->bxf; l0.by = c->byf; l0.bz = c->bzf;
+        if (c->eb_nz > 0) {
+            // the fluid layers' faces; the embedded surface (their top face)
+            // takes the cut cell's beta_cc, as setEBDirichlet is given beta_cc
+            // (ElectrostaticSolver.cpp:668-672)
+            const size_t nxy = (size_t)c->n[0] * c->n[1];
+            l0.bx.resize((size_t)(c->n[0] + 1) * c->n[1] * c->eb_nz);
+            l0.by.resize((size_t)c->n[0] * (c->n[1] + 1) * c->eb_nz);
+            l0.bz.resize(nxy * (c->eb_nz + 1));
+            for (int j = 0; j < c->n[1]; ++j)
+                for (int i = 0; i < c->n[0]; ++i)
+                    l0.bz[(size_t)i + (size_t)c->n[0] * j + nxy * c->eb_nz] = c->beta_cc(i, j, c->eb_nz - 1);
+        }
         l0.x.assign(N, 0.0); l0.r.assign(N, 0.0); l0.t.assign(N, 0.0);
         c->mg.push_back(std::move(l0));
         mg_build_coarse(c->mg);
@@ -664,7 +682,8 @@ int mg_solve(ofx_ctx* c, const double* b, double* sol, double rtol, int* iters, 
     MGLevel& l0 = c->mg[0];
     size_t N = l0.N();
     std::vector<double> res(N);
-    mg_residual(l0, sol, b, res.data(), c->V_lo, c->V_hi);
+    const double vhi = c->eb_nz > 0 ? c->eb_V : c->V_hi;   // the solve's top Dirichlet value
+    mg_residual(l0, sol, b, res.data(), c->V_lo, vhi);
     double resnorm0 = norm_inf(res.data(), N);
     double rhsnorm0 = norm_inf(b, N);
     double target = std::max(rtol, 1e-16) * std::max(resnorm0, rhsnorm0);
@@ -675,7 +694,7 @@ int mg_solve(ofx_ctx* c, const double* b, double* sol, double rtol, int* iters, 
         l0.r = res;
         mg_vcycle(c->mg, 0);
         for (size_t q = 0; q < N; ++q) sol[q] += l0.x[q];
-        mg_residual(l0, sol, b, res.data(), c->V_lo, c->V_hi);
+        mg_residual(l0, sol, b, res.data(), c->V_lo, vhi);
         rn = norm_inf(res.data(), N);
         ++it;
         if (c->p.verbose > 1) printf("  mg iter %d  |r|/|r0| = %g\n", it, rn / std::max(resnorm0, rhsnorm0));
@@ -1307,7 +1326,16 @@ int ofx_poisson_apply(ofx_ctx* c, const double* alpha_cc, const double* phi, int
     for (int k = 0; k < l.n[2]; ++k)
         for (int j = 0; j < l.n[1]; ++j)
             for (int i = 0; i < l.n[0]; ++i)
-                out[L3(l, i, j, k)] = apply_cell(l, phi, i, j, k, inh ? c->V_lo : 0.0, inh ? c->V_hi : 0.0);
+                out[L3(l, i, j, k)] = apply_cell(l, phi, i, j, k, inh ? c->V_lo : 0.0,
+                                                 inh ? (c->eb_nz > 0 ? c->eb_V : c->V_hi) : 0.0);
+    return 0;
+}
+
+int ofx_set_eb(ofx_ctx* c, int nz_fluid, double V) {
+    if (nz_fluid < 0 || nz_fluid >= c->n[2]) return -1;
+    c->eb_nz = nz_fluid;
+    c->eb_V = V;
+    c->mg.clear();   // the hierarchy is built for the solve's layers
     return 0;
 }
 

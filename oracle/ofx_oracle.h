@@ -113,6 +113,10 @@ int ofx_poisson_solve(ofx_ctx* c, const double* rhs, const double* alpha_cc,
                       double* phi, double rtol, int* iters_out, double* resid_out);
 int ofx_poisson_apply(ofx_ctx* c, const double* alpha_cc, const double* phi,
                       int inhomogeneous, double* out);
+// a grid-aligned embedded boundary covering the layers k >= nz_fluid (0:
+// none): later Poisson solves run on the layers below it, their top face a
+// Dirichlet face at V with the cell's own beta; call before the first solve
+int ofx_set_eb(ofx_ctx* c, int nz_fluid, double V);
 
 /* Calculate_Landau / Calculate_Grad / Calculate_Elec outputs for the current
  * P and E (3 x N each, x fastest) */

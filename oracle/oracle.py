@@ -74,6 +74,8 @@ def lib():
         L.ofx_get_beta_faces.argtypes = [vp, dp, dp, dp]
         L.ofx_poisson_solve.argtypes = [vp, dp, dp, dp, C.c_double, ip, dp]
         L.ofx_poisson_apply.argtypes = [vp, dp, dp, C.c_int, dp]
+        L.ofx_set_eb.argtypes = [vp, C.c_int, C.c_double]
+        L.ofx_set_eb.restype = C.c_int
         L.ofx_tdgl_terms.argtypes = [vp, dp, dp, dp]
         L.ofx_get_scalar.argtypes = [vp, C.c_char_p]
         L.ofx_get_scalar.restype = C.c_double
@@ -131,6 +133,9 @@ class Oracle:
         p = _inputs.ferrox_params(table)
         tph, a, b, t = _inputs.function_fields(table, p)
         o = cls(p, tph, (a, b, t), **kw)
+        eb = _inputs.embedded_boundary(table, p)
+        if eb is not None:
+            o.set_eb(*eb)
         if "fx.initial_P_file" in table:
             # the initial P file (format: ferrox_b200.decks.write_P_file)
             from ferrox_b200 import decks
@@ -138,6 +143,11 @@ class Oracle:
             for name, comp in zip(["Px", "Py", "Pz"], P):
                 o.set_field(name, np.zeros(o.shape) if comp is None else comp)
         return o
+
+    def set_eb(self, nz_fluid: int, V: float) -> None:
+        """Embedded surface on the face below layer nz_fluid (0: none), Dirichlet value V."""
+        if lib().ofx_set_eb(self.h, int(nz_fluid), float(V)) != 0:
+            raise ValueError("oracle: embedded boundary layer out of range")
 
     def __del__(self):
         if getattr(self, "h", None):

@@ -2,7 +2,8 @@
 
 The FerroX tree ships inputs decks for its regression runs
 (Exec/regression_inputs/3D_MFIM/inputs_mfim_Noeb and
-Exec/regression_inputs/MIS/input_mis) but no outputs.  The parity tests run
+Exec/regression_inputs/MIS/input_mis) and examples with an embedded metal
+boundary (Exec/Examples/inputs_mfim_eb, inputs_mfis_eb), but no outputs.  The parity tests run
 these decks through both the GPU library and the CPU oracle; the reference
 tree is not present where the GPU tests run, so the decks travel as fixtures.
 This script keeps each `key = value` line (comments and blank lines dropped,
@@ -18,6 +19,8 @@ import sys
 DECKS = {
     "3D_MFIM_inputs_mfim_Noeb.inputs": "Exec/regression_inputs/3D_MFIM/inputs_mfim_Noeb",
     "MIS_input_mis.inputs": "Exec/regression_inputs/MIS/input_mis",
+    "Examples_inputs_mfim_eb.inputs": "Exec/Examples/inputs_mfim_eb",
+    "Examples_inputs_mfis_eb.inputs": "Exec/Examples/inputs_mfis_eb",
 }
 
 

@@ -27,6 +27,9 @@ def pair(text, grains=None, P=None, precision=None, rtol=None):
     else:
         tph, a, b, t = I.function_fields(table, p)
         o = O.Oracle(p, tph, (a, b, t))
+    eb = I.embedded_boundary(table, p)
+    if eb is not None:
+        o.set_eb(*eb)
     if P is not None:
         f.set_initial_P(*P)
         for name, comp in zip(["Px", "Py", "Pz"], P):

@@ -222,13 +222,3 @@ def test_gradient_entry_points_check_arguments_before_any_device_work():
     with pytest.raises(api.FxError) as e:
         h.forward_record(np.zeros(4), 1.0)
     assert e.value.code == -3
-
-
-def test_embedded_boundary_decks_are_refused():
-    """domain.embedded_boundary = 1 selects the reference's AMReX cut-cell
-    Poisson solver, which is not restated: fx_create refuses it with
-    FX_ERR_UNSUPPORTED rather than silently solving without the boundary."""
-    with pytest.raises(api.FxError) as e:
-        api.FerroX(decks.mfim(8, 8, 12) + "domain.embedded_boundary = 1\n")
-    assert e.value.code == -3 and "embedded_boundary" in str(e.value)
-    api.FerroX(decks.mfim(8, 8, 12) + "domain.embedded_boundary = 0\n").close()
