@@ -131,6 +131,23 @@ def test_fd_semiconductor_newton():
     check_fd(make, 0.8, 10, 4, which=[0, 3, 5])
 
 
+def test_fd_embedded_boundary():
+    # the reference's MFIM deck with the embedded metal over the top 1 nm
+    # (16 x 16 lateral cells): the adjoint solves run on the fluid layers like
+    # the forward ones.  The swept top electrode lies under the metal, so v_amp
+    # has no effect and is left out
+    import os
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "decks")
+    with open(os.path.join(here, "Examples_inputs_mfim_eb.inputs")) as f:
+        text = f.read().replace("domain.n_cell = 64 64 20", "domain.n_cell = 16 16 20")
+    assert "domain.n_cell = 16 16 20" in text
+    make = maker(text, start_P((20, 16, 16), 6))
+    f = make()
+    assert f.param("eb_fluid_layers") == 18
+    f.close()
+    check_fd(make, 1.0, 16, 5, which=[0, 3, 4])
+
+
 def test_fd_per_grain_alpha():
     text, g = decks.polycrystal(16, 16, 24, ngrains=6, seed=5, nsteps=10)
     ga = np.full(6, -2.5e9) * (1.0 + 0.1 * np.arange(6))

@@ -157,3 +157,34 @@ def test_eb_deck_coupled_steps(name, precision):
         assert np.all(f.field("Phi")[kb:] == 0.0)
     finally:
         f.close()
+
+
+@pytest.mark.gpu
+def test_executable_runs_the_reference_eb_deck(tmp_path):
+    """The reference's inputs_mfim_eb file through the executable, as the
+    reference's own binary takes it: plotfiles of the full 64 x 64 x 20 grid
+    with phi 0 in the covered layers, and the library's fields to within the
+    deck's solver tolerance (the executable also writes the step-0 plotfile)."""
+    import subprocess
+
+    from ferrox_b200 import build, plotfile
+    build.build()
+    exe = os.path.join(os.path.dirname(os.path.dirname(HERE)), "..", "ferrox_b200", "ferrox_b200")
+    deck_path = tmp_path / "inputs_mfim_eb"
+    deck_path.write_text(deck(MFIM_EB))
+    r = subprocess.run([os.path.abspath(exe), str(deck_path), "nsteps=4", "plot_int=2"], cwd=tmp_path,
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    for step in (0, 2, 4):
+        assert (tmp_path / f"plt{step:08d}").is_dir(), step
+    pf = plotfile.read(str(tmp_path / "plt00000004"))
+    assert pf["n"] == [64, 64, 20] and pf["step"] == 4
+    phi = pf["fields"]["Phi"]
+    assert np.all(phi[18:] == 0.0) and np.abs(phi[:18]).max() > 0.0
+    f = api.FerroX(with_keys(deck(MFIM_EB), nsteps="4", plot_int="2"))
+    try:
+        f.step(4)
+        for name in ["Pz", "Phi", "Ez"]:
+            assert relerr(pf["fields"][name], f.field(name)) < 1e-8, name
+    finally:
+        f.close()
