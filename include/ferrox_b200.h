@@ -75,8 +75,12 @@ const char* fx_version(void);
  * masks, permittivity and the initial P on the host, as c_FerroX::InitData +
  * InitializeFerroXNamespace + InitializeMaterialMask + InitializePermittivity
  * + InitializePandRho do (Source/FerroX.cpp:150-572, main.cpp:65-226).
- * Device memory is allocated at the first call that needs the GPU.  On
- * failure *out is NULL and fx_create_error() holds the message. */
+ * Device memory is allocated at the first call that needs the GPU.  An
+ * embedded boundary (domain.embedded_boundary = 1, SetupMLMG_EB,
+ * ElectrostaticSolver.cpp:613-676) is taken when it lies on grid faces: one
+ * box with no fluid inside spanning x / y from a cell face to the top of z;
+ * other geometries give FX_ERR_UNSUPPORTED.  On failure *out is NULL and
+ * fx_create_error() holds the message. */
 int         fx_create(const char* inputs, int is_text, fx_ctx** out);
 /* message of the last failed fx_create (or fx_mean_P_noalloc) on this thread */
 const char* fx_create_error(void);
@@ -91,7 +95,10 @@ int fx_get_dims(const fx_ctx* ctx, int n_cell[3], double dx[3]);
  * run), mg_level0_planes (1 when level 0's face coefficients depend on z
  * only and are read by plane) and step_graph_ran (1 when the last step ran
  * as one CUDA graph with its Newton and multigrid loop tests on the device,
- * fx.step_graph = 1; 0 when the host-driven loop ran it). */
+ * fx.step_graph = 1; 0 when the host-driven loop ran it), eb_fluid_layers
+ * and eb_surf_soln (domain.embedded_boundary = 1: the layers below the
+ * embedded surface that the Poisson solve covers, 0 without one, and the
+ * surface's Dirichlet value). */
 int fx_get_param(const fx_ctx* ctx, const char* key, double* value);
 int fx_set_param(fx_ctx* ctx, const char* key, double value);
 
