@@ -72,7 +72,14 @@ def test_library_exports_every_declared_symbol():
     assert b"sm_100a" in L.fx_version()
 
 
-@pytest.mark.parametrize("text", [decks.mfim(16, 16, 12), decks.mfism(16, 16, 48), REF_DECK])
+def _golden(name):
+    with open(os.path.join(ROOT, "tests", "golden", "decks", name)) as f:
+        return f.read()
+
+
+@pytest.mark.parametrize("text", [decks.mfim(16, 16, 12), decks.mfism(16, 16, 48), REF_DECK,
+                                  _golden("Examples_inputs_mfis_eb.inputs")],
+                         ids=["mfim", "mfism", "ref_deck", "mfis_eb"])
 def test_setup_matches_oracle(text):
     f = api.FerroX(text)
     table = I.parse_table(text)
