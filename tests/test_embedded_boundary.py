@@ -188,3 +188,38 @@ def test_executable_runs_the_reference_eb_deck(tmp_path):
             assert relerr(pf["fields"][name], f.field(name)) < 1e-8, name
     finally:
         f.close()
+
+
+def test_oracle_embedded_face_known_answer():
+    """Without charge the layered MFIM stack under the embedded metal is a
+    chain of conductances in z: eps of the bottom cell over half a cell to the
+    electrode, the face averages 0.5 (eps_k + eps_k+1) between layers, and eps
+    of the top fluid cell over half a cell to the embedded surface.  The
+    oracle's 3D solve with the embedded face equals that chain's solution."""
+    V, Vlo = 0.5, -0.2
+    text = with_keys(deck(MFIM_EB), MyGeom__surf_soln=repr(V), Phi_Bc_lo=repr(Vlo),
+                     domain__n_cell="8 8 20", domain__max_grid_size="8 8 20")
+    o = O.Oracle.from_text(text)
+    tab = I.parse_table(text)
+    kb, _ = I.embedded_boundary(tab, I.ferrox_params(tab))
+    o.set_phi_bc()
+    phi = o.poisson_solve(np.zeros((20, 8, 8)), rtol=1e-14)[0]
+    eps = o.field("epsilon")[:kb, 0, 0]
+    assert np.all(o.field("epsilon")[:kb] == eps[:, None, None])   # layered
+    # conductances per unit area times h: bottom, the kb - 1 interior faces, top
+    g = np.concatenate([[2 * eps[0]], 0.5 * (eps[:-1] + eps[1:]), [2 * eps[-1]]])
+    A = np.zeros((kb, kb))
+    r = np.zeros(kb)
+    for k in range(kb):
+        A[k, k] = g[k] + g[k + 1]
+        if k > 0:
+            A[k, k - 1] = -g[k]
+        if k < kb - 1:
+            A[k, k + 1] = -g[k + 1]
+    r[0] += g[0] * Vlo
+    r[-1] += g[kb] * V
+    chain = np.linalg.solve(A, r)
+    for j in range(8):
+        for i in range(8):
+            assert np.allclose(phi[:kb, j, i], chain, rtol=0, atol=1e-12 * abs(V - Vlo))
+    assert np.all(phi[kb:] == 0.0)
