@@ -2249,6 +2249,13 @@ int fx_set_field(fx_ctx* c, int f, const double* in, size_t n) {
         int r = ensure_device(c);
         if (r) return r;
         FX_CUDA(c, cudaMemcpyAsync(c->d_phi, in, n * 8, cudaMemcpyHostToDevice, c->s));
+        if (c->eb_nz > 0) {
+            // the cells covered by an embedded boundary are not unknowns of the
+            // solve, which never writes them: they hold the 0 each solve of the
+            // reference starts from (ElectrostaticSolver.cpp:787)
+            const size_t n0 = c->nxy * (size_t)c->eb_nz;
+            FX_CUDA(c, cudaMemsetAsync(c->d_phi + n0, 0, (c->N - n0) * 8, c->s));
+        }
         FX_CUDA(c, cudaStreamSynchronize(c->s));
         c->E_valid = false;
         return FX_OK;
