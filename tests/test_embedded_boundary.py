@@ -223,3 +223,17 @@ def test_oracle_embedded_face_known_answer():
         for i in range(8):
             assert np.allclose(phi[:kb, j, i], chain, rtol=0, atol=1e-12 * abs(V - Vlo))
     assert np.all(phi[kb:] == 0.0)
+
+
+@pytest.mark.gpu
+def test_set_phi_keeps_covered_cells_zero():
+    """phi written through fx_set_field: the fluid layers take it, the
+    covered layers keep 0 (they are not unknowns of the solve)."""
+    f = api.FerroX(with_keys(deck(MFIM_EB), domain__n_cell="16 16 20", domain__max_grid_size="16 16 20"))
+    try:
+        kb = int(f.param("eb_fluid_layers"))
+        f.set_field("Phi", np.full((20, 16, 16), 0.25))
+        phi = f.field("Phi")
+        assert np.all(phi[:kb] == 0.25) and np.all(phi[kb:] == 0.0)
+    finally:
+        f.close()
